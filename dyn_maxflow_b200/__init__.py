@@ -1,0 +1,352 @@
+"""dyn_maxflow_b200 -- Python view of libdmf.so, the B200 dynamic max-flow engine.
+
+The compute path is the C ABI in include/dmf.h (sm_100a kernels); this module only
+binds it with ctypes.  There is no CPU fallback: the solver raises DmfError when
+no CUDA device is visible, and importing fails when libdmf.so has not been built.
+
+Names mirror the reference (ShruthiKannappan/dyn_maxflow):
+  Graph.load / num_nodes / num_edges ..... code/graph.hpp:18-233
+  load_updates ........................... code/update.hpp:52-88
+  recalculate_max_flow ................... code/dyn_data_bench.cu:171-298
+  static_recalculate ..................... code/dyn_data_bench.cu:325-492
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+__all__ = [
+    "DmfError", "Graph", "Solver", "Stats", "load_updates", "save_updates", "gen_grid", "gen_rmat",
+    "gen_batches", "recalculate_max_flow", "static_recalculate", "device_count", "VARIANTS", "lib_path",
+]
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+lib_path = os.path.join(_PKG, "libdmf.so")
+if not os.path.exists(lib_path):
+    raise ImportError(f"{lib_path} is missing: build it with `python -m dyn_maxflow_b200.build` "
+                      "(or __graft_entry__.build()); there is no CPU fallback")
+_L = C.CDLL(lib_path)
+
+VARIANTS = {"data": 0, "topo": 1, "pp": 2}
+I32P = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+U8P = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+I64P = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+VP = C.c_void_p
+PP = C.POINTER(C.c_void_p)
+
+
+class Opts(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("variant", "kernel_cycles", "relabel_interval", "tile", "max_iters",
+                                          "device", "block_threads", "flags")]
+
+
+class Stats(C.Structure):
+    _fields_ = [("flow", C.c_int64), ("outer_iters", C.c_int64), ("bfs_levels", C.c_int64),
+                ("push_rounds", C.c_int64), ("pushes", C.c_int64), ("relabels", C.c_int64),
+                ("arcs_scanned", C.c_int64), ("vertices_visited", C.c_int64), ("dead_vertices", C.c_int64),
+                ("last_ms", C.c_double), ("grid_blocks", C.c_int32), ("block_threads", C.c_int32),
+                ("tile", C.c_int32), ("pad", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
+def _sig(name, res, *args):
+    f = getattr(_L, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_sig("dmf_last_error", C.c_char_p)
+_sig("dmf_status_string", C.c_char_p, C.c_int)
+_sig("dmf_opts_default", None, C.POINTER(Opts))
+_sig("dmf_free", None, VP)
+_sig("dmf_graph_load", C.c_int, C.c_char_p, PP)
+_sig("dmf_graph_from_csr", C.c_int, C.c_int32, C.c_int32, I32P, I32P, I32P, I32P, PP)
+_sig("dmf_graph_from_edges", C.c_int, C.c_int64, I32P, I32P, I32P, PP)
+_sig("dmf_graph_save", C.c_int, VP, C.c_char_p)
+_sig("dmf_graph_info", C.c_int, VP, C.POINTER(C.c_int32), C.POINTER(C.c_int32))
+_sig("dmf_graph_arrays", C.c_int, VP, PP, PP, PP, PP)
+_sig("dmf_graph_find_arc", C.c_int64, VP, C.c_int32, C.c_int32)
+_sig("dmf_graph_set_caps", C.c_int, VP, C.c_int32, I32P, I32P, I32P)
+_sig("dmf_graph_free", None, VP)
+_sig("dmf_updates_load", C.c_int, C.c_char_p, C.POINTER(C.c_int32), PP, PP, PP)
+_sig("dmf_updates_save", C.c_int, C.c_char_p, C.c_int32, I32P, I32P, I32P)
+_sig("dmf_gen_grid", C.c_int, C.c_int32, C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, PP,
+     C.POINTER(C.c_int32), C.POINTER(C.c_int32))
+_sig("dmf_gen_rmat", C.c_int, C.c_int32, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_int32,
+     C.c_int32, C.c_int64, PP, C.POINTER(C.c_int32), C.POINTER(C.c_int32))
+_sig("dmf_gen_batches", C.c_int, VP, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,
+     C.c_int32, C.c_int32, C.c_uint64, PP, PP, PP, PP)
+_sig("dmf_solver_create", C.c_int, VP, C.c_int32, C.c_int32, C.POINTER(Opts), VP, PP)
+_sig("dmf_static_maxflow", C.c_int, VP, C.POINTER(C.c_int64))
+_sig("dmf_apply_updates", C.c_int, VP, C.c_int32, I32P, I32P, I32P, C.POINTER(C.c_int64))
+_sig("dmf_apply_updates_device", C.c_int, VP, C.c_int32, VP, VP, VP, C.POINTER(C.c_int64))
+_sig("dmf_recompute", C.c_int, VP, C.c_int32, I32P, I32P, I32P, C.POINTER(C.c_int64))
+_sig("dmf_recompute_device", C.c_int, VP, C.c_int32, VP, VP, VP, C.POINTER(C.c_int64))
+_sig("dmf_flow_value", C.c_int, VP, C.POINTER(C.c_int64))
+_sig("dmf_get_cut", C.c_int, VP, U8P)
+_sig("dmf_get_state", C.c_int, VP, VP, VP, VP, VP)
+_sig("dmf_stats_get", C.c_int, VP, C.POINTER(Stats))
+_sig("dmf_solver_set_opts", C.c_int, VP, C.POINTER(Opts))
+_sig("dmf_solver_destroy", C.c_int, VP)
+_sig("dmf_device_count", C.c_int)
+
+
+class DmfError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{_L.dmf_status_string(status).decode()}] {msg}")
+        self.status = status
+
+
+def _check(st: int) -> None:
+    if st:
+        raise DmfError(st, (_L.dmf_last_error() or b"").decode())
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a), dtype=np.int32)
+
+
+def _take_i32(ptr: C.c_void_p, count: int) -> np.ndarray:
+    if count == 0 or not ptr.value:
+        _L.dmf_free(ptr)
+        return np.zeros(0, np.int32)
+    a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_int32)), shape=(count,)).copy()
+    _L.dmf_free(ptr)
+    return a
+
+
+def device_count() -> int:
+    return int(_L.dmf_device_count())
+
+
+class Graph:
+    """Host CSR in the reference's .bin layout (code/graph.hpp:18-233)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _L.dmf_graph_free(h)
+            self._h = None
+
+    @classmethod
+    def load(cls, path: str) -> "Graph":
+        """graph::loadGraph, code/graph.hpp:202-223."""
+        h = C.c_void_p()
+        _check(_L.dmf_graph_load(os.fsencode(path), C.byref(h)))
+        return cls(h)
+
+    loadGraph = load
+
+    @classmethod
+    def from_csr(cls, index, adj, w, par) -> "Graph":
+        index, adj, w, par = _i32(index), _i32(adj), _i32(w), _i32(par)
+        h = C.c_void_p()
+        _check(_L.dmf_graph_from_csr(len(index) - 1, len(adj), index, adj, w, par, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_edges(cls, u, v, w) -> "Graph":
+        """input_create/create_bin.cpp:67-124 semantics."""
+        u, v, w = _i32(u), _i32(v), _i32(w)
+        h = C.c_void_p()
+        _check(_L.dmf_graph_from_edges(len(u), u, v, w, C.byref(h)))
+        return cls(h)
+
+    def save(self, path: str) -> None:
+        _check(_L.dmf_graph_save(self._h, os.fsencode(path)))
+
+    def num_nodes(self) -> int:
+        n, m = C.c_int32(), C.c_int32()
+        _check(_L.dmf_graph_info(self._h, C.byref(n), C.byref(m)))
+        return n.value
+
+    def num_edges(self) -> int:
+        n, m = C.c_int32(), C.c_int32()
+        _check(_L.dmf_graph_info(self._h, C.byref(n), C.byref(m)))
+        return m.value
+
+    def arrays(self):
+        """(index[n+1], adj[m], w[m], par[m]) as numpy copies."""
+        n, m = self.num_nodes(), self.num_edges()
+        ps = [C.c_void_p() for _ in range(4)]
+        _check(_L.dmf_graph_arrays(self._h, *[C.byref(p) for p in ps]))
+        out = []
+        for p, cnt in zip(ps, (n + 1, m, m, m)):
+            out.append(np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_int32)), shape=(max(cnt, 1),))[:cnt].copy())
+        return tuple(out)
+
+    def find_arc(self, src: int, dst: int) -> int:
+        return int(_L.dmf_graph_find_arc(self._h, src, dst))
+
+    def set_caps(self, src, dst, w) -> None:
+        """update_kernel (code/dyn_data_bench.cu:300-322) on the host copy."""
+        src, dst, w = _i32(src), _i32(dst), _i32(w)
+        _check(_L.dmf_graph_set_caps(self._h, len(src), src, dst, w))
+
+
+def load_updates(path: str):
+    """loadUpdateFile, code/update.hpp:52-88 -> (src, dst, w) int32 arrays."""
+    k = C.c_int32()
+    ps = [C.c_void_p() for _ in range(3)]
+    _check(_L.dmf_updates_load(os.fsencode(path), C.byref(k), *[C.byref(p) for p in ps]))
+    return tuple(_take_i32(p, k.value) for p in ps)
+
+
+def save_updates(path: str, src, dst, w) -> None:
+    src, dst, w = _i32(src), _i32(dst), _i32(w)
+    _check(_L.dmf_updates_save(os.fsencode(path), len(src), src, dst, w))
+
+
+def gen_grid(rows=256, cols=256, seed=0, cap_lo=1, cap_hi=100, st_cap=1000):
+    """-> (Graph, s, t)."""
+    h, s, t = C.c_void_p(), C.c_int32(), C.c_int32()
+    _check(_L.dmf_gen_grid(rows, cols, seed, cap_lo, cap_hi, st_cap, C.byref(h), C.byref(s), C.byref(t)))
+    return Graph(h), s.value, t.value
+
+
+def gen_rmat(scale=20, narcs=None, a=0.57, b=0.19, c=0.19, seed=0, cap_lo=1, cap_hi=1000, reserve=0):
+    """-> (Graph, s, t); narcs defaults to 16 * 2^scale."""
+    if narcs is None:
+        narcs = 16 << scale
+    h, s, t = C.c_void_p(), C.c_int32(), C.c_int32()
+    _check(_L.dmf_gen_rmat(scale, narcs, a, b, c, seed, cap_lo, cap_hi, reserve, C.byref(h), C.byref(s),
+                           C.byref(t)))
+    return Graph(h), s.value, t.value
+
+
+def gen_batches(g: Graph, nbatches, frac=0.01, p_inc=0.4, p_dec=0.4, p_ins=0.1, delta_hi=500, ins_lo=1,
+                ins_hi=1000, seed=1):
+    """-> list of (src, dst, w) per batch (successive: batch b assumes batches < b applied)."""
+    ofs, s, d, w = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+    _check(_L.dmf_gen_batches(g._h, nbatches, frac, p_inc, p_dec, p_ins, delta_hi, ins_lo, ins_hi, seed,
+                              C.byref(ofs), C.byref(s), C.byref(d), C.byref(w)))
+    o = np.ctypeslib.as_array(C.cast(ofs, C.POINTER(C.c_int64)), shape=(nbatches + 1,)).copy()
+    _L.dmf_free(ofs)
+    k = int(o[-1])
+    S, D, W = _take_i32(s, k), _take_i32(d, k), _take_i32(w, k)
+    return [(S[o[i]:o[i + 1]].copy(), D[o[i]:o[i + 1]].copy(), W[o[i]:o[i + 1]].copy()) for i in range(nbatches)]
+
+
+class Solver:
+    """Device-resident residual state of one graph on one GPU (dmf_solver)."""
+
+    def __init__(self, g: Graph, source: int, sink: int, variant="data", kernel_cycles=0, relabel_interval=0,
+                 tile=0, max_iters=0, device=-1, stream=None):
+        o = Opts()
+        _L.dmf_opts_default(C.byref(o))
+        o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
+        o.kernel_cycles, o.relabel_interval, o.tile, o.max_iters, o.device = (
+            kernel_cycles, relabel_interval, tile, max_iters, device)
+        self._h = C.c_void_p()
+        self.n, self.m = g.num_nodes(), g.num_edges()
+        stream_ptr = None if stream is None else C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+        _check(_L.dmf_solver_create(g._h, source, sink, C.byref(o), stream_ptr, C.byref(self._h)))
+        self.source, self.sink = source, sink
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _L.dmf_solver_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def static_maxflow(self) -> int:
+        f = C.c_int64()
+        _check(_L.dmf_static_maxflow(self._h, C.byref(f)))
+        return f.value
+
+    def apply_updates(self, src, dst, w) -> int:
+        src, dst, w = _i32(src), _i32(dst), _i32(w)
+        f = C.c_int64()
+        _check(_L.dmf_apply_updates(self._h, len(src), src, dst, w, C.byref(f)))
+        return f.value
+
+    def apply_updates_device(self, d_src: int, d_dst: int, d_w: int, k: int) -> int:
+        """Batch already on the device (raw device pointers, e.g. tensor.data_ptr())."""
+        f = C.c_int64()
+        _check(_L.dmf_apply_updates_device(self._h, k, C.c_void_p(d_src), C.c_void_p(d_dst), C.c_void_p(d_w),
+                                           C.byref(f)))
+        return f.value
+
+    def recompute(self, src=(), dst=(), w=()) -> int:
+        src, dst, w = _i32(src), _i32(dst), _i32(w)
+        f = C.c_int64()
+        _check(_L.dmf_recompute(self._h, len(src), src, dst, w, C.byref(f)))
+        return f.value
+
+    def recompute_device(self, d_src: int, d_dst: int, d_w: int, k: int) -> int:
+        f = C.c_int64()
+        _check(_L.dmf_recompute_device(self._h, k, C.c_void_p(d_src), C.c_void_p(d_dst), C.c_void_p(d_w),
+                                       C.byref(f)))
+        return f.value
+
+    @property
+    def flow(self) -> int:
+        f = C.c_int64()
+        _check(_L.dmf_flow_value(self._h, C.byref(f)))
+        return f.value
+
+    def cut(self) -> np.ndarray:
+        """1 = sink side (find_cut, code/dyn_pp.h:440-449)."""
+        out = np.zeros(self.n, dtype=np.uint8)
+        _check(_L.dmf_get_cut(self._h, out))
+        return out
+
+    def state(self):
+        """(cap[m], res[m], excess[n], height[n]) copied from the device."""
+        cap = np.zeros(max(self.m, 1), np.int32)
+        res = np.zeros(max(self.m, 1), np.int32)
+        ex = np.zeros(max(self.n, 1), np.int64)
+        h = np.zeros(max(self.n, 1), np.int32)
+        _check(_L.dmf_get_state(self._h, cap.ctypes.data, res.ctypes.data, ex.ctypes.data, h.ctypes.data))
+        return cap[:self.m], res[:self.m], ex[:self.n], h[:self.n]
+
+    def stats(self) -> dict:
+        st = Stats()
+        _check(_L.dmf_stats_get(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def set_opts(self, variant=None, kernel_cycles=None, relabel_interval=None, tile=None, max_iters=None):
+        o = Opts()
+        _L.dmf_opts_default(C.byref(o))
+        cur = getattr(self, "_opts", {})
+        vals = dict(variant=variant, kernel_cycles=kernel_cycles, relabel_interval=relabel_interval, tile=tile,
+                    max_iters=max_iters)
+        for k_, v_ in vals.items():
+            if v_ is None:
+                v_ = cur.get(k_, 0 if k_ != "variant" else 0)
+            if k_ == "variant" and isinstance(v_, str):
+                v_ = VARIANTS[v_]
+            setattr(o, k_, v_)
+            cur[k_] = v_
+        self._opts = cur
+        _check(_L.dmf_solver_set_opts(self._h, C.byref(o)))
+
+
+def recalculate_max_flow(g: Graph, updates, source: int, sink: int, kernel_cycles: int = 0, variant="data") -> int:
+    """Dynamic path of the reference bench (code/dyn_data_bench.cu:171-298): a fresh
+    device state of the ORIGINAL graph, static solve, one batch, flow readout."""
+    with Solver(g, source, sink, variant=variant, kernel_cycles=kernel_cycles) as sv:
+        sv.static_maxflow()
+        return sv.apply_updates(*updates)
+
+
+def static_recalculate(g: Graph, updates, source: int, sink: int, kernel_cycles: int = 0, variant="data") -> int:
+    """From-scratch path of the reference bench (code/dyn_data_bench.cu:325-492)."""
+    with Solver(g, source, sink, variant=variant, kernel_cycles=kernel_cycles) as sv:
+        return sv.recompute(*updates)

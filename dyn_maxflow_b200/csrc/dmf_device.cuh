@@ -1,0 +1,189 @@
+// dmf_device.cuh -- device-side building blocks of the sm_100a solver:
+// memory-order helpers, the bounded grid barrier, queue appends and the group
+// abstractions (a warp tile or a whole block working on one vertex).
+#pragma once
+
+#include <climits>
+#include <cstdint>
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+#include <cooperative_groups/scan.h>
+#include <cub/block/block_reduce.cuh>
+#include <cub/block/block_scan.cuh>
+
+namespace dmfd {
+
+namespace cg = cooperative_groups;
+
+// ---- error bits (Ctrl::err) ------------------------------------------------
+enum : int {
+  ERR_TIMEOUT = 1,       // a grid-barrier wait ran out of time
+  ERR_NO_CONV = 2,       // outer-iteration bound reached
+  ERR_UNKNOWN_ARC = 4,   // update names an absent arc
+  ERR_DUP_ARC = 8,       // arc twice in one batch
+  ERR_BAD_UPDATE = 16,   // vertex id out of range or capacity out of bounds
+};
+
+// Barrier wait limit: 4 s of %globaltimer.  Any single phase of a solve is
+// orders of magnitude shorter; hitting it means a block never arrived.
+constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;
+
+// Per-phase counters, triple-buffered: phase k appends into slot k%3, reads
+// slot (k-1)%3, and block 0 clears slot (k+1)%3.
+struct Slot {
+  int q;             // normal-queue tail
+  int hq;            // hub-queue tail
+  long long arcs;    // sum of degrees of appended vertices
+  int cnt;           // generic counter
+  int pad;
+};
+
+// Control block of one solver (device memory, cleared before every launch).
+struct Ctrl {
+  unsigned int bar_count;
+  unsigned int bar_gen;
+  int err;
+  int err_info;
+  Slot slot[3];
+  // per global relabel
+  int act_q, act_hq;          // active list tails built by the BFS
+  int pos_count;              // vertices with excess > 0 (not s, t, dead)
+  int reached;                // positive-excess vertices labelled so far
+  long long unexplored;       // arcs of not-yet-labelled candidate vertices
+  long long flow;             // result
+  // statistics
+  unsigned long long st_outer, st_levels, st_rounds, st_pushes, st_relabels, st_arcs, st_visits, st_dead;
+  unsigned int rounds_used;
+  int pad;
+};
+
+// ---- memory helpers ---------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_vol(const int *p) { return *(const volatile int *)p; }
+__device__ __forceinline__ long long ld_vol(const long long *p) { return *(const volatile long long *)p; }
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ long long atomic_add_ll(long long *p, long long v) {
+  return (long long)atomicAdd((unsigned long long *)p, (unsigned long long)v);
+}
+
+// ---- bounded grid barrier ---------------------------------------------------
+// All blocks of a cooperative launch call it the same number of times.  Thread
+// 0 of each block arrives on a counter; the last arrival resets it and bumps the
+// generation.  Waiters poll with a time limit and leave early once any block
+// has set an error.  Returns false (uniformly per block) when an error is set.
+__device__ __forceinline__ bool grid_barrier(Ctrl *c) {
+  __shared__ int s_err;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned gen = ld_acquire_u32(&c->bar_gen);
+    __threadfence();
+    unsigned prev = atomicAdd(&c->bar_count, 1u);
+    if (prev == gridDim.x - 1) {
+      atomicExch(&c->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&c->bar_gen, 1u);
+    } else {
+      unsigned long long t0 = globaltimer();
+      unsigned ns = 32;
+      while (ld_acquire_u32(&c->bar_gen) == gen) {
+        if (ld_vol(&c->err)) break;
+        if (globaltimer() - t0 > kBarrierTimeoutNs) {
+          atomicOr(&c->err, ERR_TIMEOUT);
+          break;
+        }
+        __nanosleep(ns);
+        if (ns < 256) ns <<= 1;
+      }
+    }
+    __threadfence();
+    s_err = ld_vol(&c->err);
+  }
+  __syncthreads();
+  return s_err == 0;
+}
+
+// ---- queue append (warp-aggregated) -----------------------------------------
+__device__ __forceinline__ void append(int *q, int *tail, int v) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  int base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(tail, (int)g.size());
+  base = g.shfl(base, 0);
+  q[base + g.thread_rank()] = v;
+}
+
+__device__ __forceinline__ void agg_add_ll(long long *p, long long v) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  long long s = cg::reduce(g, v, cg::plus<long long>());
+  if (g.thread_rank() == 0 && s) atomic_add_ll(p, s);
+}
+
+__device__ __forceinline__ void agg_add_int(int *p, int v) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  int s = cg::reduce(g, v, cg::plus<int>());
+  if (g.thread_rank() == 0 && s) atomicAdd(p, s);
+}
+
+// ---- groups: T lanes of a warp, or the whole block ---------------------------
+template <int T>
+struct TileGroup {
+  cg::thread_block_tile<T> g;
+  __device__ TileGroup() : g(cg::tiled_partition<T>(cg::this_thread_block())) {}
+  __device__ __forceinline__ int rank() const { return (int)g.thread_rank(); }
+  static constexpr int size() { return T; }
+  // exclusive prefix sum and total
+  __device__ __forceinline__ long long scan(long long x, long long &tot) {
+    long long pre = cg::exclusive_scan(g, x, cg::plus<long long>());
+    tot = g.shfl(pre + x, T - 1);
+    return pre;
+  }
+  __device__ __forceinline__ int min_all(int x) { return cg::reduce(g, x, cg::less<int>()); }
+  __device__ __forceinline__ long long sum_all(long long x) { return cg::reduce(g, x, cg::plus<long long>()); }
+};
+
+template <int BLOCK>
+struct BlockGroup {
+  typedef cub::BlockScan<long long, BLOCK> Scan;
+  typedef cub::BlockReduce<int, BLOCK> RedI;
+  typedef cub::BlockReduce<long long, BLOCK> RedL;
+  union Temp {
+    typename Scan::TempStorage scan;
+    typename RedI::TempStorage redi;
+    typename RedL::TempStorage redl;
+  };
+  Temp &tmp;
+  int *bcast_i;
+  long long *bcast_l;
+  __device__ BlockGroup(Temp &t, int *bi, long long *bl) : tmp(t), bcast_i(bi), bcast_l(bl) {}
+  __device__ __forceinline__ int rank() const { return (int)threadIdx.x; }
+  static constexpr int size() { return BLOCK; }
+  __device__ __forceinline__ long long scan(long long x, long long &tot) {
+    long long pre;
+    __syncthreads();
+    Scan(tmp.scan).ExclusiveSum(x, pre, tot);
+    return pre;
+  }
+  __device__ __forceinline__ int min_all(int x) {
+    __syncthreads();
+    int r = RedI(tmp.redi).Reduce(x, cub::Min());
+    if (threadIdx.x == 0) *bcast_i = r;
+    __syncthreads();
+    return *bcast_i;
+  }
+  __device__ __forceinline__ long long sum_all(long long x) {
+    __syncthreads();
+    long long r = RedL(tmp.redl).Sum(x);
+    if (threadIdx.x == 0) *bcast_l = r;
+    __syncthreads();
+    return *bcast_l;
+  }
+};
+
+}  // namespace dmfd

@@ -1,0 +1,39 @@
+// Internal declarations shared by the host (dmf_host.cpp) and device
+// (dmf_solver.cu) halves of libdmf.so.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "dmf.h"
+
+// Host CSR.  Arrays follow the on-disk layout of code/graph.hpp:202-223.
+// `sidx` is built on demand: for each vertex, its arc indices sorted by
+// (head, arc) -- used for O(log deg) arc lookup.
+struct dmf_graph {
+  int32_t n = 0, m = 0;
+  std::vector<int32_t> off, adj, w, par;
+  std::vector<int32_t> sidx;
+};
+
+namespace dmf {
+
+// Records a thread-local error message and returns `status`.
+int fail(int status, const char *fmt, ...);
+// Clears the thread-local message, returns DMF_OK.
+int ok();
+
+// Validates CSR structure: offsets, ids, partner involution, capacities.
+int validate(const dmf_graph &g);
+// Fills g.sidx (idempotent).
+void build_sorted_index(dmf_graph &g);
+// Arc src->dst via g.sidx (last arc index among equal heads), or -1.
+int64_t find_arc(const dmf_graph &g, int32_t src, int32_t dst);
+
+// Builds a graph with create_bin semantics from an edge list (first-touch
+// adjacency order, duplicates summed, partners created with capacity 0).
+int build_from_edges(int64_t k, const int32_t *u, const int32_t *v,
+                     const int32_t *w, dmf_graph **out);
+
+}  // namespace dmf

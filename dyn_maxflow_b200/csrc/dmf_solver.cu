@@ -1,0 +1,1074 @@
+// dmf_solver.cu -- device half of libdmf.so: the persistent push-relabel
+// solver for sm_100a and the solver entry points of the C ABI.
+//
+// One cooperative launch runs a whole solve: the update prologue (arc lookup,
+// capacity apply, over-capacity repair, source saturation), then rounds of
+//   global relabel: direction-optimising reverse BFS from t and the deficit
+//                   vertices over residual arcs, which also builds the active
+//                   worklist and proves unreachable vertices dead;
+//   push rounds:    discharge of every active vertex by a warp tile (or a whole
+//                   block for hubs), multi-arc pushes per adjacency scan, with
+//                   warp-aggregated worklist appends;
+// until a global relabel finds no active vertex, then the flow readout
+// excess(t) + sum of deficits (recalculate_max_flow_kernel_39,
+// code/dyn_data.h:208-215).  Phases are separated by a bounded grid barrier, so
+// no host round trip happens inside a solve (the reference syncs and copies a
+// flag per BFS level, code/dyn_data_bench.cu:39-47).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <mutex>
+
+#include "dmf_device.cuh"
+#include "dmf_internal.h"
+
+using namespace dmfd;
+
+namespace {
+
+constexpr int kBlock = 512;
+
+enum Mode : int { MODE_STATIC = 0, MODE_DYNAMIC = 1, MODE_RECOMPUTE = 2, MODE_CUT = 3 };
+
+// Largest capacity an update may set: keeps cap(e) + cap(partner) < 2^31 when
+// both arcs of a pair change in one batch.
+constexpr int kMaxUpdateCap = (1 << 30) - 1;
+
+struct Params {
+  int n, m, s, t;
+  const int *__restrict__ off;
+  const int *__restrict__ adj;
+  const int *__restrict__ par;
+  const int *__restrict__ sidx;
+  int *cap, *res, *height, *stamp, *astamp, *uarc;
+  long long *excess;
+  unsigned char *dead, *side;
+  int *fq[2], *fh[2], *wq[2], *wh[2], *aq, *ah;
+  const int *hubs;
+  int nhubs;
+  const int *usrc, *udst, *uw;
+  int k;
+  Ctrl *ctrl;
+  int mode, variant, cycles, interval, max_iters, hub_deg, need_cut;
+  unsigned round_base;
+  int epoch;
+};
+
+struct LStats {
+  unsigned long long pushes = 0, relabels = 0, arcs = 0, visits = 0;
+};
+
+__device__ __forceinline__ int deg_of(const Params &p, int v) { return __ldg(p.off + v + 1) - __ldg(p.off + v); }
+
+__device__ __forceinline__ void set_err(Ctrl *c, int bit, int info) {
+  if (atomicOr(&c->err, bit) == 0) c->err_info = info;
+}
+
+// ---- prologue phases ----------------------------------------------------------
+
+// staticMaxFlow_kernel_1 (code/dyn_data.h:25-35): residual = capacity, excess 0.
+__device__ void ph_init_res(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int e = gt; e < p.m; e += nt) p.res[e] = __ldcg(p.cap + e);
+  for (int v = gt; v < p.n; v += nt) p.excess[v] = 0;
+}
+
+// staticMaxFlow_kernel_7 (code/dyn_data.h:39-56) made parallel: every residual
+// arc out of s is saturated.
+__device__ void ph_saturate(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int beg = __ldg(p.off + p.s), end = __ldg(p.off + p.s + 1);
+  long long sum = 0;
+  for (int a = beg + gt; a < end; a += nt) {
+    int r = __ldcg(p.res + a);
+    if (r > 0) {
+      p.res[a] = 0;
+      atomicAdd(p.res + __ldg(p.par + a), r);
+      atomic_add_ll(p.excess + __ldg(p.adj + a), r);
+      sum += r;
+    }
+  }
+  if (sum) atomic_add_ll(p.excess + p.s, -sum);
+}
+
+// Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201) by binary search over the
+// per-vertex head-sorted index; also validates the batch.
+__device__ void ph_lookup(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int i = gt; i < p.k; i += nt) {
+    int u = __ldg(p.usrc + i), v = __ldg(p.udst + i), w = __ldg(p.uw + i);
+    p.uarc[i] = -1;
+    if (u < 0 || u >= p.n || v < 0 || v >= p.n || w < 0 || w > kMaxUpdateCap) {
+      set_err(p.ctrl, ERR_BAD_UPDATE, i);
+      continue;
+    }
+    if (u == v) continue;  // ignored, as OnAdd_kernel does (code/dyn_data.h:194)
+    int lo = __ldg(p.off + u), hi = __ldg(p.off + u + 1);
+    // last position with head <= v
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (__ldg(p.adj + __ldg(p.sidx + mid)) <= v) lo = mid + 1;
+      else hi = mid;
+    }
+    int e = -1;
+    if (lo > __ldg(p.off + u)) {
+      int cand = __ldg(p.sidx + lo - 1);
+      if (__ldg(p.adj + cand) == v) e = cand;
+    }
+    if (e < 0) {
+      set_err(p.ctrl, ERR_UNKNOWN_ARC, i);
+      continue;
+    }
+    if (atomicExch(p.astamp + e, p.epoch) == p.epoch) {
+      set_err(p.ctrl, ERR_DUP_ARC, i);
+      continue;
+    }
+    if ((long long)w + __ldcg(p.cap + __ldg(p.par + e)) > INT_MAX) {
+      set_err(p.ctrl, ERR_BAD_UPDATE, i);
+      continue;
+    }
+    p.uarc[i] = e;
+  }
+}
+
+// Capacity apply of OnAdd_kernel (code/dyn_data.h:202-205); in recompute mode
+// only the capacity is set (update_kernel, code/dyn_data_bench.cu:300-322).
+__device__ void ph_apply(const Params &p, bool residual) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int i = gt; i < p.k; i += nt) {
+    int e = __ldcg(p.uarc + i);
+    if (e < 0) continue;
+    int w = __ldg(p.uw + i);
+    int delta = w - __ldcg(p.cap + e);
+    p.cap[e] = w;
+    if (residual && delta) atomicAdd(p.res + e, delta);
+  }
+}
+
+// Over-capacity repair driven by the batch: replaces the O(m) sweeps
+// incremental_kernel_20 / _22 (code/dyn_data.h:157-183).  An arc whose residual
+// went negative carries more flow than its new capacity; the excess is returned
+// to its tail and taken from its head.  At most one arc of a pair can be
+// negative because res(e) + res(partner) = cap(e) + cap(partner) >= 0.
+__device__ void ph_repair(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int i = gt; i < p.k; i += nt) {
+    int e = __ldcg(p.uarc + i);
+    if (e < 0) continue;
+    int r = __ldcg(p.res + e);
+    if (r < 0) {
+      p.res[e] = 0;
+      atomicAdd(p.res + __ldg(p.par + e), r);
+      atomic_add_ll(p.excess + __ldg(p.usrc + i), -(long long)r);
+      atomic_add_ll(p.excess + __ldg(p.adj + e), (long long)r);
+    }
+  }
+}
+
+// Push-pull: an updated arc that now has residual from the source side A into
+// the sink side B of the kept cut is saturated (the cut part of the fused
+// incremental_kernel_20, code/dyn_pp.h:422-432, limited to touched arcs).
+__device__ void ph_cut_saturate(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int i = gt; i < p.k; i += nt) {
+    int e = __ldcg(p.uarc + i);
+    if (e < 0) continue;
+    int u = __ldg(p.usrc + i), v = __ldg(p.adj + e);
+    if (u == p.s || u == p.t || v == p.s || v == p.t) continue;
+    if (p.side[u] == 0 && p.side[v] == 1) {
+      int r = __ldcg(p.res + e);
+      if (r > 0) {
+        p.res[e] = 0;
+        atomicAdd(p.res + __ldg(p.par + e), r);
+        atomic_add_ll(p.excess + u, -(long long)r);
+        atomic_add_ll(p.excess + v, (long long)r);
+      }
+    }
+  }
+}
+
+// ---- global relabel ---------------------------------------------------------------
+
+#define UNV (p.n + 1)
+
+// Seeds (my_init_1, code/dyn_data.h:60-67): t and every deficit vertex other
+// than s get height 0; all other live vertices become unvisited.
+__device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  Ctrl *c = p.ctrl;
+  if (gt == 0) {
+    c->act_q = 0;
+    c->act_hq = 0;
+  }
+  int pos = 0;
+  long long unexpl = 0, seed_arcs = 0;
+  for (int v = gt; v < p.n; v += nt) {
+    if (reset_dead) p.dead[v] = 0;
+    else if (__ldcg(p.dead + v)) continue;
+    long long ex = __ldcg(p.excess + v);
+    int d = deg_of(p, v);
+    if (v == p.t || (v != p.s && ex < 0)) {
+      p.height[v] = 0;
+      if (d > p.hub_deg) append(p.fh[0], &out->hq, v);
+      else append(p.fq[0], &out->q, v);
+      seed_arcs += d;
+    } else {
+      p.height[v] = UNV;
+      unexpl += d;
+    }
+    if (v != p.s && v != p.t && ex > 0) pos++;
+  }
+  agg_add_int(&c->pos_count, pos);
+  agg_add_ll(&c->unexplored, unexpl);
+  agg_add_ll(&out->arcs, seed_arcs);
+}
+
+struct VisitAcc {
+  long long arcs = 0;
+  int reached = 0;
+};
+
+__device__ __forceinline__ void bfs_visit(const Params &p, Slot *out, int nxt, int w, VisitAcc &acc) {
+  int d = deg_of(p, w);
+  if (d > p.hub_deg) append(p.fh[nxt], &out->hq, w);
+  else append(p.fq[nxt], &out->q, w);
+  acc.arcs += d;
+  if (w != p.s && w != p.t && __ldcg(p.excess + w) > 0) {
+    if (d > p.hub_deg) append(p.ah, &p.ctrl->act_hq, w);
+    else append(p.aq, &p.ctrl->act_q, w);
+    acc.reached++;
+  }
+}
+
+__device__ __forceinline__ void flush_visits(const Params &p, Slot *out, VisitAcc &acc) {
+  agg_add_ll(&out->arcs, acc.arcs);
+  agg_add_int(&p.ctrl->reached, acc.reached);
+}
+
+// Top-down level (staticMaxFlow_kernel_11, code/dyn_data.h:72-87, run over the
+// frontier queue instead of all V): x at level L labels w when arc w->x has
+// residual, i.e. res[par[e]] > 0 for e = x->w.
+template <int TILE>
+__device__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cur = L & 1, nxt = cur ^ 1;
+  const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
+  const int lane = threadIdx.x % TILE;
+  VisitAcc acc;
+  for (int i = blockIdx.x; i < nh; i += gridDim.x) {
+    int x = __ldcg(p.fh[cur] + i);
+    int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
+    for (int a = beg + threadIdx.x; a < end; a += blockDim.x) {
+      int w = __ldg(p.adj + a);
+      ls.arcs++;
+      if (__ldcg(p.height + w) == UNV && __ldcg(p.res + __ldg(p.par + a)) > 0 &&
+          atomicCAS(p.height + w, UNV, L + 1) == UNV)
+        bfs_visit(p, out, nxt, w, acc);
+    }
+  }
+  for (int i = gt / TILE; i < nn; i += nt / TILE) {
+    int x = __ldcg(p.fq[cur] + i);
+    int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
+    for (int a = beg + lane; a < end; a += TILE) {
+      int w = __ldg(p.adj + a);
+      ls.arcs++;
+      if (__ldcg(p.height + w) == UNV && __ldcg(p.res + __ldg(p.par + a)) > 0 &&
+          atomicCAS(p.height + w, UNV, L + 1) == UNV)
+        bfs_visit(p, out, nxt, w, acc);
+    }
+  }
+  flush_visits(p, out, acc);
+}
+
+// Bottom-up level: every unvisited vertex looks for a residual arc into level L.
+__device__ void ph_bfs_bu(const Params &p, Slot *out, int L, LStats &ls) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nxt = (L & 1) ^ 1;
+  VisitAcc acc;
+  for (int v = gt; v < p.n; v += nt) {
+    if (__ldcg(p.height + v) != UNV) continue;
+    int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
+    for (int a = beg; a < end; a++) {
+      ls.arcs++;
+      if (__ldcg(p.res + a) > 0 && __ldcg(p.height + __ldg(p.adj + a)) == L) {
+        p.height[v] = L + 1;
+        bfs_visit(p, out, nxt, v, acc);
+        break;
+      }
+    }
+  }
+  flush_visits(p, out, acc);
+}
+
+// After the BFS: a complete BFS proves every unvisited vertex unreachable
+// (dead for the rest of this solve; the reference gives them height V); an
+// early-stopped BFS gives them the valid lower bound `floor`.
+__device__ void ph_bfs_finalize(const Params &p, bool full, int floor_h, bool write_side) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  int nd = 0;
+  for (int v = gt; v < p.n; v += nt) {
+    int h = __ldcg(p.height + v);
+    if (h == UNV) {
+      if (full) {
+        p.dead[v] = 1;
+        p.height[v] = p.n;
+        nd++;
+      } else {
+        p.height[v] = floor_h;
+      }
+    }
+    if (write_side) p.side[v] = h < p.n ? 1 : 0;
+  }
+  if (nd) atomicAdd((unsigned long long *)&p.ctrl->st_dead, (unsigned long long)nd);
+}
+
+// ---- push rounds ---------------------------------------------------------------
+
+__device__ __forceinline__ void enqueue(const Params &p, Slot *out, int buf, unsigned round_id, int v) {
+  if (atomicExch(p.stamp + v, (int)round_id) == (int)round_id) return;
+  if (deg_of(p, v) > p.hub_deg) append(p.wh[buf], &out->hq, v);
+  else append(p.wq[buf], &out->q, v);
+}
+
+// Discharge of v by a group (warp tile or block): up to `cycles` scans of the
+// adjacency; each scan pushes the excess over every admissible arc (height
+// below h) in arc order, allotted by a prefix sum, and relabels to
+// 1 + min height over the arcs still residual when excess is left.  This is the
+// push/relabel of staticMaxFlow_kernel_14 (code/dyn_data.h:89-131) with all
+// admissible arcs used per scan instead of only the lowest one.
+template <class G>
+__device__ void discharge(G &g, const Params &p, int v, Slot *out, int buf, unsigned round_id, bool enq,
+                          LStats &ls, int *seen) {
+  long long ex0;
+  int h;
+  // one read, broadcast: concurrent pushes may change excess[v] meanwhile
+  if constexpr (G::size() == kBlock) {
+    __shared__ long long s_ex;
+    __shared__ int s_h;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_ex = __ldcg(p.excess + v);
+      s_h = __ldcg(p.height + v);
+    }
+    __syncthreads();
+    ex0 = s_ex;
+    h = s_h;
+  } else {
+    long long e = 0;
+    int hh = 0;
+    if (g.rank() == 0) {
+      e = __ldcg(p.excess + v);
+      hh = __ldcg(p.height + v);
+    }
+    ex0 = g.g.shfl(e, 0);
+    h = g.g.shfl(hh, 0);
+  }
+  if (!(ex0 > 0 && h < p.n) || v == p.s || v == p.t) return;
+  if (g.rank() == 0) {
+    ls.visits++;
+    if (seen) (*seen)++;
+  }
+  long long ex = ex0;
+  const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
+  for (int cyc = 0; cyc < p.cycles && ex > 0 && h < p.n; cyc++) {
+    int minh = INT_MAX;
+    for (int base = beg; base < end; base += G::size()) {
+      const int a = base + g.rank();
+      int r = 0, w = -1, hw = INT_MAX;
+      if (a < end) {
+        r = __ldcg(p.res + a);
+        if (r > 0) {
+          w = __ldg(p.adj + a);
+          hw = __ldcg(p.height + w);
+        }
+        ls.arcs++;
+      }
+      const bool adm = r > 0 && hw < h;
+      long long tot;
+      const long long pre = g.scan(adm ? (long long)r : 0ll, tot);
+      int d = 0;
+      if (adm) {
+        long long left = ex - pre;
+        d = left <= 0 ? 0 : (left < r ? (int)left : r);
+      }
+      if (d > 0) {
+        atomicSub(p.res + a, d);
+        atomicAdd(p.res + __ldg(p.par + a), d);
+        long long old = atomic_add_ll(p.excess + w, d);
+        ls.pushes++;
+        if (enq && w != p.s && w != p.t && old + d > 0) enqueue(p, out, buf, round_id, w);
+      }
+      if (r > 0 && !(adm && d == r)) minh = min(minh, hw);
+      ex -= (tot < ex ? tot : ex);
+      if (ex == 0) break;
+    }
+    if (ex > 0) {
+      const int mh = g.min_all(minh);
+      h = mh >= p.n ? p.n : mh + 1;
+      if (g.rank() == 0) {
+        p.height[v] = h;
+        ls.relabels++;
+      }
+    }
+  }
+  if (g.rank() == 0) {
+    if (ex0 != ex) atomic_add_ll(p.excess + v, ex - ex0);
+    if (enq && ex > 0 && h < p.n) enqueue(p, out, buf, round_id, v);
+  }
+}
+
+template <int TILE, int BLOCK>
+__device__ void ph_push(const Params &p, const Slot *in, Slot *out, int r, unsigned round_id, LStats &ls,
+                        typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
+  Ctrl *c = p.ctrl;
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool topo = p.variant == DMF_VARIANT_TOPO;
+  if (r == 0 && gt == 0) {  // read during the BFS just finished; cleared for the next one
+    c->pos_count = 0;
+    c->reached = 0;
+    c->unexplored = 0;
+  }
+  const int buf = r & 1;
+  const int *nlist, *hlist;
+  int nn, nh;
+  if (topo) {
+    nlist = nullptr;
+    nn = p.n;
+    hlist = p.hubs;
+    nh = p.nhubs;
+  } else if (r == 0) {
+    nlist = p.aq;
+    nn = ld_vol(&c->act_q);
+    hlist = p.ah;
+    nh = ld_vol(&c->act_hq);
+  } else {
+    nlist = p.wq[buf ^ 1];
+    nn = ld_vol(&in->q);
+    hlist = p.wh[buf ^ 1];
+    nh = ld_vol(&in->hq);
+  }
+  int seen = 0;
+  {
+    BlockGroup<BLOCK> bg(btmp, bci, bcl);
+    for (int i = blockIdx.x; i < nh; i += gridDim.x) {
+      int v = __ldcg(hlist + i);
+      discharge(bg, p, v, out, buf, round_id, !topo, ls, topo ? &seen : nullptr);
+    }
+  }
+  {
+    TileGroup<TILE> tg;
+    for (int i = gt / TILE; i < nn; i += nt / TILE) {
+      int v = topo ? i : __ldcg(nlist + i);
+      if (topo && deg_of(p, v) > p.hub_deg) continue;
+      discharge(tg, p, v, out, buf, round_id, !topo, ls, topo ? &seen : nullptr);
+    }
+  }
+  if (topo) agg_add_int(&out->cnt, seen);
+}
+
+// recalculate_max_flow_kernel_39 (code/dyn_data.h:208-215) as a reduction:
+// flow = excess(t) + sum of negative excess over v != s, t.
+template <int BLOCK>
+__device__ void ph_flow(const Params &p, typename BlockGroup<BLOCK>::Temp &btmp) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  long long acc = 0;
+  for (int v = gt; v < p.n; v += nt) {
+    long long ex = __ldcg(p.excess + v);
+    if (v == p.t) acc += ex;
+    else if (v != p.s && ex < 0) acc += ex;
+  }
+  __syncthreads();
+  long long tot = typename BlockGroup<BLOCK>::RedL(btmp.redl).Sum(acc);
+  if (threadIdx.x == 0 && tot) atomic_add_ll(&p.ctrl->flow, tot);
+}
+
+__device__ __forceinline__ void clear_slot(Slot *s) {
+  s->q = 0;
+  s->hq = 0;
+  s->arcs = 0;
+  s->cnt = 0;
+}
+
+template <int TILE, int BLOCK>
+__device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Temp &btmp, int *bci,
+                    long long *bcl) {
+  Ctrl *c = p.ctrl;
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  int ph = 0;
+  auto slot_out = [&]() { return &c->slot[ph % 3]; };
+  auto slot_in = [&]() { return &c->slot[(ph + 2) % 3]; };
+  auto next = [&]() -> bool {
+    if (!grid_barrier(c)) return false;
+    ph++;
+    if (lead) clear_slot(&c->slot[(ph + 1) % 3]);
+    return true;
+  };
+  if (lead) clear_slot(&c->slot[1]);
+
+  // ---- prologue --------------------------------------------------------------
+  if (p.mode == MODE_STATIC) {
+    ph_init_res(p);
+    if (!next()) return;
+    ph_saturate(p);
+    if (!next()) return;
+  } else if (p.mode == MODE_DYNAMIC) {
+    ph_lookup(p);
+    if (!next()) return;
+    ph_apply(p, true);
+    if (!next()) return;
+    ph_repair(p);
+    if (!next()) return;
+    if (p.variant == DMF_VARIANT_PP) {
+      ph_cut_saturate(p);
+      if (!next()) return;
+    }
+    ph_saturate(p);
+    if (!next()) return;
+  } else if (p.mode == MODE_RECOMPUTE) {
+    ph_lookup(p);
+    if (!next()) return;
+    ph_apply(p, false);
+    if (!next()) return;
+    ph_init_res(p);
+    if (!next()) return;
+    ph_saturate(p);
+    if (!next()) return;
+  }
+
+  // ---- global relabel / push rounds ---------------------------------------------
+  unsigned round_id = p.round_base;
+  const bool cut_only = p.mode == MODE_CUT;
+  for (int it = 0;; it++) {
+    if (it >= p.max_iters) {
+      if (lead) set_err(c, ERR_NO_CONV, it);
+      return;
+    }
+    ph_bfs_init(p, slot_out(), it == 0);
+    if (!next()) return;
+    if (lead) c->st_outer++;
+    const int P = ld_vol(&c->pos_count);
+    const bool want_cut = p.need_cut || cut_only;
+    if (P == 0 && !want_cut) break;
+    long long m_u = ld_vol(&c->unexplored);
+    bool bu = false, full = true;
+    int L = 0;
+    for (;; L++) {
+      const Slot *in = slot_in();
+      const int F = ld_vol(&in->q) + ld_vol(&in->hq);
+      const long long m_f = ld_vol(&in->arcs);
+      if (F == 0) break;  // complete
+      if (!cut_only && P > 0 && ld_vol(&c->reached) == P) {
+        full = false;  // every active vertex has its exact distance
+        break;
+      }
+      if (L > 0) m_u -= m_f;
+      if (!bu && m_f * 14 > m_u) bu = true;
+      else if (bu && (long long)F * 24 < p.n) bu = false;
+      if (bu) ph_bfs_bu(p, slot_out(), L, ls);
+      else ph_bfs_td<TILE>(p, in, slot_out(), L, ls);
+      if (!next()) return;
+      if (lead) c->st_levels++;
+    }
+    ph_bfs_finalize(p, full, L + 1, full && want_cut);
+    if (!next()) return;
+    const int A = ld_vol(&c->act_q) + ld_vol(&c->act_hq);
+    if (A == 0 || cut_only) break;
+    for (int r = 0; r < p.interval; r++) {
+      round_id++;
+      ph_push<TILE, BLOCK>(p, slot_in(), slot_out(), r, round_id, ls, btmp, bci, bcl);
+      if (!next()) return;
+      if (lead) c->st_rounds++;
+      const Slot *in = slot_in();
+      const int W = p.variant == DMF_VARIANT_TOPO ? ld_vol(&in->cnt) : ld_vol(&in->q) + ld_vol(&in->hq);
+      if (W == 0) break;
+    }
+  }
+  ph_flow<BLOCK>(p, btmp);
+  if (lead) c->rounds_used = round_id - p.round_base;
+}
+
+template <int TILE, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 2) k_solve(Params p) {
+  __shared__ typename BlockGroup<BLOCK>::Temp btmp;
+  __shared__ int bci;
+  __shared__ long long bcl;
+  LStats ls;
+  run<TILE, BLOCK>(p, ls, btmp, &bci, &bcl);
+  // statistics: one atomic per block and counter
+  __syncthreads();
+  typedef cub::BlockReduce<unsigned long long, BLOCK> R;
+  __shared__ typename R::TempStorage rt;
+  unsigned long long v[4] = {ls.pushes, ls.relabels, ls.arcs, ls.visits};
+  unsigned long long *dst[4] = {&p.ctrl->st_pushes, &p.ctrl->st_relabels, &p.ctrl->st_arcs, &p.ctrl->st_visits};
+  for (int i = 0; i < 4; i++) {
+    unsigned long long s = R(rt).Sum(v[i]);
+    if (threadIdx.x == 0 && s) atomicAdd(dst[i], s);
+    __syncthreads();
+  }
+}
+
+using KernelFn = void (*)(Params);
+
+KernelFn pick_kernel(int tile) {
+  switch (tile) {
+    case 4: return k_solve<4, kBlock>;
+    case 8: return k_solve<8, kBlock>;
+    case 16: return k_solve<16, kBlock>;
+    default: return k_solve<32, kBlock>;
+  }
+}
+
+}  // namespace
+
+// ============================================================================
+// host side
+// ============================================================================
+using dmf::fail;
+using dmf::ok;
+
+struct dmf_solver {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  int n = 0, m = 0, s = 0, t = 0;
+  dmf_opts opts{};
+  int tile = 32, grid = 0, block = kBlock, hub_deg = 256;
+  int *off = nullptr, *adj = nullptr, *par = nullptr, *sidx = nullptr, *cap = nullptr, *res = nullptr;
+  int *height = nullptr, *stamp = nullptr, *astamp = nullptr, *uarc = nullptr;
+  long long *excess = nullptr;
+  unsigned char *dead = nullptr, *side = nullptr;
+  int *qbuf = nullptr;  // 10 vertex queues
+  int *hubs = nullptr;
+  int nhubs = 0;
+  int *ubuf = nullptr;  // device update staging: src | dst | w
+  int kcap = 0;
+  int *h_ubuf = nullptr;  // pinned host staging
+  int h_kcap = 0;
+  Ctrl *ctrl = nullptr;
+  Ctrl *h_ctrl = nullptr;  // pinned
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  unsigned round_base = 1;
+  int epoch = 0;
+  bool solved = false, side_valid = false;
+  dmf_stats st{};
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(e == cudaErrorMemoryAllocation ? DMF_ERR_OOM : DMF_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                  \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_fail(_e, what);  \
+  } while (0)
+
+template <class T>
+int dalloc(dmf_solver *sv, T **p, size_t count) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, sizeof(T) * std::max<size_t>(count, 1));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+  sv->allocs.push_back(q);
+  *p = (T *)q;
+  return DMF_OK;
+}
+
+void free_all(dmf_solver *sv) {
+  if (sv->dev >= 0) cudaSetDevice(sv->dev);
+  if (sv->stream) cudaStreamSynchronize(sv->stream);
+  for (void *q : sv->allocs) cudaFree(q);
+  sv->allocs.clear();
+  if (sv->h_ubuf) cudaFreeHost(sv->h_ubuf);
+  if (sv->h_ctrl) cudaFreeHost(sv->h_ctrl);
+  if (sv->ev0) cudaEventDestroy(sv->ev0);
+  if (sv->ev1) cudaEventDestroy(sv->ev1);
+  sv->h_ubuf = nullptr;
+  sv->h_ctrl = nullptr;
+  sv->ev0 = sv->ev1 = nullptr;
+}
+
+int choose_tile(const dmf_opts &o, int n, int m) {
+  if (o.tile == 1 || o.tile == 2 || o.tile == 4) return 4;
+  if (o.tile == 8 || o.tile == 16 || o.tile == 32) return o.tile;
+  double avg = n > 0 ? (double)m / n : 0;
+  if (avg <= 6) return 4;
+  if (avg <= 12) return 8;
+  if (avg <= 24) return 16;
+  return 32;
+}
+
+int configure(dmf_solver *sv) {
+  sv->tile = choose_tile(sv->opts, sv->n, sv->m);
+  sv->hub_deg = 8 * sv->tile;
+  KernelFn fn = pick_kernel(sv->tile);
+  int per_sm = 0, sms = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kBlock, 0), "occupancy");
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, sv->dev), "sm count");
+  int coop = 0;
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, sv->dev), "coop attr");
+  if (!coop || per_sm < 1) return fail(DMF_ERR_CUDA, "device does not support cooperative launch of the solver");
+  sv->grid = per_sm * sms;
+  sv->block = kBlock;
+  return DMF_OK;
+}
+
+int ensure_ubuf(dmf_solver *sv, int k) {
+  if (k <= sv->kcap) return DMF_OK;
+  int want = std::max(k, 1024);
+  int *nb = nullptr;
+  CK(cudaMalloc(&nb, sizeof(int) * 4 * (size_t)want), "cudaMalloc updates");
+  // uarc lives in the 4th quarter
+  if (sv->ubuf) {
+    cudaStreamSynchronize(sv->stream);
+    cudaFree(sv->ubuf);
+  }
+  sv->ubuf = nb;
+  sv->kcap = want;
+  return DMF_OK;
+}
+
+int ensure_host_ubuf(dmf_solver *sv, int k) {
+  if (k <= sv->h_kcap) return DMF_OK;
+  int want = std::max(k, 1024);
+  int *nb = nullptr;
+  CK(cudaMallocHost(&nb, sizeof(int) * 3 * (size_t)want), "cudaMallocHost");
+  if (sv->h_ubuf) {
+    cudaStreamSynchronize(sv->stream);
+    cudaFreeHost(sv->h_ubuf);
+  }
+  sv->h_ubuf = nb;
+  sv->h_kcap = want;
+  return DMF_OK;
+}
+
+int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, const int *d_w) {
+  Params p{};
+  p.n = sv->n;
+  p.m = sv->m;
+  p.s = sv->s;
+  p.t = sv->t;
+  p.off = sv->off;
+  p.adj = sv->adj;
+  p.par = sv->par;
+  p.sidx = sv->sidx;
+  p.cap = sv->cap;
+  p.res = sv->res;
+  p.height = sv->height;
+  p.stamp = sv->stamp;
+  p.astamp = sv->astamp;
+  p.uarc = sv->ubuf ? sv->ubuf + 3 * (size_t)sv->kcap : nullptr;
+  p.excess = sv->excess;
+  p.dead = sv->dead;
+  p.side = sv->side;
+  const size_t N = (size_t)sv->n + 1;
+  for (int i = 0; i < 2; i++) {
+    p.fq[i] = sv->qbuf + (0 + i) * N;
+    p.fh[i] = sv->qbuf + (2 + i) * N;
+    p.wq[i] = sv->qbuf + (4 + i) * N;
+    p.wh[i] = sv->qbuf + (6 + i) * N;
+  }
+  p.aq = sv->qbuf + 8 * N;
+  p.ah = sv->qbuf + 9 * N;
+  p.hubs = sv->hubs;
+  p.nhubs = sv->nhubs;
+  p.usrc = d_src;
+  p.udst = d_dst;
+  p.uw = d_w;
+  p.k = k;
+  p.ctrl = sv->ctrl;
+  p.mode = mode;
+  p.variant = sv->opts.variant;
+  const int avg = sv->n > 0 ? std::max(1, sv->m / sv->n) : 1;
+  p.cycles = sv->opts.kernel_cycles > 0 ? sv->opts.kernel_cycles : std::max(2, std::min(avg, 8));
+  p.interval = sv->opts.relabel_interval > 0 ? sv->opts.relabel_interval : 4;
+  p.max_iters = sv->opts.max_iters > 0 ? sv->opts.max_iters : 100000;
+  p.hub_deg = sv->hub_deg;
+  p.need_cut = sv->opts.variant == DMF_VARIANT_PP ? 1 : 0;
+  p.round_base = sv->round_base;
+  p.epoch = ++sv->epoch;
+  if (sv->epoch == INT_MAX) sv->epoch = 0;
+  CK(cudaMemsetAsync(sv->ctrl, 0, sizeof(Ctrl), sv->stream), "memset ctrl");
+  void *args[] = {&p};
+  CK(cudaLaunchCooperativeKernel((const void *)pick_kernel(sv->tile), dim3(sv->grid), dim3(sv->block), args, 0,
+                                 sv->stream),
+     "cooperative launch");
+  CK(cudaMemcpyAsync(sv->h_ctrl, sv->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, sv->stream), "D2H ctrl");
+  return DMF_OK;
+}
+
+// Waits for the launch sequence, records timing and maps device errors.
+int finish(dmf_solver *sv, int64_t *flow, bool need_cut_valid) {
+  CK(cudaEventRecord(sv->ev1, sv->stream), "event record");
+  CK(cudaEventSynchronize(sv->ev1), "solve");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, sv->ev0, sv->ev1);
+  const Ctrl &c = *sv->h_ctrl;
+  sv->st.last_ms = ms;
+  sv->st.outer_iters = (int64_t)c.st_outer;
+  sv->st.bfs_levels = (int64_t)c.st_levels;
+  sv->st.push_rounds = (int64_t)c.st_rounds;
+  sv->st.pushes = (int64_t)c.st_pushes;
+  sv->st.relabels = (int64_t)c.st_relabels;
+  sv->st.arcs_scanned = (int64_t)c.st_arcs;
+  sv->st.vertices_visited = (int64_t)c.st_visits;
+  sv->st.dead_vertices = (int64_t)c.st_dead;
+  sv->st.grid_blocks = sv->grid;
+  sv->st.block_threads = sv->block;
+  sv->st.tile = sv->tile;
+  sv->round_base += c.rounds_used + 2;
+  if (c.err) {
+    sv->solved = false;
+    sv->side_valid = false;
+    if (c.err & ERR_TIMEOUT) return fail(DMF_ERR_TIMEOUT, "a grid-barrier wait timed out");
+    if (c.err & ERR_UNKNOWN_ARC) {
+      // nothing was applied: lookup errors stop the launch before any change
+      sv->solved = true;
+      return fail(DMF_ERR_UNKNOWN_ARC, "update %d names an arc that is not in the graph", c.err_info);
+    }
+    if (c.err & ERR_DUP_ARC) {
+      sv->solved = true;
+      return fail(DMF_ERR_DUP_ARC, "update %d repeats an arc already in this batch", c.err_info);
+    }
+    if (c.err & ERR_BAD_UPDATE) {
+      sv->solved = true;
+      return fail(DMF_ERR_INVALID_ARG,
+                  "update %d: vertex out of range, capacity outside [0, 2^30-1], or capacity + partner "
+                  "capacity exceeds int32",
+                  c.err_info);
+    }
+    if (c.err & ERR_NO_CONV) return fail(DMF_ERR_NO_CONVERGENCE, "no convergence after %d global relabels", c.err_info);
+    return fail(DMF_ERR_CUDA, "device error flags 0x%x", c.err);
+  }
+  sv->solved = true;
+  sv->side_valid = need_cut_valid;
+  sv->st.flow = c.flow;
+  if (flow) *flow = c.flow;
+  return ok();
+}
+
+int run_mode(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, const int *d_w, int64_t *flow,
+             bool started) {
+  if (!started) CK(cudaEventRecord(sv->ev0, sv->stream), "event record");
+  int st = launch(sv, mode, k, d_src, d_dst, d_w);
+  if (st) return st;
+  return finish(sv, flow, sv->opts.variant == DMF_VARIANT_PP || mode == MODE_CUT);
+}
+
+int check_updates_args(dmf_solver *sv, int32_t k, const void *a, const void *b, const void *c) {
+  if (!sv) return fail(DMF_ERR_INVALID_ARG, "null solver");
+  if (k < 0 || (k > 0 && (!a || !b || !c))) return fail(DMF_ERR_INVALID_ARG, "bad update arrays");
+  return DMF_OK;
+}
+
+int host_updates(dmf_solver *sv, int mode, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
+                 int64_t *flow) {
+  int st = check_updates_args(sv, k, src, dst, w);
+  if (st) return st;
+  if (mode == MODE_DYNAMIC && !sv->solved) return fail(DMF_ERR_NOT_SOLVED, "apply_updates before a solve");
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  if ((st = ensure_ubuf(sv, k)) || (st = ensure_host_ubuf(sv, k))) return st;
+  const size_t K = (size_t)sv->kcap, HK = (size_t)sv->h_kcap;
+  std::memcpy(sv->h_ubuf, src, 4 * (size_t)k);
+  std::memcpy(sv->h_ubuf + HK, dst, 4 * (size_t)k);
+  std::memcpy(sv->h_ubuf + 2 * HK, w, 4 * (size_t)k);
+  CK(cudaEventRecord(sv->ev0, sv->stream), "event record");
+  if (k > 0) {
+    CK(cudaMemcpyAsync(sv->ubuf, sv->h_ubuf, 4 * (size_t)k, cudaMemcpyHostToDevice, sv->stream), "H2D src");
+    CK(cudaMemcpyAsync(sv->ubuf + K, sv->h_ubuf + HK, 4 * (size_t)k, cudaMemcpyHostToDevice, sv->stream), "H2D dst");
+    CK(cudaMemcpyAsync(sv->ubuf + 2 * K, sv->h_ubuf + 2 * HK, 4 * (size_t)k, cudaMemcpyHostToDevice, sv->stream),
+       "H2D w");
+  }
+  return run_mode(sv, mode, k, sv->ubuf, sv->ubuf + K, sv->ubuf + 2 * K, flow, true);
+}
+
+int device_updates(dmf_solver *sv, int mode, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
+                   int64_t *flow) {
+  int st = check_updates_args(sv, k, src, dst, w);
+  if (st) return st;
+  if (mode == MODE_DYNAMIC && !sv->solved) return fail(DMF_ERR_NOT_SOLVED, "apply_updates before a solve");
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  if ((st = ensure_ubuf(sv, k))) return st;  // for the per-update arc scratch
+  return run_mode(sv, mode, k, src, dst, w, flow, false);
+}
+
+}  // namespace
+
+extern "C" {
+
+int dmf_device_count(void) {
+  int c = 0;
+  if (cudaGetDeviceCount(&c) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return c;
+}
+
+int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, void *stream,
+                      dmf_solver **out) {
+  if (!g || !out) return fail(DMF_ERR_INVALID_ARG, "null argument");
+  if (g->n < 2 || s < 0 || t < 0 || s >= g->n || t >= g->n || s == t)
+    return fail(DMF_ERR_INVALID_ARG, "need n >= 2 and distinct s, t in [0, n): n=%d s=%d t=%d", g->n, s, t);
+  if ((int64_t)g->sidx.size() != g->m) return fail(DMF_ERR_INVALID_ARG, "graph has no arc index");
+  int ndev = dmf_device_count();
+  if (ndev == 0) return fail(DMF_ERR_CUDA, "no CUDA device is visible; the solver runs only on the GPU");
+  auto *sv = new dmf_solver();
+  if (opts) sv->opts = *opts;
+  else dmf_opts_default(&sv->opts);
+  if (sv->opts.variant < 0 || sv->opts.variant > 2) {
+    delete sv;
+    return fail(DMF_ERR_INVALID_ARG, "unknown variant %d", sv->opts.variant);
+  }
+  sv->n = g->n;
+  sv->m = g->m;
+  sv->s = s;
+  sv->t = t;
+  sv->stream = (cudaStream_t)stream;
+  int st = DMF_OK;
+  auto bail = [&](int code) {
+    std::string msg = dmf_last_error();
+    free_all(sv);
+    delete sv;
+    return fail(code, "%s", msg.c_str());
+  };
+  if (sv->opts.device >= 0) sv->dev = sv->opts.device;
+  else if (cudaGetDevice(&sv->dev) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "cudaGetDevice"));
+  if (cudaSetDevice(sv->dev) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "cudaSetDevice"));
+  if ((st = configure(sv))) return bail(st);
+  const size_t N = (size_t)g->n + 1, M = (size_t)g->m;
+  if ((st = dalloc(sv, &sv->off, N)) || (st = dalloc(sv, &sv->adj, M)) || (st = dalloc(sv, &sv->par, M)) ||
+      (st = dalloc(sv, &sv->sidx, M)) || (st = dalloc(sv, &sv->cap, M)) || (st = dalloc(sv, &sv->res, M)) ||
+      (st = dalloc(sv, &sv->astamp, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
+      (st = dalloc(sv, &sv->excess, N)) || (st = dalloc(sv, &sv->dead, N)) || (st = dalloc(sv, &sv->side, N)) ||
+      (st = dalloc(sv, &sv->qbuf, 10 * N)) || (st = dalloc(sv, &sv->ctrl, 1)))
+    return bail(st);
+  std::vector<int> hub_list;
+  for (int v = 0; v < g->n; v++)
+    if (g->off[v + 1] - g->off[v] > sv->hub_deg) hub_list.push_back(v);
+  sv->nhubs = (int)hub_list.size();
+  if ((st = dalloc(sv, &sv->hubs, hub_list.size()))) return bail(st);
+  cudaStream_t S = sv->stream;
+  cudaError_t e = cudaSuccess;
+  auto up = [&](void *d, const void *h, size_t bytes) {
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, S);
+  };
+  up(sv->off, g->off.data(), 4 * N);
+  up(sv->adj, g->adj.data(), 4 * M);
+  up(sv->par, g->par.data(), 4 * M);
+  up(sv->sidx, g->sidx.data(), 4 * M);
+  up(sv->cap, g->w.data(), 4 * M);
+  up(sv->hubs, hub_list.data(), 4 * hub_list.size());
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->astamp, 0, 4 * M, S);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->stamp, 0, 4 * N, S);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->dead, 0, N, S);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->side, 0, N, S);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->excess, 0, 8 * N, S);
+  if (e == cudaSuccess) e = cudaMallocHost(&sv->h_ctrl, sizeof(Ctrl));
+  if (e == cudaSuccess) e = cudaEventCreate(&sv->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&sv->ev1);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "solver upload"));
+  if ((st = ensure_ubuf(sv, 1024))) return bail(st);
+  *out = sv;
+  return ok();
+}
+
+int dmf_solver_set_opts(dmf_solver *sv, const dmf_opts *opts) {
+  if (!sv || !opts) return fail(DMF_ERR_INVALID_ARG, "null argument");
+  if (opts->variant < 0 || opts->variant > 2) return fail(DMF_ERR_INVALID_ARG, "unknown variant");
+  bool variant_changed = opts->variant != sv->opts.variant;
+  sv->opts = *opts;
+  if (cudaSetDevice(sv->dev) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaSetDevice");
+  int st = configure(sv);
+  if (st) return st;
+  if (variant_changed) sv->side_valid = false;
+  return ok();
+}
+
+int dmf_static_maxflow(dmf_solver *sv, int64_t *flow) {
+  if (!sv) return fail(DMF_ERR_INVALID_ARG, "null solver");
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  return run_mode(sv, MODE_STATIC, 0, nullptr, nullptr, nullptr, flow, false);
+}
+
+int dmf_apply_updates(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
+                      int64_t *flow) {
+  return host_updates(sv, MODE_DYNAMIC, k, src, dst, w, flow);
+}
+
+int dmf_apply_updates_device(dmf_solver *sv, int32_t k, const int32_t *d_src, const int32_t *d_dst,
+                             const int32_t *d_w, int64_t *flow) {
+  return device_updates(sv, MODE_DYNAMIC, k, d_src, d_dst, d_w, flow);
+}
+
+int dmf_recompute(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
+                  int64_t *flow) {
+  return host_updates(sv, MODE_RECOMPUTE, k, src, dst, w, flow);
+}
+
+int dmf_recompute_device(dmf_solver *sv, int32_t k, const int32_t *d_src, const int32_t *d_dst,
+                         const int32_t *d_w, int64_t *flow) {
+  return device_updates(sv, MODE_RECOMPUTE, k, d_src, d_dst, d_w, flow);
+}
+
+int dmf_flow_value(const dmf_solver *sv, int64_t *flow) {
+  if (!sv || !flow) return fail(DMF_ERR_INVALID_ARG, "null argument");
+  if (!sv->solved) return fail(DMF_ERR_NOT_SOLVED, "no solve yet");
+  *flow = sv->st.flow;
+  return ok();
+}
+
+int dmf_get_cut(dmf_solver *sv, uint8_t *sink_side) {
+  if (!sv || !sink_side) return fail(DMF_ERR_INVALID_ARG, "null argument");
+  if (!sv->solved) return fail(DMF_ERR_NOT_SOLVED, "no solve yet");
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  if (!sv->side_valid) {
+    int64_t f = sv->st.flow;
+    dmf_stats keep = sv->st;
+    int st = run_mode(sv, MODE_CUT, 0, nullptr, nullptr, nullptr, nullptr, false);
+    if (st) return st;
+    sv->st = keep;
+    sv->st.flow = f;
+    sv->side_valid = true;
+  }
+  CK(cudaMemcpyAsync(sink_side, sv->side, (size_t)sv->n, cudaMemcpyDeviceToHost, sv->stream), "D2H cut");
+  CK(cudaStreamSynchronize(sv->stream), "cut");
+  return ok();
+}
+
+int dmf_get_state(dmf_solver *sv, int32_t *cap, int32_t *res, int64_t *excess, int32_t *height) {
+  if (!sv) return fail(DMF_ERR_INVALID_ARG, "null solver");
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  const size_t M = (size_t)sv->m, N = (size_t)sv->n;
+  if (cap) CK(cudaMemcpyAsync(cap, sv->cap, 4 * M, cudaMemcpyDeviceToHost, sv->stream), "D2H cap");
+  if (res) CK(cudaMemcpyAsync(res, sv->res, 4 * M, cudaMemcpyDeviceToHost, sv->stream), "D2H res");
+  if (excess) CK(cudaMemcpyAsync(excess, sv->excess, 8 * N, cudaMemcpyDeviceToHost, sv->stream), "D2H excess");
+  if (height) CK(cudaMemcpyAsync(height, sv->height, 4 * N, cudaMemcpyDeviceToHost, sv->stream), "D2H height");
+  CK(cudaStreamSynchronize(sv->stream), "state");
+  return ok();
+}
+
+int dmf_stats_get(const dmf_solver *sv, dmf_stats *st) {
+  if (!sv || !st) return fail(DMF_ERR_INVALID_ARG, "null argument");
+  *st = sv->st;
+  return ok();
+}
+
+int dmf_solver_destroy(dmf_solver *sv) {
+  if (!sv) return ok();
+  if (sv->ubuf) {
+    cudaSetDevice(sv->dev);
+    if (sv->stream) cudaStreamSynchronize(sv->stream);
+    cudaFree(sv->ubuf);
+    sv->ubuf = nullptr;
+  }
+  free_all(sv);
+  delete sv;
+  return ok();
+}
+
+}  // extern "C"

@@ -1,0 +1,208 @@
+/*
+ * dmf.h -- C ABI of libdmf.so, the B200 dynamic s-t max-flow engine.
+ *
+ * The library is a drop-in for the hot path of ShruthiKannappan/dyn_maxflow:
+ * it reads the same CSR graph and update .bin formats and computes, after every
+ * capacity-update batch, the exact maximum s-t flow with push-relabel kernels
+ * written for sm_100a.  The reference has no library API; each entry point below
+ * names the reference function or kernel sequence it replaces (file:line in that
+ * project).
+ *
+ * Conventions
+ *   - Every function returns a dmf_status (0 = DMF_OK).  dmf_last_error()
+ *     returns a message for the last failure on the calling thread.  The
+ *     library never calls exit().
+ *   - Host arrays passed in are copied during the call; the caller keeps them.
+ *     Arrays returned through out-pointers are owned by the library and freed
+ *     with dmf_free() / dmf_graph_free().
+ *   - A dmf_solver owns all of its device memory, lives on one CUDA device and
+ *     one stream, and is not re-entrant.  Different solvers may be used
+ *     concurrently from different host threads.
+ *   - Capacities are int32 and must be >= 0; cap(e) + cap(partner(e)) must fit
+ *     in int32.  Flow values and excesses are int64.
+ *   - An update is (src, dst, w): the arc src->dst, which must already exist in
+ *     the CSR (reserved zero-capacity slots serve as insert targets), gets the
+ *     absolute new capacity w.  Updates with src == dst are ignored, as in the
+ *     reference.  An arc may appear at most once per batch.
+ */
+#ifndef DMF_H
+#define DMF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DMF_OK = 0,
+  DMF_ERR_INVALID_ARG = 1,   /* bad size, vertex id, s == t, negative capacity */
+  DMF_ERR_BAD_FILE = 2,      /* missing, truncated or inconsistent .bin */
+  DMF_ERR_UNKNOWN_ARC = 3,   /* update names an arc absent from the CSR */
+  DMF_ERR_DUP_ARC = 4,       /* an arc appears twice in one batch */
+  DMF_ERR_OOM = 5,           /* device or host allocation failed */
+  DMF_ERR_NO_CONVERGENCE = 6,/* outer-iteration bound reached */
+  DMF_ERR_CUDA = 7,          /* CUDA runtime error, or no usable device */
+  DMF_ERR_TIMEOUT = 8,       /* a bounded device-side wait gave up */
+  DMF_ERR_OVERFLOW = 9,      /* cap(e) + cap(partner) exceeds int32 */
+  DMF_ERR_NOT_SOLVED = 10    /* update or query before the first solve */
+} dmf_status;
+
+/* Algorithm variants: the three reference entry points. */
+typedef enum {
+  DMF_VARIANT_DATA = 0, /* dyn_data: worklist-driven push-relabel (code/dyn_data.h) */
+  DMF_VARIANT_TOPO = 1, /* dyn_topo: topology-driven sweeps (code/dyn_topo.h) */
+  DMF_VARIANT_PP = 2    /* dyn_pp: push-pull on the kept min-cut partition (code/dyn_pp.h) */
+} dmf_variant;
+
+typedef struct dmf_graph dmf_graph;   /* host CSR, owned by the library */
+typedef struct dmf_solver dmf_solver; /* device-resident residual state */
+
+typedef struct {
+  int32_t variant;          /* dmf_variant */
+  int32_t kernel_cycles;    /* push/relabel cycles per vertex visit; 0 = avg degree
+                               (the reference runs avg_deg-1, avg_deg, avg_deg+1,
+                               code/dyn_data_bench.cu:529-562) */
+  int32_t relabel_interval; /* push rounds between global relabels; 0 = adaptive */
+  int32_t tile;             /* lanes per vertex (1,2,4,8,16,32); 0 = chosen from degree */
+  int32_t max_iters;        /* bound on global-relabel iterations per solve; 0 = default */
+  int32_t device;           /* CUDA device ordinal; -1 = current device */
+  int32_t block_threads;    /* threads per block of the persistent kernel; 0 = 512 */
+  int32_t flags;            /* reserved, 0 */
+} dmf_opts;
+
+typedef struct {
+  int64_t flow;             /* last flow value */
+  int64_t outer_iters;      /* global relabels in the last solve */
+  int64_t bfs_levels;       /* BFS levels expanded in the last solve */
+  int64_t push_rounds;      /* worklist rounds in the last solve */
+  int64_t pushes;           /* non-zero pushes in the last solve */
+  int64_t relabels;         /* local relabels in the last solve */
+  int64_t arcs_scanned;     /* adjacency entries read in the last solve */
+  int64_t vertices_visited; /* vertex visits (BFS + push) in the last solve */
+  int64_t dead_vertices;    /* vertices proven unable to reach t or a deficit */
+  double last_ms;           /* device time of the last solve call (CUDA events) */
+  int32_t grid_blocks;      /* persistent-kernel grid */
+  int32_t block_threads;
+  int32_t tile;
+  int32_t pad;
+} dmf_stats;
+
+/* ---- errors and options ------------------------------------------------- */
+const char *dmf_last_error(void);
+const char *dmf_status_string(int status);
+void dmf_opts_default(dmf_opts *opts);
+void dmf_free(void *p);
+
+/* ---- graphs (host only; no GPU needed) ---------------------------------- */
+/* Replaces graph::loadGraph, code/graph.hpp:202-223 (no magic: int32 n, m,
+ * index[n+1], adj[m], w[m], par[m]).  Validates sizes, offsets, ids and the
+ * partner involution. */
+int dmf_graph_load(const char *path, dmf_graph **out);
+/* Builds from CSR arrays with the same validation as dmf_graph_load. */
+int dmf_graph_from_csr(int32_t n, int32_t m, const int32_t *index,
+                       const int32_t *adj, const int32_t *w, const int32_t *par,
+                       dmf_graph **out);
+/* Replaces input_create/create_bin.cpp:67-124 in O(k log k): self-loops
+ * dropped, duplicate arcs summed, a zero-capacity partner for every arc,
+ * adjacency in first-touch order (byte-identical .bin). */
+int dmf_graph_from_edges(int64_t k, const int32_t *u, const int32_t *v,
+                         const int32_t *w, dmf_graph **out);
+/* Writes the .bin, input_create/create_bin.cpp:18-64 (writeCSR). */
+int dmf_graph_save(const dmf_graph *g, const char *path);
+int dmf_graph_info(const dmf_graph *g, int32_t *n, int32_t *m);
+/* Borrowed pointers into the graph (valid until dmf_graph_free). */
+int dmf_graph_arrays(const dmf_graph *g, const int32_t **index,
+                     const int32_t **adj, const int32_t **w, const int32_t **par);
+/* Arc index of src->dst (last match, as OnAdd_kernel code/dyn_data.h:196-201),
+ * or -1. */
+int64_t dmf_graph_find_arc(const dmf_graph *g, int32_t src, int32_t dst);
+/* Sets the capacity of existing arcs on the host copy (the reference's
+ * update_kernel, code/dyn_data_bench.cu:300-322). */
+int dmf_graph_set_caps(dmf_graph *g, int32_t k, const int32_t *src,
+                       const int32_t *dst, const int32_t *w);
+void dmf_graph_free(dmf_graph *g);
+
+/* ---- update files (host only) ------------------------------------------- */
+/* Replaces loadUpdateFile, code/update.hpp:52-88 (int32 k, src[k], dst[k],
+ * w[k]); returns exactly k records (no zero-typed padding). */
+int dmf_updates_load(const char *path, int32_t *k, int32_t **src,
+                     int32_t **dst, int32_t **w);
+/* Writes the update .bin, input_create/create_update_bin.cpp:41-49. */
+int dmf_updates_save(const char *path, int32_t k, const int32_t *src,
+                     const int32_t *dst, const int32_t *w);
+
+/* ---- seeded generators (host only) -------------------------------------- */
+/* Directed 4-neighbour rows x cols grid, both directions, caps uniform
+ * [cap_lo, cap_hi] from `seed`; source = vertex (0,0) joined to every column-0
+ * vertex, sink = (rows-1, cols-1) fed by every last-column vertex, both with
+ * capacity st_cap (coinciding arcs summed, as create_bin does). */
+int dmf_gen_grid(int32_t rows, int32_t cols, uint64_t seed, int32_t cap_lo,
+                 int32_t cap_hi, int32_t st_cap, dmf_graph **out, int32_t *s,
+                 int32_t *t);
+/* R-MAT: 2^scale vertices, `narcs` directed samples with probabilities
+ * (a, b, c, 1-a-b-c); self-loops and duplicates dropped; caps uniform
+ * [cap_lo, cap_hi]; `reserve` extra distinct non-arcs added with capacity 0
+ * as insert slots.  s = max out-degree vertex, t = max in-degree vertex != s. */
+int dmf_gen_rmat(int32_t scale, int64_t narcs, double a, double b, double c,
+                 uint64_t seed, int32_t cap_lo, int32_t cap_hi, int64_t reserve,
+                 dmf_graph **out, int32_t *s, int32_t *t);
+/* Successive mixed batches over the graph's current capacities (the graph is
+ * not modified).  Each batch touches `frac` of the positive-capacity arcs
+ * (at least 1): p_inc increases (+U[1,delta_hi]), p_dec decreases
+ * (max(0, c-U[1,delta_hi])), p_ins inserts into zero-capacity slots (U[ins_lo,
+ * ins_hi]), the rest deletes (c -> 0).  Arcs are distinct within a batch.
+ * Output: batch b is [ofs[b], ofs[b+1]) of src/dst/w (library-owned). */
+int dmf_gen_batches(const dmf_graph *g, int32_t nbatches, double frac,
+                    double p_inc, double p_dec, double p_ins, int32_t delta_hi,
+                    int32_t ins_lo, int32_t ins_hi, uint64_t seed,
+                    int64_t **ofs, int32_t **src, int32_t **dst, int32_t **w);
+
+/* ---- solver (CUDA) ------------------------------------------------------ */
+/* Uploads the graph (the reference's cudaMalloc + H2D at
+ * code/dyn_data_bench.cu:182-217) and builds the device state.  `stream` is a
+ * cudaStream_t or NULL for the legacy default stream. */
+int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t,
+                      const dmf_opts *opts, void *stream, dmf_solver **out);
+/* Static solve from the solver's current capacities: replaces staticMaxFlow,
+ * code/dyn_data_bench.cu:8-97 (topo :16-75, pp code/dyn_pp_bench.cu:155-239),
+ * followed by the flow readout recalculate_max_flow_kernel_39
+ * (code/dyn_data.h:208-215). */
+int dmf_static_maxflow(dmf_solver *sv, int64_t *flow);
+/* One update batch from host arrays: replaces OnAdd_kernel
+ * (code/dyn_data.h:186-206) + Incremental (code/dyn_data_bench.cu:98-170; topo
+ * code/dyn_topo_bench.cu:76-119; pp code/dyn_pp_bench.cu:242-258) + kernel_39.
+ * Includes the H2D copy of the batch and the D2H read of the flow value. */
+int dmf_apply_updates(dmf_solver *sv, int32_t k, const int32_t *src,
+                      const int32_t *dst, const int32_t *w, int64_t *flow);
+/* The same with the batch already in device memory (device pointers). */
+int dmf_apply_updates_device(dmf_solver *sv, int32_t k, const int32_t *d_src,
+                             const int32_t *d_dst, const int32_t *d_w,
+                             int64_t *flow);
+/* From-scratch recompute after setting capacities: replaces update_kernel +
+ * static solve of static_recalculate (code/dyn_data_bench.cu:300-492). */
+int dmf_recompute(dmf_solver *sv, int32_t k, const int32_t *src,
+                  const int32_t *dst, const int32_t *w, int64_t *flow);
+int dmf_recompute_device(dmf_solver *sv, int32_t k, const int32_t *d_src,
+                         const int32_t *d_dst, const int32_t *d_w, int64_t *flow);
+/* Last flow value (host copy; no device work). */
+int dmf_flow_value(const dmf_solver *sv, int64_t *flow);
+/* Minimum-cut side per vertex: 1 = sink side (can reach t or a deficit in the
+ * residual graph), 0 = source side.  Replaces find_cut, code/dyn_pp.h:440-449. */
+int dmf_get_cut(dmf_solver *sv, uint8_t *sink_side);
+/* Device state copied to host (any pointer may be NULL): capacities and
+ * residuals per arc, excess and height per vertex. */
+int dmf_get_state(dmf_solver *sv, int32_t *cap, int32_t *res, int64_t *excess,
+                  int32_t *height);
+int dmf_stats_get(const dmf_solver *sv, dmf_stats *st);
+/* Replaces the option set of a live solver (variant, cycles, interval, tile). */
+int dmf_solver_set_opts(dmf_solver *sv, const dmf_opts *opts);
+int dmf_solver_destroy(dmf_solver *sv);
+
+/* Number of CUDA devices visible (0 without a GPU); never fails. */
+int dmf_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DMF_H */
