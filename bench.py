@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark: milliseconds to the exact max-flow per update batch.
+
+Workload (the reference's GPU-scale configuration): R-MAT scale 20
+(1,048,576 vertices, 16,777,216 directed samples, a=0.57 b=0.19 c=0.19,
+self-loops and duplicates dropped, capacities uniform [1,1000], source = max
+out-degree vertex, sink = max in-degree other vertex), then successive 1% update
+batches (40% increases, 40% decreases, 10% inserts into reserved zero-capacity
+slots, 10% deletes).  Inputs are synthetic and seeded.  One step = one batch.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--variant data|pp|topo]
+  python bench.py --impl reference ...   (the reference algorithm restated on the
+                                          host cores: oracle/, OpenMP)
+
+Prints one JSON line (rank 0).  `value` is the p50 device time per batch with the
+batch already in HBM (dmf_apply_updates_device, CUDA events on the solver's
+stream); `e2e` is the same metric through the host-array entry point
+dmf_apply_updates (pinned staging, H2D of the batch, D2H of the flow value)
+timed by the host clock.  Every batch's final device state is certified by the
+oracle's certificate checker outside the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms to exact maxflow per update batch (p50)"
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_solve_rmat20_traffic.json")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", default="data", choices=["data", "topo", "pp"])
+    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--kernel-cycles", type=int, default=0)
+    ap.add_argument("--relabel-interval", type=int, default=0)
+    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-certify", action="store_true")
+    ap.add_argument("--cpu-batches", type=int, default=3)
+    return ap.parse_args()
+
+
+def workload(scale: int, nbatches: int):
+    import dyn_maxflow_b200 as D
+    narcs = 16 << scale
+    reserve = int(0.1 * 0.01 * narcs * nbatches) + 16
+    g, s, t = D.gen_rmat(scale, narcs, 0.57, 0.19, 0.19, seed=0, cap_lo=1, cap_hi=1000, reserve=reserve)
+    batches = D.gen_batches(g, nbatches, frac=0.01, p_inc=0.4, p_dec=0.4, p_ins=0.1, delta_hi=500, ins_lo=1,
+                            ins_hi=1000, seed=1)
+    return g, s, t, batches
+
+
+def config_dict(args, g, s, t, batches):
+    return {
+        "workload": f"rmat{args.scale}-10x1pct-mixed",
+        "graph": f"R-MAT scale {args.scale} a=0.57 b=0.19 c=0.19, 16*2^scale samples, caps U[1,1000]",
+        "vertices": g.num_nodes(), "csr_arcs": g.num_edges(), "source": s, "sink": t,
+        "batch_updates": int(len(batches[0][0])), "batch_mix": "40% inc / 40% dec / 10% insert / 10% delete",
+        "variant": args.variant, "successive_batches": True,
+        "l2": "flushed before every timed batch (256 MiB write); working set > L2 as well",
+    }
+
+
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = (len(xs) - 1) * q
+    lo, hi = int(k), min(int(k) + 1, len(xs) - 1)
+    return xs[lo] + (xs[hi] - xs[lo]) * (k - lo)
+
+
+# ---------------------------------------------------------------------------
+def cpu_port_run(g, s, t, batches, nthreads):
+    """The reference's data-driven algorithm restated in oracle/ (OpenMP)."""
+    from oracle import build as OB
+    OB.build_oracle()
+    from oracle import oracle as O
+    off, adj, w, par = g.arrays()
+    n = g.num_nodes()
+    kc = max(1, g.num_edges() // n)
+    _, flows, ms = O.ref_run_successive("data", n, off, adj, w, par, s, t, kc, batches, nthreads=nthreads)
+    return list(flows), list(ms)
+
+
+class ClockSampler:
+    def __init__(self, device_index: int):
+        self.proc = None
+        self.path = os.path.join("/tmp", f"dmf_clocks_{os.getpid()}.csv")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(device_index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(st: dict, n: int, k: int, deg_s: int) -> int:
+    """Bytes a single solve must move, from the solver's own counters:
+    64 B per update (triple, lookup probes, stamps, apply, repair), 16 B per source
+    arc, 36 B per vertex per global relabel (seed/init + finalize passes), 12 B per
+    adjacency entry scanned (head, residual, neighbour label), 16 B per vertex
+    discharge, 24 B per push (two residual atomics, one 8-byte excess atomic), and
+    8 B per vertex for the flow reduction."""
+    return int(64 * k + 16 * deg_s + 36 * n * max(1, st["outer_iters"]) + 12 * st["arcs_scanned"]
+               + 16 * st["vertices_visited"] + 24 * st["pushes"] + 8 * n)
+
+
+def load_measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            d = json.load(open(p))
+            return float(d["hbm_gbs"]), "measured"
+        except (ValueError, KeyError):
+            pass
+    return 6650.0, "fallback"
+
+
+def run_ours(args, rank: int, world: int):
+    import numpy as np
+    import torch
+    import dyn_maxflow_b200 as D
+    from oracle import oracle as O
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    nb = args.warmup + args.steps
+    g, s, t, batches = workload(args.scale, nb)
+    n = g.num_nodes()
+    off, adj, w, par = g.arrays()
+    deg_s = int(off[s + 1] - off[s])
+    stream = torch.cuda.Stream()
+    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")  # 256 MiB > 126 MB L2
+    # ---- device-resident pass (value) ----
+    dbat = [[torch.as_tensor(x, dtype=torch.int32).cuda() for x in b] for b in batches]
+    torch.cuda.synchronize()
+    sv = D.Solver(g, s, t, variant=args.variant, kernel_cycles=args.kernel_cycles,
+                  relabel_interval=args.relabel_interval, tile=args.tile, stream=stream)
+    static_flow = sv.static_maxflow()
+    flows, times, stats = [], [], []
+    certified = True
+    sampler = None
+    t_region = None
+    for i, b in enumerate(dbat):
+        timed = i >= args.warmup
+        if timed and sampler is None:
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            sampler = ClockSampler(dev)
+            t_region = time.perf_counter()
+        flush.fill_(i)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        f = sv.apply_updates_device(b[0].data_ptr(), b[1].data_ptr(), b[2].data_ptr(), int(b[0].numel()))
+        e1.record(stream)
+        e1.synchronize()
+        if timed:
+            times.append(e0.elapsed_time(e1))
+            stats.append(sv.stats())
+        flows.append(f)
+        if not args.no_certify and timed:
+            cap, res, ex, _ = sv.state()
+            rc, val, cut = O.certify(n, off, adj, cap, par, res, s, t)
+            certified &= (rc == 0 and val == f == cut)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    region_s = time.perf_counter() - t_region
+    clocks = sampler.stop() if sampler else None
+    sv.close()
+    # ---- end-to-end pass through the host-array entry point ----
+    sv2 = D.Solver(g, s, t, variant=args.variant, kernel_cycles=args.kernel_cycles,
+                   relabel_interval=args.relabel_interval, tile=args.tile, stream=stream)
+    assert sv2.static_maxflow() == static_flow
+    e2e = []
+    flows2 = []
+    for i, b in enumerate(batches):
+        flush.fill_(i)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f = sv2.apply_updates(*b)
+        dt = (time.perf_counter() - t0) * 1e3
+        flows2.append(f)
+        if i >= args.warmup:
+            e2e.append(dt)
+    sv2.close()
+    consistent = flows == flows2
+    # ---- roofline of the solve kernel ----
+    abytes = [algorithmic_bytes(st, n, int(len(batches[args.warmup + j][0])), deg_s) for j, st in enumerate(stats)]
+    avg_bytes = sum(abytes) / len(abytes)
+    avg_ms = sum(times) / len(times)
+    peak, peak_kind = load_measured_peak()
+    achieved = avg_bytes / (avg_ms * 1e-3) / 1e9
+    traffic = None
+    if os.path.exists(PROFILE_SUMMARY):
+        try:
+            traffic = json.load(open(PROFILE_SUMMARY)).get("dram_bytes_per_launch")
+        except ValueError:
+            traffic = None
+    p50, p99 = pct(times, 0.5), pct(times, 0.99)
+    res = {
+        "metric": METRIC, "value": round(p50, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(avg_ms, 4), "p50_ms": round(p50, 4), "p99_ms": round(p99, 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int32 (int64 excess)",
+        "data": "synthetic (seeded R-MAT and update generators)", "config": config_dict(args, g, s, t, batches),
+        "parallelism": "replicas" if world > 1 else "single",
+        "static_flow": static_flow, "flows": flows[args.warmup:], "certified": bool(certified and consistent),
+        "timed_region_s": round(region_s, 3),
+        "e2e": {"value": round(pct(e2e, 0.5), 4), "unit": "ms", "p99": round(pct(e2e, 0.99), 4),
+                "h2d_bytes_per_step": int(12 * len(batches[-1][0])), "d2h_bytes_per_step": 8,
+                "api": "dmf_apply_updates (host arrays)"},
+        "gpu_launches": len(times),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_solve", "algorithmic_bytes_per_launch": int(avg_bytes)},
+        "solver_stats_mean": {k: round(sum(st[k] for st in stats) / len(stats), 1)
+                              for k in ("outer_iters", "bfs_levels", "push_rounds", "pushes", "relabels",
+                                        "arcs_scanned", "vertices_visited", "dead_vertices")},
+        "clocks": clocks,
+    }
+    if world > 1:
+        tt = torch.tensor([p50, avg_ms, pct(e2e, 0.5)], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        res["value"], res["ms_per_step"], res["e2e"]["value"] = [round(x, 4) for x in tt.tolist()]
+        res["throughput_batches_per_s"] = round(world * 1e3 / res["ms_per_step"], 2)
+    if rank == 0 and not args.no_cpu_baseline:
+        nth = os.cpu_count() or 1
+        k = max(1, min(args.cpu_batches, len(batches)))
+        t0 = time.perf_counter()
+        cflows, cms = cpu_port_run(g, s, t, batches[:k], nth)
+        res["cpu_baseline"] = {"value": round(statistics.median(cms), 3), "unit": "ms", "cores": nth,
+                               "kind": "port",
+                               "sample": f"first {k} successive batches of the same workload after an untimed "
+                                         f"static solve ({time.perf_counter() - t0:.1f} s total)",
+                               "flows_match": [int(x) for x in cflows] == flows[:k]}
+    return res
+
+
+def run_reference(args, rank: int):
+    if rank != 0:
+        return None
+    nb = args.warmup + args.steps
+    g, s, t, batches = workload(args.scale, nb)
+    nth = os.cpu_count() or 1
+    flows, ms = cpu_port_run(g, s, t, batches, nth)
+    timed = ms[args.warmup:]
+    p50 = pct(timed, 0.5)
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(p50, 3), "unit": "ms", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sum(timed) / len(timed), 3),
+        "p99_ms": round(pct(timed, 0.99), 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32 (int64 excess)", "data": "synthetic (seeded R-MAT and update generators)",
+        "config": config_dict(args, g, s, t, batches),
+        "cpu_baseline": {"value": round(p50, 3), "unit": "ms", "cores": nth, "kind": "port",
+                         "sample": f"{args.steps} timed successive batches (after {args.warmup} warm-up) of the "
+                                   "full workload, reference data-driven algorithm restated in oracle/ (OpenMP)"},
+        "e2e": {"value": round(p50, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "flows": [int(x) for x in flows[args.warmup:]],
+    }
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    distributed = world > 1 and args.impl == "ours"
+    if distributed:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        res = run_reference(args, rank) if args.impl == "reference" else run_ours(args, rank, world)
+    finally:
+        if distributed:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+    if rank == 0 and res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()
