@@ -179,8 +179,9 @@ def run_ours(args, rank: int, world: int):
     dbat = [[torch.as_tensor(x, dtype=torch.int32).cuda() for x in b] for b in batches]
     torch.cuda.synchronize()
     sv = D.Solver(g, s, t, variant=args.variant, kernel_cycles=args.kernel_cycles,
-                  relabel_interval=args.relabel_interval, tile=args.tile, stream=stream)
+                  relabel_interval=args.relabel_interval, tile=args.tile, stream=stream, trace=True)
     static_flow = sv.static_maxflow()
+    phase_us = {}
     flows, times, stats = [], [], []
     certified = True
     sampler = None
@@ -203,6 +204,11 @@ def run_ours(args, rank: int, world: int):
         if timed:
             times.append(e0.elapsed_time(e1))
             stats.append(sv.stats())
+            tr = sv.trace()
+            for (k0, t0_), (k1, t1_) in zip(tr, tr[1:]):
+                d = phase_us.setdefault(k1, [0.0, 0])
+                d[0] += t1_ - t0_
+                d[1] += 1
         flows.append(f)
         if not args.no_certify and timed:
             cap, res, ex, _ = sv.state()
@@ -263,6 +269,8 @@ def run_ours(args, rank: int, world: int):
                               for k in ("outer_iters", "bfs_levels", "push_rounds", "pushes", "relabels",
                                         "arcs_scanned", "vertices_visited", "dead_vertices")},
         "clocks": clocks,
+        "phases_us_per_batch": {k: {"us": round(v[0] / len(times), 1), "count": round(v[1] / len(times), 1)}
+                                for k, v in sorted(phase_us.items(), key=lambda kv: -kv[1][0])},
     }
     if world > 1:
         tt = torch.tensor([p50, avg_ms, pct(e2e, 0.5)], dtype=torch.float64, device="cuda")

@@ -92,6 +92,8 @@ _sig("dmf_flow_value", C.c_int, VP, C.POINTER(C.c_int64))
 _sig("dmf_get_cut", C.c_int, VP, U8P)
 _sig("dmf_get_state", C.c_int, VP, VP, VP, VP, VP)
 _sig("dmf_stats_get", C.c_int, VP, C.POINTER(Stats))
+_sig("dmf_trace_get", C.c_int, VP, C.c_int32, I32P, np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"),
+     C.POINTER(C.c_int32))
 _sig("dmf_solver_set_opts", C.c_int, VP, C.POINTER(Opts))
 _sig("dmf_solver_destroy", C.c_int, VP)
 _sig("dmf_device_count", C.c_int)
@@ -240,12 +242,13 @@ class Solver:
     """Device-resident residual state of one graph on one GPU (dmf_solver)."""
 
     def __init__(self, g: Graph, source: int, sink: int, variant="data", kernel_cycles=0, relabel_interval=0,
-                 tile=0, max_iters=0, device=-1, stream=None):
+                 tile=0, max_iters=0, device=-1, stream=None, trace=False):
         o = Opts()
         _L.dmf_opts_default(C.byref(o))
         o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
         o.kernel_cycles, o.relabel_interval, o.tile, o.max_iters, o.device = (
             kernel_cycles, relabel_interval, tile, max_iters, device)
+        o.flags = 1 if trace else 0
         self._h = C.c_void_p()
         self.n, self.m = g.num_nodes(), g.num_edges()
         stream_ptr = None if stream is None else C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
@@ -315,6 +318,19 @@ class Solver:
         h = np.zeros(max(self.n, 1), np.int32)
         _check(_L.dmf_get_state(self._h, cap.ctypes.data, res.ctypes.data, ex.ctypes.data, h.ctypes.data))
         return cap[:self.m], res[:self.m], ex[:self.n], h[:self.n]
+
+    TRACE_KINDS = {0: "start", 1: "init_res", 2: "saturate", 3: "lookup", 4: "apply", 5: "repair",
+                   6: "cut_saturate", 7: "bfs_init", 8: "bfs_td", 9: "bfs_bu", 10: "bfs_finalize", 11: "push",
+                   12: "flow"}
+
+    def trace(self):
+        """[(phase kind, end time in us since kernel start)] of the last solve (trace=True)."""
+        cnt = C.c_int32()
+        cap = 8192
+        kinds = np.zeros(cap, np.int32)
+        t = np.zeros(cap, np.float64)
+        _check(_L.dmf_trace_get(self._h, cap, kinds, t, C.byref(cnt)))
+        return [(self.TRACE_KINDS.get(int(k), str(k)), float(x)) for k, x in zip(kinds[:cnt.value], t[:cnt.value])]
 
     def stats(self) -> dict:
         st = Stats()

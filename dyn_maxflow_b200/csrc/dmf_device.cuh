@@ -34,7 +34,7 @@ struct Slot {
   int q;             // normal-queue tail
   int hq;            // hub-queue tail
   long long arcs;    // sum of degrees of appended vertices
-  int cnt;           // generic counter
+  int cnt;           // generic counter (BFS: active vertices labelled; topo push: active seen)
   int pad;
 };
 
@@ -48,13 +48,13 @@ struct Ctrl {
   // per global relabel
   int act_q, act_hq;          // active list tails built by the BFS
   int pos_count;              // vertices with excess > 0 (not s, t, dead)
-  int reached;                // positive-excess vertices labelled so far
+  int pad0;
   long long unexplored;       // arcs of not-yet-labelled candidate vertices
   long long flow;             // result
   // statistics
   unsigned long long st_outer, st_levels, st_rounds, st_pushes, st_relabels, st_arcs, st_visits, st_dead;
   unsigned int rounds_used;
-  int pad;
+  int trace_len;              // entries written to the optional timeline
 };
 
 // ---- memory helpers ---------------------------------------------------------
@@ -137,7 +137,7 @@ struct TileGroup {
   cg::thread_block_tile<T> g;
   __device__ TileGroup() : g(cg::tiled_partition<T>(cg::this_thread_block())) {}
   __device__ __forceinline__ int rank() const { return (int)g.thread_rank(); }
-  static constexpr int size() { return T; }
+  __host__ __device__ static constexpr int size() { return T; }
   // exclusive prefix sum and total
   __device__ __forceinline__ long long scan(long long x, long long &tot) {
     long long pre = cg::exclusive_scan(g, x, cg::plus<long long>());
@@ -163,7 +163,7 @@ struct BlockGroup {
   long long *bcast_l;
   __device__ BlockGroup(Temp &t, int *bi, long long *bl) : tmp(t), bcast_i(bi), bcast_l(bl) {}
   __device__ __forceinline__ int rank() const { return (int)threadIdx.x; }
-  static constexpr int size() { return BLOCK; }
+  __host__ __device__ static constexpr int size() { return BLOCK; }
   __device__ __forceinline__ long long scan(long long x, long long &tot) {
     long long pre;
     __syncthreads();

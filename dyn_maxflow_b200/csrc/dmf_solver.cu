@@ -32,6 +32,13 @@ constexpr int kBlock = 512;
 
 enum Mode : int { MODE_STATIC = 0, MODE_DYNAMIC = 1, MODE_RECOMPUTE = 2, MODE_CUT = 3 };
 
+// Phase kinds of the optional timeline (dmf_trace_get); values are part of the ABI.
+enum TraceKind : int {
+  TR_START = 0, TR_INIT_RES = 1, TR_SATURATE = 2, TR_LOOKUP = 3, TR_APPLY = 4, TR_REPAIR = 5,
+  TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
+  TR_FLOW = 12
+};
+
 // Largest capacity an update may set: keeps cap(e) + cap(partner) < 2^31 when
 // both arcs of a pair change in one batch.
 constexpr int kMaxUpdateCap = (1 << 30) - 1;
@@ -54,6 +61,8 @@ struct Params {
   int mode, variant, cycles, interval, max_iters, hub_deg, need_cut;
   unsigned round_base;
   int epoch;
+  unsigned long long *trace;  // optional phase timeline: 2 words per entry
+  int trace_cap;
 };
 
 struct LStats {
@@ -205,8 +214,13 @@ __device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
   int pos = 0;
   long long unexpl = 0, seed_arcs = 0;
   for (int v = gt; v < p.n; v += nt) {
-    if (reset_dead) p.dead[v] = 0;
-    else if (__ldcg(p.dead + v)) continue;
+    bool was_dead = false;
+    if (reset_dead) {
+      was_dead = __ldcg(p.dead + v) != 0;
+      if (was_dead) p.dead[v] = 0;
+    } else if (__ldcg(p.dead + v)) {
+      continue;
+    }
     long long ex = __ldcg(p.excess + v);
     int d = deg_of(p, v);
     if (v == p.t || (v != p.s && ex < 0)) {
@@ -216,7 +230,9 @@ __device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
       seed_arcs += d;
     } else {
       p.height[v] = UNV;
-      unexpl += d;
+      // direction heuristic: vertices that could not reach t or a deficit at the
+      // end of the previous solve are not expected to be labelled now
+      if (!was_dead) unexpl += d;
     }
     if (v != p.s && v != p.t && ex > 0) pos++;
   }
@@ -242,9 +258,11 @@ __device__ __forceinline__ void bfs_visit(const Params &p, Slot *out, int nxt, i
   }
 }
 
+// Counts go to the phase's own slot: a cross-phase counter would be read by a
+// slow block after a fast block already added to it in the next phase.
 __device__ __forceinline__ void flush_visits(const Params &p, Slot *out, VisitAcc &acc) {
   agg_add_ll(&out->arcs, acc.arcs);
-  agg_add_int(&p.ctrl->reached, acc.reached);
+  agg_add_int(&out->cnt, acc.reached);
 }
 
 // Top-down level (staticMaxFlow_kernel_11, code/dyn_data.h:72-87, run over the
@@ -282,21 +300,60 @@ __device__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LSt
   flush_visits(p, out, acc);
 }
 
-// Bottom-up level: every unvisited vertex looks for a residual arc into level L.
+// Bottom-up level: every unvisited vertex looks for a residual arc into level
+// L and stops at the first one.  Hubs are searched by a whole block (strided,
+// with a shared found-flag polled every 8 strides); other vertices by a tile.
+template <int TILE>
 __device__ void ph_bfs_bu(const Params &p, Slot *out, int L, LStats &ls) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int nxt = (L & 1) ^ 1;
   VisitAcc acc;
-  for (int v = gt; v < p.n; v += nt) {
-    if (__ldcg(p.height + v) != UNV) continue;
-    int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
-    for (int a = beg; a < end; a++) {
+  __shared__ int s_found;
+  for (int i = blockIdx.x; i < p.nhubs; i += gridDim.x) {
+    const int v = __ldg(p.hubs + i);
+    if (__ldcg(p.height + v) != UNV) continue;  // block-uniform: only v's block writes it
+    if (threadIdx.x == 0) s_found = 0;
+    __syncthreads();
+    const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
+    int it = 0;
+    for (int a = beg + threadIdx.x; a < end; a += blockDim.x, it++) {
+      if ((it & 7) == 7 && *(volatile int *)&s_found) break;
       ls.arcs++;
       if (__ldcg(p.res + a) > 0 && __ldcg(p.height + __ldg(p.adj + a)) == L) {
-        p.height[v] = L + 1;
-        bfs_visit(p, out, nxt, v, acc);
+        s_found = 1;
         break;
       }
+    }
+    __syncthreads();
+    const bool found = s_found != 0;
+    if (found && threadIdx.x == 0) {
+      p.height[v] = L + 1;
+      bfs_visit(p, out, nxt, v, acc);
+    }
+    __syncthreads();
+  }
+  cg::thread_block_tile<TILE> tile = cg::tiled_partition<TILE>(cg::this_thread_block());
+  const int lane = tile.thread_rank();
+  for (int v = gt / TILE; v < p.n; v += nt / TILE) {
+    if (__ldcg(p.height + v) != UNV) continue;  // same address for the whole tile
+    const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
+    if (end - beg > p.hub_deg) continue;
+    bool found = false;
+    for (int base = beg; base < end; base += TILE) {
+      const int a = base + lane;
+      bool hit = false;
+      if (a < end) {
+        ls.arcs++;
+        hit = __ldcg(p.res + a) > 0 && __ldcg(p.height + __ldg(p.adj + a)) == L;
+      }
+      if (tile.any(hit)) {
+        found = true;
+        break;
+      }
+    }
+    if (found && lane == 0) {
+      p.height[v] = L + 1;
+      bfs_visit(p, out, nxt, v, acc);
     }
   }
   flush_visits(p, out, acc);
@@ -332,12 +389,29 @@ __device__ __forceinline__ void enqueue(const Params &p, Slot *out, int buf, uns
   else append(p.wq[buf], &out->q, v);
 }
 
-// Discharge of v by a group (warp tile or block): up to `cycles` scans of the
-// adjacency; each scan pushes the excess over every admissible arc (height
-// below h) in arc order, allotted by a prefix sum, and relabels to
-// 1 + min height over the arcs still residual when excess is left.  This is the
-// push/relabel of staticMaxFlow_kernel_14 (code/dyn_data.h:89-131) with all
-// admissible arcs used per scan instead of only the lowest one.
+__device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, Slot *out, int buf, unsigned round_id,
+                                         bool enq, LStats &ls) {
+  atomicSub(p.res + a, d);
+  atomicAdd(p.res + __ldg(p.par + a), d);
+  long long old = atomic_add_ll(p.excess + w, d);
+  ls.pushes++;
+  if (enq && w != p.s && w != p.t && old + d > 0) enqueue(p, out, buf, round_id, w);
+}
+
+// Discharge of v by a group (warp tile or block): up to `cycles` rounds of
+// push-then-relabel, the push/relabel of staticMaxFlow_kernel_14
+// (code/dyn_data.h:89-131) with every admissible arc (head below h) used per
+// round instead of only the lowest one.
+//  * adjacency within one group width: one load per lane, the excess is split
+//    over the admissible arcs in arc order by a group prefix sum;
+//  * longer adjacency (hubs): pass 1 has every lane sum the admissible residual
+//    and the minimum non-admissible height over its strided arcs (independent
+//    loads, no group synchronisation inside the loop); a group prefix sum turns
+//    the sums into per-lane budgets; pass 2 pushes each lane's budget greedily.
+// When every admissible arc was saturated and excess is left, h becomes
+// 1 + the minimum height over the arcs still residual.  Concurrent relabels only
+// raise heights, so a pass-2 arc that lost admissibility is skipped and the round
+// is retried instead of relabelled.
 template <class G>
 __device__ void discharge(G &g, const Params &p, int v, Slot *out, int buf, unsigned round_id, bool enq,
                           LStats &ls, int *seen) {
@@ -372,10 +446,10 @@ __device__ void discharge(G &g, const Params &p, int v, Slot *out, int buf, unsi
   }
   long long ex = ex0;
   const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
+  constexpr int S = G::size();
   for (int cyc = 0; cyc < p.cycles && ex > 0 && h < p.n; cyc++) {
-    int minh = INT_MAX;
-    for (int base = beg; base < end; base += G::size()) {
-      const int a = base + g.rank();
+    if (end - beg <= S) {
+      const int a = beg + g.rank();
       int r = 0, w = -1, hw = INT_MAX;
       if (a < end) {
         r = __ldcg(p.res + a);
@@ -393,25 +467,59 @@ __device__ void discharge(G &g, const Params &p, int v, Slot *out, int buf, unsi
         long long left = ex - pre;
         d = left <= 0 ? 0 : (left < r ? (int)left : r);
       }
-      if (d > 0) {
-        atomicSub(p.res + a, d);
-        atomicAdd(p.res + __ldg(p.par + a), d);
-        long long old = atomic_add_ll(p.excess + w, d);
-        ls.pushes++;
-        if (enq && w != p.s && w != p.t && old + d > 0) enqueue(p, out, buf, round_id, w);
-      }
-      if (r > 0 && !(adm && d == r)) minh = min(minh, hw);
+      if (d > 0) push_arc(p, a, w, d, out, buf, round_id, enq, ls);
       ex -= (tot < ex ? tot : ex);
-      if (ex == 0) break;
+      if (ex > 0) {
+        const int mh = g.min_all(r > 0 && !(adm && d == r) ? hw : INT_MAX);
+        h = mh >= p.n ? p.n : mh + 1;
+        if (g.rank() == 0) {
+          p.height[v] = h;
+          ls.relabels++;
+        }
+      }
+      continue;
     }
-    if (ex > 0) {
-      const int mh = g.min_all(minh);
+    // pass 1
+    long long tsum = 0;
+    int tmin = INT_MAX;
+#pragma unroll 4
+    for (int a = beg + g.rank(); a < end; a += S) {
+      const int r = __ldcg(p.res + a);
+      if (r > 0) {
+        const int hw = __ldcg(p.height + __ldg(p.adj + a));
+        if (hw < h) tsum += r;
+        else tmin = min(tmin, hw);
+      }
+    }
+    ls.arcs += (unsigned long long)((end - beg - g.rank() + S - 1) / S);
+    long long tot;
+    const long long pre = g.scan(tsum, tot);
+    // pass 2
+    long long budget = ex - pre;
+    budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
+    long long done = 0;
+    for (int a = beg + g.rank(); a < end && budget > 0; a += S) {
+      const int r = __ldcg(p.res + a);
+      if (r <= 0) continue;
+      const int w = __ldg(p.adj + a);
+      if (__ldcg(p.height + w) >= h) continue;
+      const int d = (int)(r < budget ? r : budget);
+      push_arc(p, a, w, d, out, buf, round_id, enq, ls);
+      budget -= d;
+      done += d;
+    }
+    const long long moved = g.sum_all(done);
+    const long long planned = tot < ex ? tot : ex;
+    ex -= moved;
+    if (ex > 0 && moved == tot) {  // all admissible arcs saturated: relabel
+      const int mh = g.min_all(tmin);
       h = mh >= p.n ? p.n : mh + 1;
       if (g.rank() == 0) {
         p.height[v] = h;
         ls.relabels++;
       }
     }
+    (void)planned;
   }
   if (g.rank() == 0) {
     if (ex0 != ex) atomic_add_ll(p.excess + v, ex - ex0);
@@ -427,7 +535,6 @@ __device__ void ph_push(const Params &p, const Slot *in, Slot *out, int r, unsig
   const bool topo = p.variant == DMF_VARIANT_TOPO;
   if (r == 0 && gt == 0) {  // read during the BFS just finished; cleared for the next one
     c->pos_count = 0;
-    c->reached = 0;
     c->unexplored = 0;
   }
   const int buf = r & 1;
@@ -497,42 +604,62 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
   Ctrl *c = p.ctrl;
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   int ph = 0;
+  int kind = 0;  // phase kind, recorded in the optional timeline
   auto slot_out = [&]() { return &c->slot[ph % 3]; };
   auto slot_in = [&]() { return &c->slot[(ph + 2) % 3]; };
+  auto record = [&]() {
+    if (lead && p.trace && ph < p.trace_cap) {
+      p.trace[2 * ph] = (unsigned long long)kind;
+      p.trace[2 * ph + 1] = globaltimer();
+    }
+  };
   auto next = [&]() -> bool {
     if (!grid_barrier(c)) return false;
     ph++;
+    record();
     if (lead) clear_slot(&c->slot[(ph + 1) % 3]);
     return true;
   };
+  record();
   if (lead) clear_slot(&c->slot[1]);
 
   // ---- prologue --------------------------------------------------------------
   if (p.mode == MODE_STATIC) {
+    kind = TR_INIT_RES;
     ph_init_res(p);
     if (!next()) return;
+    kind = TR_SATURATE;
     ph_saturate(p);
     if (!next()) return;
   } else if (p.mode == MODE_DYNAMIC) {
+    kind = TR_LOOKUP;
     ph_lookup(p);
     if (!next()) return;
+    kind = TR_APPLY;
     ph_apply(p, true);
     if (!next()) return;
+    kind = TR_REPAIR;
     ph_repair(p);
     if (!next()) return;
     if (p.variant == DMF_VARIANT_PP) {
+      kind = TR_CUT_SATURATE;
       ph_cut_saturate(p);
       if (!next()) return;
     }
+    kind = TR_SATURATE;
     ph_saturate(p);
     if (!next()) return;
   } else if (p.mode == MODE_RECOMPUTE) {
+    kind = TR_LOOKUP;
     ph_lookup(p);
     if (!next()) return;
+    kind = TR_APPLY;
     ph_apply(p, false);
     if (!next()) return;
+    kind = TR_INIT_RES;
     ph_init_res(p);
     if (!next()) return;
+    kind = TR_SATURATE;
     ph_saturate(p);
     if (!next()) return;
   }
@@ -545,6 +672,7 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
       if (lead) set_err(c, ERR_NO_CONV, it);
       return;
     }
+    kind = TR_BFS_INIT;
     ph_bfs_init(p, slot_out(), it == 0);
     if (!next()) return;
     if (lead) c->st_outer++;
@@ -553,40 +681,50 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
     if (P == 0 && !want_cut) break;
     long long m_u = ld_vol(&c->unexplored);
     bool bu = false, full = true;
-    int L = 0;
+    int L = 0, reached = 0;
     for (;; L++) {
       const Slot *in = slot_in();
       const int F = ld_vol(&in->q) + ld_vol(&in->hq);
       const long long m_f = ld_vol(&in->arcs);
+      reached += ld_vol(&in->cnt);
       if (F == 0) break;  // complete
-      if (!cut_only && P > 0 && ld_vol(&c->reached) == P) {
+      if (!cut_only && P > 0 && reached == P) {
         full = false;  // every active vertex has its exact distance
         break;
       }
       if (L > 0) m_u -= m_f;
       if (!bu && m_f * 14 > m_u) bu = true;
       else if (bu && (long long)F * 24 < p.n) bu = false;
-      if (bu) ph_bfs_bu(p, slot_out(), L, ls);
+      kind = bu ? TR_BFS_BU : TR_BFS_TD;
+      if (bu) ph_bfs_bu<TILE>(p, slot_out(), L, ls);
       else ph_bfs_td<TILE>(p, in, slot_out(), L, ls);
       if (!next()) return;
       if (lead) c->st_levels++;
     }
+    kind = TR_BFS_FINALIZE;
     ph_bfs_finalize(p, full, L + 1, full && want_cut);
     if (!next()) return;
     const int A = ld_vol(&c->act_q) + ld_vol(&c->act_hq);
     if (A == 0 || cut_only) break;
     for (int r = 0; r < p.interval; r++) {
       round_id++;
+      kind = TR_PUSH;
       ph_push<TILE, BLOCK>(p, slot_in(), slot_out(), r, round_id, ls, btmp, bci, bcl);
       if (!next()) return;
-      if (lead) c->st_rounds++;
+      if (lead) {
+        c->st_rounds++;
+        c->rounds_used = round_id - p.round_base;
+      }
       const Slot *in = slot_in();
       const int W = p.variant == DMF_VARIANT_TOPO ? ld_vol(&in->cnt) : ld_vol(&in->q) + ld_vol(&in->hq);
       if (W == 0) break;
     }
   }
+  kind = TR_FLOW;
   ph_flow<BLOCK>(p, btmp);
   if (lead) c->rounds_used = round_id - p.round_base;
+  // the flow phase ends without a barrier; its end is the kernel's end
+  if (lead && p.trace && ph + 1 < p.trace_cap) c->trace_len = ph + 1;
 }
 
 template <int TILE, int BLOCK>
@@ -647,6 +785,8 @@ struct dmf_solver {
   int h_kcap = 0;
   Ctrl *ctrl = nullptr;
   Ctrl *h_ctrl = nullptr;  // pinned
+  unsigned long long *trace = nullptr;  // device timeline (opts.flags & DMF_FLAG_TRACE)
+  int trace_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   unsigned round_base = 1;
   int epoch = 0;
@@ -789,6 +929,8 @@ int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, 
   p.hub_deg = sv->hub_deg;
   p.need_cut = sv->opts.variant == DMF_VARIANT_PP ? 1 : 0;
   p.round_base = sv->round_base;
+  p.trace = (sv->opts.flags & DMF_FLAG_TRACE) ? sv->trace : nullptr;
+  p.trace_cap = sv->trace_cap;
   p.epoch = ++sv->epoch;
   if (sv->epoch == INT_MAX) sv->epoch = 0;
   CK(cudaMemsetAsync(sv->ctrl, 0, sizeof(Ctrl), sv->stream), "memset ctrl");
@@ -973,6 +1115,8 @@ int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *
   if (e == cudaSuccess) e = cudaStreamSynchronize(S);
   if (e != cudaSuccess) return bail(cuda_fail(e, "solver upload"));
   if ((st = ensure_ubuf(sv, 1024))) return bail(st);
+  sv->trace_cap = 8192;
+  if ((st = dalloc(sv, &sv->trace, 2 * (size_t)sv->trace_cap))) return bail(st);
   *out = sv;
   return ok();
 }
@@ -1049,6 +1193,22 @@ int dmf_get_state(dmf_solver *sv, int32_t *cap, int32_t *res, int64_t *excess, i
   if (excess) CK(cudaMemcpyAsync(excess, sv->excess, 8 * N, cudaMemcpyDeviceToHost, sv->stream), "D2H excess");
   if (height) CK(cudaMemcpyAsync(height, sv->height, 4 * N, cudaMemcpyDeviceToHost, sv->stream), "D2H height");
   CK(cudaStreamSynchronize(sv->stream), "state");
+  return ok();
+}
+
+int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us, int32_t *count) {
+  if (!sv || !count || cap < 0 || (cap > 0 && (!kinds || !t_us))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  const int len = std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap);
+  *count = len;
+  if (len == 0 || cap == 0) return ok();
+  std::vector<unsigned long long> h(2 * (size_t)len);
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  CK(cudaMemcpyAsync(h.data(), sv->trace, 16 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
+  CK(cudaStreamSynchronize(sv->stream), "trace");
+  for (int i = 0; i < std::min(len, cap); i++) {
+    kinds[i] = (int32_t)h[2 * i];
+    t_us[i] = (double)(h[2 * i + 1] - h[1]) * 1e-3;
+  }
   return ok();
 }
 

@@ -55,6 +55,9 @@ typedef enum {
   DMF_VARIANT_PP = 2    /* dyn_pp: push-pull on the kept min-cut partition (code/dyn_pp.h) */
 } dmf_variant;
 
+/* dmf_opts.flags bits */
+#define DMF_FLAG_TRACE 1 /* record a per-phase device timeline (dmf_trace_get) */
+
 typedef struct dmf_graph dmf_graph;   /* host CSR, owned by the library */
 typedef struct dmf_solver dmf_solver; /* device-resident residual state */
 
@@ -68,7 +71,7 @@ typedef struct {
   int32_t max_iters;        /* bound on global-relabel iterations per solve; 0 = default */
   int32_t device;           /* CUDA device ordinal; -1 = current device */
   int32_t block_threads;    /* threads per block of the persistent kernel; 0 = 512 */
-  int32_t flags;            /* reserved, 0 */
+  int32_t flags;            /* DMF_FLAG_* bits */
 } dmf_opts;
 
 typedef struct {
@@ -195,6 +198,15 @@ int dmf_get_cut(dmf_solver *sv, uint8_t *sink_side);
 int dmf_get_state(dmf_solver *sv, int32_t *cap, int32_t *res, int64_t *excess,
                   int32_t *height);
 int dmf_stats_get(const dmf_solver *sv, dmf_stats *st);
+/* Phase timeline of the last solve call (needs DMF_FLAG_TRACE): entry 0 is the
+ * kernel start (kind 0); entry i > 0 is the end of a phase of kind kinds[i] at
+ * t_us[i] microseconds after the start.  Kinds: 1 init residuals, 2 source
+ * saturation, 3 arc lookup, 4 capacity apply, 5 over-capacity repair, 6 cut
+ * saturation, 7 BFS seeds, 8 BFS top-down level, 9 BFS bottom-up level,
+ * 10 BFS finalize, 11 push round.  No counterpart in the reference (which
+ * times whole calls with cudaEvents, code/dyn_data_bench.cu:246-258). */
+int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us,
+                  int32_t *count);
 /* Replaces the option set of a live solver (variant, cycles, interval, tile). */
 int dmf_solver_set_opts(dmf_solver *sv, const dmf_opts *opts);
 int dmf_solver_destroy(dmf_solver *sv);
