@@ -94,6 +94,7 @@ _sig("dmf_get_state", C.c_int, VP, VP, VP, VP, VP)
 _sig("dmf_stats_get", C.c_int, VP, C.POINTER(Stats))
 _sig("dmf_trace_get", C.c_int, VP, C.c_int32, I32P, np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"),
      C.POINTER(C.c_int32))
+_sig("dmf_trace_items", C.c_int, VP, C.c_int32, I64P, I64P)
 _sig("dmf_solver_set_opts", C.c_int, VP, C.POINTER(Opts))
 _sig("dmf_solver_destroy", C.c_int, VP)
 _sig("dmf_device_count", C.c_int)
@@ -321,7 +322,7 @@ class Solver:
 
     TRACE_KINDS = {0: "start", 1: "init_res", 2: "saturate", 3: "lookup", 4: "apply", 5: "repair",
                    6: "cut_saturate", 7: "bfs_init", 8: "bfs_td", 9: "bfs_bu", 10: "bfs_finalize", 11: "push",
-                   12: "flow"}
+                   12: "flow", 13: "push_hub", 14: "push_hub_finish"}
 
     def trace(self):
         """[(phase kind, end time in us since kernel start)] of the last solve (trace=True)."""
@@ -330,7 +331,12 @@ class Solver:
         kinds = np.zeros(cap, np.int32)
         t = np.zeros(cap, np.float64)
         _check(_L.dmf_trace_get(self._h, cap, kinds, t, C.byref(cnt)))
-        return [(self.TRACE_KINDS.get(int(k), str(k)), float(x)) for k, x in zip(kinds[:cnt.value], t[:cnt.value])]
+        n = cnt.value
+        items = np.zeros(max(n, 1), np.int64)
+        hubs = np.zeros(max(n, 1), np.int64)
+        _check(_L.dmf_trace_items(self._h, n, items, hubs))
+        self.last_trace_items = list(zip(items[:n].tolist(), hubs[:n].tolist()))
+        return [(self.TRACE_KINDS.get(int(k), str(k)), float(x)) for k, x in zip(kinds[:n], t[:n])]
 
     def stats(self) -> dict:
         st = Stats()

@@ -55,6 +55,9 @@ struct Ctrl {
   unsigned long long st_outer, st_levels, st_rounds, st_pushes, st_relabels, st_arcs, st_visits, st_dead;
   unsigned int rounds_used;
   int trace_len;              // entries written to the optional timeline
+  // push-round worklist tails and topology-driven active counts, round r uses [r % 3]
+  int wtail[3], whtail[3], seen[3];
+  int pad1;
 };
 
 // ---- memory helpers ---------------------------------------------------------
@@ -131,7 +134,19 @@ __device__ __forceinline__ void agg_add_int(int *p, int v) {
   if (g.thread_rank() == 0 && s) atomicAdd(p, s);
 }
 
-// ---- groups: T lanes of a warp, or the whole block ---------------------------
+// ---- groups: one thread, T lanes of a warp, or the whole block ----------------
+struct ThreadGroup {
+  __device__ __forceinline__ int rank() const { return 0; }
+  __host__ __device__ static constexpr int size() { return 1; }
+  __device__ __forceinline__ long long scan(long long x, long long &tot) {
+    tot = x;
+    return 0;
+  }
+  __device__ __forceinline__ int min_all(int x) { return x; }
+  __device__ __forceinline__ long long sum_all(long long x) { return x; }
+  __device__ __forceinline__ bool any(bool x) { return x; }
+};
+
 template <int T>
 struct TileGroup {
   cg::thread_block_tile<T> g;
@@ -146,6 +161,7 @@ struct TileGroup {
   }
   __device__ __forceinline__ int min_all(int x) { return cg::reduce(g, x, cg::less<int>()); }
   __device__ __forceinline__ long long sum_all(long long x) { return cg::reduce(g, x, cg::plus<long long>()); }
+  __device__ __forceinline__ bool any(bool x) { return g.any(x); }
 };
 
 template <int BLOCK>

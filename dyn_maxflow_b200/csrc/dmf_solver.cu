@@ -18,8 +18,8 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
-#include <mutex>
 
 #include "dmf_device.cuh"
 #include "dmf_internal.h"
@@ -29,6 +29,7 @@ using namespace dmfd;
 namespace {
 
 constexpr int kBlock = 512;
+constexpr int kChunk = 2048;  // arcs per hub chunk (one block item)
 
 enum Mode : int { MODE_STATIC = 0, MODE_DYNAMIC = 1, MODE_RECOMPUTE = 2, MODE_CUT = 3 };
 
@@ -36,7 +37,7 @@ enum Mode : int { MODE_STATIC = 0, MODE_DYNAMIC = 1, MODE_RECOMPUTE = 2, MODE_CU
 enum TraceKind : int {
   TR_START = 0, TR_INIT_RES = 1, TR_SATURATE = 2, TR_LOOKUP = 3, TR_APPLY = 4, TR_REPAIR = 5,
   TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
-  TR_FLOW = 12
+  TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14
 };
 
 // Largest capacity an update may set: keeps cap(e) + cap(partner) < 2^31 when
@@ -52,13 +53,16 @@ struct Params {
   int *cap, *res, *height, *stamp, *astamp, *uarc;
   long long *excess;
   unsigned char *dead, *side;
-  int *fq[2], *fh[2], *wq[2], *wh[2], *aq, *ah;
-  const int *hubs;
-  int nhubs;
+  int *fq[2], *wq[2], *aq;     // non-hub vertex queues
+  int2 *fh[2], *wh[2], *ah;    // hub chunk queues
+  const int2 *hch;             // every hub's chunks (bottom-up BFS, topology-driven rounds)
+  int nhch;
+  long long *hc_tsum, *hc_ex, *hc_moved;  // per hub-chunk scratch of a push round
+  int *hc_tmin;
   const int *usrc, *udst, *uw;
   int k;
   Ctrl *ctrl;
-  int mode, variant, cycles, interval, max_iters, hub_deg, need_cut;
+  int mode, variant, cycles, interval, max_iters, hub_deg, small_deg, need_cut;
   unsigned round_base;
   int epoch;
   unsigned long long *trace;  // optional phase timeline: 2 words per entry
@@ -99,7 +103,7 @@ __device__ void ph_saturate(const Params &p) {
       sum += r;
     }
   }
-  if (sum) atomic_add_ll(p.excess + p.s, -sum);
+  agg_add_ll(p.excess + p.s, -sum);
 }
 
 // Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201) by binary search over the
@@ -198,6 +202,56 @@ __device__ void ph_cut_saturate(const Params &p) {
   }
 }
 
+// ---- degree tiers ------------------------------------------------------------------
+// Items of a vertex list (or all vertices when list == nullptr) are taken TILE
+// at a time by a tile: vertices of degree <= small_deg are handled by their own
+// lane, larger ones (up to hub_deg; hubs are split into arc chunks and done
+// block-wide) one after another by the whole tile.  `f(group, v)` does the work
+// for one vertex.
+template <int TILE, class F>
+__device__ __forceinline__ void for_tiered(const Params &p, const int *list, int nn, F &&f) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  TileGroup<TILE> tg;
+  for (int base = (gt / TILE) * TILE; base < nn; base += nt) {
+    const int i = base + tg.rank();
+    int v = -1, d = 0;
+    if (i < nn) {
+      v = list ? __ldcg(list + i) : i;
+      d = deg_of(p, v);
+      if (d > p.hub_deg) v = -1;
+    }
+    const bool small = v >= 0 && d <= p.small_deg;
+    if (small) {
+      ThreadGroup th;
+      f(th, v);
+    }
+    tg.g.sync();
+    unsigned big = tg.g.ballot(v >= 0 && !small);
+    while (big) {
+      const int j = __ffs(big) - 1;
+      big &= big - 1;
+      f(tg, tg.g.shfl(v, j));
+    }
+  }
+}
+
+// A hub (degree > hub_deg) enters a queue as ceil(deg / kChunk) consecutive
+// items (v, c), chunk c covering arcs [off[v] + c*kChunk, +kChunk).  Every item
+// is one block's work, so a hub's adjacency is spread over many blocks.
+__device__ __forceinline__ int nchunks(int d) { return (d + kChunk - 1) / kChunk; }
+
+__device__ __forceinline__ void append_hub(const Params &p, int2 *q, int *tail, int v) {
+  const int k = nchunks(deg_of(p, v));
+  const int base = atomicAdd(tail, k);
+  for (int c = 0; c < k; c++) q[base + c] = make_int2(v, c);
+}
+
+__device__ __forceinline__ void chunk_range(const Params &p, int2 it, int &beg, int &end) {
+  const int b0 = __ldg(p.off + it.x), e0 = __ldg(p.off + it.x + 1);
+  beg = b0 + it.y * kChunk;
+  end = min(e0, beg + kChunk);
+}
+
 // ---- global relabel ---------------------------------------------------------------
 
 #define UNV (p.n + 1)
@@ -210,14 +264,13 @@ __device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
   if (gt == 0) {
     c->act_q = 0;
     c->act_hq = 0;
+    c->wtail[0] = c->whtail[0] = c->seen[0] = 0;  // written by push round 0
   }
   int pos = 0;
   long long unexpl = 0, seed_arcs = 0;
   for (int v = gt; v < p.n; v += nt) {
-    bool was_dead = false;
     if (reset_dead) {
-      was_dead = __ldcg(p.dead + v) != 0;
-      if (was_dead) p.dead[v] = 0;
+      if (__ldcg(p.dead + v)) p.dead[v] = 0;
     } else if (__ldcg(p.dead + v)) {
       continue;
     }
@@ -225,14 +278,14 @@ __device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
     int d = deg_of(p, v);
     if (v == p.t || (v != p.s && ex < 0)) {
       p.height[v] = 0;
-      if (d > p.hub_deg) append(p.fh[0], &out->hq, v);
+      if (d > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
       else append(p.fq[0], &out->q, v);
       seed_arcs += d;
     } else {
       p.height[v] = UNV;
-      // direction heuristic: vertices that could not reach t or a deficit at the
-      // end of the previous solve are not expected to be labelled now
-      if (!was_dead) unexpl += d;
+      // a bottom-up level scans the arcs of every unvisited vertex, so the
+      // direction heuristic weighs the frontier against all of them
+      unexpl += d;
     }
     if (v != p.s && v != p.t && ex > 0) pos++;
   }
@@ -248,11 +301,12 @@ struct VisitAcc {
 
 __device__ __forceinline__ void bfs_visit(const Params &p, Slot *out, int nxt, int w, VisitAcc &acc) {
   int d = deg_of(p, w);
-  if (d > p.hub_deg) append(p.fh[nxt], &out->hq, w);
+  const bool hub = d > p.hub_deg;
+  if (hub) append_hub(p, p.fh[nxt], &out->hq, w);
   else append(p.fq[nxt], &out->q, w);
   acc.arcs += d;
   if (w != p.s && w != p.t && __ldcg(p.excess + w) > 0) {
-    if (d > p.hub_deg) append(p.ah, &p.ctrl->act_hq, w);
+    if (hub) append_hub(p, p.ah, &p.ctrl->act_hq, w);
     else append(p.aq, &p.ctrl->act_q, w);
     acc.reached++;
   }
@@ -268,94 +322,83 @@ __device__ __forceinline__ void flush_visits(const Params &p, Slot *out, VisitAc
 // Top-down level (staticMaxFlow_kernel_11, code/dyn_data.h:72-87, run over the
 // frontier queue instead of all V): x at level L labels w when arc w->x has
 // residual, i.e. res[par[e]] > 0 for e = x->w.
+__device__ __forceinline__ void td_arc(const Params &p, Slot *out, int nxt, int a, int L, LStats &ls,
+                                       VisitAcc &acc) {
+  const int w = __ldg(p.adj + a);
+  ls.arcs++;
+  if (__ldcg(p.height + w) == UNV && __ldcg(p.res + __ldg(p.par + a)) > 0 &&
+      atomicCAS(p.height + w, UNV, L + 1) == UNV)
+    bfs_visit(p, out, nxt, w, acc);
+}
+
 template <int TILE>
 __device__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int cur = L & 1, nxt = cur ^ 1;
   const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
-  const int lane = threadIdx.x % TILE;
   VisitAcc acc;
   for (int i = blockIdx.x; i < nh; i += gridDim.x) {
-    int x = __ldcg(p.fh[cur] + i);
-    int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
-    for (int a = beg + threadIdx.x; a < end; a += blockDim.x) {
-      int w = __ldg(p.adj + a);
-      ls.arcs++;
-      if (__ldcg(p.height + w) == UNV && __ldcg(p.res + __ldg(p.par + a)) > 0 &&
-          atomicCAS(p.height + w, UNV, L + 1) == UNV)
-        bfs_visit(p, out, nxt, w, acc);
-    }
+    int beg, end;
+    chunk_range(p, p.fh[cur][i], beg, end);
+    for (int a = beg + threadIdx.x; a < end; a += blockDim.x) td_arc(p, out, nxt, a, L, ls, acc);
   }
-  for (int i = gt / TILE; i < nn; i += nt / TILE) {
-    int x = __ldcg(p.fq[cur] + i);
-    int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
-    for (int a = beg + lane; a < end; a += TILE) {
-      int w = __ldg(p.adj + a);
-      ls.arcs++;
-      if (__ldcg(p.height + w) == UNV && __ldcg(p.res + __ldg(p.par + a)) > 0 &&
-          atomicCAS(p.height + w, UNV, L + 1) == UNV)
-        bfs_visit(p, out, nxt, w, acc);
-    }
-  }
+  for_tiered<TILE>(p, p.fq[cur], nn, [&](auto &g, int x) {
+    const int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
+    for (int a = beg + g.rank(); a < end; a += g.size()) td_arc(p, out, nxt, a, L, ls, acc);
+  });
   flush_visits(p, out, acc);
 }
 
 // Bottom-up level: every unvisited vertex looks for a residual arc into level
-// L and stops at the first one.  Hubs are searched by a whole block (strided,
-// with a shared found-flag polled every 8 strides); other vertices by a tile.
+// L and stops at the first one.  Hub chunks are searched by whole blocks
+// (strided, with a shared found-flag polled every 8 strides; the first chunk of
+// a hub to succeed labels it); other vertices by a lane or a tile.
 template <int TILE>
 __device__ void ph_bfs_bu(const Params &p, Slot *out, int L, LStats &ls) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int nxt = (L & 1) ^ 1;
   VisitAcc acc;
-  __shared__ int s_found;
-  for (int i = blockIdx.x; i < p.nhubs; i += gridDim.x) {
-    const int v = __ldg(p.hubs + i);
-    if (__ldcg(p.height + v) != UNV) continue;  // block-uniform: only v's block writes it
-    if (threadIdx.x == 0) s_found = 0;
+  __shared__ int s_flag;
+  for (int i = blockIdx.x; i < p.nhch; i += gridDim.x) {
+    const int2 it = p.hch[i];
     __syncthreads();
-    const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
-    int it = 0;
-    for (int a = beg + threadIdx.x; a < end; a += blockDim.x, it++) {
-      if ((it & 7) == 7 && *(volatile int *)&s_found) break;
+    if (threadIdx.x == 0) s_flag = __ldcg(p.height + it.x) == UNV ? 0 : -1;
+    __syncthreads();
+    if (s_flag < 0) continue;  // labelled already (block-uniform through shared memory)
+    int beg, end;
+    chunk_range(p, it, beg, end);
+    int k = 0;
+    for (int a = beg + threadIdx.x; a < end; a += blockDim.x, k++) {
+      if ((k & 7) == 7 && *(volatile int *)&s_flag) break;
       ls.arcs++;
       if (__ldcg(p.res + a) > 0 && __ldcg(p.height + __ldg(p.adj + a)) == L) {
-        s_found = 1;
+        s_flag = 1;
         break;
       }
     }
     __syncthreads();
-    const bool found = s_found != 0;
-    if (found && threadIdx.x == 0) {
-      p.height[v] = L + 1;
-      bfs_visit(p, out, nxt, v, acc);
-    }
-    __syncthreads();
+    if (s_flag > 0 && threadIdx.x == 0 && atomicCAS(p.height + it.x, UNV, L + 1) == UNV)
+      bfs_visit(p, out, nxt, it.x, acc);
   }
-  cg::thread_block_tile<TILE> tile = cg::tiled_partition<TILE>(cg::this_thread_block());
-  const int lane = tile.thread_rank();
-  for (int v = gt / TILE; v < p.n; v += nt / TILE) {
-    if (__ldcg(p.height + v) != UNV) continue;  // same address for the whole tile
+  for_tiered<TILE>(p, nullptr, p.n, [&](auto &g, int v) {
+    if (__ldcg(p.height + v) != UNV) return;  // only v's group writes it in this phase
     const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
-    if (end - beg > p.hub_deg) continue;
     bool found = false;
-    for (int base = beg; base < end; base += TILE) {
-      const int a = base + lane;
+    for (int base = beg; base < end; base += g.size()) {
+      const int a = base + g.rank();
       bool hit = false;
       if (a < end) {
         ls.arcs++;
         hit = __ldcg(p.res + a) > 0 && __ldcg(p.height + __ldg(p.adj + a)) == L;
       }
-      if (tile.any(hit)) {
+      if (g.any(hit)) {
         found = true;
         break;
       }
     }
-    if (found && lane == 0) {
+    if (found && g.rank() == 0) {
       p.height[v] = L + 1;
       bfs_visit(p, out, nxt, v, acc);
     }
-  }
+  });
   flush_visits(p, out, acc);
 }
 
@@ -378,57 +421,52 @@ __device__ void ph_bfs_finalize(const Params &p, bool full, int floor_h, bool wr
     }
     if (write_side) p.side[v] = h < p.n ? 1 : 0;
   }
-  if (nd) atomicAdd((unsigned long long *)&p.ctrl->st_dead, (unsigned long long)nd);
+  agg_add_ll((long long *)&p.ctrl->st_dead, nd);
 }
 
 // ---- push rounds ---------------------------------------------------------------
+// Round r reads the worklists of round r-1 (the BFS active lists for r = 0) and
+// appends to buffers r&1 with tails wtail/whtail[r%3]; tails are triple-buffered
+// for the same reason as the phase slots.
 
-__device__ __forceinline__ void enqueue(const Params &p, Slot *out, int buf, unsigned round_id, int v) {
+__device__ __forceinline__ void enqueue(const Params &p, int r, unsigned round_id, int v) {
   if (atomicExch(p.stamp + v, (int)round_id) == (int)round_id) return;
-  if (deg_of(p, v) > p.hub_deg) append(p.wh[buf], &out->hq, v);
-  else append(p.wq[buf], &out->q, v);
+  if (deg_of(p, v) > p.hub_deg) append_hub(p, p.wh[r & 1], &p.ctrl->whtail[r % 3], v);
+  else append(p.wq[r & 1], &p.ctrl->wtail[r % 3], v);
 }
 
-__device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, Slot *out, int buf, unsigned round_id,
-                                         bool enq, LStats &ls) {
+__device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, int r, unsigned round_id, bool enq,
+                                         LStats &ls) {
   atomicSub(p.res + a, d);
   atomicAdd(p.res + __ldg(p.par + a), d);
   long long old = atomic_add_ll(p.excess + w, d);
   ls.pushes++;
-  if (enq && w != p.s && w != p.t && old + d > 0) enqueue(p, out, buf, round_id, w);
+  if (enq && w != p.s && w != p.t && old + d > 0) enqueue(p, r, round_id, w);
 }
 
-// Discharge of v by a group (warp tile or block): up to `cycles` rounds of
+// Discharge of a non-hub v by a lane or a tile: up to `cycles` rounds of
 // push-then-relabel, the push/relabel of staticMaxFlow_kernel_14
 // (code/dyn_data.h:89-131) with every admissible arc (head below h) used per
 // round instead of only the lowest one.
-//  * adjacency within one group width: one load per lane, the excess is split
+//  * adjacency within the group width: one load per lane, the excess is split
 //    over the admissible arcs in arc order by a group prefix sum;
-//  * longer adjacency (hubs): pass 1 has every lane sum the admissible residual
-//    and the minimum non-admissible height over its strided arcs (independent
-//    loads, no group synchronisation inside the loop); a group prefix sum turns
-//    the sums into per-lane budgets; pass 2 pushes each lane's budget greedily.
+//  * longer adjacency: pass 1 has every lane sum the admissible residual and the
+//    minimum non-admissible height over its strided arcs (independent loads); a
+//    group prefix sum turns the sums into per-lane budgets; pass 2 pushes each
+//    lane's budget greedily.
 // When every admissible arc was saturated and excess is left, h becomes
 // 1 + the minimum height over the arcs still residual.  Concurrent relabels only
-// raise heights, so a pass-2 arc that lost admissibility is skipped and the round
-// is retried instead of relabelled.
+// raise heights, so a pass-2 arc that lost admissibility is skipped and the
+// round is retried instead of relabelled.
 template <class G>
-__device__ void discharge(G &g, const Params &p, int v, Slot *out, int buf, unsigned round_id, bool enq,
-                          LStats &ls, int *seen) {
+__device__ void discharge(G &g, const Params &p, int v, int r, unsigned round_id, bool enq, LStats &ls,
+                          int *seen) {
   long long ex0;
   int h;
   // one read, broadcast: concurrent pushes may change excess[v] meanwhile
-  if constexpr (G::size() == kBlock) {
-    __shared__ long long s_ex;
-    __shared__ int s_h;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_ex = __ldcg(p.excess + v);
-      s_h = __ldcg(p.height + v);
-    }
-    __syncthreads();
-    ex0 = s_ex;
-    h = s_h;
+  if constexpr (G::size() == 1) {
+    ex0 = __ldcg(p.excess + v);
+    h = __ldcg(p.height + v);
   } else {
     long long e = 0;
     int hh = 0;
@@ -450,27 +488,27 @@ __device__ void discharge(G &g, const Params &p, int v, Slot *out, int buf, unsi
   for (int cyc = 0; cyc < p.cycles && ex > 0 && h < p.n; cyc++) {
     if (end - beg <= S) {
       const int a = beg + g.rank();
-      int r = 0, w = -1, hw = INT_MAX;
+      int rr = 0, w = -1, hw = INT_MAX;
       if (a < end) {
-        r = __ldcg(p.res + a);
-        if (r > 0) {
+        rr = __ldcg(p.res + a);
+        if (rr > 0) {
           w = __ldg(p.adj + a);
           hw = __ldcg(p.height + w);
         }
         ls.arcs++;
       }
-      const bool adm = r > 0 && hw < h;
+      const bool adm = rr > 0 && hw < h;
       long long tot;
-      const long long pre = g.scan(adm ? (long long)r : 0ll, tot);
+      const long long pre = g.scan(adm ? (long long)rr : 0ll, tot);
       int d = 0;
       if (adm) {
         long long left = ex - pre;
-        d = left <= 0 ? 0 : (left < r ? (int)left : r);
+        d = left <= 0 ? 0 : (left < rr ? (int)left : rr);
       }
-      if (d > 0) push_arc(p, a, w, d, out, buf, round_id, enq, ls);
+      if (d > 0) push_arc(p, a, w, d, r, round_id, enq, ls);
       ex -= (tot < ex ? tot : ex);
       if (ex > 0) {
-        const int mh = g.min_all(r > 0 && !(adm && d == r) ? hw : INT_MAX);
+        const int mh = g.min_all(rr > 0 && !(adm && d == rr) ? hw : INT_MAX);
         h = mh >= p.n ? p.n : mh + 1;
         if (g.rank() == 0) {
           p.height[v] = h;
@@ -484,10 +522,10 @@ __device__ void discharge(G &g, const Params &p, int v, Slot *out, int buf, unsi
     int tmin = INT_MAX;
 #pragma unroll 4
     for (int a = beg + g.rank(); a < end; a += S) {
-      const int r = __ldcg(p.res + a);
-      if (r > 0) {
+      const int rr = __ldcg(p.res + a);
+      if (rr > 0) {
         const int hw = __ldcg(p.height + __ldg(p.adj + a));
-        if (hw < h) tsum += r;
+        if (hw < h) tsum += rr;
         else tmin = min(tmin, hw);
       }
     }
@@ -499,17 +537,16 @@ __device__ void discharge(G &g, const Params &p, int v, Slot *out, int buf, unsi
     budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
     long long done = 0;
     for (int a = beg + g.rank(); a < end && budget > 0; a += S) {
-      const int r = __ldcg(p.res + a);
-      if (r <= 0) continue;
+      const int rr = __ldcg(p.res + a);
+      if (rr <= 0) continue;
       const int w = __ldg(p.adj + a);
       if (__ldcg(p.height + w) >= h) continue;
-      const int d = (int)(r < budget ? r : budget);
-      push_arc(p, a, w, d, out, buf, round_id, enq, ls);
+      const int d = (int)(rr < budget ? rr : budget);
+      push_arc(p, a, w, d, r, round_id, enq, ls);
       budget -= d;
       done += d;
     }
     const long long moved = g.sum_all(done);
-    const long long planned = tot < ex ? tot : ex;
     ex -= moved;
     if (ex > 0 && moved == tot) {  // all admissible arcs saturated: relabel
       const int mh = g.min_all(tmin);
@@ -519,60 +556,197 @@ __device__ void discharge(G &g, const Params &p, int v, Slot *out, int buf, unsi
         ls.relabels++;
       }
     }
-    (void)planned;
   }
   if (g.rank() == 0) {
     if (ex0 != ex) atomic_add_ll(p.excess + v, ex - ex0);
-    if (enq && ex > 0 && h < p.n) enqueue(p, out, buf, round_id, v);
+    if (enq && ex > 0 && h < p.n) enqueue(p, r, round_id, v);
   }
 }
 
-template <int TILE, int BLOCK>
-__device__ void ph_push(const Params &p, const Slot *in, Slot *out, int r, unsigned round_id, LStats &ls,
-                        typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
+// Inputs of push round r: non-hub vertices and hub chunks.
+struct RoundIn {
+  const int *nlist;
+  int nn;
+  const int2 *hlist;
+  int nh;
+};
+
+__device__ __forceinline__ RoundIn round_inputs(const Params &p, int r) {
   Ctrl *c = p.ctrl;
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool topo = p.variant == DMF_VARIANT_TOPO;
-  if (r == 0 && gt == 0) {  // read during the BFS just finished; cleared for the next one
-    c->pos_count = 0;
-    c->unexplored = 0;
-  }
-  const int buf = r & 1;
-  const int *nlist, *hlist;
-  int nn, nh;
-  if (topo) {
-    nlist = nullptr;
-    nn = p.n;
-    hlist = p.hubs;
-    nh = p.nhubs;
+  RoundIn in;
+  if (p.variant == DMF_VARIANT_TOPO) {
+    in.nlist = nullptr;
+    in.nn = p.n;
+    in.hlist = p.hch;
+    in.nh = p.nhch;
   } else if (r == 0) {
-    nlist = p.aq;
-    nn = ld_vol(&c->act_q);
-    hlist = p.ah;
-    nh = ld_vol(&c->act_hq);
+    in.nlist = p.aq;
+    in.nn = ld_vol(&c->act_q);
+    in.hlist = p.ah;
+    in.nh = ld_vol(&c->act_hq);
   } else {
-    nlist = p.wq[buf ^ 1];
-    nn = ld_vol(&in->q);
-    hlist = p.wh[buf ^ 1];
-    nh = ld_vol(&in->hq);
+    in.nlist = p.wq[(r - 1) & 1];
+    in.nn = ld_vol(&c->wtail[(r - 1) % 3]);
+    in.hlist = p.wh[(r - 1) & 1];
+    in.nh = ld_vol(&c->whtail[(r - 1) % 3]);
+  }
+  return in;
+}
+
+// Push round, phase 1: non-hub vertices are discharged completely; every hub
+// chunk computes its admissible residual sum and its minimum non-admissible
+// height (chunk 0 also snapshots the hub's excess).
+template <int TILE, int BLOCK>
+__device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls,
+                         typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
+  Ctrl *c = p.ctrl;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool topo = p.variant == DMF_VARIANT_TOPO;
+  if (gt == 0) {
+    if (r == 0) {  // read during the BFS just finished; cleared for the next one
+      c->pos_count = 0;
+      c->unexplored = 0;
+    }
+    c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
+  }
+  __shared__ int s_h;
+  BlockGroup<BLOCK> bg(btmp, bci, bcl);
+  for (int i = blockIdx.x; i < in.nh; i += gridDim.x) {
+    const int2 it = __ldcg(in.hlist + i);
+    const int v = it.x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_h = __ldcg(p.height + v);
+      if (it.y == 0) {
+        p.hc_ex[i] = __ldcg(p.excess + v);
+        p.hc_moved[i] = 0;
+      }
+    }
+    __syncthreads();
+    const int h = s_h;
+    long long tsum = 0;
+    int tmin = INT_MAX;
+    if (h < p.n && v != p.s && v != p.t) {
+      int beg, end;
+      chunk_range(p, it, beg, end);
+#pragma unroll 4
+      for (int a = beg + threadIdx.x; a < end; a += BLOCK) {
+        const int rr = __ldcg(p.res + a);
+        ls.arcs++;
+        if (rr > 0) {
+          const int hw = __ldcg(p.height + __ldg(p.adj + a));
+          if (hw < h) tsum += rr;
+          else tmin = min(tmin, hw);
+        }
+      }
+    }
+    const long long ts = bg.sum_all(tsum);
+    const int tm = bg.min_all(tmin);
+    if (threadIdx.x == 0) {
+      p.hc_tsum[i] = ts;
+      p.hc_tmin[i] = tm;
+    }
   }
   int seen = 0;
-  {
-    BlockGroup<BLOCK> bg(btmp, bci, bcl);
-    for (int i = blockIdx.x; i < nh; i += gridDim.x) {
-      int v = __ldcg(hlist + i);
-      discharge(bg, p, v, out, buf, round_id, !topo, ls, topo ? &seen : nullptr);
+  for_tiered<TILE>(p, in.nlist, in.nn, [&](auto &g, int v) {
+    discharge(g, p, v, r, round_id, !topo, ls, topo ? &seen : nullptr);
+  });
+  if (topo) agg_add_int(&c->seen[r % 3], seen);
+}
+
+// Push round, phase 2: each hub chunk pushes its share of the hub's excess
+// (excess minus the admissible residual of the chunks before it, capped at its
+// own) over its admissible arcs: lane budgets from a block prefix sum, then a
+// greedy pass.  Moved amounts are summed per hub.
+template <int BLOCK>
+__device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls,
+                         typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
+  const bool topo = p.variant == DMF_VARIANT_TOPO;
+  __shared__ int s_h;
+  __shared__ long long s_ex;
+  BlockGroup<BLOCK> bg(btmp, bci, bcl);
+  for (int i = blockIdx.x; i < in.nh; i += gridDim.x) {
+    const int2 it = __ldcg(in.hlist + i);
+    const int v = it.x, base = i - it.y;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_h = __ldcg(p.height + v);
+      s_ex = __ldcg(p.hc_ex + base);
     }
-  }
-  {
-    TileGroup<TILE> tg;
-    for (int i = gt / TILE; i < nn; i += nt / TILE) {
-      int v = topo ? i : __ldcg(nlist + i);
-      if (topo && deg_of(p, v) > p.hub_deg) continue;
-      discharge(tg, p, v, out, buf, round_id, !topo, ls, topo ? &seen : nullptr);
+    __syncthreads();
+    const int h = s_h;
+    const long long ex0 = s_ex;
+    if (!(ex0 > 0 && h < p.n) || v == p.s || v == p.t) continue;
+    long long prior = 0;
+    for (int j = threadIdx.x; j < it.y; j += BLOCK) prior += __ldcg(p.hc_tsum + base + j);
+    prior = bg.sum_all(prior);
+    long long cb = ex0 - prior;
+    const long long mine = __ldcg(p.hc_tsum + i);
+    cb = cb < 0 ? 0 : (cb > mine ? mine : cb);
+    if (cb == 0) continue;  // block-uniform
+    int beg, end;
+    chunk_range(p, it, beg, end);
+    long long tsum = 0;
+#pragma unroll 4
+    for (int a = beg + threadIdx.x; a < end; a += BLOCK) {
+      const int rr = __ldcg(p.res + a);
+      if (rr > 0 && __ldcg(p.height + __ldg(p.adj + a)) < h) tsum += rr;
     }
+    long long tot;
+    const long long pre = bg.scan(tsum, tot);
+    long long budget = cb - pre;
+    budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
+    long long done = 0;
+    for (int a = beg + threadIdx.x; a < end && budget > 0; a += BLOCK) {
+      const int rr = __ldcg(p.res + a);
+      if (rr <= 0) continue;
+      const int w = __ldg(p.adj + a);
+      if (__ldcg(p.height + w) >= h) continue;
+      const int d = (int)(rr < budget ? rr : budget);
+      push_arc(p, a, w, d, r, round_id, !topo, ls);
+      budget -= d;
+      done += d;
+    }
+    const long long moved = bg.sum_all(done);
+    if (threadIdx.x == 0 && moved) atomic_add_ll(p.hc_moved + base, moved);
   }
-  if (topo) agg_add_int(&out->cnt, seen);
+}
+
+// Push round, phase 3: per hub (its chunk 0), the moved total leaves its
+// excess; when every chunk's admissible residual was pushed and excess is left,
+// the hub is relabelled to 1 + the minimum non-admissible height; a hub with
+// excess left is queued for the next round.
+__device__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool topo = p.variant == DMF_VARIANT_TOPO;
+  int seen = 0;
+  for (int i = gt; i < in.nh; i += nt) {
+    const int2 it = __ldcg(in.hlist + i);
+    if (it.y != 0) continue;
+    const int v = it.x;
+    const long long ex0 = __ldcg(p.hc_ex + i);
+    int h = __ldcg(p.height + v);
+    if (!(ex0 > 0 && h < p.n) || v == p.s || v == p.t) continue;
+    seen++;
+    ls.visits++;
+    const int k = nchunks(deg_of(p, v));
+    long long tot = 0;
+    int mh = INT_MAX;
+    for (int j = 0; j < k; j++) {
+      tot += __ldcg(p.hc_tsum + i + j);
+      mh = min(mh, __ldcg(p.hc_tmin + i + j));
+    }
+    const long long moved = __ldcg(p.hc_moved + i);
+    const long long ex = ex0 - moved;
+    if (moved) atomic_add_ll(p.excess + v, -moved);
+    if (ex > 0 && moved == tot) {
+      h = mh >= p.n ? p.n : mh + 1;
+      p.height[v] = h;
+      ls.relabels++;
+    }
+    if (!topo && ex > 0 && h < p.n) enqueue(p, r, round_id, v);
+  }
+  if (topo) agg_add_int(&p.ctrl->seen[r % 3], seen);
 }
 
 // recalculate_max_flow_kernel_39 (code/dyn_data.h:208-215) as a reduction:
@@ -605,11 +779,13 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   int ph = 0;
   int kind = 0;  // phase kind, recorded in the optional timeline
+  long long items = 0, hubitems = 0;  // work of the phase, recorded with it
   auto slot_out = [&]() { return &c->slot[ph % 3]; };
   auto slot_in = [&]() { return &c->slot[(ph + 2) % 3]; };
   auto record = [&]() {
     if (lead && p.trace && ph < p.trace_cap) {
-      p.trace[2 * ph] = (unsigned long long)kind;
+      p.trace[2 * ph] = (unsigned long long)kind | ((unsigned long long)(items & 0xffffffffll) << 8) |
+                        ((unsigned long long)(hubitems & 0xffffff) << 40);
       p.trace[2 * ph + 1] = globaltimer();
     }
   };
@@ -667,12 +843,14 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
   // ---- global relabel / push rounds ---------------------------------------------
   unsigned round_id = p.round_base;
   const bool cut_only = p.mode == MODE_CUT;
+  const bool topo = p.variant == DMF_VARIANT_TOPO;
   for (int it = 0;; it++) {
     if (it >= p.max_iters) {
       if (lead) set_err(c, ERR_NO_CONV, it);
       return;
     }
     kind = TR_BFS_INIT;
+    items = hubitems = 0;
     ph_bfs_init(p, slot_out(), it == 0);
     if (!next()) return;
     if (lead) c->st_outer++;
@@ -696,31 +874,45 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
       if (!bu && m_f * 14 > m_u) bu = true;
       else if (bu && (long long)F * 24 < p.n) bu = false;
       kind = bu ? TR_BFS_BU : TR_BFS_TD;
+      items = ld_vol(&in->q);
+      hubitems = ld_vol(&in->hq);
       if (bu) ph_bfs_bu<TILE>(p, slot_out(), L, ls);
       else ph_bfs_td<TILE>(p, in, slot_out(), L, ls);
       if (!next()) return;
       if (lead) c->st_levels++;
     }
     kind = TR_BFS_FINALIZE;
+    items = hubitems = 0;
     ph_bfs_finalize(p, full, L + 1, full && want_cut);
     if (!next()) return;
     const int A = ld_vol(&c->act_q) + ld_vol(&c->act_hq);
     if (A == 0 || cut_only) break;
     for (int r = 0; r < p.interval; r++) {
       round_id++;
+      const RoundIn in = round_inputs(p, r);
       kind = TR_PUSH;
-      ph_push<TILE, BLOCK>(p, slot_in(), slot_out(), r, round_id, ls, btmp, bci, bcl);
+      items = in.nn;
+      hubitems = in.nh;
+      ph_push1<TILE, BLOCK>(p, in, r, round_id, ls, btmp, bci, bcl);
       if (!next()) return;
+      if (in.nh > 0) {
+        kind = TR_PUSH_HUB;
+        ph_push2<BLOCK>(p, in, r, round_id, ls, btmp, bci, bcl);
+        if (!next()) return;
+        kind = TR_PUSH_HUB_FINISH;
+        ph_push3(p, in, r, round_id, ls);
+        if (!next()) return;
+      }
       if (lead) {
         c->st_rounds++;
         c->rounds_used = round_id - p.round_base;
       }
-      const Slot *in = slot_in();
-      const int W = p.variant == DMF_VARIANT_TOPO ? ld_vol(&in->cnt) : ld_vol(&in->q) + ld_vol(&in->hq);
+      const int W = topo ? ld_vol(&c->seen[r % 3]) : ld_vol(&c->wtail[r % 3]) + ld_vol(&c->whtail[r % 3]);
       if (W == 0) break;
     }
   }
   kind = TR_FLOW;
+  items = hubitems = 0;
   ph_flow<BLOCK>(p, btmp);
   if (lead) c->rounds_used = round_id - p.round_base;
   // the flow phase ends without a barrier; its end is the kernel's end
@@ -771,14 +963,18 @@ struct dmf_solver {
   cudaStream_t stream = nullptr;
   int n = 0, m = 0, s = 0, t = 0;
   dmf_opts opts{};
-  int tile = 32, grid = 0, block = kBlock, hub_deg = 256;
+  int tile = 32, grid = 0, block = kBlock, hub_deg = 256, small_deg = 8;
   int *off = nullptr, *adj = nullptr, *par = nullptr, *sidx = nullptr, *cap = nullptr, *res = nullptr;
   int *height = nullptr, *stamp = nullptr, *astamp = nullptr, *uarc = nullptr;
   long long *excess = nullptr;
   unsigned char *dead = nullptr, *side = nullptr;
-  int *qbuf = nullptr;  // 10 vertex queues
-  int *hubs = nullptr;
-  int nhubs = 0;
+  int *qbuf = nullptr;    // 5 vertex queues (frontier x2, worklist x2, active)
+  int2 *hqbuf = nullptr;  // 5 hub-chunk queues, same roles
+  int2 *hch = nullptr;    // every hub's chunks
+  int nchunk = 0;         // total hub chunks = capacity of each hub-chunk queue
+  long long *hc_tsum = nullptr, *hc_ex = nullptr, *hc_moved = nullptr;
+  int *hc_tmin = nullptr;
+  bool thresholds_set = false;
   int *ubuf = nullptr;  // device update staging: src | dst | w
   int kcap = 0;
   int *h_ubuf = nullptr;  // pinned host staging
@@ -843,7 +1039,14 @@ int choose_tile(const dmf_opts &o, int n, int m) {
 
 int configure(dmf_solver *sv) {
   sv->tile = choose_tile(sv->opts, sv->n, sv->m);
-  sv->hub_deg = 8 * sv->tile;
+  if (!sv->thresholds_set) {  // fixed for the solver's life: they size the hub-chunk queues
+    sv->hub_deg = 8 * sv->tile;
+    sv->small_deg = 8;
+    // tuning overrides (thread-per-vertex and chunked-hub degree bounds)
+    if (const char *e = std::getenv("DMF_SMALL_DEG")) sv->small_deg = std::max(0, std::atoi(e));
+    if (const char *e = std::getenv("DMF_HUB_DEG")) sv->hub_deg = std::max(32, std::atoi(e));
+    sv->thresholds_set = true;
+  }
   KernelFn fn = pick_kernel(sv->tile);
   int per_sm = 0, sms = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kBlock, 0), "occupancy");
@@ -905,16 +1108,21 @@ int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, 
   p.dead = sv->dead;
   p.side = sv->side;
   const size_t N = (size_t)sv->n + 1;
+  const size_t NC = (size_t)std::max(sv->nchunk, 1);
   for (int i = 0; i < 2; i++) {
     p.fq[i] = sv->qbuf + (0 + i) * N;
-    p.fh[i] = sv->qbuf + (2 + i) * N;
-    p.wq[i] = sv->qbuf + (4 + i) * N;
-    p.wh[i] = sv->qbuf + (6 + i) * N;
+    p.wq[i] = sv->qbuf + (2 + i) * N;
+    p.fh[i] = sv->hqbuf + (0 + i) * NC;
+    p.wh[i] = sv->hqbuf + (2 + i) * NC;
   }
-  p.aq = sv->qbuf + 8 * N;
-  p.ah = sv->qbuf + 9 * N;
-  p.hubs = sv->hubs;
-  p.nhubs = sv->nhubs;
+  p.aq = sv->qbuf + 4 * N;
+  p.ah = sv->hqbuf + 4 * NC;
+  p.hch = sv->hch;
+  p.nhch = sv->nchunk;
+  p.hc_tsum = sv->hc_tsum;
+  p.hc_ex = sv->hc_ex;
+  p.hc_moved = sv->hc_moved;
+  p.hc_tmin = sv->hc_tmin;
   p.usrc = d_src;
   p.udst = d_dst;
   p.uw = d_w;
@@ -923,10 +1131,12 @@ int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, 
   p.mode = mode;
   p.variant = sv->opts.variant;
   const int avg = sv->n > 0 ? std::max(1, sv->m / sv->n) : 1;
-  p.cycles = sv->opts.kernel_cycles > 0 ? sv->opts.kernel_cycles : std::max(2, std::min(avg, 8));
-  p.interval = sv->opts.relabel_interval > 0 ? sv->opts.relabel_interval : 4;
+  (void)avg;
+  p.cycles = sv->opts.kernel_cycles > 0 ? sv->opts.kernel_cycles : 2;
+  p.interval = sv->opts.relabel_interval > 0 ? sv->opts.relabel_interval : 3;
   p.max_iters = sv->opts.max_iters > 0 ? sv->opts.max_iters : 100000;
   p.hub_deg = sv->hub_deg;
+  p.small_deg = sv->small_deg;
   p.need_cut = sv->opts.variant == DMF_VARIANT_PP ? 1 : 0;
   p.round_base = sv->round_base;
   p.trace = (sv->opts.flags & DMF_FLAG_TRACE) ? sv->trace : nullptr;
@@ -1086,13 +1296,20 @@ int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *
       (st = dalloc(sv, &sv->sidx, M)) || (st = dalloc(sv, &sv->cap, M)) || (st = dalloc(sv, &sv->res, M)) ||
       (st = dalloc(sv, &sv->astamp, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
       (st = dalloc(sv, &sv->excess, N)) || (st = dalloc(sv, &sv->dead, N)) || (st = dalloc(sv, &sv->side, N)) ||
-      (st = dalloc(sv, &sv->qbuf, 10 * N)) || (st = dalloc(sv, &sv->ctrl, 1)))
+      (st = dalloc(sv, &sv->qbuf, 5 * N)) || (st = dalloc(sv, &sv->ctrl, 1)))
     return bail(st);
-  std::vector<int> hub_list;
-  for (int v = 0; v < g->n; v++)
-    if (g->off[v + 1] - g->off[v] > sv->hub_deg) hub_list.push_back(v);
-  sv->nhubs = (int)hub_list.size();
-  if ((st = dalloc(sv, &sv->hubs, hub_list.size()))) return bail(st);
+  std::vector<int2> hub_chunks;
+  for (int v = 0; v < g->n; v++) {
+    const int d = g->off[v + 1] - g->off[v];
+    if (d > sv->hub_deg)
+      for (int c = 0; c * kChunk < d; c++) hub_chunks.push_back(make_int2(v, c));
+  }
+  sv->nchunk = (int)hub_chunks.size();
+  const size_t NC = (size_t)std::max(sv->nchunk, 1);
+  if ((st = dalloc(sv, &sv->hqbuf, 5 * NC)) || (st = dalloc(sv, &sv->hch, NC)) ||
+      (st = dalloc(sv, &sv->hc_tsum, NC)) || (st = dalloc(sv, &sv->hc_ex, NC)) ||
+      (st = dalloc(sv, &sv->hc_moved, NC)) || (st = dalloc(sv, &sv->hc_tmin, NC)))
+    return bail(st);
   cudaStream_t S = sv->stream;
   cudaError_t e = cudaSuccess;
   auto up = [&](void *d, const void *h, size_t bytes) {
@@ -1103,7 +1320,7 @@ int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *
   up(sv->par, g->par.data(), 4 * M);
   up(sv->sidx, g->sidx.data(), 4 * M);
   up(sv->cap, g->w.data(), 4 * M);
-  up(sv->hubs, hub_list.data(), 4 * hub_list.size());
+  up(sv->hch, hub_chunks.data(), sizeof(int2) * hub_chunks.size());
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->astamp, 0, 4 * M, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->stamp, 0, 4 * N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->dead, 0, N, S);
@@ -1196,6 +1413,21 @@ int dmf_get_state(dmf_solver *sv, int32_t *cap, int32_t *res, int64_t *excess, i
   return ok();
 }
 
+int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs) {
+  if (!sv || cap < 0 || (cap > 0 && (!items || !hubs))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  const int len = std::min(std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap), cap);
+  if (len <= 0) return ok();
+  std::vector<unsigned long long> h(2 * (size_t)len);
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  CK(cudaMemcpyAsync(h.data(), sv->trace, 16 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
+  CK(cudaStreamSynchronize(sv->stream), "trace");
+  for (int i = 0; i < len; i++) {
+    items[i] = (int64_t)((h[2 * i] >> 8) & 0xffffffffull);
+    hubs[i] = (int64_t)(h[2 * i] >> 40);
+  }
+  return ok();
+}
+
 int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us, int32_t *count) {
   if (!sv || !count || cap < 0 || (cap > 0 && (!kinds || !t_us))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
   const int len = std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap);
@@ -1206,7 +1438,7 @@ int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us, int
   CK(cudaMemcpyAsync(h.data(), sv->trace, 16 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
   CK(cudaStreamSynchronize(sv->stream), "trace");
   for (int i = 0; i < std::min(len, cap); i++) {
-    kinds[i] = (int32_t)h[2 * i];
+    kinds[i] = (int32_t)(h[2 * i] & 0xff);
     t_us[i] = (double)(h[2 * i + 1] - h[1]) * 1e-3;
   }
   return ok();

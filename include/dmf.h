@@ -207,6 +207,9 @@ int dmf_stats_get(const dmf_solver *sv, dmf_stats *st);
  * times whole calls with cudaEvents, code/dyn_data_bench.cu:246-258). */
 int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us,
                   int32_t *count);
+/* Work of each timeline entry: items[i] = vertices in the frontier or worklist
+ * processed by that phase, hubs[i] = of which hubs (block-wide vertices). */
+int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs);
 /* Replaces the option set of a live solver (variant, cycles, interval, tile). */
 int dmf_solver_set_opts(dmf_solver *sv, const dmf_opts *opts);
 int dmf_solver_destroy(dmf_solver *sv);
