@@ -29,7 +29,7 @@ using namespace dmfd;
 namespace {
 
 constexpr int kBlock = 512;
-constexpr int kChunk = 2048;  // arcs per hub chunk (one block item)
+constexpr int kChunk = 256;  // arcs per hub chunk: one warp item, 8 arcs per lane
 
 enum Mode : int { MODE_STATIC = 0, MODE_DYNAMIC = 1, MODE_RECOMPUTE = 2, MODE_CUT = 3 };
 
@@ -57,8 +57,10 @@ struct Params {
   int2 *fh[2], *wh[2], *ah;    // hub chunk queues
   const int2 *hch;             // every hub's chunks (bottom-up BFS, topology-driven rounds)
   int nhch;
-  long long *hc_tsum, *hc_ex, *hc_moved;  // per hub-chunk scratch of a push round
-  int *hc_tmin;
+  // per hub-chunk scratch of a push round, indexed by list position: tsum/tmin
+  // per chunk; ex/alloc/moved/min at the hub's first chunk
+  long long *hc_tsum, *hc_ex, *hc_moved, *hc_alloc;
+  int *hc_tmin, *hc_min;
   const int *usrc, *udst, *uw;
   int k;
   Ctrl *ctrl;
@@ -237,7 +239,8 @@ __device__ __forceinline__ void for_tiered(const Params &p, const int *list, int
 
 // A hub (degree > hub_deg) enters a queue as ceil(deg / kChunk) consecutive
 // items (v, c), chunk c covering arcs [off[v] + c*kChunk, +kChunk).  Every item
-// is one block's work, so a hub's adjacency is spread over many blocks.
+// is one warp's work, so a hub's adjacency is spread over many warps and no
+// block-wide synchronisation is needed.
 __device__ __forceinline__ int nchunks(int d) { return (d + kChunk - 1) / kChunk; }
 
 __device__ __forceinline__ void append_hub(const Params &p, int2 *q, int *tail, int v) {
@@ -336,10 +339,11 @@ __device__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LSt
   const int cur = L & 1, nxt = cur ^ 1;
   const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
   VisitAcc acc;
-  for (int i = blockIdx.x; i < nh; i += gridDim.x) {
+  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nh; i += nwarps) {
     int beg, end;
-    chunk_range(p, p.fh[cur][i], beg, end);
-    for (int a = beg + threadIdx.x; a < end; a += blockDim.x) td_arc(p, out, nxt, a, L, ls, acc);
+    chunk_range(p, __ldcg(p.fh[cur] + i), beg, end);
+    for (int a = beg + lane; a < end; a += 32) td_arc(p, out, nxt, a, L, ls, acc);
   }
   for_tiered<TILE>(p, p.fq[cur], nn, [&](auto &g, int x) {
     const int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
@@ -349,34 +353,30 @@ __device__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LSt
 }
 
 // Bottom-up level: every unvisited vertex looks for a residual arc into level
-// L and stops at the first one.  Hub chunks are searched by whole blocks
-// (strided, with a shared found-flag polled every 8 strides; the first chunk of
-// a hub to succeed labels it); other vertices by a lane or a tile.
+// L and stops at the first one.  Hub chunks are searched by warps (the first
+// chunk of a hub to succeed labels it); other vertices by a lane or a tile.
 template <int TILE>
 __device__ void ph_bfs_bu(const Params &p, Slot *out, int L, LStats &ls) {
   const int nxt = (L & 1) ^ 1;
   VisitAcc acc;
-  __shared__ int s_flag;
-  for (int i = blockIdx.x; i < p.nhch; i += gridDim.x) {
-    const int2 it = p.hch[i];
-    __syncthreads();
-    if (threadIdx.x == 0) s_flag = __ldcg(p.height + it.x) == UNV ? 0 : -1;
-    __syncthreads();
-    if (s_flag < 0) continue;  // labelled already (block-uniform through shared memory)
-    int beg, end;
-    chunk_range(p, it, beg, end);
-    int k = 0;
-    for (int a = beg + threadIdx.x; a < end; a += blockDim.x, k++) {
-      if ((k & 7) == 7 && *(volatile int *)&s_flag) break;
-      ls.arcs++;
-      if (__ldcg(p.res + a) > 0 && __ldcg(p.height + __ldg(p.adj + a)) == L) {
-        s_flag = 1;
-        break;
+  {
+    TileGroup<32> wg;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < p.nhch; i += nwarps) {
+      const int2 it = __ldg(p.hch + i);
+      int hv = 0;
+      if (wg.rank() == 0) hv = __ldcg(p.height + it.x);
+      if (wg.g.shfl(hv, 0) != UNV) continue;  // labelled already (possibly by another chunk)
+      int beg, end;
+      chunk_range(p, it, beg, end);
+      bool hit = false;
+      for (int a = beg + wg.rank(); a < end && !hit; a += 32) {
+        ls.arcs++;
+        hit = __ldcg(p.res + a) > 0 && __ldcg(p.height + __ldg(p.adj + a)) == L;
       }
+      if (wg.any(hit) && wg.rank() == 0 && atomicCAS(p.height + it.x, UNV, L + 1) == UNV)
+        bfs_visit(p, out, nxt, it.x, acc);
     }
-    __syncthreads();
-    if (s_flag > 0 && threadIdx.x == 0 && atomicCAS(p.height + it.x, UNV, L + 1) == UNV)
-      bfs_visit(p, out, nxt, it.x, acc);
   }
   for_tiered<TILE>(p, nullptr, p.n, [&](auto &g, int v) {
     if (__ldcg(p.height + v) != UNV) return;  // only v's group writes it in this phase
@@ -595,7 +595,7 @@ __device__ __forceinline__ RoundIn round_inputs(const Params &p, int r) {
 
 // Push round, phase 1: non-hub vertices are discharged completely; every hub
 // chunk computes its admissible residual sum and its minimum non-admissible
-// height (chunk 0 also snapshots the hub's excess).
+// height (chunk 0 also snapshots the hub's excess and clears its totals).
 template <int TILE, int BLOCK>
 __device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls,
                          typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
@@ -609,42 +609,45 @@ __device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned rou
     }
     c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
   }
-  __shared__ int s_h;
-  BlockGroup<BLOCK> bg(btmp, bci, bcl);
-  for (int i = blockIdx.x; i < in.nh; i += gridDim.x) {
-    const int2 it = __ldcg(in.hlist + i);
-    const int v = it.x;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_h = __ldcg(p.height + v);
-      if (it.y == 0) {
-        p.hc_ex[i] = __ldcg(p.excess + v);
-        p.hc_moved[i] = 0;
-      }
-    }
-    __syncthreads();
-    const int h = s_h;
-    long long tsum = 0;
-    int tmin = INT_MAX;
-    if (h < p.n && v != p.s && v != p.t) {
-      int beg, end;
-      chunk_range(p, it, beg, end);
-#pragma unroll 4
-      for (int a = beg + threadIdx.x; a < end; a += BLOCK) {
-        const int rr = __ldcg(p.res + a);
-        ls.arcs++;
-        if (rr > 0) {
-          const int hw = __ldcg(p.height + __ldg(p.adj + a));
-          if (hw < h) tsum += rr;
-          else tmin = min(tmin, hw);
+  {
+    TileGroup<32> wg;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = gt >> 5; i < in.nh; i += nwarps) {
+      const int2 it = __ldcg(in.hlist + i);
+      const int v = it.x;
+      int hh = 0;
+      if (wg.rank() == 0) {
+        hh = __ldcg(p.height + v);
+        if (it.y == 0) {
+          p.hc_ex[i] = __ldcg(p.excess + v);
+          p.hc_alloc[i] = 0;
+          p.hc_moved[i] = 0;
+          p.hc_min[i] = INT_MAX;
         }
       }
-    }
-    const long long ts = bg.sum_all(tsum);
-    const int tm = bg.min_all(tmin);
-    if (threadIdx.x == 0) {
-      p.hc_tsum[i] = ts;
-      p.hc_tmin[i] = tm;
+      const int h = wg.g.shfl(hh, 0);
+      long long tsum = 0;
+      int tmin = INT_MAX;
+      if (h < p.n && v != p.s && v != p.t) {
+        int beg, end;
+        chunk_range(p, it, beg, end);
+#pragma unroll 4
+        for (int a = beg + wg.rank(); a < end; a += 32) {
+          const int rr = __ldcg(p.res + a);
+          ls.arcs++;
+          if (rr > 0) {
+            const int hw = __ldcg(p.height + __ldg(p.adj + a));
+            if (hw < h) tsum += rr;
+            else tmin = min(tmin, hw);
+          }
+        }
+      }
+      const long long ts = wg.sum_all(tsum);
+      const int tm = wg.min_all(tmin);
+      if (wg.rank() == 0) {
+        p.hc_tsum[i] = ts;
+        p.hc_tmin[i] = tm;
+      }
     }
   }
   int seen = 0;
@@ -654,50 +657,54 @@ __device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned rou
   if (topo) agg_add_int(&c->seen[r % 3], seen);
 }
 
-// Push round, phase 2: each hub chunk pushes its share of the hub's excess
-// (excess minus the admissible residual of the chunks before it, capped at its
-// own) over its admissible arcs: lane budgets from a block prefix sum, then a
-// greedy pass.  Moved amounts are summed per hub.
-template <int BLOCK>
-__device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls,
-                         typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
+// Push round, phase 2: each hub chunk takes its share of the hub's excess by an
+// atomic prefix over the chunks' admissible residual sums (the order of the
+// atomics decides which chunk pushes first; the sum pushed is exactly
+// min(excess, total admissible residual)), then pushes it over its admissible
+// arcs: lane budgets from a warp prefix sum, then a greedy pass.  The same
+// atomics leave the hub's total admissible residual, minimum non-admissible
+// height and moved amount at its first chunk.
+__device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls) {
   const bool topo = p.variant == DMF_VARIANT_TOPO;
-  __shared__ int s_h;
-  __shared__ long long s_ex;
-  BlockGroup<BLOCK> bg(btmp, bci, bcl);
-  for (int i = blockIdx.x; i < in.nh; i += gridDim.x) {
+  TileGroup<32> wg;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < in.nh; i += nwarps) {
     const int2 it = __ldcg(in.hlist + i);
     const int v = it.x, base = i - it.y;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_h = __ldcg(p.height + v);
-      s_ex = __ldcg(p.hc_ex + base);
+    long long e0 = 0, old = 0, mine = 0;
+    int hh = 0;
+    if (wg.rank() == 0) {
+      hh = __ldcg(p.height + v);
+      e0 = __ldcg(p.hc_ex + base);
+      if (e0 > 0 && hh < p.n && v != p.s && v != p.t) {
+        mine = __ldcg(p.hc_tsum + i);
+        old = atomic_add_ll(p.hc_alloc + base, mine);
+        const int tm = __ldcg(p.hc_tmin + i);
+        if (tm != INT_MAX) atomicMin(p.hc_min + base, tm);
+      }
     }
-    __syncthreads();
-    const int h = s_h;
-    const long long ex0 = s_ex;
+    const int h = wg.g.shfl(hh, 0);
+    const long long ex0 = wg.g.shfl(e0, 0);
     if (!(ex0 > 0 && h < p.n) || v == p.s || v == p.t) continue;
-    long long prior = 0;
-    for (int j = threadIdx.x; j < it.y; j += BLOCK) prior += __ldcg(p.hc_tsum + base + j);
-    prior = bg.sum_all(prior);
-    long long cb = ex0 - prior;
-    const long long mine = __ldcg(p.hc_tsum + i);
+    old = wg.g.shfl(old, 0);
+    mine = wg.g.shfl(mine, 0);
+    long long cb = ex0 - old;
     cb = cb < 0 ? 0 : (cb > mine ? mine : cb);
-    if (cb == 0) continue;  // block-uniform
+    if (cb == 0) continue;  // warp-uniform
     int beg, end;
     chunk_range(p, it, beg, end);
     long long tsum = 0;
 #pragma unroll 4
-    for (int a = beg + threadIdx.x; a < end; a += BLOCK) {
+    for (int a = beg + wg.rank(); a < end; a += 32) {
       const int rr = __ldcg(p.res + a);
       if (rr > 0 && __ldcg(p.height + __ldg(p.adj + a)) < h) tsum += rr;
     }
     long long tot;
-    const long long pre = bg.scan(tsum, tot);
+    const long long pre = wg.scan(tsum, tot);
     long long budget = cb - pre;
     budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
     long long done = 0;
-    for (int a = beg + threadIdx.x; a < end && budget > 0; a += BLOCK) {
+    for (int a = beg + wg.rank(); a < end && budget > 0; a += 32) {
       const int rr = __ldcg(p.res + a);
       if (rr <= 0) continue;
       const int w = __ldg(p.adj + a);
@@ -707,15 +714,15 @@ __device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned rou
       budget -= d;
       done += d;
     }
-    const long long moved = bg.sum_all(done);
-    if (threadIdx.x == 0 && moved) atomic_add_ll(p.hc_moved + base, moved);
+    const long long moved = wg.sum_all(done);
+    if (wg.rank() == 0 && moved) atomic_add_ll(p.hc_moved + base, moved);
   }
 }
 
-// Push round, phase 3: per hub (its chunk 0), the moved total leaves its
-// excess; when every chunk's admissible residual was pushed and excess is left,
-// the hub is relabelled to 1 + the minimum non-admissible height; a hub with
-// excess left is queued for the next round.
+// Push round, phase 3: per hub (its first chunk), the moved total leaves its
+// excess; when all of the hub's admissible residual was pushed and excess is
+// left, the hub is relabelled to 1 + the minimum non-admissible height; a hub
+// with excess left is queued for the next round.
 __device__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   const bool topo = p.variant == DMF_VARIANT_TOPO;
@@ -729,13 +736,8 @@ __device__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned rou
     if (!(ex0 > 0 && h < p.n) || v == p.s || v == p.t) continue;
     seen++;
     ls.visits++;
-    const int k = nchunks(deg_of(p, v));
-    long long tot = 0;
-    int mh = INT_MAX;
-    for (int j = 0; j < k; j++) {
-      tot += __ldcg(p.hc_tsum + i + j);
-      mh = min(mh, __ldcg(p.hc_tmin + i + j));
-    }
+    const long long tot = __ldcg(p.hc_alloc + i);
+    const int mh = __ldcg(p.hc_min + i);
     const long long moved = __ldcg(p.hc_moved + i);
     const long long ex = ex0 - moved;
     if (moved) atomic_add_ll(p.excess + v, -moved);
@@ -897,7 +899,7 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
       if (!next()) return;
       if (in.nh > 0) {
         kind = TR_PUSH_HUB;
-        ph_push2<BLOCK>(p, in, r, round_id, ls, btmp, bci, bcl);
+        ph_push2(p, in, r, round_id, ls);
         if (!next()) return;
         kind = TR_PUSH_HUB_FINISH;
         ph_push3(p, in, r, round_id, ls);
@@ -972,8 +974,8 @@ struct dmf_solver {
   int2 *hqbuf = nullptr;  // 5 hub-chunk queues, same roles
   int2 *hch = nullptr;    // every hub's chunks
   int nchunk = 0;         // total hub chunks = capacity of each hub-chunk queue
-  long long *hc_tsum = nullptr, *hc_ex = nullptr, *hc_moved = nullptr;
-  int *hc_tmin = nullptr;
+  long long *hc_tsum = nullptr, *hc_ex = nullptr, *hc_moved = nullptr, *hc_alloc = nullptr;
+  int *hc_tmin = nullptr, *hc_min = nullptr;
   bool thresholds_set = false;
   int *ubuf = nullptr;  // device update staging: src | dst | w
   int kcap = 0;
@@ -1123,6 +1125,8 @@ int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, 
   p.hc_ex = sv->hc_ex;
   p.hc_moved = sv->hc_moved;
   p.hc_tmin = sv->hc_tmin;
+  p.hc_alloc = sv->hc_alloc;
+  p.hc_min = sv->hc_min;
   p.usrc = d_src;
   p.udst = d_dst;
   p.uw = d_w;
@@ -1308,7 +1312,8 @@ int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *
   const size_t NC = (size_t)std::max(sv->nchunk, 1);
   if ((st = dalloc(sv, &sv->hqbuf, 5 * NC)) || (st = dalloc(sv, &sv->hch, NC)) ||
       (st = dalloc(sv, &sv->hc_tsum, NC)) || (st = dalloc(sv, &sv->hc_ex, NC)) ||
-      (st = dalloc(sv, &sv->hc_moved, NC)) || (st = dalloc(sv, &sv->hc_tmin, NC)))
+      (st = dalloc(sv, &sv->hc_moved, NC)) || (st = dalloc(sv, &sv->hc_tmin, NC)) ||
+      (st = dalloc(sv, &sv->hc_alloc, NC)) || (st = dalloc(sv, &sv->hc_min, NC)))
     return bail(st);
   cudaStream_t S = sv->stream;
   cudaError_t e = cudaSuccess;
