@@ -94,7 +94,7 @@ _sig("dmf_get_state", C.c_int, VP, VP, VP, VP, VP)
 _sig("dmf_stats_get", C.c_int, VP, C.POINTER(Stats))
 _sig("dmf_trace_get", C.c_int, VP, C.c_int32, I32P, np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"),
      C.POINTER(C.c_int32))
-_sig("dmf_trace_items", C.c_int, VP, C.c_int32, I64P, I64P)
+_sig("dmf_trace_items", C.c_int, VP, C.c_int32, I64P, I64P, I64P, I64P)
 _sig("dmf_solver_set_opts", C.c_int, VP, C.POINTER(Opts))
 _sig("dmf_solver_destroy", C.c_int, VP)
 _sig("dmf_device_count", C.c_int)
@@ -243,13 +243,13 @@ class Solver:
     """Device-resident residual state of one graph on one GPU (dmf_solver)."""
 
     def __init__(self, g: Graph, source: int, sink: int, variant="data", kernel_cycles=0, relabel_interval=0,
-                 tile=0, max_iters=0, device=-1, stream=None, trace=False):
+                 tile=0, max_iters=0, device=-1, stream=None, trace=False, probe=False):
         o = Opts()
         _L.dmf_opts_default(C.byref(o))
         o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
         o.kernel_cycles, o.relabel_interval, o.tile, o.max_iters, o.device = (
             kernel_cycles, relabel_interval, tile, max_iters, device)
-        o.flags = 1 if trace else 0
+        o.flags = (1 if trace or probe else 0) | (2 if probe else 0)
         self._h = C.c_void_p()
         self.n, self.m = g.num_nodes(), g.num_edges()
         stream_ptr = None if stream is None else C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
@@ -334,8 +334,10 @@ class Solver:
         n = cnt.value
         items = np.zeros(max(n, 1), np.int64)
         hubs = np.zeros(max(n, 1), np.int64)
-        _check(_L.dmf_trace_items(self._h, n, items, hubs))
-        self.last_trace_items = list(zip(items[:n].tolist(), hubs[:n].tolist()))
+        sns = np.zeros(max(n, 1), np.int64)
+        sv_ = np.zeros(max(n, 1), np.int64)
+        _check(_L.dmf_trace_items(self._h, n, items, hubs, sns, sv_))
+        self.last_trace_items = list(zip(items[:n].tolist(), hubs[:n].tolist(), sns[:n].tolist(), sv_[:n].tolist()))
         return [(self.TRACE_KINDS.get(int(k), str(k)), float(x)) for k, x in zip(kinds[:n], t[:n])]
 
     def stats(self) -> dict:

@@ -58,6 +58,7 @@ struct Ctrl {
   // push-round worklist tails and topology-driven active counts, round r uses [r % 3]
   int wtail[3], whtail[3], seen[3];
   int pad1;
+  unsigned long long probe[2];  // longest work item of a phase, (ns << 32) | vertex
 };
 
 // ---- memory helpers ---------------------------------------------------------

@@ -61,18 +61,44 @@ struct Params {
   // per chunk; ex/alloc/moved/min at the hub's first chunk
   long long *hc_tsum, *hc_ex, *hc_moved, *hc_alloc;
   int *hc_tmin, *hc_min;
+  // Exhausted hub chunks: a chunk with no admissible arc at hub height h stays
+  // so until the hub's height changes or the next global relabel (heights only
+  // rise in between, and a reverse residual only opens from a higher head).
+  // mark = (relabel epoch << 32) | h, indexed by hub_base[v] + chunk.
+  const int *hub_base;
+  unsigned long long *chunk_mark;
+  int *chunk_tmin;
+  unsigned relabel_base;
   const int *usrc, *udst, *uw;
   int k;
   Ctrl *ctrl;
   int mode, variant, cycles, interval, max_iters, hub_deg, small_deg, need_cut;
   unsigned round_base;
   int epoch;
-  unsigned long long *trace;  // optional phase timeline: 2 words per entry
+  unsigned long long *trace;  // optional phase timeline: 4 words per entry
   int trace_cap;
+  int probe;                  // time work items (DMF_FLAG_PROBE)
 };
 
 struct LStats {
   unsigned long long pushes = 0, relabels = 0, arcs = 0, visits = 0;
+  unsigned long long probe = 0;  // (longest single item in ns << 32) | vertex, this phase
+};
+
+// Optional probe (DMF_FLAG_PROBE): times every work item and keeps the longest.
+struct ItemTimer {
+  unsigned long long t0;
+  bool on;
+  __device__ __forceinline__ ItemTimer(const Params &p) : t0(0), on(p.probe) {
+    if (on) t0 = globaltimer();
+  }
+  __device__ __forceinline__ void done(LStats &ls, int v) {
+    if (!on) return;
+    unsigned long long dt = globaltimer() - t0;
+    if (dt > 0xffffffffull) dt = 0xffffffffull;
+    const unsigned long long key = (dt << 32) | (unsigned)v;
+    if (key > ls.probe) ls.probe = key;
+  }
 };
 
 __device__ __forceinline__ int deg_of(const Params &p, int v) { return __ldg(p.off + v + 1) - __ldg(p.off + v); }
@@ -211,7 +237,7 @@ __device__ void ph_cut_saturate(const Params &p) {
 // block-wide) one after another by the whole tile.  `f(group, v)` does the work
 // for one vertex.
 template <int TILE, class F>
-__device__ __forceinline__ void for_tiered(const Params &p, const int *list, int nn, F &&f) {
+__device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const int *list, int nn, F &&f) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   TileGroup<TILE> tg;
   for (int base = (gt / TILE) * TILE; base < nn; base += nt) {
@@ -225,14 +251,19 @@ __device__ __forceinline__ void for_tiered(const Params &p, const int *list, int
     const bool small = v >= 0 && d <= p.small_deg;
     if (small) {
       ThreadGroup th;
+      ItemTimer tm(p);
       f(th, v);
+      tm.done(ls, v);
     }
     tg.g.sync();
     unsigned big = tg.g.ballot(v >= 0 && !small);
     while (big) {
       const int j = __ffs(big) - 1;
       big &= big - 1;
-      f(tg, tg.g.shfl(v, j));
+      const int vj = tg.g.shfl(v, j);
+      ItemTimer tm(p);
+      f(tg, vj);
+      tm.done(ls, vj);
     }
   }
 }
@@ -325,13 +356,57 @@ __device__ __forceinline__ void flush_visits(const Params &p, Slot *out, VisitAc
 // Top-down level (staticMaxFlow_kernel_11, code/dyn_data.h:72-87, run over the
 // frontier queue instead of all V): x at level L labels w when arc w->x has
 // residual, i.e. res[par[e]] > 0 for e = x->w.
-__device__ __forceinline__ void td_arc(const Params &p, Slot *out, int nxt, int a, int L, LStats &ls,
-                                       VisitAcc &acc) {
-  const int w = __ldg(p.adj + a);
-  ls.arcs++;
-  if (__ldcg(p.height + w) == UNV && __ldcg(p.res + __ldg(p.par + a)) > 0 &&
-      atomicCAS(p.height + w, UNV, L + 1) == UNV)
-    bfs_visit(p, out, nxt, w, acc);
+__device__ __forceinline__ void visit_claimed(const Params &p, Slot *out, int nxt, int w, int d, long long ex,
+                                              VisitAcc &acc) {
+  const bool hub = d > p.hub_deg;
+  if (hub) append_hub(p, p.fh[nxt], &out->hq, w);
+  else append(p.fq[nxt], &out->q, w);
+  acc.arcs += d;
+  if (w != p.s && w != p.t && ex > 0) {
+    if (hub) append_hub(p, p.ah, &p.ctrl->act_hq, w);
+    else append(p.aq, &p.ctrl->act_q, w);
+    acc.reached++;
+  }
+}
+
+// Arcs first, first+stride, ... < end of a frontier vertex, in register
+// batches of kBatch so that the gathers of a batch are in flight together:
+// heads, then head labels, then the reverse residuals, then the claims, then
+// the claimed heads' degree and excess.
+constexpr int kBatch = 8;   // arcs per lane per batch (a hub chunk is one batch)
+constexpr int kTdBatch = 4;  // smaller for top-down, which keeps more state per arc
+__device__ __forceinline__ void td_range(const Params &p, Slot *out, int nxt, int first, int end, int stride, int L,
+                                         LStats &ls, VisitAcc &acc) {
+  for (int a0 = first; a0 < end; a0 += kTdBatch * stride) {
+    int w[kTdBatch];
+    bool c[kTdBatch];
+#pragma unroll
+    for (int k = 0; k < kTdBatch; k++) {
+      const int a = a0 + k * stride;
+      w[k] = a < end ? __ldg(p.adj + a) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < kTdBatch; k++) c[k] = w[k] >= 0 && __ldcg(p.height + w[k]) == UNV;
+#pragma unroll
+    for (int k = 0; k < kTdBatch; k++)
+      if (c[k]) c[k] = __ldcg(p.res + __ldg(p.par + a0 + k * stride)) > 0;
+#pragma unroll
+    for (int k = 0; k < kTdBatch; k++)
+      if (c[k]) c[k] = atomicCAS(p.height + w[k], UNV, L + 1) == UNV;
+    int d[kTdBatch];
+    long long ex[kTdBatch];
+#pragma unroll
+    for (int k = 0; k < kTdBatch; k++)
+      if (c[k]) {
+        d[k] = deg_of(p, w[k]);
+        ex[k] = __ldcg(p.excess + w[k]);
+      }
+#pragma unroll
+    for (int k = 0; k < kTdBatch; k++) {
+      if (w[k] >= 0) ls.arcs++;
+      if (c[k]) visit_claimed(p, out, nxt, w[k], d[k], ex[k], acc);
+    }
+  }
 }
 
 template <int TILE>
@@ -342,14 +417,36 @@ __device__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LSt
   const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nh; i += nwarps) {
     int beg, end;
-    chunk_range(p, __ldcg(p.fh[cur] + i), beg, end);
-    for (int a = beg + lane; a < end; a += 32) td_arc(p, out, nxt, a, L, ls, acc);
+    const int2 it = __ldcg(p.fh[cur] + i);
+    ItemTimer tm(p);
+    chunk_range(p, it, beg, end);
+    td_range(p, out, nxt, beg + lane, end, 32, L, ls, acc);
+    tm.done(ls, it.x);
   }
-  for_tiered<TILE>(p, p.fq[cur], nn, [&](auto &g, int x) {
+  for_tiered<TILE>(p, ls, p.fq[cur], nn, [&](auto &g, int x) {
     const int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
-    for (int a = beg + g.rank(); a < end; a += g.size()) td_arc(p, out, nxt, a, L, ls, acc);
+    td_range(p, out, nxt, beg + g.rank(), end, g.size(), L, ls, acc);
   });
   flush_visits(p, out, acc);
+}
+
+// Whether one of the arcs first, first+stride, ... < end (at most kBatch of them)
+// has residual into a vertex labelled L; loads batched as in td_range.
+__device__ __forceinline__ bool bu_batch(const Params &p, int first, int end, int stride, int L, LStats &ls) {
+  int r[kBatch], w[kBatch];
+#pragma unroll
+  for (int k = 0; k < kBatch; k++) {
+    const int a = first + k * stride;
+    r[k] = a < end ? __ldcg(p.res + a) : 0;
+    w[k] = a < end ? __ldg(p.adj + a) : -1;
+  }
+  bool hit = false;
+#pragma unroll
+  for (int k = 0; k < kBatch; k++) {
+    if (w[k] >= 0) ls.arcs++;
+    hit |= r[k] > 0 && __ldcg(p.height + w[k]) == L;
+  }
+  return hit;
 }
 
 // Bottom-up level: every unvisited vertex looks for a residual arc into level
@@ -369,27 +466,17 @@ __device__ void ph_bfs_bu(const Params &p, Slot *out, int L, LStats &ls) {
       if (wg.g.shfl(hv, 0) != UNV) continue;  // labelled already (possibly by another chunk)
       int beg, end;
       chunk_range(p, it, beg, end);
-      bool hit = false;
-      for (int a = beg + wg.rank(); a < end && !hit; a += 32) {
-        ls.arcs++;
-        hit = __ldcg(p.res + a) > 0 && __ldcg(p.height + __ldg(p.adj + a)) == L;
-      }
+      const bool hit = bu_batch(p, beg + wg.rank(), end, 32, L, ls);  // 256 arcs = one batch
       if (wg.any(hit) && wg.rank() == 0 && atomicCAS(p.height + it.x, UNV, L + 1) == UNV)
         bfs_visit(p, out, nxt, it.x, acc);
     }
   }
-  for_tiered<TILE>(p, nullptr, p.n, [&](auto &g, int v) {
+  for_tiered<TILE>(p, ls, nullptr, p.n, [&](auto &g, int v) {
     if (__ldcg(p.height + v) != UNV) return;  // only v's group writes it in this phase
     const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
     bool found = false;
-    for (int base = beg; base < end; base += g.size()) {
-      const int a = base + g.rank();
-      bool hit = false;
-      if (a < end) {
-        ls.arcs++;
-        hit = __ldcg(p.res + a) > 0 && __ldcg(p.height + __ldg(p.adj + a)) == L;
-      }
-      if (g.any(hit)) {
+    for (int base = beg; base < end; base += kBatch * g.size()) {
+      if (g.any(bu_batch(p, base + g.rank(), end, g.size(), L, ls))) {
         found = true;
         break;
       }
@@ -597,7 +684,7 @@ __device__ __forceinline__ RoundIn round_inputs(const Params &p, int r) {
 // chunk computes its admissible residual sum and its minimum non-admissible
 // height (chunk 0 also snapshots the hub's excess and clears its totals).
 template <int TILE, int BLOCK>
-__device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls,
+__device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned round_id, unsigned gepoch, LStats &ls,
                          typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
   Ctrl *c = p.ctrl;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -615,6 +702,7 @@ __device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned rou
     for (int i = gt >> 5; i < in.nh; i += nwarps) {
       const int2 it = __ldcg(in.hlist + i);
       const int v = it.x;
+      ItemTimer tmr(p);
       int hh = 0;
       if (wg.rank() == 0) {
         hh = __ldcg(p.height + v);
@@ -626,32 +714,52 @@ __device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned rou
         }
       }
       const int h = wg.g.shfl(hh, 0);
-      long long tsum = 0;
-      int tmin = INT_MAX;
-      if (h < p.n && v != p.s && v != p.t) {
+      const int cidx = __ldg(p.hub_base + v) + it.y;
+      const unsigned long long key = ((unsigned long long)gepoch << 32) | (unsigned)h;
+      unsigned long long mk = 0;
+      if (wg.rank() == 0) mk = __ldcg(p.chunk_mark + cidx);
+      mk = wg.g.shfl(mk, 0);
+      long long ts = 0;
+      int tm = INT_MAX;
+      if (mk == key) {  // exhausted at this height: only its minimum head height matters
+        if (wg.rank() == 0) tm = __ldcg(p.chunk_tmin + cidx);
+      } else if (h < p.n && v != p.s && v != p.t) {
         int beg, end;
         chunk_range(p, it, beg, end);
-#pragma unroll 4
-        for (int a = beg + wg.rank(); a < end; a += 32) {
-          const int rr = __ldcg(p.res + a);
-          ls.arcs++;
-          if (rr > 0) {
-            const int hw = __ldcg(p.height + __ldg(p.adj + a));
-            if (hw < h) tsum += rr;
+        int rr[kBatch], w[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) {
+          const int a = beg + wg.rank() + 32 * k;
+          rr[k] = a < end ? __ldcg(p.res + a) : 0;
+          w[k] = a < end ? __ldg(p.adj + a) : 0;
+        }
+        long long tsum = 0;
+        int tmin = INT_MAX;
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) {
+          if (rr[k] > 0) {
+            const int hw = __ldcg(p.height + w[k]);
+            if (hw < h) tsum += rr[k];
             else tmin = min(tmin, hw);
           }
         }
+        ls.arcs += kBatch;
+        ts = wg.sum_all(tsum);
+        tm = wg.min_all(tmin);
+        if (ts == 0 && wg.rank() == 0) {
+          p.chunk_mark[cidx] = key;
+          p.chunk_tmin[cidx] = tm;
+        }
       }
-      const long long ts = wg.sum_all(tsum);
-      const int tm = wg.min_all(tmin);
       if (wg.rank() == 0) {
         p.hc_tsum[i] = ts;
         p.hc_tmin[i] = tm;
       }
+      tmr.done(ls, v);
     }
   }
   int seen = 0;
-  for_tiered<TILE>(p, in.nlist, in.nn, [&](auto &g, int v) {
+  for_tiered<TILE>(p, ls, in.nlist, in.nn, [&](auto &g, int v) {
     discharge(g, p, v, r, round_id, !topo, ls, topo ? &seen : nullptr);
   });
   if (topo) agg_add_int(&c->seen[r % 3], seen);
@@ -664,7 +772,8 @@ __device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned rou
 // arcs: lane budgets from a warp prefix sum, then a greedy pass.  The same
 // atomics leave the hub's total admissible residual, minimum non-admissible
 // height and moved amount at its first chunk.
-__device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls) {
+__device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned round_id, unsigned gepoch,
+                         LStats &ls) {
   const bool topo = p.variant == DMF_VARIANT_TOPO;
   TileGroup<32> wg;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -693,29 +802,44 @@ __device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned rou
     if (cb == 0) continue;  // warp-uniform
     int beg, end;
     chunk_range(p, it, beg, end);
+    int rr[kBatch], w[kBatch];
+    bool adm[kBatch];
     long long tsum = 0;
-#pragma unroll 4
-    for (int a = beg + wg.rank(); a < end; a += 32) {
-      const int rr = __ldcg(p.res + a);
-      if (rr > 0 && __ldcg(p.height + __ldg(p.adj + a)) < h) tsum += rr;
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) {
+      const int a = beg + wg.rank() + 32 * k;
+      rr[k] = a < end ? __ldcg(p.res + a) : 0;
+      w[k] = a < end ? __ldg(p.adj + a) : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) {
+      adm[k] = rr[k] > 0 && __ldcg(p.height + w[k]) < h;
+      if (adm[k]) tsum += rr[k];
     }
     long long tot;
     const long long pre = wg.scan(tsum, tot);
     long long budget = cb - pre;
     budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
     long long done = 0;
-    for (int a = beg + wg.rank(); a < end && budget > 0; a += 32) {
-      const int rr = __ldcg(p.res + a);
-      if (rr <= 0) continue;
-      const int w = __ldg(p.adj + a);
-      if (__ldcg(p.height + w) >= h) continue;
-      const int d = (int)(rr < budget ? rr : budget);
-      push_arc(p, a, w, d, r, round_id, !topo, ls);
-      budget -= d;
-      done += d;
+    // residuals only grew since the loads (reverse pushes), so rr is a safe amount
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) {
+      if (adm[k] && budget > 0) {
+        const int d = (int)(rr[k] < budget ? rr[k] : budget);
+        push_arc(p, beg + wg.rank() + 32 * k, w[k], d, r, round_id, !topo, ls);
+        budget -= d;
+        done += d;
+      }
     }
     const long long moved = wg.sum_all(done);
-    if (wg.rank() == 0 && moved) atomic_add_ll(p.hc_moved + base, moved);
+    if (wg.rank() == 0) {
+      if (moved) atomic_add_ll(p.hc_moved + base, moved);
+      if (moved == mine && cb == mine) {  // every admissible arc of the chunk saturated
+        const int cidx = __ldg(p.hub_base + v) + it.y;
+        p.chunk_mark[cidx] = ((unsigned long long)gepoch << 32) | (unsigned)h;
+        p.chunk_tmin[cidx] = __ldcg(p.hc_tmin + i);
+      }
+    }
   }
 }
 
@@ -786,12 +910,20 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
   auto slot_in = [&]() { return &c->slot[(ph + 2) % 3]; };
   auto record = [&]() {
     if (lead && p.trace && ph < p.trace_cap) {
-      p.trace[2 * ph] = (unsigned long long)kind | ((unsigned long long)(items & 0xffffffffll) << 8) |
+      p.trace[4 * ph] = (unsigned long long)kind | ((unsigned long long)(items & 0xffffffffll) << 8) |
                         ((unsigned long long)(hubitems & 0xffffff) << 40);
-      p.trace[2 * ph + 1] = globaltimer();
+      p.trace[4 * ph + 1] = globaltimer();
+      p.trace[4 * ph + 2] = ph > 0 ? ld_vol((const long long *)&c->probe[(ph + 1) & 1]) : 0;
+      c->probe[(ph + 1) & 1] = 0;
     }
   };
   auto next = [&]() -> bool {
+    if (p.probe) {  // longest item of the phase that is ending
+      cg::thread_block_tile<32> w = cg::tiled_partition<32>(cg::this_thread_block());
+      const unsigned long long mx = cg::reduce(w, ls.probe, cg::greater<unsigned long long>());
+      if (w.thread_rank() == 0 && mx) atomicMax(&c->probe[ph & 1], mx);
+      ls.probe = 0;
+    }
     if (!grid_barrier(c)) return false;
     ph++;
     record();
@@ -895,11 +1027,11 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
       kind = TR_PUSH;
       items = in.nn;
       hubitems = in.nh;
-      ph_push1<TILE, BLOCK>(p, in, r, round_id, ls, btmp, bci, bcl);
+      ph_push1<TILE, BLOCK>(p, in, r, round_id, p.relabel_base + it, ls, btmp, bci, bcl);
       if (!next()) return;
       if (in.nh > 0) {
         kind = TR_PUSH_HUB;
-        ph_push2(p, in, r, round_id, ls);
+        ph_push2(p, in, r, round_id, p.relabel_base + it, ls);
         if (!next()) return;
         kind = TR_PUSH_HUB_FINISH;
         ph_push3(p, in, r, round_id, ls);
@@ -921,8 +1053,8 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
   if (lead && p.trace && ph + 1 < p.trace_cap) c->trace_len = ph + 1;
 }
 
-template <int TILE, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 2) k_solve(Params p) {
+template <int TILE, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_solve(Params p) {
   __shared__ typename BlockGroup<BLOCK>::Temp btmp;
   __shared__ int bci;
   __shared__ long long bcl;
@@ -943,12 +1075,22 @@ __global__ void __launch_bounds__(BLOCK, 2) k_solve(Params p) {
 
 using KernelFn = void (*)(Params);
 
-KernelFn pick_kernel(int tile) {
+// minb = resident blocks per SM the register budget is sized for (1: up to 128
+// registers a thread, 2: up to 64).
+KernelFn pick_kernel(int tile, int minb) {
+  if (minb == 1) {
+    switch (tile) {
+      case 4: return k_solve<4, kBlock, 1>;
+      case 8: return k_solve<8, kBlock, 1>;
+      case 16: return k_solve<16, kBlock, 1>;
+      default: return k_solve<32, kBlock, 1>;
+    }
+  }
   switch (tile) {
-    case 4: return k_solve<4, kBlock>;
-    case 8: return k_solve<8, kBlock>;
-    case 16: return k_solve<16, kBlock>;
-    default: return k_solve<32, kBlock>;
+    case 4: return k_solve<4, kBlock, 2>;
+    case 8: return k_solve<8, kBlock, 2>;
+    case 16: return k_solve<16, kBlock, 2>;
+    default: return k_solve<32, kBlock, 2>;
   }
 }
 
@@ -965,7 +1107,7 @@ struct dmf_solver {
   cudaStream_t stream = nullptr;
   int n = 0, m = 0, s = 0, t = 0;
   dmf_opts opts{};
-  int tile = 32, grid = 0, block = kBlock, hub_deg = 256, small_deg = 8;
+  int tile = 32, grid = 0, block = kBlock, hub_deg = 256, small_deg = 8, minb = 1;
   int *off = nullptr, *adj = nullptr, *par = nullptr, *sidx = nullptr, *cap = nullptr, *res = nullptr;
   int *height = nullptr, *stamp = nullptr, *astamp = nullptr, *uarc = nullptr;
   long long *excess = nullptr;
@@ -976,6 +1118,10 @@ struct dmf_solver {
   int nchunk = 0;         // total hub chunks = capacity of each hub-chunk queue
   long long *hc_tsum = nullptr, *hc_ex = nullptr, *hc_moved = nullptr, *hc_alloc = nullptr;
   int *hc_tmin = nullptr, *hc_min = nullptr;
+  int *hub_base = nullptr;
+  unsigned long long *chunk_mark = nullptr;
+  int *chunk_tmin = nullptr;
+  unsigned relabel_base = 1;
   bool thresholds_set = false;
   int *ubuf = nullptr;  // device update staging: src | dst | w
   int kcap = 0;
@@ -1049,7 +1195,9 @@ int configure(dmf_solver *sv) {
     if (const char *e = std::getenv("DMF_HUB_DEG")) sv->hub_deg = std::max(32, std::atoi(e));
     sv->thresholds_set = true;
   }
-  KernelFn fn = pick_kernel(sv->tile);
+  sv->minb = 1;
+  if (const char *e = std::getenv("DMF_MINB")) sv->minb = std::atoi(e) == 2 ? 2 : 1;
+  KernelFn fn = pick_kernel(sv->tile, sv->minb);
   int per_sm = 0, sms = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kBlock, 0), "occupancy");
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, sv->dev), "sm count");
@@ -1127,6 +1275,10 @@ int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, 
   p.hc_tmin = sv->hc_tmin;
   p.hc_alloc = sv->hc_alloc;
   p.hc_min = sv->hc_min;
+  p.hub_base = sv->hub_base;
+  p.chunk_mark = sv->chunk_mark;
+  p.chunk_tmin = sv->chunk_tmin;
+  p.relabel_base = sv->relabel_base;
   p.usrc = d_src;
   p.udst = d_dst;
   p.uw = d_w;
@@ -1144,12 +1296,13 @@ int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, 
   p.need_cut = sv->opts.variant == DMF_VARIANT_PP ? 1 : 0;
   p.round_base = sv->round_base;
   p.trace = (sv->opts.flags & DMF_FLAG_TRACE) ? sv->trace : nullptr;
+  p.probe = (sv->opts.flags & DMF_FLAG_PROBE) && p.trace ? 1 : 0;
   p.trace_cap = sv->trace_cap;
   p.epoch = ++sv->epoch;
   if (sv->epoch == INT_MAX) sv->epoch = 0;
   CK(cudaMemsetAsync(sv->ctrl, 0, sizeof(Ctrl), sv->stream), "memset ctrl");
   void *args[] = {&p};
-  CK(cudaLaunchCooperativeKernel((const void *)pick_kernel(sv->tile), dim3(sv->grid), dim3(sv->block), args, 0,
+  CK(cudaLaunchCooperativeKernel((const void *)pick_kernel(sv->tile, sv->minb), dim3(sv->grid), dim3(sv->block), args, 0,
                                  sv->stream),
      "cooperative launch");
   CK(cudaMemcpyAsync(sv->h_ctrl, sv->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, sv->stream), "D2H ctrl");
@@ -1176,6 +1329,7 @@ int finish(dmf_solver *sv, int64_t *flow, bool need_cut_valid) {
   sv->st.block_threads = sv->block;
   sv->st.tile = sv->tile;
   sv->round_base += c.rounds_used + 2;
+  sv->relabel_base += (unsigned)c.st_outer + 2;
   if (c.err) {
     sv->solved = false;
     sv->side_valid = false;
@@ -1303,17 +1457,22 @@ int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *
       (st = dalloc(sv, &sv->qbuf, 5 * N)) || (st = dalloc(sv, &sv->ctrl, 1)))
     return bail(st);
   std::vector<int2> hub_chunks;
+  std::vector<int> hub_base(g->n, -1);
   for (int v = 0; v < g->n; v++) {
     const int d = g->off[v + 1] - g->off[v];
-    if (d > sv->hub_deg)
+    if (d > sv->hub_deg) {
+      hub_base[v] = (int)hub_chunks.size();
       for (int c = 0; c * kChunk < d; c++) hub_chunks.push_back(make_int2(v, c));
+    }
   }
   sv->nchunk = (int)hub_chunks.size();
   const size_t NC = (size_t)std::max(sv->nchunk, 1);
   if ((st = dalloc(sv, &sv->hqbuf, 5 * NC)) || (st = dalloc(sv, &sv->hch, NC)) ||
       (st = dalloc(sv, &sv->hc_tsum, NC)) || (st = dalloc(sv, &sv->hc_ex, NC)) ||
       (st = dalloc(sv, &sv->hc_moved, NC)) || (st = dalloc(sv, &sv->hc_tmin, NC)) ||
-      (st = dalloc(sv, &sv->hc_alloc, NC)) || (st = dalloc(sv, &sv->hc_min, NC)))
+      (st = dalloc(sv, &sv->hc_alloc, NC)) || (st = dalloc(sv, &sv->hc_min, NC)) ||
+      (st = dalloc(sv, &sv->hub_base, N)) || (st = dalloc(sv, &sv->chunk_mark, NC)) ||
+      (st = dalloc(sv, &sv->chunk_tmin, NC)))
     return bail(st);
   cudaStream_t S = sv->stream;
   cudaError_t e = cudaSuccess;
@@ -1326,6 +1485,8 @@ int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *
   up(sv->sidx, g->sidx.data(), 4 * M);
   up(sv->cap, g->w.data(), 4 * M);
   up(sv->hch, hub_chunks.data(), sizeof(int2) * hub_chunks.size());
+  up(sv->hub_base, hub_base.data(), 4 * (size_t)g->n);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->chunk_mark, 0, 8 * NC, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->astamp, 0, 4 * M, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->stamp, 0, 4 * N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->dead, 0, N, S);
@@ -1338,7 +1499,7 @@ int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *
   if (e != cudaSuccess) return bail(cuda_fail(e, "solver upload"));
   if ((st = ensure_ubuf(sv, 1024))) return bail(st);
   sv->trace_cap = 8192;
-  if ((st = dalloc(sv, &sv->trace, 2 * (size_t)sv->trace_cap))) return bail(st);
+  if ((st = dalloc(sv, &sv->trace, 4 * (size_t)sv->trace_cap))) return bail(st);
   *out = sv;
   return ok();
 }
@@ -1418,17 +1579,20 @@ int dmf_get_state(dmf_solver *sv, int32_t *cap, int32_t *res, int64_t *excess, i
   return ok();
 }
 
-int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs) {
+int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs, int64_t *slow_ns,
+                    int64_t *slow_v) {
   if (!sv || cap < 0 || (cap > 0 && (!items || !hubs))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
   const int len = std::min(std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap), cap);
   if (len <= 0) return ok();
-  std::vector<unsigned long long> h(2 * (size_t)len);
+  std::vector<unsigned long long> h(4 * (size_t)len);
   CK(cudaSetDevice(sv->dev), "cudaSetDevice");
-  CK(cudaMemcpyAsync(h.data(), sv->trace, 16 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
+  CK(cudaMemcpyAsync(h.data(), sv->trace, 32 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
   CK(cudaStreamSynchronize(sv->stream), "trace");
   for (int i = 0; i < len; i++) {
-    items[i] = (int64_t)((h[2 * i] >> 8) & 0xffffffffull);
-    hubs[i] = (int64_t)(h[2 * i] >> 40);
+    items[i] = (int64_t)((h[4 * i] >> 8) & 0xffffffffull);
+    hubs[i] = (int64_t)(h[4 * i] >> 40);
+    if (slow_ns) slow_ns[i] = (int64_t)(h[4 * i + 2] >> 32);
+    if (slow_v) slow_v[i] = (int64_t)(h[4 * i + 2] & 0xffffffffull);
   }
   return ok();
 }
@@ -1438,13 +1602,13 @@ int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us, int
   const int len = std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap);
   *count = len;
   if (len == 0 || cap == 0) return ok();
-  std::vector<unsigned long long> h(2 * (size_t)len);
+  std::vector<unsigned long long> h(4 * (size_t)len);
   CK(cudaSetDevice(sv->dev), "cudaSetDevice");
-  CK(cudaMemcpyAsync(h.data(), sv->trace, 16 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
+  CK(cudaMemcpyAsync(h.data(), sv->trace, 32 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
   CK(cudaStreamSynchronize(sv->stream), "trace");
   for (int i = 0; i < std::min(len, cap); i++) {
-    kinds[i] = (int32_t)(h[2 * i] & 0xff);
-    t_us[i] = (double)(h[2 * i + 1] - h[1]) * 1e-3;
+    kinds[i] = (int32_t)(h[4 * i] & 0xff);
+    t_us[i] = (double)(h[4 * i + 1] - h[1]) * 1e-3;
   }
   return ok();
 }

@@ -57,6 +57,7 @@ typedef enum {
 
 /* dmf_opts.flags bits */
 #define DMF_FLAG_TRACE 1 /* record a per-phase device timeline (dmf_trace_get) */
+#define DMF_FLAG_PROBE 2 /* with TRACE: also time every work item (dmf_trace_items) */
 
 typedef struct dmf_graph dmf_graph;   /* host CSR, owned by the library */
 typedef struct dmf_solver dmf_solver; /* device-resident residual state */
@@ -208,8 +209,11 @@ int dmf_stats_get(const dmf_solver *sv, dmf_stats *st);
 int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us,
                   int32_t *count);
 /* Work of each timeline entry: items[i] = vertices in the frontier or worklist
- * processed by that phase, hubs[i] = of which hubs (block-wide vertices). */
-int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs);
+ * processed by that phase, hubs[i] = hub chunks among them; with
+ * DMF_FLAG_PROBE, slow_ns[i] / slow_v[i] = duration and vertex of the phase's
+ * longest single work item (slow_ns / slow_v may be NULL). */
+int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs,
+                    int64_t *slow_ns, int64_t *slow_v);
 /* Replaces the option set of a live solver (variant, cycles, interval, tile). */
 int dmf_solver_set_opts(dmf_solver *sv, const dmf_opts *opts);
 int dmf_solver_destroy(dmf_solver *sv);
