@@ -73,6 +73,7 @@ struct Params {
   int k;
   Ctrl *ctrl;
   int mode, variant, cycles, interval, max_iters, hub_deg, small_deg, need_cut;
+  int bu_alpha;  // bottom-up when frontier arcs * bu_alpha > unexplored arcs (0: never)
   unsigned round_base;
   int epoch;
   unsigned long long *trace;  // optional phase timeline: 4 words per entry
@@ -231,40 +232,34 @@ __device__ void ph_cut_saturate(const Params &p) {
 }
 
 // ---- degree tiers ------------------------------------------------------------------
-// Items of a vertex list (or all vertices when list == nullptr) are taken TILE
-// at a time by a tile: vertices of degree <= small_deg are handled by their own
-// lane, larger ones (up to hub_deg; hubs are split into arc chunks and done
-// block-wide) one after another by the whole tile.  `f(group, v)` does the work
-// for one vertex.
+// Items of a vertex list (or all vertices when list == nullptr) in two passes:
+// vertices of degree <= small_deg one per thread over the whole grid, then the
+// larger ones (up to hub_deg; hubs are split into arc chunks and done by warps)
+// one per tile.  `f(group, v)` does the work for one vertex.
 template <int TILE, class F>
 __device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const int *list, int nn, F &&f) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int i = gt; i < nn; i += nt) {
+    const int v = list ? __ldcg(list + i) : i;
+    if (deg_of(p, v) > p.small_deg) continue;
+    ThreadGroup th;
+    ItemTimer tm(p);
+    f(th, v);
+    tm.done(ls, v);
+  }
   TileGroup<TILE> tg;
-  for (int base = (gt / TILE) * TILE; base < nn; base += nt) {
-    const int i = base + tg.rank();
-    int v = -1, d = 0;
-    if (i < nn) {
+  for (int i = gt / TILE; i < nn; i += nt / TILE) {
+    int v = 0, d = 0;
+    if (tg.rank() == 0) {
       v = list ? __ldcg(list + i) : i;
       d = deg_of(p, v);
-      if (d > p.hub_deg) v = -1;
     }
-    const bool small = v >= 0 && d <= p.small_deg;
-    if (small) {
-      ThreadGroup th;
-      ItemTimer tm(p);
-      f(th, v);
-      tm.done(ls, v);
-    }
-    tg.g.sync();
-    unsigned big = tg.g.ballot(v >= 0 && !small);
-    while (big) {
-      const int j = __ffs(big) - 1;
-      big &= big - 1;
-      const int vj = tg.g.shfl(v, j);
-      ItemTimer tm(p);
-      f(tg, vj);
-      tm.done(ls, vj);
-    }
+    v = tg.g.shfl(v, 0);
+    d = tg.g.shfl(d, 0);
+    if (d <= p.small_deg || d > p.hub_deg) continue;  // tile-uniform
+    ItemTimer tm(p);
+    f(tg, v);
+    tm.done(ls, v);
   }
 }
 
@@ -1005,7 +1000,7 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
         break;
       }
       if (L > 0) m_u -= m_f;
-      if (!bu && m_f * 14 > m_u) bu = true;
+      if (!bu && p.bu_alpha > 0 && m_f * p.bu_alpha > m_u) bu = true;
       else if (bu && (long long)F * 24 < p.n) bu = false;
       kind = bu ? TR_BFS_BU : TR_BFS_TD;
       items = ld_vol(&in->q);
@@ -1107,7 +1102,7 @@ struct dmf_solver {
   cudaStream_t stream = nullptr;
   int n = 0, m = 0, s = 0, t = 0;
   dmf_opts opts{};
-  int tile = 32, grid = 0, block = kBlock, hub_deg = 256, small_deg = 8, minb = 1;
+  int tile = 32, grid = 0, block = kBlock, hub_deg = 256, small_deg = 8, minb = 2, bu_alpha = 2;
   int *off = nullptr, *adj = nullptr, *par = nullptr, *sidx = nullptr, *cap = nullptr, *res = nullptr;
   int *height = nullptr, *stamp = nullptr, *astamp = nullptr, *uarc = nullptr;
   long long *excess = nullptr;
@@ -1193,10 +1188,11 @@ int configure(dmf_solver *sv) {
     // tuning overrides (thread-per-vertex and chunked-hub degree bounds)
     if (const char *e = std::getenv("DMF_SMALL_DEG")) sv->small_deg = std::max(0, std::atoi(e));
     if (const char *e = std::getenv("DMF_HUB_DEG")) sv->hub_deg = std::max(32, std::atoi(e));
+    if (const char *e = std::getenv("DMF_BU_ALPHA")) sv->bu_alpha = std::max(0, std::atoi(e));
     sv->thresholds_set = true;
   }
-  sv->minb = 1;
-  if (const char *e = std::getenv("DMF_MINB")) sv->minb = std::atoi(e) == 2 ? 2 : 1;
+  sv->minb = 2;
+  if (const char *e = std::getenv("DMF_MINB")) sv->minb = std::atoi(e) == 1 ? 1 : 2;
   KernelFn fn = pick_kernel(sv->tile, sv->minb);
   int per_sm = 0, sms = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kBlock, 0), "occupancy");
@@ -1289,10 +1285,11 @@ int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, 
   const int avg = sv->n > 0 ? std::max(1, sv->m / sv->n) : 1;
   (void)avg;
   p.cycles = sv->opts.kernel_cycles > 0 ? sv->opts.kernel_cycles : 2;
-  p.interval = sv->opts.relabel_interval > 0 ? sv->opts.relabel_interval : 3;
+  p.interval = sv->opts.relabel_interval > 0 ? sv->opts.relabel_interval : 6;
   p.max_iters = sv->opts.max_iters > 0 ? sv->opts.max_iters : 100000;
   p.hub_deg = sv->hub_deg;
   p.small_deg = sv->small_deg;
+  p.bu_alpha = sv->bu_alpha;
   p.need_cut = sv->opts.variant == DMF_VARIANT_PP ? 1 : 0;
   p.round_base = sv->round_base;
   p.trace = (sv->opts.flags & DMF_FLAG_TRACE) ? sv->trace : nullptr;
