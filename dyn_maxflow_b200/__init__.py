@@ -21,6 +21,7 @@ import numpy as np
 __all__ = [
     "DmfError", "Graph", "Solver", "Stats", "load_updates", "save_updates", "gen_grid", "gen_rmat",
     "gen_batches", "recalculate_max_flow", "static_recalculate", "device_count", "VARIANTS", "lib_path",
+    "static_maxflow_noalloc",
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -98,6 +99,18 @@ _sig("dmf_trace_items", C.c_int, VP, C.c_int32, I64P, I64P, I64P, I64P)
 _sig("dmf_solver_set_opts", C.c_int, VP, C.POINTER(Opts))
 _sig("dmf_solver_destroy", C.c_int, VP)
 _sig("dmf_device_count", C.c_int)
+_sig("dmf_static_maxflow_noalloc", C.c_int, C.c_int32, C.c_int32, VP, VP, VP, VP, C.c_int32, C.c_int32, VP,
+     C.POINTER(C.c_int64), VP)
+
+
+def static_maxflow_noalloc(n, m, d_index, d_adj, d_cap, d_par, s, t, d_res, stream=None) -> int:
+    """dmf_static_maxflow_noalloc over caller-owned device buffers (raw pointers):
+    the solver allocates nothing; its scratch is a static device array (n <= 262144)."""
+    f = C.c_int64()
+    st = None if stream is None else C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+    _check(_L.dmf_static_maxflow_noalloc(n, m, C.c_void_p(d_index), C.c_void_p(d_adj), C.c_void_p(d_cap),
+                                         C.c_void_p(d_par), s, t, C.c_void_p(d_res), C.byref(f), st))
+    return f.value
 
 
 class DmfError(RuntimeError):

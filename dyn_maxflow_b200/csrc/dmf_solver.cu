@@ -20,6 +20,7 @@
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "dmf_device.cuh"
 #include "dmf_internal.h"
@@ -1402,9 +1403,149 @@ int device_updates(dmf_solver *sv, int mode, int32_t k, const int32_t *src, cons
   return run_mode(sv, mode, k, src, dst, w, flow, false);
 }
 
+// ---- allocation-free static solve ------------------------------------------------
+// Some callers cannot allocate device memory while they run: code inside a
+// pre-sized memory pool or arena, a host that forbids cudaMalloc after start-up,
+// or a deployment that must never grow its footprint mid-flight.  For them
+// dmf_static_maxflow_noalloc keeps all solver scratch (control block, labels,
+// excess, stamps, dead/side marks, vertex queues) in the file-scope array below
+// instead of memory the library allocates; the caller supplies the graph and
+// the residual output in its own device memory.  The array is sized for
+// kNoAllocMaxVertices vertices (about 10 MiB); every GPU that loads the library
+// holds it until the process exits.
+constexpr int kNoAllocMaxVertices = 1 << 18;
+constexpr size_t kNoAllocAlign = 256;
+constexpr size_t na_round(size_t b) { return (b + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign; }
+constexpr size_t kNoAllocV = (size_t)kNoAllocMaxVertices + 1;
+constexpr size_t kNoAllocBytes = na_round(sizeof(Ctrl)) + na_round(4 * kNoAllocV) /* height */ +
+                                 na_round(4 * kNoAllocV) /* stamp */ + na_round(8 * kNoAllocV) /* excess */ +
+                                 na_round(kNoAllocV) /* dead */ + na_round(kNoAllocV) /* side */ +
+                                 5 * na_round(4 * kNoAllocV) /* queues */ + 4 * kNoAllocAlign /* unused hub slots */;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch, looked up once per device (the name is
+// only a host-side stand-in for the array; a kernel must be given this address).
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[128] = {};
+
+int noalloc_scratch(int dev, unsigned char **out) {
+  if (dev < 0 || dev >= 128) return fail(DMF_ERR_CUDA, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
+    g_noalloc_addr[dev] = ptr;
+  }
+  *out = (unsigned char *)g_noalloc_addr[dev];
+  return DMF_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, const int32_t *d_adj,
+                               const int32_t *d_cap, const int32_t *d_par, int32_t s, int32_t t, int32_t *d_res,
+                               int64_t *flow, void *stream) {
+  if (n < 2 || m < 0 || !d_index || !flow || (m > 0 && (!d_adj || !d_cap || !d_par || !d_res)))
+    return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  if (n > kNoAllocMaxVertices)
+    return fail(DMF_ERR_INVALID_ARG, "n=%d exceeds the %d vertices the allocation-free scratch holds", n,
+                kNoAllocMaxVertices);
+  if (s < 0 || t < 0 || s >= n || t >= n || s == t)
+    return fail(DMF_ERR_INVALID_ARG, "need distinct s, t in [0, n): s=%d t=%d", s, t);
+  int dev = 0;
+  CK(cudaGetDevice(&dev), "cudaGetDevice");
+  unsigned char *base = nullptr;
+  int st = noalloc_scratch(dev, &base);
+  if (st) return st;
+  const int tile = n > 0 && (double)m / n <= 6 ? 4 : (double)m / n <= 12 ? 8 : (double)m / n <= 24 ? 16 : 32;
+  KernelFn fn = pick_kernel(tile, 2);
+  int per_sm = 0, sms = 0, coop = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kBlock, 0), "occupancy");
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "coop attr");
+  if (!coop || per_sm < 1) return fail(DMF_ERR_CUDA, "device does not support cooperative launch of the solver");
+  // carve the scratch
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    unsigned char *q = base + off;
+    off += na_round(bytes);
+    return q;
+  };
+  const size_t N = (size_t)n + 1;
+  Ctrl *ctrl = (Ctrl *)carve(sizeof(Ctrl));
+  Params p{};
+  p.height = (int *)carve(4 * N);
+  p.stamp = (int *)carve(4 * N);
+  p.excess = (long long *)carve(8 * N);
+  p.dead = carve(N);
+  p.side = carve(N);
+  p.fq[0] = (int *)carve(4 * N);
+  p.fq[1] = (int *)carve(4 * N);
+  p.wq[0] = (int *)carve(4 * N);
+  p.wq[1] = (int *)carve(4 * N);
+  p.aq = (int *)carve(4 * N);
+  // no hubs in this mode (hub_deg = INT_MAX): the hub structures are never read
+  int2 *hub_dummy = (int2 *)carve(kNoAllocAlign);
+  long long *ll_dummy = (long long *)carve(kNoAllocAlign);
+  int *int_dummy = (int *)carve(kNoAllocAlign);
+  unsigned long long *mark_dummy = (unsigned long long *)carve(kNoAllocAlign);
+  if (off > kNoAllocBytes) return fail(DMF_ERR_CUDA, "internal: scratch layout exceeds the array");
+  p.fh[0] = p.fh[1] = p.wh[0] = p.wh[1] = p.ah = hub_dummy;
+  p.hch = hub_dummy;
+  p.nhch = 0;
+  p.hc_tsum = p.hc_ex = p.hc_moved = p.hc_alloc = ll_dummy;
+  p.hc_tmin = p.hc_min = int_dummy;
+  p.hub_base = int_dummy;
+  p.chunk_mark = mark_dummy;
+  p.chunk_tmin = int_dummy;
+  p.n = n;
+  p.m = m;
+  p.s = s;
+  p.t = t;
+  p.off = d_index;
+  p.adj = d_adj;
+  p.par = d_par;
+  p.sidx = nullptr;
+  p.cap = const_cast<int *>(d_cap);  // read only in static mode
+  p.res = d_res;
+  p.astamp = nullptr;
+  p.uarc = nullptr;
+  p.ctrl = ctrl;
+  p.mode = MODE_STATIC;
+  p.variant = DMF_VARIANT_DATA;
+  p.cycles = 2;
+  p.interval = 6;
+  p.max_iters = 100000;
+  p.hub_deg = INT_MAX;
+  p.small_deg = 8;
+  p.bu_alpha = 2;
+  p.need_cut = 0;
+  p.round_base = 1;
+  p.relabel_base = 1;
+  p.epoch = 1;
+  p.trace = nullptr;
+  p.trace_cap = 0;
+  p.probe = 0;
+  cudaStream_t S = (cudaStream_t)stream;
+  // the array keeps the previous call's contents: the control block and the
+  // worklist stamps must start at zero (everything else is written before use)
+  CK(cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), S), "memset control");
+  CK(cudaMemsetAsync(p.stamp, 0, 4 * N, S), "memset stamps");
+  void *args[] = {&p};
+  CK(cudaLaunchCooperativeKernel((const void *)fn, dim3(per_sm * sms), dim3(kBlock), args, 0, S),
+     "cooperative launch");
+  Ctrl hc;
+  CK(cudaMemcpyAsync(&hc, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, S), "D2H control");
+  CK(cudaStreamSynchronize(S), "solve");
+  if (hc.err & ERR_TIMEOUT) return fail(DMF_ERR_TIMEOUT, "a grid-barrier wait timed out");
+  if (hc.err & ERR_NO_CONV) return fail(DMF_ERR_NO_CONVERGENCE, "no convergence");
+  if (hc.err) return fail(DMF_ERR_CUDA, "device error flags 0x%x", hc.err);
+  *flow = hc.flow;
+  return ok();
+}
 
 int dmf_device_count(void) {
   int c = 0;

@@ -218,6 +218,24 @@ int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs,
 int dmf_solver_set_opts(dmf_solver *sv, const dmf_opts *opts);
 int dmf_solver_destroy(dmf_solver *sv);
 
+/* Static solve that allocates nothing, for callers that cannot allocate device
+ * memory while they run (code inside a fixed memory pool or arena, or a host
+ * that forbids cudaMalloc after start-up).  No counterpart in the reference.
+ * The caller passes the CSR (index[n+1], adj[m], cap[m], par[m], the layout of
+ * dmf_graph_from_csr, already validated) and d_res[m] for the residuals of the
+ * maximum flow, all in its own device memory; *flow receives the value.  All
+ * other scratch lives in one static device array inside the library, sized for
+ * n <= 262144 vertices (about 10 MiB, held by every GPU that loads the library
+ * until the process exits); larger n is rejected with DMF_ERR_INVALID_ARG.
+ * The first call on a device looks up that array's device address (so make it
+ * before any stream capture).  Calls share the array: calls that overlap on the
+ * GPU race and give wrong results, so serialise them.  The call waits for the
+ * result on `stream` (a cudaStream_t, NULL = legacy default stream). */
+int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index,
+                               const int32_t *d_adj, const int32_t *d_cap,
+                               const int32_t *d_par, int32_t s, int32_t t,
+                               int32_t *d_res, int64_t *flow, void *stream);
+
 /* Number of CUDA devices visible (0 without a GPU); never fails. */
 int dmf_device_count(void);
 
