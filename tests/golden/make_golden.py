@@ -119,8 +119,6 @@ _KC = re.compile(r"=======kernel cycles (-?\d+) =======")
 def parse_bench(out: str):
     """Per kernel_cycles block: dynamic flow, static flow (equal unless PANIC), times."""
     runs = []
-    for blk in _KC.split(out)[1:]:
-        pass
     parts = _KC.split(out)
     for i in range(1, len(parts), 2):
         kc, body = int(parts[i]), parts[i + 1]
@@ -135,7 +133,7 @@ def parse_bench(out: str):
     return runs
 
 
-def cmd_reference(configs, timeout: float, variants, builds) -> None:
+def cmd_reference(configs, timeout: float, variants, builds, files_sel=None) -> None:
     import dyn_maxflow_b200 as D
     results = {}
     if os.path.exists(OUT_JSON):
@@ -155,7 +153,7 @@ def cmd_reference(configs, timeout: float, variants, builds) -> None:
             for build in builds:
                 exe = os.path.join(REF_BIN, f"dyn_{variant}_bench_large" + ("_sm100a" if build == "sm100a" else ""))
                 per_file = []
-                for i in range(1, len(files) + 1):
+                for i in (files_sel or range(1, len(files) + 1)):
                     t0 = time.time()
                     try:
                         r = subprocess.run([exe, gpath, os.path.join(tmp, name), str(s), str(t), str(i)],
@@ -169,6 +167,10 @@ def cmd_reference(configs, timeout: float, variants, builds) -> None:
                     if rc == "timeout":
                         break
                 entry["runs"][f"{variant}/{build}"] = per_file
+        old = results.get(name)
+        if old and old.get("sha256") == entry["sha256"]:
+            old["runs"].update(entry["runs"])
+            entry = old
         results[name] = entry
         with open(OUT_JSON, "w") as f:
             json.dump(results, f, indent=1, sort_keys=True)
@@ -182,8 +184,10 @@ if __name__ == "__main__":
     ap.add_argument("--variants", default="data,topo,pp")
     ap.add_argument("--builds", default="sm100a")
     ap.add_argument("--timeout", type=float, default=300)
+    ap.add_argument("--files", default="", help="comma-separated file numbers (default: all)")
     a = ap.parse_args()
     if a.what == "fixtures":
         cmd_fixtures()
     else:
-        cmd_reference(a.configs.split(","), a.timeout, a.variants.split(","), a.builds.split(","))
+        sel = [int(x) for x in a.files.split(",")] if a.files else None
+        cmd_reference(a.configs.split(","), a.timeout, a.variants.split(","), a.builds.split(","), sel)
