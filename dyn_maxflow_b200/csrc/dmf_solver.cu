@@ -31,6 +31,7 @@ namespace {
 
 constexpr int kBlock = 512;
 constexpr int kChunk = 256;  // arcs per hub chunk: one warp item, 8 arcs per lane
+constexpr int kPPIters = 4;  // push-pull phase-1 relabel rounds before the general solve
 
 enum Mode : int { MODE_STATIC = 0, MODE_DYNAMIC = 1, MODE_RECOMPUTE = 2, MODE_CUT = 3 };
 
@@ -38,7 +39,8 @@ enum Mode : int { MODE_STATIC = 0, MODE_DYNAMIC = 1, MODE_RECOMPUTE = 2, MODE_CU
 enum TraceKind : int {
   TR_START = 0, TR_INIT_RES = 1, TR_SATURATE = 2, TR_LOOKUP = 3, TR_APPLY = 4, TR_REPAIR = 5,
   TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
-  TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14
+  TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14, TR_PP_INIT = 15, TR_PP_BFS = 16, TR_PP_FINALIZE = 17,
+  TR_PP_ROUND = 18
 };
 
 // Largest capacity an update may set: keeps cap(e) + cap(partner) < 2^31 when
@@ -894,6 +896,219 @@ __device__ __forceinline__ void clear_slot(Slot *s) {
   s->cnt = 0;
 }
 
+// ---- push-pull, phase 1 (code/dyn_pp_bench.cu:6-88, part_pp) --------------------
+// The cut kept from the previous solve splits the vertices into the sink side B
+// (side = 1) and the source side A (side = 0).  Phase 1 works inside each side:
+// B pushes its excess towards t and B's deficits (heights: residual distance to
+// them within B, pp_bfs code/dyn_pp.h:99-120), A pulls its deficits from A's
+// excess (heights: residual distance from an excess vertex within A; pull_kernel
+// code/dyn_pp.h:237-280), both in the same rounds.  Arcs between the sides are
+// not touched.  Phase 2, the general solve, then finishes exactly.
+
+__device__ __forceinline__ bool pp_active(const Params &p, int v, long long ex) {
+  if (v == p.s || v == p.t) return false;
+  return p.side[v] ? ex > 0 : ex < 0;
+}
+
+// Seeds (pp_bfs_init, code/dyn_pp.h:76-83): t, B's deficits and A's excess.
+__device__ void ph_pp_init(const Params &p, Slot *out) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  Ctrl *c = p.ctrl;
+  if (gt == 0) {
+    c->act_q = 0;
+    c->act_hq = 0;
+    c->wtail[0] = c->whtail[0] = c->seen[0] = 0;
+  }
+  int pos = 0;
+  for (int v = gt; v < p.n; v += nt) {
+    const long long ex = __ldcg(p.excess + v);
+    const int sd = p.side[v];
+    const bool seed = v == p.t || (v != p.s && (sd ? ex < 0 : ex > 0));
+    if (seed) {
+      p.height[v] = 0;
+      if (deg_of(p, v) > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
+      else append(p.fq[0], &out->q, v);
+    } else {
+      p.height[v] = UNV;
+    }
+    if (pp_active(p, v, ex)) pos++;
+  }
+  agg_add_int(&c->pos_count, pos);
+}
+
+// One level over the frontier: a B vertex x labels B neighbours w with residual
+// w->x, an A vertex x labels A neighbours w with residual x->w; s and t are
+// never labelled.  All phase-1 actives go to the non-hub active list.
+__device__ __forceinline__ void pp_td_range(const Params &p, Slot *out, int nxt, int x, int first, int end,
+                                            int stride, int L, LStats &ls, VisitAcc &acc) {
+  const int sx = p.side[x];
+  for (int a = first; a < end; a += stride) {
+    const int w = __ldg(p.adj + a);
+    ls.arcs++;
+    if (w == p.s || w == p.t || p.side[w] != sx) continue;
+    if (__ldcg(p.height + w) != UNV) continue;
+    const int r = sx ? __ldcg(p.res + __ldg(p.par + a)) : __ldcg(p.res + a);
+    if (r <= 0 || atomicCAS(p.height + w, UNV, L + 1) != UNV) continue;
+    const int d = deg_of(p, w);
+    if (d > p.hub_deg) append_hub(p, p.fh[nxt], &out->hq, w);
+    else append(p.fq[nxt], &out->q, w);
+    if (pp_active(p, w, __ldcg(p.excess + w))) {
+      append(p.aq, &p.ctrl->act_q, w);
+      acc.reached++;
+    }
+  }
+}
+
+template <int TILE>
+__device__ void ph_pp_bfs(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
+  const int cur = L & 1, nxt = cur ^ 1;
+  const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
+  VisitAcc acc;
+  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nh; i += nwarps) {
+    const int2 it = __ldcg(p.fh[cur] + i);
+    int beg, end;
+    chunk_range(p, it, beg, end);
+    pp_td_range(p, out, nxt, it.x, beg + lane, end, 32, L, ls, acc);
+  }
+  for_tiered<TILE>(p, ls, p.fq[cur], nn, [&](auto &g, int x) {
+    const int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
+    pp_td_range(p, out, nxt, x, beg + g.rank(), end, g.size(), L, ls, acc);
+  });
+  flush_visits(p, out, acc);
+}
+
+// Unlabelled vertices cannot reach a target within their side: inactive for
+// phase 1 (not dead: the general solve decides that).
+__device__ void ph_pp_finalize(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt == 0) p.ctrl->pos_count = 0;  // read by every block before this phase
+  for (int v = gt; v < p.n; v += nt)
+    if (__ldcg(p.height + v) == UNV) p.height[v] = p.n;
+}
+
+__device__ __forceinline__ void pp_enqueue(const Params &p, int r, unsigned round_id, int v) {
+  if (atomicExch(p.stamp + v, (int)round_id) == (int)round_id) return;
+  append(p.wq[r & 1], &p.ctrl->wtail[r % 3], v);
+}
+
+// Push (B vertex, to B neighbours) or pull (A vertex, from A neighbours) of one
+// vertex by a group, two passes per cycle as in discharge: pass 1 sums the
+// admissible residual (head / tail labelled below h) and the minimum label over
+// the other residual arcs; a group prefix sum gives lane budgets; pass 2 moves
+// them.  A pull of d from w along w->v lowers res(w->v) and excess(w).
+template <class G>
+__device__ void pp_discharge(G &g, const Params &p, int v, int r, unsigned round_id, LStats &ls) {
+  long long e0 = 0;
+  int hh = 0;
+  if (g.rank() == 0) {
+    e0 = __ldcg(p.excess + v);
+    hh = __ldcg(p.height + v);
+  }
+  long long ex0;
+  int h;
+  if constexpr (G::size() == 1) {
+    ex0 = e0;
+    h = hh;
+  } else {
+    ex0 = g.g.shfl(e0, 0);
+    h = g.g.shfl(hh, 0);
+  }
+  const bool pull = p.side[v] == 0;
+  if (!pp_active(p, v, ex0) || h >= p.n) return;
+  if (g.rank() == 0) ls.visits++;
+  long long need = pull ? -ex0 : ex0;
+  const long long need0 = need;
+  const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
+  constexpr int S = G::size();
+  for (int cyc = 0; cyc < p.cycles && need > 0 && h < p.n; cyc++) {
+    long long tsum = 0;
+    int tmin = INT_MAX;
+    for (int a = beg + g.rank(); a < end; a += S) {
+      const int w = __ldg(p.adj + a);
+      ls.arcs++;
+      // B pushes to B (t included); A pulls from A (s excluded: its arcs are saturated)
+      if (w == p.s || p.side[w] != (pull ? 0 : 1)) continue;
+      const int rr = pull ? __ldcg(p.res + __ldg(p.par + a)) : __ldcg(p.res + a);
+      if (rr <= 0) continue;
+      const int hw = __ldcg(p.height + w);
+      if (hw < h) tsum += rr;
+      else tmin = min(tmin, hw);
+    }
+    long long tot;
+    const long long pre = g.scan(tsum, tot);
+    long long budget = need - pre;
+    budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
+    long long done = 0;
+    for (int a = beg + g.rank(); a < end && budget > 0; a += S) {
+      const int w = __ldg(p.adj + a);
+      if (w == p.s || p.side[w] != (pull ? 0 : 1)) continue;
+      const int pa = __ldg(p.par + a);
+      const int rr = pull ? __ldcg(p.res + pa) : __ldcg(p.res + a);
+      if (rr <= 0 || __ldcg(p.height + w) >= h) continue;
+      const int d = (int)(rr < budget ? rr : budget);
+      if (pull) {
+        atomicSub(p.res + pa, d);
+        atomicAdd(p.res + a, d);
+        const long long old = atomic_add_ll(p.excess + w, -(long long)d);
+        if (old - d < 0 && old >= 0) pp_enqueue(p, r, round_id, w);  // w now has a deficit
+      } else {
+        atomicSub(p.res + a, d);
+        atomicAdd(p.res + pa, d);
+        const long long old = atomic_add_ll(p.excess + w, (long long)d);
+        if (old + d > 0 && old <= 0) pp_enqueue(p, r, round_id, w);  // w now has excess
+      }
+      ls.pushes++;
+      budget -= d;
+      done += d;
+    }
+    const long long moved = g.sum_all(done);
+    need -= moved;
+    if (need > 0 && moved == tot) {
+      const int mh = g.min_all(tmin);
+      h = mh >= p.n ? p.n : mh + 1;
+      if (g.rank() == 0) {
+        p.height[v] = h;
+        ls.relabels++;
+      }
+    }
+  }
+  if (g.rank() == 0) {
+    const long long moved_total = need0 - need;
+    if (moved_total) atomic_add_ll(p.excess + v, pull ? moved_total : -moved_total);
+    if (need > 0 && h < p.n) pp_enqueue(p, r, round_id, v);
+  }
+}
+
+template <int TILE>
+__device__ void ph_pp_round(const Params &p, int r, unsigned round_id, LStats &ls) {
+  Ctrl *c = p.ctrl;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt == 0) c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
+  const int *list = r == 0 ? p.aq : p.wq[(r - 1) & 1];
+  const int nn = r == 0 ? ld_vol(&c->act_q) : ld_vol(&c->wtail[(r - 1) % 3]);
+  // every degree goes through a lane or a tile here (no hub chunks in phase 1)
+  const int nt = gridDim.x * blockDim.x;
+  for (int i = gt; i < nn; i += nt) {
+    const int v = __ldcg(list + i);
+    if (deg_of(p, v) > p.small_deg) continue;
+    ThreadGroup th;
+    pp_discharge(th, p, v, r, round_id, ls);
+  }
+  TileGroup<TILE> tg;
+  for (int i = gt / TILE; i < nn; i += nt / TILE) {
+    int v = 0, d = 0;
+    if (tg.rank() == 0) {
+      v = __ldcg(list + i);
+      d = deg_of(p, v);
+    }
+    v = tg.g.shfl(v, 0);
+    d = tg.g.shfl(d, 0);
+    if (d <= p.small_deg) continue;
+    pp_discharge(tg, p, v, r, round_id, ls);
+  }
+}
+
 template <int TILE, int BLOCK>
 __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Temp &btmp, int *bci,
                     long long *bcl) {
@@ -970,8 +1185,48 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
     if (!next()) return;
   }
 
-  // ---- global relabel / push rounds ---------------------------------------------
   unsigned round_id = p.round_base;
+
+  // ---- push-pull phase 1 (dynamic batches of the push-pull variant) ----------------
+  if (p.variant == DMF_VARIANT_PP && p.mode == MODE_DYNAMIC) {
+    for (int it1 = 0; it1 < kPPIters; it1++) {
+      kind = TR_PP_INIT;
+      items = hubitems = 0;
+      ph_pp_init(p, slot_out());
+      if (!next()) return;
+      const int P = ld_vol(&c->pos_count);
+      int reached = 0;
+      for (int L = 0;; L++) {
+        const Slot *in = slot_in();
+        const int F = ld_vol(&in->q) + ld_vol(&in->hq);
+        reached += ld_vol(&in->cnt);
+        if (F == 0 || P == 0 || reached == P) break;
+        kind = TR_PP_BFS;
+        items = ld_vol(&in->q);
+        hubitems = ld_vol(&in->hq);
+        ph_pp_bfs<TILE>(p, in, slot_out(), L, ls);
+        if (!next()) return;
+      }
+      kind = TR_PP_FINALIZE;
+      items = hubitems = 0;
+      ph_pp_finalize(p);
+      if (!next()) return;
+      const int A = ld_vol(&c->act_q);
+      if (A == 0) break;
+      for (int r = 0; r < p.interval; r++) {
+        round_id++;
+        kind = TR_PP_ROUND;
+        items = r == 0 ? A : ld_vol(&c->wtail[(r - 1) % 3]);
+        hubitems = 0;
+        ph_pp_round<TILE>(p, r, round_id, ls);
+        if (!next()) return;
+        if (lead) c->rounds_used = round_id - p.round_base;
+        if (ld_vol(&c->wtail[r % 3]) == 0) break;
+      }
+    }
+  }
+
+  // ---- global relabel / push rounds ---------------------------------------------
   const bool cut_only = p.mode == MODE_CUT;
   const bool topo = p.variant == DMF_VARIANT_TOPO;
   for (int it = 0;; it++) {
