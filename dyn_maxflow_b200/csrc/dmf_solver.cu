@@ -31,7 +31,7 @@ namespace {
 
 constexpr int kBlock = 512;
 constexpr int kChunk = 256;  // arcs per hub chunk: one warp item, 8 arcs per lane
-constexpr int kPPIters = 4;  // push-pull phase-1 relabel rounds before the general solve
+constexpr int kPPIters = 1;  // push-pull phase-1 relabel rounds before the general solve
 
 enum Mode : int { MODE_STATIC = 0, MODE_DYNAMIC = 1, MODE_RECOMPUTE = 2, MODE_CUT = 3 };
 
@@ -1087,7 +1087,7 @@ __device__ void ph_pp_round(const Params &p, int r, unsigned round_id, LStats &l
   if (gt == 0) c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
   const int *list = r == 0 ? p.aq : p.wq[(r - 1) & 1];
   const int nn = r == 0 ? ld_vol(&c->act_q) : ld_vol(&c->wtail[(r - 1) % 3]);
-  // every degree goes through a lane or a tile here (no hub chunks in phase 1)
+  // small vertices by a lane, medium ones by a tile; hubs wait for phase 2
   const int nt = gridDim.x * blockDim.x;
   for (int i = gt; i < nn; i += nt) {
     const int v = __ldcg(list + i);
@@ -1104,7 +1104,7 @@ __device__ void ph_pp_round(const Params &p, int r, unsigned round_id, LStats &l
     }
     v = tg.g.shfl(v, 0);
     d = tg.g.shfl(d, 0);
-    if (d <= p.small_deg) continue;
+    if (d <= p.small_deg || d > p.hub_deg) continue;  // hubs are left to the general solve
     pp_discharge(tg, p, v, r, round_id, ls);
   }
 }
