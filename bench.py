@@ -273,10 +273,11 @@ def run_ours(args, rank: int, world: int):
                                 for k, v in sorted(phase_us.items(), key=lambda kv: -kv[1][0])},
     }
     if world > 1:
-        tt = torch.tensor([p50, avg_ms, pct(e2e, 0.5)], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        res["value"], res["ms_per_step"], res["e2e"]["value"] = [round(x, 4) for x in tt.tolist()]
-        res["throughput_batches_per_s"] = round(world * 1e3 / res["ms_per_step"], 2)
+        from dyn_maxflow_b200.replicas import replica_summary
+        rs = replica_summary(p50, avg_ms, pct(e2e, 0.5), world)
+        res["value"], res["ms_per_step"] = round(rs["p50_ms"], 4), round(rs["ms_per_step"], 4)
+        res["e2e"]["value"] = round(rs["e2e_p50_ms"], 4)
+        res["throughput_batches_per_s"] = round(rs["throughput_batches_per_s"], 2)
     if rank == 0 and not args.no_cpu_baseline:
         nth = os.cpu_count() or 1
         k = max(1, min(args.cpu_batches, len(batches)))

@@ -6,6 +6,8 @@
 * ``bin/dyn_data_bench``, ``bin/dyn_topo_bench``, ``bin/dyn_pp_bench`` and the
   ``*_large`` forms -- the drop-in command-line entry points (csrc/dmf_cli.cpp),
   linked against libdmf.so.
+* ``bin/dmf_tool`` -- input tooling (csrc/dmf_tool.cpp): weighting, text -> .bin
+  graph and update conversion, seeded generators.
 """
 from __future__ import annotations
 
@@ -80,9 +82,20 @@ def build_cli(force: bool = False, verbose: bool = False) -> list[str]:
     return outs
 
 
+def build_tool(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(BIN, exist_ok=True)
+    src = os.path.join(CSRC, "dmf_tool.cpp")
+    out = os.path.join(BIN, "dmf_tool")
+    if force or _stale(out, [src, LIB, os.path.join(INCLUDE, "dmf.h")]):
+        _run(["g++", "-std=c++17", "-O2", "-I", INCLUDE, src, "-o", out, "-L", PKG, "-ldmf",
+              "-Wl,-rpath,$ORIGIN/.."], verbose)
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> None:
     build_lib(force, verbose)
     build_cli(force, verbose)
+    build_tool(force, verbose)
 
 
 if __name__ == "__main__":
