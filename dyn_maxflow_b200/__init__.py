@@ -21,7 +21,7 @@ import numpy as np
 __all__ = [
     "DmfError", "Graph", "Solver", "Stats", "load_updates", "save_updates", "gen_grid", "gen_rmat",
     "gen_batches", "recalculate_max_flow", "static_recalculate", "device_count", "VARIANTS", "lib_path",
-    "static_maxflow_noalloc",
+    "static_maxflow_noalloc", "MultiSolver",
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -41,7 +41,7 @@ PP = C.POINTER(C.c_void_p)
 
 class Opts(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("variant", "kernel_cycles", "relabel_interval", "tile", "max_iters",
-                                          "device", "block_threads", "flags")]
+                                          "device", "block_threads", "flags", "small_deg", "grid_blocks")]
 
 
 class Stats(C.Structure):
@@ -99,6 +99,12 @@ _sig("dmf_trace_items", C.c_int, VP, C.c_int32, I64P, I64P, I64P, I64P)
 _sig("dmf_solver_set_opts", C.c_int, VP, C.POINTER(Opts))
 _sig("dmf_solver_destroy", C.c_int, VP)
 _sig("dmf_device_count", C.c_int)
+_sig("dmf_multi_create", C.c_int, C.c_int32, C.POINTER(C.c_void_p), I32P, I32P, C.POINTER(Opts), VP, PP)
+_sig("dmf_multi_info", C.c_int, VP, C.POINTER(C.c_int32), I32P)
+_sig("dmf_multi_static_maxflow", C.c_int, VP, I64P)
+_sig("dmf_multi_apply_updates", C.c_int, VP, C.c_int32, I32P, I32P, I32P, I32P, I64P)
+_sig("dmf_multi_run_batches", C.c_int, VP, C.c_int32, I64P, VP, VP, VP, C.c_int32, I64P, C.POINTER(C.c_double))
+_sig("dmf_autotune", C.c_int, VP, C.c_int32, C.POINTER(Opts))
 _sig("dmf_static_maxflow_noalloc", C.c_int, C.c_int32, C.c_int32, VP, VP, VP, VP, C.c_int32, C.c_int32, VP,
      C.POINTER(C.c_int64), VP)
 
@@ -359,6 +365,12 @@ class Solver:
         _check(_L.dmf_stats_get(self._h, C.byref(st)))
         return st.as_dict()
 
+    def autotune(self, repeats=2) -> dict:
+        """dmf_autotune: picks tile / per-thread degree bound / relabel interval / cycles."""
+        o = Opts()
+        _check(_L.dmf_autotune(self._h, repeats, C.byref(o)))
+        return {k: getattr(o, k) for k, _ in Opts._fields_}
+
     def set_opts(self, variant=None, kernel_cycles=None, relabel_interval=None, tile=None, max_iters=None):
         o = Opts()
         _L.dmf_opts_default(C.byref(o))
@@ -388,3 +400,50 @@ def static_recalculate(g: Graph, updates, source: int, sink: int, kernel_cycles:
     """From-scratch path of the reference bench (code/dyn_data_bench.cu:325-492)."""
     with Solver(g, source, sink, variant=variant, kernel_cycles=kernel_cycles) as sv:
         return sv.recompute(*updates)
+
+
+class MultiSolver(Solver):
+    """Many independent graphs in one device state (dmf_multi_*): one persistent
+    launch per call serves every instance; flows come back per instance."""
+
+    def __init__(self, graphs, sources, sinks, variant="data", kernel_cycles=0, relabel_interval=0, tile=0,
+                 device=-1, stream=None, small_deg=0):
+        o = Opts()
+        _L.dmf_opts_default(C.byref(o))
+        o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
+        o.kernel_cycles, o.relabel_interval, o.tile, o.device, o.small_deg = (
+            kernel_cycles, relabel_interval, tile, device, small_deg)
+        self._h = C.c_void_p()
+        self.graphs = list(graphs)
+        arr = (C.c_void_p * len(self.graphs))(*[g._h.value for g in self.graphs])
+        stream_ptr = None if stream is None else C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+        _check(_L.dmf_multi_create(len(self.graphs), arr, _i32(sources), _i32(sinks), C.byref(o), stream_ptr,
+                                   C.byref(self._h)))
+        self.count = len(self.graphs)
+        self.n = sum(g.num_nodes() for g in self.graphs)
+        self.m = sum(g.num_edges() for g in self.graphs)
+        cnt = C.c_int32()
+        base = np.zeros(self.count, np.int32)
+        _check(_L.dmf_multi_info(self._h, C.byref(cnt), base))
+        self.vertex_base = base
+
+    def static_maxflow_all(self) -> np.ndarray:
+        out = np.zeros(self.count, np.int64)
+        _check(_L.dmf_multi_static_maxflow(self._h, out))
+        return out
+
+    def apply_updates_all(self, inst, src, dst, w) -> np.ndarray:
+        inst, src, dst, w = _i32(inst), _i32(src), _i32(dst), _i32(w)
+        out = np.zeros(self.count, np.int64)
+        _check(_L.dmf_multi_apply_updates(self._h, len(src), inst, src, dst, w, out))
+        return out
+
+    def run_batches(self, ofs, d_src: int, d_dst: int, d_w: int, use_graph=True):
+        """Successive device-resident batches (union vertex ids); -> (flows[steps, count], ms)."""
+        ofs = np.ascontiguousarray(ofs, dtype=np.int64)
+        steps = len(ofs) - 1
+        out = np.zeros(steps * self.count, np.int64)
+        ms = C.c_double()
+        _check(_L.dmf_multi_run_batches(self._h, steps, ofs, C.c_void_p(d_src), C.c_void_p(d_dst), C.c_void_p(d_w),
+                                        1 if use_graph else 0, out, C.byref(ms)))
+        return out.reshape(steps, self.count), ms.value

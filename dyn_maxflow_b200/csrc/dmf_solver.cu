@@ -74,6 +74,14 @@ struct Params {
   unsigned relabel_base;
   const int *usrc, *udst, *uw;
   int k;
+  // Several independent instances in one residual graph (batched mode): role
+  // bit 0 = a source, bit 1 = a sink, inst = instance of each vertex, flows per
+  // instance.  Single instance: role == nullptr, s and t above.
+  const unsigned char *role;
+  const int *inst;
+  long long *inst_flow;
+  const int *srcs;  // every source vertex (just s for one instance)
+  int nsrc;
   Ctrl *ctrl;
   int mode, variant, cycles, interval, max_iters, hub_deg, small_deg, need_cut;
   int bu_alpha;  // bottom-up when frontier arcs * bu_alpha > unexplored arcs (0: never)
@@ -107,6 +115,10 @@ struct ItemTimer {
 
 __device__ __forceinline__ int deg_of(const Params &p, int v) { return __ldg(p.off + v + 1) - __ldg(p.off + v); }
 
+__device__ __forceinline__ bool is_src(const Params &p, int v) { return p.role ? (p.role[v] & 1) : v == p.s; }
+__device__ __forceinline__ bool is_snk(const Params &p, int v) { return p.role ? (p.role[v] & 2) : v == p.t; }
+__device__ __forceinline__ bool is_term(const Params &p, int v) { return p.role ? p.role[v] != 0 : (v == p.s || v == p.t); }
+
 __device__ __forceinline__ void set_err(Ctrl *c, int bit, int info) {
   if (atomicOr(&c->err, bit) == 0) c->err_info = info;
 }
@@ -121,21 +133,24 @@ __device__ void ph_init_res(const Params &p) {
 }
 
 // staticMaxFlow_kernel_7 (code/dyn_data.h:39-56) made parallel: every residual
-// arc out of s is saturated.
+// arc out of every source is saturated (one warp per source, lanes over arcs).
 __device__ void ph_saturate(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int beg = __ldg(p.off + p.s), end = __ldg(p.off + p.s + 1);
-  long long sum = 0;
-  for (int a = beg + gt; a < end; a += nt) {
-    int r = __ldcg(p.res + a);
-    if (r > 0) {
-      p.res[a] = 0;
-      atomicAdd(p.res + __ldg(p.par + a), r);
-      atomic_add_ll(p.excess + __ldg(p.adj + a), r);
-      sum += r;
+  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < p.nsrc; i += nwarps) {
+    const int s = __ldg(p.srcs + i);
+    const int beg = __ldg(p.off + s), end = __ldg(p.off + s + 1);
+    long long sum = 0;
+    for (int a = beg + lane; a < end; a += 32) {
+      int r = __ldcg(p.res + a);
+      if (r > 0) {
+        p.res[a] = 0;
+        atomicAdd(p.res + __ldg(p.par + a), r);
+        atomic_add_ll(p.excess + __ldg(p.adj + a), r);
+        sum += r;
+      }
     }
+    agg_add_ll(p.excess + s, -sum);
   }
-  agg_add_ll(p.excess + p.s, -sum);
 }
 
 // Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201) by binary search over the
@@ -221,7 +236,7 @@ __device__ void ph_cut_saturate(const Params &p) {
     int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
     int u = __ldg(p.usrc + i), v = __ldg(p.adj + e);
-    if (u == p.s || u == p.t || v == p.s || v == p.t) continue;
+    if (is_term(p, u) || is_term(p, v)) continue;
     if (p.side[u] == 0 && p.side[v] == 1) {
       int r = __ldcg(p.res + e);
       if (r > 0) {
@@ -308,7 +323,7 @@ __device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
     }
     long long ex = __ldcg(p.excess + v);
     int d = deg_of(p, v);
-    if (v == p.t || (v != p.s && ex < 0)) {
+    if (is_snk(p, v) || (!is_src(p, v) && ex < 0)) {
       p.height[v] = 0;
       if (d > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
       else append(p.fq[0], &out->q, v);
@@ -319,7 +334,7 @@ __device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
       // direction heuristic weighs the frontier against all of them
       unexpl += d;
     }
-    if (v != p.s && v != p.t && ex > 0) pos++;
+    if (!is_term(p, v) && ex > 0) pos++;
   }
   agg_add_int(&c->pos_count, pos);
   agg_add_ll(&c->unexplored, unexpl);
@@ -337,7 +352,7 @@ __device__ __forceinline__ void bfs_visit(const Params &p, Slot *out, int nxt, i
   if (hub) append_hub(p, p.fh[nxt], &out->hq, w);
   else append(p.fq[nxt], &out->q, w);
   acc.arcs += d;
-  if (w != p.s && w != p.t && __ldcg(p.excess + w) > 0) {
+  if (!is_term(p, w) && __ldcg(p.excess + w) > 0) {
     if (hub) append_hub(p, p.ah, &p.ctrl->act_hq, w);
     else append(p.aq, &p.ctrl->act_q, w);
     acc.reached++;
@@ -360,7 +375,7 @@ __device__ __forceinline__ void visit_claimed(const Params &p, Slot *out, int nx
   if (hub) append_hub(p, p.fh[nxt], &out->hq, w);
   else append(p.fq[nxt], &out->q, w);
   acc.arcs += d;
-  if (w != p.s && w != p.t && ex > 0) {
+  if (!is_term(p, w) && ex > 0) {
     if (hub) append_hub(p, p.ah, &p.ctrl->act_hq, w);
     else append(p.aq, &p.ctrl->act_q, w);
     acc.reached++;
@@ -526,7 +541,7 @@ __device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, i
   atomicAdd(p.res + __ldg(p.par + a), d);
   long long old = atomic_add_ll(p.excess + w, d);
   ls.pushes++;
-  if (enq && w != p.s && w != p.t && old + d > 0) enqueue(p, r, round_id, w);
+  if (enq && !is_term(p, w) && old + d > 0) enqueue(p, r, round_id, w);
 }
 
 // Discharge of a non-hub v by a lane or a tile: up to `cycles` rounds of
@@ -562,7 +577,7 @@ __device__ void discharge(G &g, const Params &p, int v, int r, unsigned round_id
     ex0 = g.g.shfl(e, 0);
     h = g.g.shfl(hh, 0);
   }
-  if (!(ex0 > 0 && h < p.n) || v == p.s || v == p.t) return;
+  if (!(ex0 > 0 && h < p.n) || is_term(p, v)) return;
   if (g.rank() == 0) {
     ls.visits++;
     if (seen) (*seen)++;
@@ -721,7 +736,7 @@ __device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned rou
       int tm = INT_MAX;
       if (mk == key) {  // exhausted at this height: only its minimum head height matters
         if (wg.rank() == 0) tm = __ldcg(p.chunk_tmin + cidx);
-      } else if (h < p.n && v != p.s && v != p.t) {
+      } else if (h < p.n && !is_term(p, v)) {
         int beg, end;
         chunk_range(p, it, beg, end);
         int rr[kBatch], w[kBatch];
@@ -783,7 +798,7 @@ __device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned rou
     if (wg.rank() == 0) {
       hh = __ldcg(p.height + v);
       e0 = __ldcg(p.hc_ex + base);
-      if (e0 > 0 && hh < p.n && v != p.s && v != p.t) {
+      if (e0 > 0 && hh < p.n && !is_term(p, v)) {
         mine = __ldcg(p.hc_tsum + i);
         old = atomic_add_ll(p.hc_alloc + base, mine);
         const int tm = __ldcg(p.hc_tmin + i);
@@ -792,7 +807,7 @@ __device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned rou
     }
     const int h = wg.g.shfl(hh, 0);
     const long long ex0 = wg.g.shfl(e0, 0);
-    if (!(ex0 > 0 && h < p.n) || v == p.s || v == p.t) continue;
+    if (!(ex0 > 0 && h < p.n) || is_term(p, v)) continue;
     old = wg.g.shfl(old, 0);
     mine = wg.g.shfl(mine, 0);
     long long cb = ex0 - old;
@@ -855,7 +870,7 @@ __device__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned rou
     const int v = it.x;
     const long long ex0 = __ldcg(p.hc_ex + i);
     int h = __ldcg(p.height + v);
-    if (!(ex0 > 0 && h < p.n) || v == p.s || v == p.t) continue;
+    if (!(ex0 > 0 && h < p.n) || is_term(p, v)) continue;
     seen++;
     ls.visits++;
     const long long tot = __ldcg(p.hc_alloc + i);
@@ -874,16 +889,24 @@ __device__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned rou
 }
 
 // recalculate_max_flow_kernel_39 (code/dyn_data.h:208-215) as a reduction:
-// flow = excess(t) + sum of negative excess over v != s, t.
+// flow = excess(t) + sum of negative excess over v != s, t (per instance in
+// batched mode).
 template <int BLOCK>
 __device__ void ph_flow(const Params &p, typename BlockGroup<BLOCK>::Temp &btmp) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   long long acc = 0;
   for (int v = gt; v < p.n; v += nt) {
-    long long ex = __ldcg(p.excess + v);
-    if (v == p.t) acc += ex;
-    else if (v != p.s && ex < 0) acc += ex;
+    const long long ex = __ldcg(p.excess + v);
+    long long c = 0;
+    if (is_snk(p, v)) c = ex;
+    else if (!is_src(p, v) && ex < 0) c = ex;
+    if (p.inst) {
+      if (c) atomic_add_ll(p.inst_flow + __ldg(p.inst + v), c);
+    } else {
+      acc += c;
+    }
   }
+  if (p.inst) return;
   __syncthreads();
   long long tot = typename BlockGroup<BLOCK>::RedL(btmp.redl).Sum(acc);
   if (threadIdx.x == 0 && tot) atomic_add_ll(&p.ctrl->flow, tot);
@@ -906,7 +929,7 @@ __device__ __forceinline__ void clear_slot(Slot *s) {
 // not touched.  Phase 2, the general solve, then finishes exactly.
 
 __device__ __forceinline__ bool pp_active(const Params &p, int v, long long ex) {
-  if (v == p.s || v == p.t) return false;
+  if (is_term(p, v)) return false;
   return p.side[v] ? ex > 0 : ex < 0;
 }
 
@@ -923,7 +946,7 @@ __device__ void ph_pp_init(const Params &p, Slot *out) {
   for (int v = gt; v < p.n; v += nt) {
     const long long ex = __ldcg(p.excess + v);
     const int sd = p.side[v];
-    const bool seed = v == p.t || (v != p.s && (sd ? ex < 0 : ex > 0));
+    const bool seed = is_snk(p, v) || (!is_src(p, v) && (sd ? ex < 0 : ex > 0));
     if (seed) {
       p.height[v] = 0;
       if (deg_of(p, v) > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
@@ -945,7 +968,7 @@ __device__ __forceinline__ void pp_td_range(const Params &p, Slot *out, int nxt,
   for (int a = first; a < end; a += stride) {
     const int w = __ldg(p.adj + a);
     ls.arcs++;
-    if (w == p.s || w == p.t || p.side[w] != sx) continue;
+    if (is_term(p, w) || p.side[w] != sx) continue;
     if (__ldcg(p.height + w) != UNV) continue;
     const int r = sx ? __ldcg(p.res + __ldg(p.par + a)) : __ldcg(p.res + a);
     if (r <= 0 || atomicCAS(p.height + w, UNV, L + 1) != UNV) continue;
@@ -1028,7 +1051,7 @@ __device__ void pp_discharge(G &g, const Params &p, int v, int r, unsigned round
       const int w = __ldg(p.adj + a);
       ls.arcs++;
       // B pushes to B (t included); A pulls from A (s excluded: its arcs are saturated)
-      if (w == p.s || p.side[w] != (pull ? 0 : 1)) continue;
+      if (is_src(p, w) || p.side[w] != (pull ? 0 : 1)) continue;
       const int rr = pull ? __ldcg(p.res + __ldg(p.par + a)) : __ldcg(p.res + a);
       if (rr <= 0) continue;
       const int hw = __ldcg(p.height + w);
@@ -1042,7 +1065,7 @@ __device__ void pp_discharge(G &g, const Params &p, int v, int r, unsigned round
     long long done = 0;
     for (int a = beg + g.rank(); a < end && budget > 0; a += S) {
       const int w = __ldg(p.adj + a);
-      if (w == p.s || p.side[w] != (pull ? 0 : 1)) continue;
+      if (is_src(p, w) || p.side[w] != (pull ? 0 : 1)) continue;
       const int pa = __ldg(p.par + a);
       const int rr = pull ? __ldcg(p.res + pa) : __ldcg(p.res + a);
       if (rr <= 0 || __ldcg(p.height + w) >= h) continue;
@@ -1374,6 +1397,17 @@ struct dmf_solver {
   int *chunk_tmin = nullptr;
   unsigned relabel_base = 1;
   bool thresholds_set = false;
+  // batched instances (dmf_multi_*): roles, instance ids, sources, per-instance flows
+  int ninst = 1;
+  unsigned char *role = nullptr;
+  int *inst = nullptr;
+  int *srcs = nullptr;
+  int nsrc = 1;
+  long long *inst_flow = nullptr;
+  long long *h_inst_flow = nullptr;  // pinned
+  std::vector<int> vbase;            // first vertex of each instance in the union
+  std::vector<int64_t> flows;        // last per-instance flows
+  cudaStream_t own_stream = nullptr; // for graph capture when the user stream is the legacy one
   int *ubuf = nullptr;  // device update staging: src | dst | w
   int kcap = 0;
   int *h_ubuf = nullptr;  // pinned host staging
@@ -1419,6 +1453,10 @@ void free_all(dmf_solver *sv) {
   sv->allocs.clear();
   if (sv->h_ubuf) cudaFreeHost(sv->h_ubuf);
   if (sv->h_ctrl) cudaFreeHost(sv->h_ctrl);
+  if (sv->h_inst_flow) cudaFreeHost(sv->h_inst_flow);
+  sv->h_inst_flow = nullptr;
+  if (sv->own_stream) cudaStreamDestroy(sv->own_stream);
+  sv->own_stream = nullptr;
   if (sv->ev0) cudaEventDestroy(sv->ev0);
   if (sv->ev1) cudaEventDestroy(sv->ev1);
   sv->h_ubuf = nullptr;
@@ -1457,6 +1495,9 @@ int configure(dmf_solver *sv) {
   CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, sv->dev), "coop attr");
   if (!coop || per_sm < 1) return fail(DMF_ERR_CUDA, "device does not support cooperative launch of the solver");
   sv->grid = per_sm * sms;
+  if (sv->opts.grid_blocks > 0) sv->grid = std::min(sv->grid, sv->opts.grid_blocks);
+  if (sv->opts.small_deg > 0) sv->small_deg = sv->opts.small_deg;
+  else if (sv->opts.small_deg < 0) sv->small_deg = 0;  // no thread tier
   sv->block = kBlock;
   return DMF_OK;
 }
@@ -1490,7 +1531,7 @@ int ensure_host_ubuf(dmf_solver *sv, int k) {
   return DMF_OK;
 }
 
-int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, const int *d_w) {
+Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, const int *d_w) {
   Params p{};
   p.n = sv->n;
   p.m = sv->m;
@@ -1528,6 +1569,11 @@ int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, 
   p.hc_alloc = sv->hc_alloc;
   p.hc_min = sv->hc_min;
   p.hub_base = sv->hub_base;
+  p.role = sv->role;
+  p.inst = sv->inst;
+  p.inst_flow = sv->inst_flow;
+  p.srcs = sv->srcs;
+  p.nsrc = sv->nsrc;
   p.chunk_mark = sv->chunk_mark;
   p.chunk_tmin = sv->chunk_tmin;
   p.relabel_base = sv->relabel_base;
@@ -1553,12 +1599,21 @@ int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, 
   p.trace_cap = sv->trace_cap;
   p.epoch = ++sv->epoch;
   if (sv->epoch == INT_MAX) sv->epoch = 0;
+  return p;
+}
+
+int launch(dmf_solver *sv, int mode, int k, const int *d_src, const int *d_dst, const int *d_w) {
+  Params p = make_params(sv, mode, k, d_src, d_dst, d_w);
   CK(cudaMemsetAsync(sv->ctrl, 0, sizeof(Ctrl), sv->stream), "memset ctrl");
+  if (sv->inst_flow) CK(cudaMemsetAsync(sv->inst_flow, 0, 8 * (size_t)sv->ninst, sv->stream), "memset flows");
   void *args[] = {&p};
   CK(cudaLaunchCooperativeKernel((const void *)pick_kernel(sv->tile, sv->minb), dim3(sv->grid), dim3(sv->block), args, 0,
                                  sv->stream),
      "cooperative launch");
   CK(cudaMemcpyAsync(sv->h_ctrl, sv->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, sv->stream), "D2H ctrl");
+  if (sv->inst_flow)
+    CK(cudaMemcpyAsync(sv->h_inst_flow, sv->inst_flow, 8 * (size_t)sv->ninst, cudaMemcpyDeviceToHost, sv->stream),
+       "D2H flows");
   return DMF_OK;
 }
 
@@ -1608,8 +1663,16 @@ int finish(dmf_solver *sv, int64_t *flow, bool need_cut_valid) {
   }
   sv->solved = true;
   sv->side_valid = need_cut_valid;
-  sv->st.flow = c.flow;
-  if (flow) *flow = c.flow;
+  if (sv->inst_flow) {
+    sv->flows.assign(sv->h_inst_flow, sv->h_inst_flow + sv->ninst);
+    int64_t tot = 0;
+    for (int64_t f : sv->flows) tot += f;
+    sv->st.flow = tot;
+  } else {
+    sv->st.flow = c.flow;
+    sv->flows.assign(1, c.flow);
+  }
+  if (flow) *flow = sv->st.flow;
   return ok();
 }
 
@@ -1635,9 +1698,11 @@ int host_updates(dmf_solver *sv, int mode, int32_t k, const int32_t *src, const 
   CK(cudaSetDevice(sv->dev), "cudaSetDevice");
   if ((st = ensure_ubuf(sv, k)) || (st = ensure_host_ubuf(sv, k))) return st;
   const size_t K = (size_t)sv->kcap, HK = (size_t)sv->h_kcap;
-  std::memcpy(sv->h_ubuf, src, 4 * (size_t)k);
-  std::memcpy(sv->h_ubuf + HK, dst, 4 * (size_t)k);
-  std::memcpy(sv->h_ubuf + 2 * HK, w, 4 * (size_t)k);
+  if (k > 0) {
+    std::memcpy(sv->h_ubuf, src, 4 * (size_t)k);
+    std::memcpy(sv->h_ubuf + HK, dst, 4 * (size_t)k);
+    std::memcpy(sv->h_ubuf + 2 * HK, w, 4 * (size_t)k);
+  }
   CK(cudaEventRecord(sv->ev0, sv->stream), "event record");
   if (k > 0) {
     CK(cudaMemcpyAsync(sv->ubuf, sv->h_ubuf, 4 * (size_t)k, cudaMemcpyHostToDevice, sv->stream), "H2D src");
@@ -1811,8 +1876,19 @@ int dmf_device_count(void) {
   return c;
 }
 
-int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, void *stream,
-                      dmf_solver **out) {
+}  // extern "C"
+
+namespace {
+
+struct MultiSpec {
+  int count = 0;
+  std::vector<int> vbase, srcs;
+  std::vector<unsigned char> role;
+  std::vector<int> inst;
+};
+
+int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, void *stream, const MultiSpec *ms,
+                dmf_solver **out) {
   if (!g || !out) return fail(DMF_ERR_INVALID_ARG, "null argument");
   if (g->n < 2 || s < 0 || t < 0 || s >= g->n || t >= g->n || s == t)
     return fail(DMF_ERR_INVALID_ARG, "need n >= 2 and distinct s, t in [0, n): n=%d s=%d t=%d", g->n, s, t);
@@ -1891,9 +1967,303 @@ int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *
   if (e == cudaSuccess) e = cudaStreamSynchronize(S);
   if (e != cudaSuccess) return bail(cuda_fail(e, "solver upload"));
   if ((st = ensure_ubuf(sv, 1024))) return bail(st);
+  // sources (and, for batched instances, roles, instance ids, per-instance flows)
+  {
+    const std::vector<int> one(1, s);
+    const std::vector<int> &sl = ms ? ms->srcs : one;
+    sv->nsrc = (int)sl.size();
+    sv->ninst = ms ? ms->count : 1;
+    if ((st = dalloc(sv, &sv->srcs, sl.size()))) return bail(st);
+    if (cudaMemcpy(sv->srcs, sl.data(), 4 * sl.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(cuda_fail(cudaGetLastError(), "H2D sources"));
+    if (ms) {
+      sv->vbase = ms->vbase;
+      if ((st = dalloc(sv, &sv->role, N)) || (st = dalloc(sv, &sv->inst, N)) ||
+          (st = dalloc(sv, &sv->inst_flow, (size_t)ms->count)))
+        return bail(st);
+      if (cudaMemcpy(sv->role, ms->role.data(), ms->role.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMemcpy(sv->inst, ms->inst.data(), 4 * ms->inst.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMallocHost(&sv->h_inst_flow, 8 * (size_t)ms->count) != cudaSuccess)
+        return bail(cuda_fail(cudaGetLastError(), "batched-instance upload"));
+    }
+  }
   sv->trace_cap = 8192;
   if ((st = dalloc(sv, &sv->trace, 4 * (size_t)sv->trace_cap))) return bail(st);
   *out = sv;
+  return ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, void *stream,
+                      dmf_solver **out) {
+  return create_impl(g, s, t, opts, stream, nullptr, out);
+}
+
+int dmf_multi_create(int32_t count, const dmf_graph *const *graphs, const int32_t *s, const int32_t *t,
+                     const dmf_opts *opts, void *stream, dmf_solver **out) {
+  if (count < 1 || !graphs || !s || !t || !out) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  int64_t N = 0, M = 0;
+  for (int i = 0; i < count; i++) {
+    const dmf_graph *g = graphs[i];
+    if (!g || g->n < 2 || s[i] < 0 || t[i] < 0 || s[i] >= g->n || t[i] >= g->n || s[i] == t[i])
+      return fail(DMF_ERR_INVALID_ARG, "instance %d: need a graph with n >= 2 and distinct s, t in [0, n)", i);
+    if ((int64_t)g->sidx.size() != g->m) return fail(DMF_ERR_INVALID_ARG, "instance %d has no arc index", i);
+    N += g->n;
+    M += g->m;
+  }
+  if (N >= INT32_MAX || M >= INT32_MAX) return fail(DMF_ERR_INVALID_ARG, "union too large for int32 ids");
+  dmf_graph U;
+  U.n = (int32_t)N;
+  U.m = (int32_t)M;
+  U.off.resize((size_t)N + 1);
+  U.adj.resize((size_t)M);
+  U.w.resize((size_t)M);
+  U.par.resize((size_t)M);
+  U.sidx.resize((size_t)M);
+  MultiSpec ms;
+  ms.count = count;
+  ms.vbase.resize((size_t)count + 1);
+  ms.srcs.resize(count);
+  ms.role.assign((size_t)N + 1, 0);
+  ms.inst.resize((size_t)N + 1);
+  std::vector<int64_t> abase((size_t)count + 1, 0);
+  int64_t vb = 0;
+  for (int i = 0; i < count; i++) {
+    ms.vbase[i] = (int)vb;
+    abase[i + 1] = abase[i] + graphs[i]->m;
+    vb += graphs[i]->n;
+  }
+  ms.vbase[count] = (int)vb;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < count; i++) {
+    const dmf_graph &g = *graphs[i];
+    const int vb_i = ms.vbase[i];
+    const int ab = (int)abase[i];
+    for (int v = 0; v < g.n; v++) {
+      U.off[vb_i + v] = ab + g.off[v];
+      ms.inst[vb_i + v] = i;
+    }
+    for (int e = 0; e < g.m; e++) {
+      U.adj[ab + e] = vb_i + g.adj[e];
+      U.w[ab + e] = g.w[e];
+      U.par[ab + e] = ab + g.par[e];
+      U.sidx[ab + e] = ab + g.sidx[e];
+    }
+  }
+  U.off[N] = (int32_t)M;
+  for (int i = 0; i < count; i++) {
+    ms.srcs[i] = ms.vbase[i] + s[i];
+    ms.role[ms.vbase[i] + s[i]] |= 1;
+    ms.role[ms.vbase[i] + t[i]] |= 2;
+  }
+  return create_impl(&U, ms.srcs[0], ms.vbase[0] + t[0], opts, stream, &ms, out);
+}
+
+int dmf_multi_info(const dmf_solver *sv, int32_t *count, int32_t *vertex_base) {
+  if (!sv || !count) return fail(DMF_ERR_INVALID_ARG, "null argument");
+  *count = sv->ninst;
+  if (vertex_base) {
+    if (sv->vbase.empty()) vertex_base[0] = 0;
+    else for (int i = 0; i < sv->ninst; i++) vertex_base[i] = sv->vbase[i];
+  }
+  return ok();
+}
+
+int dmf_multi_static_maxflow(dmf_solver *sv, int64_t *flows) {
+  if (!sv || !flows) return fail(DMF_ERR_INVALID_ARG, "null argument");
+  int st = dmf_static_maxflow(sv, nullptr);
+  if (st) return st;
+  for (int i = 0; i < sv->ninst; i++) flows[i] = sv->flows[i];
+  return ok();
+}
+
+int dmf_multi_apply_updates(dmf_solver *sv, int32_t k, const int32_t *inst, const int32_t *src, const int32_t *dst,
+                            const int32_t *w, int64_t *flows) {
+  if (!sv || !flows || k < 0 || (k > 0 && (!inst || !src || !dst || !w)))
+    return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  std::vector<int32_t> gs(k), gd(k);
+  for (int32_t i = 0; i < k; i++) {
+    const int in = inst[i];
+    if (in < 0 || in >= sv->ninst) return fail(DMF_ERR_INVALID_ARG, "update %d: instance %d out of range", i, in);
+    const int b = sv->vbase.empty() ? 0 : sv->vbase[in];
+    const int nloc = sv->vbase.empty() ? sv->n : sv->vbase[in + 1] - b;
+    if (src[i] < 0 || dst[i] < 0 || src[i] >= nloc || dst[i] >= nloc)
+      return fail(DMF_ERR_INVALID_ARG, "update %d: vertex out of range for instance %d", i, in);
+    gs[i] = b + src[i];
+    gd[i] = b + dst[i];
+  }
+  int st = host_updates(sv, MODE_DYNAMIC, k, gs.data(), gd.data(), w, nullptr);
+  if (st) return st;
+  for (int i = 0; i < sv->ninst; i++) flows[i] = sv->flows[i];
+  return ok();
+}
+
+int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs, const int32_t *d_src,
+                          const int32_t *d_dst, const int32_t *d_w, int32_t use_graph, int64_t *flows, double *ms) {
+  if (!sv || steps < 1 || !ofs || !flows || !d_src || !d_dst || !d_w) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  if (!sv->solved) return fail(DMF_ERR_NOT_SOLVED, "run_batches before a solve");
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  int64_t kmax = 0;
+  for (int b = 0; b < steps; b++) {
+    if (ofs[b + 1] < ofs[b]) return fail(DMF_ERR_INVALID_ARG, "offsets decrease at step %d", b);
+    kmax = std::max(kmax, ofs[b + 1] - ofs[b]);
+  }
+  if (kmax > INT32_MAX) return fail(DMF_ERR_INVALID_ARG, "batch too large");
+  int st = ensure_ubuf(sv, (int)kmax);
+  if (st) return st;
+  cudaStream_t S = sv->stream;
+  if (use_graph && !S) {  // the legacy default stream cannot be captured
+    if (!sv->own_stream) CK(cudaStreamCreateWithFlags(&sv->own_stream, cudaStreamNonBlocking), "stream create");
+    CK(cudaStreamSynchronize(nullptr), "sync");
+    S = sv->own_stream;
+  }
+  const int cnt = sv->ninst;
+  Ctrl *h_ctrl = nullptr;
+  long long *h_fl = nullptr;
+  CK(cudaMallocHost(&h_ctrl, sizeof(Ctrl) * (size_t)steps), "pinned control");
+  if (cudaMallocHost(&h_fl, 8 * (size_t)steps * cnt) != cudaSuccess) {
+    cudaFreeHost(h_ctrl);
+    return fail(DMF_ERR_OOM, "pinned flows");
+  }
+  // step b uses its own range of round ids, relabel epochs and batch stamp
+  constexpr unsigned kRoundStride = 1u << 20, kRelabelStride = 1u << 18;
+  KernelFn fn = pick_kernel(sv->tile, sv->minb);
+  auto enqueue_steps = [&]() -> cudaError_t {
+    for (int b = 0; b < steps; b++) {
+      Params p = make_params(sv, MODE_DYNAMIC, (int)(ofs[b + 1] - ofs[b]), d_src + ofs[b], d_dst + ofs[b],
+                             d_w + ofs[b]);
+      p.round_base = sv->round_base + (unsigned)b * kRoundStride;
+      p.relabel_base = sv->relabel_base + (unsigned)b * kRelabelStride;
+      p.trace = nullptr;
+      p.probe = 0;
+      cudaError_t e = cudaMemsetAsync(sv->ctrl, 0, sizeof(Ctrl), S);
+      if (e == cudaSuccess && sv->inst_flow) e = cudaMemsetAsync(sv->inst_flow, 0, 8 * (size_t)cnt, S);
+      if (e != cudaSuccess) return e;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(sv->grid);
+      cfg.blockDim = dim3(sv->block);
+      cfg.dynamicSmemBytes = 0;
+      cfg.stream = S;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      e = cudaLaunchKernelEx(&cfg, fn, p);
+      if (e != cudaSuccess) return e;
+      e = cudaMemcpyAsync(h_ctrl + b, sv->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, S);
+      if (e == cudaSuccess) {
+        if (sv->inst_flow)
+          e = cudaMemcpyAsync(h_fl + (size_t)b * cnt, sv->inst_flow, 8 * (size_t)cnt, cudaMemcpyDeviceToHost, S);
+        else
+          e = cudaMemcpyAsync(h_fl + b, &sv->ctrl->flow, 8, cudaMemcpyDeviceToHost, S);
+      }
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+  cudaError_t e = cudaSuccess;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  if (use_graph) {
+    e = cudaStreamBeginCapture(S, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      cudaError_t e2 = enqueue_steps();
+      e = cudaStreamEndCapture(S, &graph);
+      if (e2 != cudaSuccess) e = e2;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(sv->ev0, S);
+  if (e == cudaSuccess) e = use_graph ? cudaGraphLaunch(exec, S) : enqueue_steps();
+  if (e == cudaSuccess) e = cudaEventRecord(sv->ev1, S);
+  if (e == cudaSuccess) e = cudaEventSynchronize(sv->ev1);
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaFreeHost(h_ctrl);
+    cudaFreeHost(h_fl);
+    return cuda_fail(e, use_graph ? "graph-captured batch loop" : "batch loop");
+  }
+  float t_ms = 0;
+  cudaEventElapsedTime(&t_ms, sv->ev0, sv->ev1);
+  if (ms) *ms = t_ms;
+  int rc = DMF_OK;
+  unsigned outer = 0;
+  for (int b = 0; b < steps && !rc; b++) {
+    const Ctrl &c = h_ctrl[b];
+    outer += (unsigned)c.st_outer;
+    if (c.err) rc = fail(c.err & ERR_TIMEOUT ? DMF_ERR_TIMEOUT
+                         : c.err & ERR_NO_CONV ? DMF_ERR_NO_CONVERGENCE
+                         : c.err & (ERR_UNKNOWN_ARC | ERR_DUP_ARC | ERR_BAD_UPDATE) ? DMF_ERR_INVALID_ARG
+                                                                                    : DMF_ERR_CUDA,
+                         "step %d: device error flags 0x%x (update %d)", b, c.err, c.err_info);
+  }
+  for (size_t i = 0; i < (size_t)steps * cnt; i++) flows[i] = h_fl[i];
+  sv->round_base += (unsigned)steps * kRoundStride;
+  sv->relabel_base += (unsigned)steps * kRelabelStride;
+  if (!rc) {
+    sv->flows.assign(h_fl + (size_t)(steps - 1) * cnt, h_fl + (size_t)steps * cnt);
+    int64_t tot = 0;
+    for (int64_t f : sv->flows) tot += f;
+    sv->st.flow = tot;
+    sv->st.last_ms = t_ms;
+    sv->st.outer_iters = outer;
+    sv->side_valid = false;
+  } else {
+    sv->solved = false;
+  }
+  cudaFreeHost(h_ctrl);
+  cudaFreeHost(h_fl);
+  return rc ? rc : ok();
+}
+
+int dmf_autotune(dmf_solver *sv, int32_t repeats, dmf_opts *chosen) {
+  if (!sv) return fail(DMF_ERR_INVALID_ARG, "null solver");
+  if (repeats < 1) repeats = 1;
+  dmf_opts best = sv->opts;
+  auto cost = [&](const dmf_opts &o, double *out) -> int {
+    sv->opts = o;
+    int st = configure(sv);
+    if (st) return st;
+    double b = 1e30;
+    for (int r = 0; r < repeats; r++) {
+      st = host_updates(sv, MODE_RECOMPUTE, 0, nullptr, nullptr, nullptr, nullptr);
+      if (st) return st;
+      b = std::min(b, sv->st.last_ms);
+    }
+    *out = b;
+    return DMF_OK;
+  };
+  double best_ms = 0;
+  int st = cost(best, &best_ms);
+  if (st) return st;
+  auto try_dim = [&](int32_t dmf_opts::*field, std::initializer_list<int32_t> vals) -> int {
+    for (int32_t v : vals) {
+      dmf_opts o = best;
+      if (o.*field == v) continue;
+      o.*field = v;
+      double ms = 0;
+      int s2 = cost(o, &ms);
+      if (s2) return s2;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = o;
+      }
+    }
+    return DMF_OK;
+  };
+  if ((st = try_dim(&dmf_opts::tile, {4, 8, 16, 32})) || (st = try_dim(&dmf_opts::small_deg, {-1, 4, 8, 16, 32})) ||
+      (st = try_dim(&dmf_opts::relabel_interval, {2, 3, 6, 12})) || (st = try_dim(&dmf_opts::kernel_cycles, {1, 2, 4})))
+    return st;
+  sv->opts = best;
+  if ((st = configure(sv))) return st;
+  st = host_updates(sv, MODE_RECOMPUTE, 0, nullptr, nullptr, nullptr, nullptr);  // leave a solved state
+  if (st) return st;
+  if (chosen) *chosen = best;
   return ok();
 }
 

@@ -73,6 +73,11 @@ typedef struct {
   int32_t device;           /* CUDA device ordinal; -1 = current device */
   int32_t block_threads;    /* threads per block of the persistent kernel; 0 = 512 */
   int32_t flags;            /* DMF_FLAG_* bits */
+  int32_t small_deg;        /* vertices of degree <= small_deg are handled one per
+                               thread, larger ones one per tile (thread-vs-warp
+                               per vertex); 0 = 8, -1 = no per-thread tier */
+  int32_t grid_blocks;      /* cap on the persistent grid (0 = every SM); a smaller
+                               grid lets several solvers run side by side */
 } dmf_opts;
 
 typedef struct {
@@ -217,6 +222,42 @@ int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs,
 /* Replaces the option set of a live solver (variant, cycles, interval, tile). */
 int dmf_solver_set_opts(dmf_solver *sv, const dmf_opts *opts);
 int dmf_solver_destroy(dmf_solver *sv);
+
+/* ---- batched instances ---------------------------------------------------- */
+/* Many independent graphs (each with its own s, t) in one device state: their
+ * disjoint union, solved by one persistent launch per call, every instance's
+ * flow read out separately.  No counterpart in the reference (which solves one
+ * graph per process).  Vertex v of instance i is vertex vertex_base[i] + v of the
+ * union. */
+int dmf_multi_create(int32_t count, const dmf_graph *const *graphs,
+                     const int32_t *s, const int32_t *t, const dmf_opts *opts,
+                     void *stream, dmf_solver **out);
+int dmf_multi_info(const dmf_solver *sv, int32_t *count, int32_t *vertex_base);
+/* Static solve of every instance; flows[count]. */
+int dmf_multi_static_maxflow(dmf_solver *sv, int64_t *flows);
+/* One batch whose updates may touch any instances: inst[k] names the instance,
+ * src/dst are that instance's vertex ids; flows[count] after the batch. */
+int dmf_multi_apply_updates(dmf_solver *sv, int32_t k, const int32_t *inst,
+                            const int32_t *src, const int32_t *dst,
+                            const int32_t *w, int64_t *flows);
+/* `steps` successive batches already in device memory (union vertex ids; batch
+ * b is [ofs[b], ofs[b+1]) of d_src/d_dst/d_w, ofs on the host), run back to back
+ * on the solver's stream; with use_graph != 0 the whole loop is captured once
+ * into a CUDA graph and launched as one graph.  flows[steps*count] receives the
+ * per-instance flows after every step; *ms the device time of the loop. */
+int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs,
+                          const int32_t *d_src, const int32_t *d_dst,
+                          const int32_t *d_w, int32_t use_graph,
+                          int64_t *flows, double *ms);
+
+/* ---- launch geometry autotuner --------------------------------------------- */
+/* Times from-scratch solves of the solver's current capacities under candidate
+ * tile widths, per-thread degree bounds (thread vs warp per vertex), relabel
+ * intervals and cycle counts (coordinate descent, best of `repeats` runs each),
+ * keeps the fastest in the solver and returns it in *chosen.  Every candidate
+ * computes the same exact flow; the state afterwards is a maximum flow of the
+ * current capacities. */
+int dmf_autotune(dmf_solver *sv, int32_t repeats, dmf_opts *chosen);
 
 /* Static solve that allocates nothing, for callers that cannot allocate device
  * memory while they run (code inside a fixed memory pool or arena, or a host
