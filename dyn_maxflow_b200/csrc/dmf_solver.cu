@@ -1740,7 +1740,8 @@ constexpr size_t kNoAllocV = (size_t)kNoAllocMaxVertices + 1;
 constexpr size_t kNoAllocBytes = na_round(sizeof(Ctrl)) + na_round(4 * kNoAllocV) /* height */ +
                                  na_round(4 * kNoAllocV) /* stamp */ + na_round(8 * kNoAllocV) /* excess */ +
                                  na_round(kNoAllocV) /* dead */ + na_round(kNoAllocV) /* side */ +
-                                 5 * na_round(4 * kNoAllocV) /* queues */ + 4 * kNoAllocAlign /* unused hub slots */;
+                                 5 * na_round(4 * kNoAllocV) /* queues */ + 4 * kNoAllocAlign /* unused hub slots */ +
+                                 kNoAllocAlign /* source list */;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // Device address of g_noalloc_scratch, looked up once per device (the name is
@@ -1812,7 +1813,13 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
   long long *ll_dummy = (long long *)carve(kNoAllocAlign);
   int *int_dummy = (int *)carve(kNoAllocAlign);
   unsigned long long *mark_dummy = (unsigned long long *)carve(kNoAllocAlign);
+  int *src_list = (int *)carve(kNoAllocAlign);
   if (off > kNoAllocBytes) return fail(DMF_ERR_CUDA, "internal: scratch layout exceeds the array");
+  p.srcs = src_list;  // one source; filled below by a plain copy (no allocation)
+  p.nsrc = 1;
+  p.role = nullptr;
+  p.inst = nullptr;
+  p.inst_flow = nullptr;
   p.fh[0] = p.fh[1] = p.wh[0] = p.wh[1] = p.ah = hub_dummy;
   p.hch = hub_dummy;
   p.nhch = 0;
@@ -1854,6 +1861,8 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
   // worklist stamps must start at zero (everything else is written before use)
   CK(cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), S), "memset control");
   CK(cudaMemsetAsync(p.stamp, 0, 4 * N, S), "memset stamps");
+  const int32_t src_host = s;
+  CK(cudaMemcpyAsync(src_list, &src_host, sizeof(src_host), cudaMemcpyHostToDevice, S), "H2D source");
   void *args[] = {&p};
   CK(cudaLaunchCooperativeKernel((const void *)fn, dim3(per_sm * sms), dim3(kBlock), args, 0, S),
      "cooperative launch");
