@@ -21,7 +21,7 @@ import numpy as np
 __all__ = [
     "DmfError", "Graph", "Solver", "Stats", "load_updates", "save_updates", "gen_grid", "gen_rmat",
     "gen_batches", "recalculate_max_flow", "static_recalculate", "device_count", "VARIANTS", "lib_path",
-    "static_maxflow_noalloc", "MultiSolver",
+    "static_maxflow_noalloc", "MultiSolver", "Server",
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -105,6 +105,12 @@ _sig("dmf_multi_static_maxflow", C.c_int, VP, I64P)
 _sig("dmf_multi_apply_updates", C.c_int, VP, C.c_int32, I32P, I32P, I32P, I32P, I64P)
 _sig("dmf_multi_run_batches", C.c_int, VP, C.c_int32, I64P, VP, VP, VP, C.c_int32, I64P, C.POINTER(C.c_double))
 _sig("dmf_autotune", C.c_int, VP, C.c_int32, C.POINTER(Opts))
+_sig("dmf_server_create", C.c_int, C.c_int32, C.POINTER(C.c_void_p), I32P, I32P, C.c_int64, C.POINTER(Opts), PP)
+_sig("dmf_server_info", C.c_int, VP, C.POINTER(C.c_int32), C.POINTER(C.c_int64))
+_sig("dmf_server_submit", C.c_int, VP, C.c_int32, C.c_int32, I32P, I32P, I32P, C.POINTER(C.c_int64))
+_sig("dmf_server_wait", C.c_int, VP, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double))
+_sig("dmf_server_stats", C.c_int, VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_double))
+_sig("dmf_server_destroy", C.c_int, VP)
 _sig("dmf_static_maxflow_noalloc", C.c_int, C.c_int32, C.c_int32, VP, VP, VP, VP, C.c_int32, C.c_int32, VP,
      C.POINTER(C.c_int64), VP)
 
@@ -447,3 +453,51 @@ class MultiSolver(Solver):
         _check(_L.dmf_multi_run_batches(self._h, steps, ofs, C.c_void_p(d_src), C.c_void_p(d_dst), C.c_void_p(d_w),
                                         1 if use_graph else 0, out, C.byref(ms)))
         return out.reshape(steps, self.count), ms.value
+
+
+class Server:
+    """Serving loop (dmf_server_*): device-resident graphs admitted by HBM budget,
+    continuous batching of update-batch requests.  submit() returns a ticket;
+    wait(ticket) -> (flow, latency_ms).  Thread-safe."""
+
+    def __init__(self, graphs, sources, sinks, hbm_budget_bytes, variant="data"):
+        o = Opts()
+        _L.dmf_opts_default(C.byref(o))
+        o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
+        self.graphs = list(graphs)  # kept alive for the server
+        arr = (C.c_void_p * len(self.graphs))(*[g._h.value for g in self.graphs])
+        self._h = C.c_void_p()
+        _check(_L.dmf_server_create(len(self.graphs), arr, _i32(sources), _i32(sinks), int(hbm_budget_bytes),
+                                    C.byref(o), C.byref(self._h)))
+        adm, by = C.c_int32(), C.c_int64()
+        _check(_L.dmf_server_info(self._h, C.byref(adm), C.byref(by)))
+        self.admitted, self.device_bytes = adm.value, by.value
+
+    def submit(self, graph, src, dst, w) -> int:
+        src, dst, w = _i32(src), _i32(dst), _i32(w)
+        tk = C.c_int64()
+        _check(_L.dmf_server_submit(self._h, graph, len(src), src, dst, w, C.byref(tk)))
+        return tk.value
+
+    def wait(self, ticket):
+        f, lat = C.c_int64(), C.c_double()
+        _check(_L.dmf_server_wait(self._h, ticket, C.byref(f), C.byref(lat)))
+        return f.value, lat.value
+
+    def stats(self) -> dict:
+        a, b, c = C.c_int64(), C.c_int64(), C.c_double()
+        _check(_L.dmf_server_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"ticks": a.value, "served": b.value, "mean_requests_per_tick": c.value}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _L.dmf_server_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,246 @@
+// dmf_server.cpp -- serving loop over device-resident residual graphs.
+//
+// Admission: graphs are admitted in the order given while the estimated device
+// footprint of their residual state fits the HBM budget; each admitted graph
+// stays resident for the server's life, and every batch a request carries is
+// applied to it (successive batches per graph, in submission order).
+//
+// Continuous batching: all admitted graphs live in one batched-instance solver
+// (dmf_multi_*).  A worker thread runs ticks; a tick takes, for every graph,
+// its oldest waiting request (while the tick's batch stays inside the staging
+// budget) and serves them all with one persistent launch, which relabels and
+// pushes only inside the touched graphs.  Requests that arrive during a tick
+// join the next one.  Instances are independent, so each result equals the
+// result of the same request sequence served alone.  No counterpart in the
+// reference (a one-shot bench).
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "dmf_internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  int64_t ticket;
+  int32_t graph;
+  std::vector<int32_t> src, dst, w;
+  Clock::time_point t_submit;
+  bool done = false;
+  int status = DMF_OK;
+  std::string error;
+  int64_t flow = 0;
+  double latency_ms = 0;
+};
+
+}  // namespace
+
+struct dmf_server {
+  std::vector<const dmf_graph *> graphs;  // admitted (borrowed; caller keeps them alive)
+  std::vector<int32_t> s, t;
+  int64_t budget = 0, device_bytes = 0, stage_budget = 0;
+  dmf_solver *sv = nullptr;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::vector<std::deque<Request *>> pending;  // per graph, FIFO
+  std::map<int64_t, Request *> all;
+  int64_t next_ticket = 1;
+  bool stop = false;
+  std::thread worker;
+  int64_t ticks = 0, served = 0, batched_sum = 0;
+};
+
+static int64_t footprint(const dmf_graph *g) {
+  // residual state bytes per arc and per vertex (see the solver's data layout)
+  return 28LL * g->m + 64LL * g->n;
+}
+
+static void tick_loop(dmf_server *S) {
+  const int G = (int)S->graphs.size();
+  std::vector<int64_t> flows(G);
+  for (;;) {
+    std::vector<Request *> batch;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_work.wait(lk, [&] {
+        if (S->stop) return true;
+        for (auto &q : S->pending)
+          if (!q.empty()) return true;
+        return false;
+      });
+      if (S->stop) return;
+      int64_t bytes = 0;
+      for (int g = 0; g < G; g++) {
+        if (S->pending[g].empty()) continue;
+        Request *r = S->pending[g].front();
+        const int64_t b = 16LL * (int64_t)r->src.size();
+        if (!batch.empty() && bytes + b > S->stage_budget) continue;  // waits for the next tick
+        bytes += b;
+        S->pending[g].pop_front();
+        batch.push_back(r);
+      }
+    }
+    std::vector<int32_t> I, A, B, W;
+    for (Request *r : batch) {
+      I.insert(I.end(), r->src.size(), r->graph);
+      A.insert(A.end(), r->src.begin(), r->src.end());
+      B.insert(B.end(), r->dst.begin(), r->dst.end());
+      W.insert(W.end(), r->w.begin(), r->w.end());
+    }
+    int st = dmf_multi_apply_updates(S->sv, (int32_t)A.size(), I.data(), A.data(), B.data(), W.data(), flows.data());
+    std::string err = st ? dmf_last_error() : "";
+    const auto now = Clock::now();
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      for (Request *r : batch) {
+        r->status = st;
+        r->error = err;
+        r->flow = flows[r->graph];
+        r->latency_ms = std::chrono::duration<double, std::milli>(now - r->t_submit).count();
+        r->done = true;
+      }
+      S->ticks++;
+      S->served += (int64_t)batch.size();
+      S->batched_sum += (int64_t)batch.size();
+    }
+    S->cv_done.notify_all();
+  }
+}
+
+extern "C" {
+
+int dmf_server_create(int32_t count, const dmf_graph *const *graphs, const int32_t *s, const int32_t *t,
+                      int64_t hbm_budget, const dmf_opts *opts, dmf_server **out) {
+  if (count < 1 || !graphs || !s || !t || !out || hbm_budget <= 0)
+    return dmf::fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  auto *S = new dmf_server();
+  S->budget = hbm_budget;
+  for (int i = 0; i < count; i++) {
+    if (!graphs[i]) {
+      delete S;
+      return dmf::fail(DMF_ERR_INVALID_ARG, "graph %d is null", i);
+    }
+    const int64_t f = footprint(graphs[i]);
+    if (S->device_bytes + f > hbm_budget) continue;  // not admitted
+    S->device_bytes += f;
+    S->graphs.push_back(graphs[i]);
+    S->s.push_back(s[i]);
+    S->t.push_back(t[i]);
+  }
+  if (S->graphs.empty()) {
+    delete S;
+    return dmf::fail(DMF_ERR_OOM, "no graph fits the HBM budget of %lld bytes", (long long)hbm_budget);
+  }
+  S->stage_budget = std::max<int64_t>(hbm_budget - S->device_bytes, 16LL << 20);
+  int st = dmf_multi_create((int32_t)S->graphs.size(), S->graphs.data(), S->s.data(), S->t.data(), opts, nullptr,
+                            &S->sv);
+  if (st) {
+    delete S;
+    return st;
+  }
+  std::vector<int64_t> f(S->graphs.size());
+  if ((st = dmf_multi_static_maxflow(S->sv, f.data()))) {
+    dmf_solver_destroy(S->sv);
+    delete S;
+    return st;
+  }
+  S->pending.resize(S->graphs.size());
+  S->worker = std::thread(tick_loop, S);
+  *out = S;
+  return dmf::ok();
+}
+
+int dmf_server_info(const dmf_server *S, int32_t *admitted, int64_t *device_bytes) {
+  if (!S) return dmf::fail(DMF_ERR_INVALID_ARG, "null server");
+  if (admitted) *admitted = (int32_t)S->graphs.size();
+  if (device_bytes) *device_bytes = S->device_bytes;
+  return dmf::ok();
+}
+
+int dmf_server_submit(dmf_server *S, int32_t graph, int32_t k, const int32_t *src, const int32_t *dst,
+                      const int32_t *w, int64_t *ticket) {
+  if (!S || !ticket || k < 0 || (k > 0 && (!src || !dst || !w))) return dmf::fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  if (graph < 0 || graph >= (int32_t)S->graphs.size())
+    return dmf::fail(DMF_ERR_INVALID_ARG, "graph %d was not admitted", graph);
+  const dmf_graph *g = S->graphs[graph];
+  // requests are checked on their own, so one bad request never fails a tick
+  std::vector<int64_t> arcs;
+  for (int32_t i = 0; i < k; i++) {
+    if (src[i] < 0 || dst[i] < 0 || src[i] >= g->n || dst[i] >= g->n)
+      return dmf::fail(DMF_ERR_INVALID_ARG, "update %d: vertex out of range", i);
+    if (w[i] < 0 || w[i] > (1 << 30) - 1) return dmf::fail(DMF_ERR_INVALID_ARG, "update %d: capacity out of range", i);
+    if (src[i] == dst[i]) continue;
+    const int64_t e = dmf::find_arc(*g, src[i], dst[i]);
+    if (e < 0) return dmf::fail(DMF_ERR_UNKNOWN_ARC, "update %d: arc %d->%d not in graph %d", i, src[i], dst[i], graph);
+    arcs.push_back(e);
+  }
+  std::sort(arcs.begin(), arcs.end());
+  if (std::adjacent_find(arcs.begin(), arcs.end()) != arcs.end())
+    return dmf::fail(DMF_ERR_DUP_ARC, "an arc repeats within the request");
+  auto *r = new Request();
+  r->graph = graph;
+  r->src.assign(src, src + k);
+  r->dst.assign(dst, dst + k);
+  r->w.assign(w, w + k);
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    r->ticket = S->next_ticket++;
+    S->all[r->ticket] = r;
+    S->pending[graph].push_back(r);
+  }
+  S->cv_work.notify_one();
+  *ticket = r->ticket;
+  return dmf::ok();
+}
+
+int dmf_server_wait(dmf_server *S, int64_t ticket, int64_t *flow, double *latency_ms) {
+  if (!S) return dmf::fail(DMF_ERR_INVALID_ARG, "null server");
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->all.find(ticket);
+  if (it == S->all.end()) return dmf::fail(DMF_ERR_INVALID_ARG, "unknown ticket %lld", (long long)ticket);
+  Request *r = it->second;
+  S->cv_done.wait(lk, [&] { return r->done; });
+  S->all.erase(it);
+  const int st = r->status;
+  const std::string err = r->error;
+  if (flow) *flow = r->flow;
+  if (latency_ms) *latency_ms = r->latency_ms;
+  delete r;
+  lk.unlock();
+  return st ? dmf::fail(st, "%s", err.c_str()) : dmf::ok();
+}
+
+int dmf_server_stats(const dmf_server *S, int64_t *ticks, int64_t *served, double *mean_per_tick) {
+  if (!S) return dmf::fail(DMF_ERR_INVALID_ARG, "null server");
+  auto *M = const_cast<dmf_server *>(S);
+  std::lock_guard<std::mutex> lk(M->mu);
+  if (ticks) *ticks = S->ticks;
+  if (served) *served = S->served;
+  if (mean_per_tick) *mean_per_tick = S->ticks ? (double)S->batched_sum / S->ticks : 0.0;
+  return dmf::ok();
+}
+
+int dmf_server_destroy(dmf_server *S) {
+  if (!S) return dmf::ok();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->cv_work.notify_all();
+  if (S->worker.joinable()) S->worker.join();
+  for (auto &kv : S->all) delete kv.second;
+  dmf_solver_destroy(S->sv);
+  delete S;
+  return dmf::ok();
+}
+
+}  // extern "C"

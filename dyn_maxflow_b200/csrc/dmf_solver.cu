@@ -82,6 +82,9 @@ struct Params {
   long long *inst_flow;
   const int *srcs;  // every source vertex (just s for one instance)
   int nsrc;
+  // instances a batched call works on (nullptr: all); the others are left as they
+  // are: not seeded, not saturated, not read out
+  const unsigned char *inst_active;
   Ctrl *ctrl;
   int mode, variant, cycles, interval, max_iters, hub_deg, small_deg, need_cut;
   int bu_alpha;  // bottom-up when frontier arcs * bu_alpha > unexplored arcs (0: never)
@@ -137,6 +140,7 @@ __device__ void ph_init_res(const Params &p) {
 __device__ void ph_saturate(const Params &p) {
   const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < p.nsrc; i += nwarps) {
+    if (p.inst_active && !p.inst_active[i]) continue;  // source i belongs to instance i
     const int s = __ldg(p.srcs + i);
     const int beg = __ldg(p.off + s), end = __ldg(p.off + s + 1);
     long long sum = 0;
@@ -316,6 +320,13 @@ __device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
   int pos = 0;
   long long unexpl = 0, seed_arcs = 0;
   for (int v = gt; v < p.n; v += nt) {
+    if (p.inst_active && !p.inst_active[__ldg(p.inst + v)]) {
+      if (reset_dead) {
+        p.dead[v] = 1;
+        p.height[v] = p.n;
+      }
+      continue;
+    }
     if (reset_dead) {
       if (__ldcg(p.dead + v)) p.dead[v] = 0;
     } else if (__ldcg(p.dead + v)) {
@@ -519,7 +530,7 @@ __device__ void ph_bfs_finalize(const Params &p, bool full, int floor_h, bool wr
         p.height[v] = floor_h;
       }
     }
-    if (write_side) p.side[v] = h < p.n ? 1 : 0;
+    if (write_side && (!p.inst_active || p.inst_active[__ldg(p.inst + v)])) p.side[v] = h < p.n ? 1 : 0;
   }
   agg_add_ll((long long *)&p.ctrl->st_dead, nd);
 }
@@ -901,7 +912,7 @@ __device__ void ph_flow(const Params &p, typename BlockGroup<BLOCK>::Temp &btmp)
     if (is_snk(p, v)) c = ex;
     else if (!is_src(p, v) && ex < 0) c = ex;
     if (p.inst) {
-      if (c) atomic_add_ll(p.inst_flow + __ldg(p.inst + v), c);
+      if (c && (!p.inst_active || p.inst_active[__ldg(p.inst + v)])) atomic_add_ll(p.inst_flow + __ldg(p.inst + v), c);
     } else {
       acc += c;
     }
@@ -1295,7 +1306,12 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
     if (!next()) return;
     const int A = ld_vol(&c->act_q) + ld_vol(&c->act_hq);
     if (A == 0 || cut_only) break;
-    for (int r = 0; r < p.interval; r++) {
+    // a global relabel costs about one phase per BFS level and a push round moves
+    // excess about one hop: on deep graphs (grids) allow as many rounds as the
+    // relabel had levels before relabelling again (the loop ends early when the
+    // worklist empties)
+    const int rounds = p.interval > L ? p.interval : L;
+    for (int r = 0; r < rounds; r++) {
       round_id++;
       const RoundIn in = round_inputs(p, r);
       kind = TR_PUSH;
@@ -1408,6 +1424,9 @@ struct dmf_solver {
   std::vector<int> vbase;            // first vertex of each instance in the union
   std::vector<int64_t> flows;        // last per-instance flows
   cudaStream_t own_stream = nullptr; // for graph capture when the user stream is the legacy one
+  unsigned char *inst_active = nullptr;     // device mask for the next launch (batched mode)
+  unsigned char *h_inst_active = nullptr;   // pinned staging
+  bool use_active = false;
   int *ubuf = nullptr;  // device update staging: src | dst | w
   int kcap = 0;
   int *h_ubuf = nullptr;  // pinned host staging
@@ -1455,6 +1474,8 @@ void free_all(dmf_solver *sv) {
   if (sv->h_ctrl) cudaFreeHost(sv->h_ctrl);
   if (sv->h_inst_flow) cudaFreeHost(sv->h_inst_flow);
   sv->h_inst_flow = nullptr;
+  if (sv->h_inst_active) cudaFreeHost(sv->h_inst_active);
+  sv->h_inst_active = nullptr;
   if (sv->own_stream) cudaStreamDestroy(sv->own_stream);
   sv->own_stream = nullptr;
   if (sv->ev0) cudaEventDestroy(sv->ev0);
@@ -1574,6 +1595,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.inst_flow = sv->inst_flow;
   p.srcs = sv->srcs;
   p.nsrc = sv->nsrc;
+  p.inst_active = sv->use_active ? sv->inst_active : nullptr;
   p.chunk_mark = sv->chunk_mark;
   p.chunk_tmin = sv->chunk_tmin;
   p.relabel_base = sv->relabel_base;
@@ -1664,7 +1686,12 @@ int finish(dmf_solver *sv, int64_t *flow, bool need_cut_valid) {
   sv->solved = true;
   sv->side_valid = need_cut_valid;
   if (sv->inst_flow) {
-    sv->flows.assign(sv->h_inst_flow, sv->h_inst_flow + sv->ninst);
+    if (sv->use_active && (int)sv->flows.size() == sv->ninst) {
+      for (int i = 0; i < sv->ninst; i++)
+        if (sv->h_inst_active[i]) sv->flows[i] = sv->h_inst_flow[i];
+    } else {
+      sv->flows.assign(sv->h_inst_flow, sv->h_inst_flow + sv->ninst);
+    }
     int64_t tot = 0;
     for (int64_t f : sv->flows) tot += f;
     sv->st.flow = tot;
@@ -1988,8 +2015,11 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
     if (ms) {
       sv->vbase = ms->vbase;
       if ((st = dalloc(sv, &sv->role, N)) || (st = dalloc(sv, &sv->inst, N)) ||
-          (st = dalloc(sv, &sv->inst_flow, (size_t)ms->count)))
+          (st = dalloc(sv, &sv->inst_flow, (size_t)ms->count)) ||
+          (st = dalloc(sv, &sv->inst_active, (size_t)ms->count)))
         return bail(st);
+      if (cudaMallocHost(&sv->h_inst_active, (size_t)ms->count) != cudaSuccess)
+        return bail(cuda_fail(cudaGetLastError(), "pinned mask"));
       if (cudaMemcpy(sv->role, ms->role.data(), ms->role.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
           cudaMemcpy(sv->inst, ms->inst.data(), 4 * ms->inst.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
           cudaMallocHost(&sv->h_inst_flow, 8 * (size_t)ms->count) != cudaSuccess)
@@ -2104,7 +2134,16 @@ int dmf_multi_apply_updates(dmf_solver *sv, int32_t k, const int32_t *inst, cons
     gs[i] = b + src[i];
     gd[i] = b + dst[i];
   }
+  // only the instances this batch touches are relabelled, pushed and read out
+  if (sv->inst_active && (int)sv->flows.size() == sv->ninst && sv->solved) {
+    std::memset(sv->h_inst_active, 0, (size_t)sv->ninst);
+    for (int32_t i = 0; i < k; i++) sv->h_inst_active[inst[i]] = 1;
+    CK(cudaMemcpyAsync(sv->inst_active, sv->h_inst_active, (size_t)sv->ninst, cudaMemcpyHostToDevice, sv->stream),
+       "H2D mask");
+    sv->use_active = true;
+  }
   int st = host_updates(sv, MODE_DYNAMIC, k, gs.data(), gd.data(), w, nullptr);
+  sv->use_active = false;
   if (st) return st;
   for (int i = 0; i < sv->ninst; i++) flows[i] = sv->flows[i];
   return ok();

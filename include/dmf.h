@@ -250,6 +250,32 @@ int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs,
                           const int32_t *d_w, int32_t use_graph,
                           int64_t *flows, double *ms);
 
+/* ---- serving loop ------------------------------------------------------------ */
+/* Device-resident graphs serving update-batch requests.  Graphs are admitted in
+ * the given order while the estimated device footprint of their residual state
+ * (28 B per arc + 64 B per vertex) fits `hbm_budget` bytes; the rest are not
+ * admitted (ids of admitted graphs are their positions among the admitted ones,
+ * dmf_server_info).  The caller keeps the graphs alive until destroy.
+ * Continuous batching: a worker thread serves, per tick, the oldest waiting
+ * request of every graph with one persistent launch (dmf_multi_apply_updates),
+ * while the tick's batch stays inside the staging budget (what the graphs leave
+ * of hbm_budget, at least 16 MiB); requests arriving during a tick join the
+ * next.  Batches of one graph apply in submission order.  submit() validates a
+ * request on the host (vertex ranges, existing arcs, no repeats) and copies it;
+ * wait() blocks until it is served and returns the graph's exact max-flow after
+ * it and its latency from submission.  No counterpart in the reference. */
+typedef struct dmf_server dmf_server;
+int dmf_server_create(int32_t count, const dmf_graph *const *graphs,
+                      const int32_t *s, const int32_t *t, int64_t hbm_budget,
+                      const dmf_opts *opts, dmf_server **out);
+int dmf_server_info(const dmf_server *srv, int32_t *admitted, int64_t *device_bytes);
+int dmf_server_submit(dmf_server *srv, int32_t graph, int32_t k, const int32_t *src,
+                      const int32_t *dst, const int32_t *w, int64_t *ticket);
+int dmf_server_wait(dmf_server *srv, int64_t ticket, int64_t *flow, double *latency_ms);
+int dmf_server_stats(const dmf_server *srv, int64_t *ticks, int64_t *served,
+                     double *mean_requests_per_tick);
+int dmf_server_destroy(dmf_server *srv);
+
 /* ---- launch geometry autotuner --------------------------------------------- */
 /* Times from-scratch solves of the solver's current capacities under candidate
  * tile widths, per-thread degree bounds (thread vs warp per vertex), relabel

@@ -1,0 +1,84 @@
+"""Serving loop: graphs admitted by HBM budget, continuous batching of
+update-batch requests; each result is the same alone and in the mix."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _graphs(dmf):
+    from dyn_maxflow_b200 import workloads
+    return workloads.batched(count=8, steps=4, seed=11, median=600, lo=64, hi=3000)
+
+
+def test_admission_by_budget(dmf):
+    inst = _graphs(dmf)
+    graphs = [x[0] for x in inst]
+    need = [28 * g.num_edges() + 64 * g.num_nodes() for g in graphs]
+    budget = sum(need[:3]) + need[3] // 2  # room for the first three only
+    with dmf.Server(graphs, [x[1] for x in inst], [x[2] for x in inst], budget) as srv:
+        assert srv.admitted == 3 and srv.device_bytes == sum(need[:3])
+        with pytest.raises(dmf.DmfError):
+            srv.submit(3, [0], [1], [1])  # not admitted
+    with pytest.raises(dmf.DmfError) as ei:
+        dmf.Server(graphs, [x[1] for x in inst], [x[2] for x in inst], 16)
+    assert ei.value.status == 5
+
+
+def test_mixed_results_equal_alone(dmf, oracle):
+    inst = _graphs(dmf)
+    graphs, S, T = [x[0] for x in inst], [x[1] for x in inst], [x[2] for x in inst]
+    # alone: each graph's request sequence on its own solver, one request at a time
+    alone = []
+    for g, s, t, batches in inst:
+        with dmf.Solver(g, s, t) as sv:
+            sv.static_maxflow()
+            alone.append([sv.apply_updates(*b) for b in batches])
+    # and independently: Dinic on the capacities after each request
+    for i, (g, s, t, batches) in enumerate(inst):
+        off, adj, w, par = g.arrays()
+        cur = w.copy()
+        for j, b in enumerate(batches):
+            for a, c, x in zip(*b):
+                cur[g.find_arc(int(a), int(c))] = x
+            assert alone[i][j] == oracle.dinic(g.num_nodes(), off, adj, cur, par, s, t)
+    # in the mix: every graph's requests submitted from its own thread, all at once
+    got = [[None] * len(inst[0][3]) for _ in inst]
+    lat = []
+    with dmf.Server(graphs, S, T, 1 << 34) as srv:
+        assert srv.admitted == len(inst)
+
+        def client(i):
+            tickets = [srv.submit(i, *b) for b in inst[i][3]]
+            for j, tk in enumerate(tickets):
+                got[i][j], l = srv.wait(tk)
+                lat.append(l)
+
+        th = [threading.Thread(target=client, args=(i,)) for i in range(len(inst))]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        st = srv.stats()
+    assert got == alone
+    assert st["served"] == sum(len(x[3]) for x in inst)
+    assert st["mean_requests_per_tick"] > 1.0  # requests of different graphs shared launches
+    assert min(lat) > 0
+
+
+def test_bad_requests_are_rejected_alone(dmf):
+    inst = _graphs(dmf)
+    g, s, t, batches = inst[0]
+    with dmf.Server([g], [s], [t], 1 << 30) as srv:
+        n = g.num_nodes()
+        missing = next((a, b) for a in range(n) for b in range(n) if a != b and g.find_arc(a, b) < 0)
+        with pytest.raises(dmf.DmfError) as ei:
+            srv.submit(0, [missing[0]], [missing[1]], [3])
+        assert ei.value.status == 3
+        tk = srv.submit(0, *batches[0])
+        f, _ = srv.wait(tk)
+        with dmf.Solver(g, s, t) as sv:
+            sv.static_maxflow()
+            assert f == sv.apply_updates(*batches[0])
