@@ -47,6 +47,8 @@ def parse_args():
     ap.add_argument("--kernel-cycles", type=int, default=0)
     ap.add_argument("--relabel-interval", type=int, default=0)
     ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--fixed-interval", action="store_true",
+                    help="exactly --relabel-interval push rounds per global relabel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-certify", action="store_true")
     ap.add_argument("--cpu-batches", type=int, default=3)
@@ -184,7 +186,8 @@ def run_ours(args, rank: int, world: int):
     dbat = [[torch.as_tensor(x, dtype=torch.int32).cuda() for x in b] for b in batches]
     torch.cuda.synchronize()
     sv = D.Solver(g, s, t, variant=args.variant, kernel_cycles=args.kernel_cycles,
-                  relabel_interval=args.relabel_interval, tile=args.tile, stream=stream, trace=True)
+                  relabel_interval=args.relabel_interval, tile=args.tile, stream=stream, trace=True,
+                  fixed_interval=args.fixed_interval)
     static_flow = sv.static_maxflow()
     phase_us = {}
     flows, times, stats = [], [], []
@@ -227,7 +230,8 @@ def run_ours(args, rank: int, world: int):
     sv.close()
     # ---- end-to-end pass through the host-array entry point ----
     sv2 = D.Solver(g, s, t, variant=args.variant, kernel_cycles=args.kernel_cycles,
-                   relabel_interval=args.relabel_interval, tile=args.tile, stream=stream)
+                   relabel_interval=args.relabel_interval, tile=args.tile, stream=stream,
+                   fixed_interval=args.fixed_interval)
     assert sv2.static_maxflow() == static_flow
     e2e = []
     flows2 = []

@@ -268,13 +268,13 @@ class Solver:
     """Device-resident residual state of one graph on one GPU (dmf_solver)."""
 
     def __init__(self, g: Graph, source: int, sink: int, variant="data", kernel_cycles=0, relabel_interval=0,
-                 tile=0, max_iters=0, device=-1, stream=None, trace=False, probe=False):
+                 tile=0, max_iters=0, device=-1, stream=None, trace=False, probe=False, fixed_interval=False):
         o = Opts()
         _L.dmf_opts_default(C.byref(o))
         o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
         o.kernel_cycles, o.relabel_interval, o.tile, o.max_iters, o.device = (
             kernel_cycles, relabel_interval, tile, max_iters, device)
-        o.flags = (1 if trace or probe else 0) | (2 if probe else 0)
+        o.flags = (1 if trace or probe else 0) | (2 if probe else 0) | (4 if fixed_interval else 0)
         self._h = C.c_void_p()
         self.n, self.m = g.num_nodes(), g.num_edges()
         stream_ptr = None if stream is None else C.c_void_p(int(getattr(stream, "cuda_stream", stream)))

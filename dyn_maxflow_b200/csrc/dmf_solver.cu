@@ -81,6 +81,9 @@ struct Params {
   const int *inst;
   long long *inst_flow;
   const int *srcs;  // every source vertex (just s for one instance)
+  // prefix sums of the sources' degrees (nsrc + 1 entries), or null: the
+  // saturation then walks the sources one after the other
+  const int *src_off;
   int nsrc;
   // instances a batched call works on (nullptr: all); the others are left as they
   // are: not seeded, not saturated, not read out
@@ -88,6 +91,7 @@ struct Params {
   Ctrl *ctrl;
   int mode, variant, cycles, interval, max_iters, hub_deg, small_deg, need_cut;
   int bu_alpha;  // bottom-up when frontier arcs * bu_alpha > unexplored arcs (0: never)
+  int adaptive;  // push rounds per relabel at least the depth of the last relabel BFS
   unsigned round_base;
   int epoch;
   unsigned long long *trace;  // optional phase timeline: 4 words per entry
@@ -136,25 +140,55 @@ __device__ void ph_init_res(const Params &p) {
 }
 
 // staticMaxFlow_kernel_7 (code/dyn_data.h:39-56) made parallel: every residual
-// arc out of every source is saturated (one warp per source, lanes over arcs).
+// arc out of every source is saturated.  The arcs of all sources form one index
+// space (src_off) walked grid-stride, so one source of very high degree (R-MAT's
+// s) is spread over the whole grid and many small sources cost one pass.
+__device__ __forceinline__ long long saturate_arc(const Params &p, int a) {
+  const int r = __ldcg(p.res + a);
+  if (r <= 0) return 0;
+  p.res[a] = 0;
+  atomicAdd(p.res + __ldg(p.par + a), r);
+  atomic_add_ll(p.excess + __ldg(p.adj + a), r);
+  return r;
+}
+
 __device__ void ph_saturate(const Params &p) {
-  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < p.nsrc; i += nwarps) {
-    if (p.inst_active && !p.inst_active[i]) continue;  // source i belongs to instance i
-    const int s = __ldg(p.srcs + i);
-    const int beg = __ldg(p.off + s), end = __ldg(p.off + s + 1);
-    long long sum = 0;
-    for (int a = beg + lane; a < end; a += 32) {
-      int r = __ldcg(p.res + a);
-      if (r > 0) {
-        p.res[a] = 0;
-        atomicAdd(p.res + __ldg(p.par + a), r);
-        atomic_add_ll(p.excess + __ldg(p.adj + a), r);
-        sum += r;
-      }
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!p.src_off) {
+    for (int i = 0; i < p.nsrc; i++) {
+      if (p.inst_active && !p.inst_active[i]) continue;  // source i belongs to instance i
+      const int s = __ldg(p.srcs + i);
+      const int beg = __ldg(p.off + s), end = __ldg(p.off + s + 1);
+      long long sum = 0;
+      for (int a = beg + gt; a < end; a += nt) sum += saturate_arc(p, a);
+      agg_add_ll(p.excess + s, -sum);
     }
-    agg_add_ll(p.excess + s, -sum);
+    return;
   }
+  const int total = __ldg(p.src_off + p.nsrc);
+  int cur = -1;  // source whose arcs this thread is summing
+  long long sum = 0;
+  for (int j = gt; j < total; j += nt) {
+    int lo = 0, hi = p.nsrc;  // last i with src_off[i] <= j
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(p.src_off + mid) <= j) lo = mid;
+      else hi = mid;
+    }
+    if (p.inst_active && !p.inst_active[lo]) continue;
+    if (lo != cur) {
+      if (sum) atomic_add_ll(p.excess + __ldg(p.srcs + cur), -sum);
+      cur = lo;
+      sum = 0;
+    }
+    const int s = __ldg(p.srcs + lo);
+    sum += saturate_arc(p, __ldg(p.off + s) + (j - __ldg(p.src_off + lo)));
+  }
+  // threads of a warp that ended on the same source add once
+  cg::coalesced_group g = cg::coalesced_threads();
+  cg::coalesced_group same = cg::labeled_partition(g, cur);
+  sum = cg::reduce(same, sum, cg::plus<long long>());
+  if (same.thread_rank() == 0 && cur >= 0 && sum) atomic_add_ll(p.excess + __ldg(p.srcs + cur), -sum);
 }
 
 // Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201) by binary search over the
@@ -339,6 +373,14 @@ __device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
       if (d > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
       else append(p.fq[0], &out->q, v);
       seed_arcs += d;
+    } else if (is_src(p, v)) {
+      // Sources stay at height V and are never labelled: with a finite label
+      // (the reference's BFS gives s its distance) a run of local relabels can
+      // lift vertices above s while t is still reachable, excess drains back
+      // into s, and the solve ends with an augmenting path open.  Excess that
+      // cannot reach a sink or a deficit is parked on dead vertices instead,
+      // so nothing ever has to return to s.
+      p.height[v] = p.n;
     } else {
       p.height[v] = UNV;
       // a bottom-up level scans the arcs of every unvisited vertex, so the
@@ -1310,7 +1352,7 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
     // excess about one hop: on deep graphs (grids) allow as many rounds as the
     // relabel had levels before relabelling again (the loop ends early when the
     // worklist empties)
-    const int rounds = p.interval > L ? p.interval : L;
+    const int rounds = (p.interval > L || !p.adaptive) ? p.interval : L;
     for (int r = 0; r < rounds; r++) {
       round_id++;
       const RoundIn in = round_inputs(p, r);
@@ -1418,6 +1460,7 @@ struct dmf_solver {
   unsigned char *role = nullptr;
   int *inst = nullptr;
   int *srcs = nullptr;
+  int *src_off = nullptr;  // prefix sums of the sources' degrees
   int nsrc = 1;
   long long *inst_flow = nullptr;
   long long *h_inst_flow = nullptr;  // pinned
@@ -1594,6 +1637,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.inst = sv->inst;
   p.inst_flow = sv->inst_flow;
   p.srcs = sv->srcs;
+  p.src_off = sv->src_off;
   p.nsrc = sv->nsrc;
   p.inst_active = sv->use_active ? sv->inst_active : nullptr;
   p.chunk_mark = sv->chunk_mark;
@@ -1614,6 +1658,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.hub_deg = sv->hub_deg;
   p.small_deg = sv->small_deg;
   p.bu_alpha = sv->bu_alpha;
+  p.adaptive = (sv->opts.flags & DMF_FLAG_FIXED_INTERVAL) ? 0 : 1;
   p.need_cut = sv->opts.variant == DMF_VARIANT_PP ? 1 : 0;
   p.round_base = sv->round_base;
   p.trace = (sv->opts.flags & DMF_FLAG_TRACE) ? sv->trace : nullptr;
@@ -2009,8 +2054,15 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
     const std::vector<int> &sl = ms ? ms->srcs : one;
     sv->nsrc = (int)sl.size();
     sv->ninst = ms ? ms->count : 1;
-    if ((st = dalloc(sv, &sv->srcs, sl.size()))) return bail(st);
-    if (cudaMemcpy(sv->srcs, sl.data(), 4 * sl.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    std::vector<int> so(sl.size() + 1, 0);
+    for (size_t i = 0; i < sl.size(); i++) {
+      const long long nx = (long long)so[i] + g->off[sl[i] + 1] - g->off[sl[i]];
+      if (nx > INT_MAX) return bail(fail(DMF_ERR_INVALID_ARG, "sources have more than 2^31 arcs in total"));
+      so[i + 1] = (int)nx;
+    }
+    if ((st = dalloc(sv, &sv->srcs, sl.size())) || (st = dalloc(sv, &sv->src_off, so.size()))) return bail(st);
+    if (cudaMemcpy(sv->srcs, sl.data(), 4 * sl.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(sv->src_off, so.data(), 4 * so.size(), cudaMemcpyHostToDevice) != cudaSuccess)
       return bail(cuda_fail(cudaGetLastError(), "H2D sources"));
     if (ms) {
       sv->vbase = ms->vbase;

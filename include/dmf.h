@@ -58,6 +58,8 @@ typedef enum {
 /* dmf_opts.flags bits */
 #define DMF_FLAG_TRACE 1 /* record a per-phase device timeline (dmf_trace_get) */
 #define DMF_FLAG_PROBE 2 /* with TRACE: also time every work item (dmf_trace_items) */
+#define DMF_FLAG_FIXED_INTERVAL 4 /* exactly relabel_interval push rounds per global relabel
+                                     (default: at least the depth of the last relabel BFS) */
 
 typedef struct dmf_graph dmf_graph;   /* host CSR, owned by the library */
 typedef struct dmf_solver dmf_solver; /* device-resident residual state */

@@ -72,6 +72,22 @@ def test_grid256_static_and_batch(dmf, oracle, variant):
         assert sv.recompute() == want1
 
 
+@pytest.mark.parametrize("fixed", [False, True])
+@pytest.mark.parametrize("interval", [1, 24, 400])
+def test_long_push_phases_keep_the_source_closed(dmf, oracle, interval, fixed):
+    """Many push rounds between global relabels lift vertices far above their
+    BFS distance; excess must still never drain back into s (a source with a
+    finite label lets it, and the solve then ends with an augmenting path)."""
+    g, s, t, (batch,) = make_config("grid256")
+    off, adj, w, par = g.arrays()
+    want0 = oracle.dinic(g.num_nodes(), off, adj, w, par, s, t)
+    with dmf.Solver(g, s, t, relabel_interval=interval, fixed_interval=fixed) as sv:
+        assert sv.static_maxflow() == want0
+        certify(oracle, g, sv, s, t, want0)
+        cap, res, ex, h = sv.state()
+        assert h[s] >= g.num_nodes()
+
+
 @pytest.mark.parametrize("name", ["rmat12", "rmat14"])
 @pytest.mark.parametrize("variant", VARIANTS)
 def test_rmat_successive_batches(dmf, oracle, name, variant):
