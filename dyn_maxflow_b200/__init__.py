@@ -353,7 +353,8 @@ class Solver:
     def trace(self):
         """[(phase kind, end time in us since kernel start)] of the last solve (trace=True)."""
         cnt = C.c_int32()
-        cap = 8192
+        _check(_L.dmf_trace_get(self._h, 0, np.zeros(1, np.int32), np.zeros(1), C.byref(cnt)))
+        cap = max(cnt.value, 1)
         kinds = np.zeros(cap, np.int32)
         t = np.zeros(cap, np.float64)
         _check(_L.dmf_trace_get(self._h, cap, kinds, t, C.byref(cnt)))

@@ -40,8 +40,8 @@ struct Slot {
 
 // Control block of one solver (device memory, cleared before every launch).
 struct Ctrl {
-  unsigned int bar_count;
-  unsigned int bar_gen;
+  unsigned int bar_count;     // grid barrier: arrivals (low bits) and generation (top bit)
+  unsigned int bar_gen;       // unused
   int err;
   int err_info;
   Slot slot[3];
@@ -80,35 +80,51 @@ __device__ __forceinline__ long long atomic_add_ll(long long *p, long long v) {
 
 // ---- bounded grid barrier ---------------------------------------------------
 // All blocks of a cooperative launch call it the same number of times.  Thread
-// 0 of each block arrives on a counter; the last arrival resets it and bumps the
-// generation.  Waiters poll with a time limit and leave early once any block
-// has set an error.  Returns false (uniformly per block) when an error is set.
-__device__ __forceinline__ bool grid_barrier(Ctrl *c) {
+// 0 of each block arrives with ONE atomic on bar_count: block 0 adds
+// 2^31 - (G - 1), every other block adds 1, so the counter's top bit flips
+// exactly when the last of the G blocks arrives (and the low bits return to
+// where they were: nothing has to be reset between barriers).  A waiter polls
+// until the top bit differs from the value its own arrival saw; a block that
+// is already in the next barrier cannot flip it back, because that flip needs
+// every block, the waiter included.  Polls check the error word and a 4 s
+// %globaltimer limit every 64 iterations.
+//
+// After the wait, warp 0 copies the whole control block into `snap` (shared
+// memory): the phase that follows reads the counters the previous phase
+// produced from there, so a phase costs G control-block reads instead of one
+// per warp on a single L2 line.  Returns false (uniformly per block) when an
+// error is set.
+__device__ __forceinline__ bool grid_barrier(Ctrl *c, Ctrl *snap) {
   __shared__ int s_err;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned gen = ld_acquire_u32(&c->bar_gen);
-    __threadfence();
-    unsigned prev = atomicAdd(&c->bar_count, 1u);
-    if (prev == gridDim.x - 1) {
-      atomicExch(&c->bar_count, 0u);
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) {
+      const unsigned nb = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
       __threadfence();
-      atomicAdd(&c->bar_gen, 1u);
-    } else {
-      unsigned long long t0 = globaltimer();
-      unsigned ns = 32;
-      while (ld_acquire_u32(&c->bar_gen) == gen) {
-        if (ld_vol(&c->err)) break;
-        if (globaltimer() - t0 > kBarrierTimeoutNs) {
-          atomicOr(&c->err, ERR_TIMEOUT);
-          break;
+      const unsigned old = atomicAdd(&c->bar_count, nb);
+      unsigned long long t0 = 0;
+      int spins = 0;
+      while (((ld_acquire_u32(&c->bar_count) ^ old) & 0x80000000u) == 0) {
+        __nanosleep(32);
+        if ((++spins & 63) == 0) {
+          if (ld_vol(&c->err)) break;
+          const unsigned long long now = globaltimer();
+          if (!t0) {
+            t0 = now;
+          } else if (now - t0 > kBarrierTimeoutNs) {
+            atomicOr(&c->err, ERR_TIMEOUT);
+            break;
+          }
         }
-        __nanosleep(ns);
-        if (ns < 256) ns <<= 1;
       }
+      __threadfence();
     }
-    __threadfence();
-    s_err = ld_vol(&c->err);
+    __syncwarp();
+    const int *src = (const int *)c;
+    int *dst = (int *)snap;
+    for (int w = threadIdx.x; w < (int)(sizeof(Ctrl) / 4); w += 32) dst[w] = __ldcg(src + w);
+    __syncwarp();
+    if (threadIdx.x == 0) s_err = snap->err;
   }
   __syncthreads();
   return s_err == 0;

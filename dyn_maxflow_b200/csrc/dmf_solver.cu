@@ -724,8 +724,7 @@ struct RoundIn {
   int nh;
 };
 
-__device__ __forceinline__ RoundIn round_inputs(const Params &p, int r) {
-  Ctrl *c = p.ctrl;
+__device__ __forceinline__ RoundIn round_inputs(const Params &p, const Ctrl *c, int r) {
   RoundIn in;
   if (p.variant == DMF_VARIANT_TOPO) {
     in.nlist = nullptr;
@@ -1157,12 +1156,12 @@ __device__ void pp_discharge(G &g, const Params &p, int v, int r, unsigned round
 }
 
 template <int TILE>
-__device__ void ph_pp_round(const Params &p, int r, unsigned round_id, LStats &ls) {
+__device__ void ph_pp_round(const Params &p, const Ctrl *sc, int r, unsigned round_id, LStats &ls) {
   Ctrl *c = p.ctrl;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   if (gt == 0) c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
   const int *list = r == 0 ? p.aq : p.wq[(r - 1) & 1];
-  const int nn = r == 0 ? ld_vol(&c->act_q) : ld_vol(&c->wtail[(r - 1) % 3]);
+  const int nn = r == 0 ? sc->act_q : sc->wtail[(r - 1) % 3];
   // small vertices by a lane, medium ones by a tile; hubs wait for phase 2
   const int nt = gridDim.x * blockDim.x;
   for (int i = gt; i < nn; i += nt) {
@@ -1187,14 +1186,17 @@ __device__ void ph_pp_round(const Params &p, int r, unsigned round_id, LStats &l
 
 template <int TILE, int BLOCK>
 __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Temp &btmp, int *bci,
-                    long long *bcl) {
+                    long long *bcl, Ctrl *sc) {
+  // c: the control block in global memory (atomics, writes by the lead);
+  // sc: this block's copy taken at the last barrier, for every read of a count
+  // the previous phase produced
   Ctrl *c = p.ctrl;
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   int ph = 0;
   int kind = 0;  // phase kind, recorded in the optional timeline
   long long items = 0, hubitems = 0;  // work of the phase, recorded with it
   auto slot_out = [&]() { return &c->slot[ph % 3]; };
-  auto slot_in = [&]() { return &c->slot[(ph + 2) % 3]; };
+  auto slot_in = [&]() { return &sc->slot[(ph + 2) % 3]; };
   auto record = [&]() {
     if (lead && p.trace && ph < p.trace_cap) {
       p.trace[4 * ph] = (unsigned long long)kind | ((unsigned long long)(items & 0xffffffffll) << 8) |
@@ -1211,7 +1213,7 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
       if (w.thread_rank() == 0 && mx) atomicMax(&c->probe[ph & 1], mx);
       ls.probe = 0;
     }
-    if (!grid_barrier(c)) return false;
+    if (!grid_barrier(c, sc)) return false;
     ph++;
     record();
     if (lead) clear_slot(&c->slot[(ph + 1) % 3]);
@@ -1270,16 +1272,16 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
       items = hubitems = 0;
       ph_pp_init(p, slot_out());
       if (!next()) return;
-      const int P = ld_vol(&c->pos_count);
+      const int P = sc->pos_count;
       int reached = 0;
       for (int L = 0;; L++) {
         const Slot *in = slot_in();
-        const int F = ld_vol(&in->q) + ld_vol(&in->hq);
-        reached += ld_vol(&in->cnt);
+        const int F = in->q + in->hq;
+        reached += in->cnt;
         if (F == 0 || P == 0 || reached == P) break;
         kind = TR_PP_BFS;
-        items = ld_vol(&in->q);
-        hubitems = ld_vol(&in->hq);
+        items = in->q;
+        hubitems = in->hq;
         ph_pp_bfs<TILE>(p, in, slot_out(), L, ls);
         if (!next()) return;
       }
@@ -1287,17 +1289,17 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
       items = hubitems = 0;
       ph_pp_finalize(p);
       if (!next()) return;
-      const int A = ld_vol(&c->act_q);
+      const int A = sc->act_q;
       if (A == 0) break;
       for (int r = 0; r < p.interval; r++) {
         round_id++;
         kind = TR_PP_ROUND;
-        items = r == 0 ? A : ld_vol(&c->wtail[(r - 1) % 3]);
+        items = r == 0 ? A : sc->wtail[(r - 1) % 3];
         hubitems = 0;
-        ph_pp_round<TILE>(p, r, round_id, ls);
+        ph_pp_round<TILE>(p, sc, r, round_id, ls);
         if (!next()) return;
         if (lead) c->rounds_used = round_id - p.round_base;
-        if (ld_vol(&c->wtail[r % 3]) == 0) break;
+        if (sc->wtail[r % 3] == 0) break;
       }
     }
   }
@@ -1315,17 +1317,17 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
     ph_bfs_init(p, slot_out(), it == 0);
     if (!next()) return;
     if (lead) c->st_outer++;
-    const int P = ld_vol(&c->pos_count);
+    const int P = sc->pos_count;
     const bool want_cut = p.need_cut || cut_only;
     if (P == 0 && !want_cut) break;
-    long long m_u = ld_vol(&c->unexplored);
+    long long m_u = sc->unexplored;
     bool bu = false, full = true;
     int L = 0, reached = 0;
     for (;; L++) {
       const Slot *in = slot_in();
-      const int F = ld_vol(&in->q) + ld_vol(&in->hq);
-      const long long m_f = ld_vol(&in->arcs);
-      reached += ld_vol(&in->cnt);
+      const int F = in->q + in->hq;
+      const long long m_f = in->arcs;
+      reached += in->cnt;
       if (F == 0) break;  // complete
       if (!cut_only && P > 0 && reached == P) {
         full = false;  // every active vertex has its exact distance
@@ -1335,8 +1337,8 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
       if (!bu && p.bu_alpha > 0 && m_f * p.bu_alpha > m_u) bu = true;
       else if (bu && (long long)F * 24 < p.n) bu = false;
       kind = bu ? TR_BFS_BU : TR_BFS_TD;
-      items = ld_vol(&in->q);
-      hubitems = ld_vol(&in->hq);
+      items = in->q;
+      hubitems = in->hq;
       if (bu) ph_bfs_bu<TILE>(p, slot_out(), L, ls);
       else ph_bfs_td<TILE>(p, in, slot_out(), L, ls);
       if (!next()) return;
@@ -1346,7 +1348,7 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
     items = hubitems = 0;
     ph_bfs_finalize(p, full, L + 1, full && want_cut);
     if (!next()) return;
-    const int A = ld_vol(&c->act_q) + ld_vol(&c->act_hq);
+    const int A = sc->act_q + sc->act_hq;
     if (A == 0 || cut_only) break;
     // a global relabel costs about one phase per BFS level and a push round moves
     // excess about one hop: on deep graphs (grids) allow as many rounds as the
@@ -1355,7 +1357,7 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
     const int rounds = (p.interval > L || !p.adaptive) ? p.interval : L;
     for (int r = 0; r < rounds; r++) {
       round_id++;
-      const RoundIn in = round_inputs(p, r);
+      const RoundIn in = round_inputs(p, sc, r);
       kind = TR_PUSH;
       items = in.nn;
       hubitems = in.nh;
@@ -1373,7 +1375,7 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
         c->st_rounds++;
         c->rounds_used = round_id - p.round_base;
       }
-      const int W = topo ? ld_vol(&c->seen[r % 3]) : ld_vol(&c->wtail[r % 3]) + ld_vol(&c->whtail[r % 3]);
+      const int W = topo ? sc->seen[r % 3] : sc->wtail[r % 3] + sc->whtail[r % 3];
       if (W == 0) break;
     }
   }
@@ -1390,8 +1392,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_solve(Params p) {
   __shared__ typename BlockGroup<BLOCK>::Temp btmp;
   __shared__ int bci;
   __shared__ long long bcl;
+  __shared__ Ctrl snap;
   LStats ls;
-  run<TILE, BLOCK>(p, ls, btmp, &bci, &bcl);
+  run<TILE, BLOCK>(p, ls, btmp, &bci, &bcl, &snap);
   // statistics: one atomic per block and counter
   __syncthreads();
   typedef cub::BlockReduce<unsigned long long, BLOCK> R;
@@ -2078,7 +2081,7 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
         return bail(cuda_fail(cudaGetLastError(), "batched-instance upload"));
     }
   }
-  sv->trace_cap = 8192;
+  sv->trace_cap = 1 << 16;
   if ((st = dalloc(sv, &sv->trace, 4 * (size_t)sv->trace_cap))) return bail(st);
   *out = sv;
   return ok();
