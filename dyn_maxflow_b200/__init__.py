@@ -96,6 +96,7 @@ _sig("dmf_stats_get", C.c_int, VP, C.POINTER(Stats))
 _sig("dmf_trace_get", C.c_int, VP, C.c_int32, I32P, np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"),
      C.POINTER(C.c_int32))
 _sig("dmf_trace_items", C.c_int, VP, C.c_int32, I64P, I64P, I64P, I64P)
+_sig("dmf_trace_blocks", C.c_int, VP, C.c_int32, I64P)
 _sig("dmf_solver_set_opts", C.c_int, VP, C.POINTER(Opts))
 _sig("dmf_solver_destroy", C.c_int, VP)
 _sig("dmf_device_count", C.c_int)
@@ -364,7 +365,11 @@ class Solver:
         sns = np.zeros(max(n, 1), np.int64)
         sv_ = np.zeros(max(n, 1), np.int64)
         _check(_L.dmf_trace_items(self._h, n, items, hubs, sns, sv_))
-        self.last_trace_items = list(zip(items[:n].tolist(), hubs[:n].tolist(), sns[:n].tolist(), sv_[:n].tolist()))
+        blk = np.zeros(max(n, 1), np.int64)
+        _check(_L.dmf_trace_blocks(self._h, n, blk))
+        # per phase: (items, hub chunks, longest item ns, its vertex, longest block work ns)
+        self.last_trace_items = list(zip(items[:n].tolist(), hubs[:n].tolist(), sns[:n].tolist(), sv_[:n].tolist(),
+                                         blk[:n].tolist()))
         return [(self.TRACE_KINDS.get(int(k), str(k)), float(x)) for k, x in zip(kinds[:n], t[:n])]
 
     def stats(self) -> dict:

@@ -59,6 +59,7 @@ struct Ctrl {
   int wtail[3], whtail[3], seen[3];
   int pad1;
   unsigned long long probe[2];  // longest work item of a phase, (ns << 32) | vertex
+  unsigned long long blk[2];    // longest block work of a phase (ns), barrier exit to arrival
 };
 
 // ---- memory helpers ---------------------------------------------------------
@@ -128,6 +129,21 @@ __device__ __forceinline__ bool grid_barrier(Ctrl *c, Ctrl *snap) {
   }
   __syncthreads();
   return s_err == 0;
+}
+
+// ---- work-item numbering ----------------------------------------------------
+// Worklist items are numbered blocks first: thread t of block b is worker
+// t * G + b (G blocks), so items 0 .. G-1 go to G different blocks -- every SM
+// -- before any block takes a second one.  A short list (a BFS level on a
+// grid, a push round late in a solve) is then worked on by all SMs at once
+// instead of filling the first blocks, whose load/store units would serialise
+// its scattered accesses.  Loops over every vertex keep the contiguous
+// numbering, which keeps their per-vertex array accesses coalesced.
+__device__ __forceinline__ int spread_thread() { return threadIdx.x * gridDim.x + blockIdx.x; }
+// The same for groups of T consecutive threads (T divides the block size).
+template <int T>
+__device__ __forceinline__ int spread_group() {
+  return (int)(threadIdx.x / T) * gridDim.x + blockIdx.x;
 }
 
 // ---- queue append (warp-aggregated) -----------------------------------------

@@ -102,6 +102,7 @@ struct Params {
 struct LStats {
   unsigned long long pushes = 0, relabels = 0, arcs = 0, visits = 0;
   unsigned long long probe = 0;  // (longest single item in ns << 32) | vertex, this phase
+  unsigned long long t_phase = 0;  // thread 0: when this block left the last barrier
 };
 
 // Optional probe (DMF_FLAG_PROBE): times every work item and keeps the longest.
@@ -133,7 +134,7 @@ __device__ __forceinline__ void set_err(Ctrl *c, int bit, int info) {
 // ---- prologue phases ----------------------------------------------------------
 
 // staticMaxFlow_kernel_1 (code/dyn_data.h:25-35): residual = capacity, excess 0.
-__device__ void ph_init_res(const Params &p) {
+__device__ __forceinline__ void ph_init_res(const Params &p) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   for (int e = gt; e < p.m; e += nt) p.res[e] = __ldcg(p.cap + e);
   for (int v = gt; v < p.n; v += nt) p.excess[v] = 0;
@@ -152,7 +153,7 @@ __device__ __forceinline__ long long saturate_arc(const Params &p, int a) {
   return r;
 }
 
-__device__ void ph_saturate(const Params &p) {
+__device__ __forceinline__ void ph_saturate(const Params &p) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   if (!p.src_off) {
     for (int i = 0; i < p.nsrc; i++) {
@@ -193,8 +194,8 @@ __device__ void ph_saturate(const Params &p) {
 
 // Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201) by binary search over the
 // per-vertex head-sorted index; also validates the batch.
-__device__ void ph_lookup(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ph_lookup(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   for (int i = gt; i < p.k; i += nt) {
     int u = __ldg(p.usrc + i), v = __ldg(p.udst + i), w = __ldg(p.uw + i);
     p.uarc[i] = -1;
@@ -233,8 +234,8 @@ __device__ void ph_lookup(const Params &p) {
 
 // Capacity apply of OnAdd_kernel (code/dyn_data.h:202-205); in recompute mode
 // only the capacity is set (update_kernel, code/dyn_data_bench.cu:300-322).
-__device__ void ph_apply(const Params &p, bool residual) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ph_apply(const Params &p, bool residual) {
+  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   for (int i = gt; i < p.k; i += nt) {
     int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
@@ -250,8 +251,8 @@ __device__ void ph_apply(const Params &p, bool residual) {
 // went negative carries more flow than its new capacity; the excess is returned
 // to its tail and taken from its head.  At most one arc of a pair can be
 // negative because res(e) + res(partner) = cap(e) + cap(partner) >= 0.
-__device__ void ph_repair(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ph_repair(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   for (int i = gt; i < p.k; i += nt) {
     int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
@@ -268,8 +269,8 @@ __device__ void ph_repair(const Params &p) {
 // Push-pull: an updated arc that now has residual from the source side A into
 // the sink side B of the kept cut is saturated (the cut part of the fused
 // incremental_kernel_20, code/dyn_pp.h:422-432, limited to touched arcs).
-__device__ void ph_cut_saturate(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ph_cut_saturate(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   for (int i = gt; i < p.k; i += nt) {
     int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
@@ -294,7 +295,8 @@ __device__ void ph_cut_saturate(const Params &p) {
 // one per tile.  `f(group, v)` does the work for one vertex.
 template <int TILE, class F>
 __device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const int *list, int nn, F &&f) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nt = gridDim.x * blockDim.x;
+  const int gt = list ? spread_thread() : blockIdx.x * blockDim.x + threadIdx.x;
   for (int i = gt; i < nn; i += nt) {
     const int v = list ? __ldcg(list + i) : i;
     if (deg_of(p, v) > p.small_deg) continue;
@@ -304,7 +306,8 @@ __device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const in
     tm.done(ls, v);
   }
   TileGroup<TILE> tg;
-  for (int i = gt / TILE; i < nn; i += nt / TILE) {
+  const int gi = list ? spread_group<TILE>() : (int)((blockIdx.x * blockDim.x + threadIdx.x) / TILE);
+  for (int i = gi; i < nn; i += nt / TILE) {
     int v = 0, d = 0;
     if (tg.rank() == 0) {
       v = list ? __ldcg(list + i) : i;
@@ -343,7 +346,7 @@ __device__ __forceinline__ void chunk_range(const Params &p, int2 it, int &beg, 
 
 // Seeds (my_init_1, code/dyn_data.h:60-67): t and every deficit vertex other
 // than s get height 0; all other live vertices become unvisited.
-__device__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
+__device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   Ctrl *c = p.ctrl;
   if (gt == 0) {
@@ -476,12 +479,12 @@ __device__ __forceinline__ void td_range(const Params &p, Slot *out, int nxt, in
 }
 
 template <int TILE>
-__device__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
+__device__ __forceinline__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
   const int cur = L & 1, nxt = cur ^ 1;
   const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
   VisitAcc acc;
   const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nh; i += nwarps) {
+  for (int i = spread_group<32>(); i < nh; i += nwarps) {
     int beg, end;
     const int2 it = __ldcg(p.fh[cur] + i);
     ItemTimer tm(p);
@@ -519,13 +522,13 @@ __device__ __forceinline__ bool bu_batch(const Params &p, int first, int end, in
 // L and stops at the first one.  Hub chunks are searched by warps (the first
 // chunk of a hub to succeed labels it); other vertices by a lane or a tile.
 template <int TILE>
-__device__ void ph_bfs_bu(const Params &p, Slot *out, int L, LStats &ls) {
+__device__ __forceinline__ void ph_bfs_bu(const Params &p, Slot *out, int L, LStats &ls) {
   const int nxt = (L & 1) ^ 1;
   VisitAcc acc;
   {
     TileGroup<32> wg;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < p.nhch; i += nwarps) {
+    for (int i = spread_group<32>(); i < p.nhch; i += nwarps) {
       const int2 it = __ldg(p.hch + i);
       int hv = 0;
       if (wg.rank() == 0) hv = __ldcg(p.height + it.x);
@@ -558,7 +561,7 @@ __device__ void ph_bfs_bu(const Params &p, Slot *out, int L, LStats &ls) {
 // After the BFS: a complete BFS proves every unvisited vertex unreachable
 // (dead for the rest of this solve; the reference gives them height V); an
 // early-stopped BFS gives them the valid lower bound `floor`.
-__device__ void ph_bfs_finalize(const Params &p, bool full, int floor_h, bool write_side) {
+__device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int floor_h, bool write_side) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   int nd = 0;
   for (int v = gt; v < p.n; v += nt) {
@@ -597,6 +600,117 @@ __device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, i
   if (enq && !is_term(p, w) && old + d > 0) enqueue(p, r, round_id, w);
 }
 
+// Reserves `cnt` consecutive slots behind *tail for this thread with one atomic
+// per group of threads that call it together.
+__device__ __forceinline__ int reserve(int *tail, int cnt) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  const int pre = cg::exclusive_scan(g, cnt, cg::plus<int>());
+  int base = 0;
+  if (g.thread_rank() == g.size() - 1) base = atomicAdd(tail, pre + cnt);
+  return g.shfl(base, g.size() - 1) + pre;
+}
+
+// Adjacency bound of the register-resident thread discharge below.
+constexpr int kSmallMax = 8;
+
+// Discharge of a vertex of degree <= kSmallMax by one thread, with the same
+// push/relabel rule as discharge() but laid out for latency: per cycle the
+// residuals and head heights of all arcs are loaded together, the pushes are
+// decided in registers (excess spread over the admissible arcs in arc order),
+// and every atomic of the cycle is in flight before any result is used; the
+// heads that became active are deduplicated by their stamps together and
+// appended with one reservation.  A head height may be one load old when it is
+// used (a concurrent relabel only raises it), which can leave a label above
+// the exact distance for a while; labels only steer the pushes -- dead
+// vertices and termination are decided by the exact BFS of each relabel.
+__device__ __forceinline__ void discharge_small(const Params &p, int v, int beg, int deg, long long ex0, int h, int r,
+                                unsigned round_id, bool enq, LStats &ls) {
+  int rr[kSmallMax], w[kSmallMax], hw[kSmallMax];
+#pragma unroll
+  for (int k = 0; k < kSmallMax; k++) {
+    rr[k] = k < deg ? __ldcg(p.res + beg + k) : 0;
+    w[k] = k < deg ? __ldg(p.adj + beg + k) : 0;
+  }
+  unsigned cand = 0;  // bit k: head k may have become active; bit kSmallMax: v itself
+  long long ex = ex0;
+  for (int cyc = 0; cyc < p.cycles && ex > 0 && h < p.n; cyc++) {
+    if (cyc > 0) {
+#pragma unroll
+      for (int k = 0; k < kSmallMax; k++)
+        if (k < deg) rr[k] = __ldcg(p.res + beg + k);
+    }
+#pragma unroll
+    for (int k = 0; k < kSmallMax; k++) hw[k] = k < deg ? __ldcg(p.height + w[k]) : INT_MAX;
+    ls.arcs += deg;
+    int dd[kSmallMax];
+    long long left = ex;
+#pragma unroll
+    for (int k = 0; k < kSmallMax; k++) {
+      dd[k] = 0;
+      if (rr[k] > 0 && hw[k] < h && left > 0) {
+        dd[k] = (int)(rr[k] < left ? rr[k] : left);
+        left -= dd[k];
+      }
+    }
+    long long old[kSmallMax];
+#pragma unroll
+    for (int k = 0; k < kSmallMax; k++)
+      if (dd[k] > 0) {
+        atomicSub(p.res + beg + k, dd[k]);
+        old[k] = atomic_add_ll(p.excess + w[k], dd[k]);
+      }
+#pragma unroll
+    for (int k = 0; k < kSmallMax; k++)
+      if (dd[k] > 0) {
+        atomicAdd(p.res + __ldg(p.par + beg + k), dd[k]);
+        rr[k] -= dd[k];
+        ls.pushes++;
+        if (enq && !is_term(p, w[k]) && old[k] + dd[k] > 0) cand |= 1u << k;
+      }
+    ex = left;
+    if (ex > 0) {  // every admissible arc is saturated: relabel
+      int mh = INT_MAX;
+#pragma unroll
+      for (int k = 0; k < kSmallMax; k++)
+        if (rr[k] > 0) mh = min(mh, hw[k]);
+      h = mh >= p.n ? p.n : mh + 1;
+      p.height[v] = h;
+      ls.relabels++;
+    }
+  }
+  if (ex0 != ex) atomic_add_ll(p.excess + v, ex - ex0);
+  if (enq && ex > 0 && h < p.n) cand |= 1u << kSmallMax;
+  if (!cand) return;
+  // stamps of all candidates in flight together, then their degrees
+  unsigned keep = 0;
+#pragma unroll
+  for (int k = 0; k <= kSmallMax; k++)
+    if ((cand >> k) & 1) {
+      const int x = k < kSmallMax ? w[k] : v;
+      if (atomicExch(p.stamp + x, (int)round_id) != (int)round_id) keep |= 1u << k;
+    }
+  if (!keep) return;
+  int cnt = 0;
+  unsigned small = 0;
+#pragma unroll
+  for (int k = 0; k <= kSmallMax; k++)
+    if ((keep >> k) & 1) {
+      const int x = k < kSmallMax ? w[k] : v;
+      if (deg_of(p, x) > p.hub_deg) {
+        append_hub(p, p.wh[r & 1], &p.ctrl->whtail[r % 3], x);
+      } else {
+        small |= 1u << k;
+        cnt++;
+      }
+    }
+  if (!cnt) return;
+  int pos = reserve(&p.ctrl->wtail[r % 3], cnt);
+  int *q = p.wq[r & 1];
+#pragma unroll
+  for (int k = 0; k <= kSmallMax; k++)
+    if ((small >> k) & 1) q[pos++] = k < kSmallMax ? w[k] : v;
+}
+
 // Discharge of a non-hub v by a lane or a tile: up to `cycles` rounds of
 // push-then-relabel, the push/relabel of staticMaxFlow_kernel_14
 // (code/dyn_data.h:89-131) with every admissible arc (head below h) used per
@@ -612,7 +726,7 @@ __device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, i
 // raise heights, so a pass-2 arc that lost admissibility is skipped and the
 // round is retried instead of relabelled.
 template <class G>
-__device__ void discharge(G &g, const Params &p, int v, int r, unsigned round_id, bool enq, LStats &ls,
+__device__ __forceinline__ void discharge(G &g, const Params &p, int v, int r, unsigned round_id, bool enq, LStats &ls,
                           int *seen) {
   long long ex0;
   int h;
@@ -638,6 +752,12 @@ __device__ void discharge(G &g, const Params &p, int v, int r, unsigned round_id
   long long ex = ex0;
   const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
   constexpr int S = G::size();
+  if constexpr (S == 1) {
+    if (end - beg <= kSmallMax) {
+      discharge_small(p, v, beg, end - beg, ex0, h, r, round_id, enq, ls);
+      return;
+    }
+  }
   for (int cyc = 0; cyc < p.cycles && ex > 0 && h < p.n; cyc++) {
     if (end - beg <= S) {
       const int a = beg + g.rank();
@@ -749,7 +869,7 @@ __device__ __forceinline__ RoundIn round_inputs(const Params &p, const Ctrl *c, 
 // chunk computes its admissible residual sum and its minimum non-admissible
 // height (chunk 0 also snapshots the hub's excess and clears its totals).
 template <int TILE, int BLOCK>
-__device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned round_id, unsigned gepoch, LStats &ls,
+__device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned round_id, unsigned gepoch, LStats &ls,
                          typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
   Ctrl *c = p.ctrl;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -764,7 +884,7 @@ __device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned rou
   {
     TileGroup<32> wg;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = gt >> 5; i < in.nh; i += nwarps) {
+    for (int i = spread_group<32>(); i < in.nh; i += nwarps) {
       const int2 it = __ldcg(in.hlist + i);
       const int v = it.x;
       ItemTimer tmr(p);
@@ -837,12 +957,12 @@ __device__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned rou
 // arcs: lane budgets from a warp prefix sum, then a greedy pass.  The same
 // atomics leave the hub's total admissible residual, minimum non-admissible
 // height and moved amount at its first chunk.
-__device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned round_id, unsigned gepoch,
+__device__ __forceinline__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned round_id, unsigned gepoch,
                          LStats &ls) {
   const bool topo = p.variant == DMF_VARIANT_TOPO;
   TileGroup<32> wg;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < in.nh; i += nwarps) {
+  for (int i = spread_group<32>(); i < in.nh; i += nwarps) {
     const int2 it = __ldcg(in.hlist + i);
     const int v = it.x, base = i - it.y;
     long long e0 = 0, old = 0, mine = 0;
@@ -912,11 +1032,11 @@ __device__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned rou
 // excess; when all of the hub's admissible residual was pushed and excess is
 // left, the hub is relabelled to 1 + the minimum non-admissible height; a hub
 // with excess left is queued for the next round.
-__device__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls) {
+  const int nt = gridDim.x * blockDim.x;
   const bool topo = p.variant == DMF_VARIANT_TOPO;
   int seen = 0;
-  for (int i = gt; i < in.nh; i += nt) {
+  for (int i = spread_thread(); i < in.nh; i += nt) {
     const int2 it = __ldcg(in.hlist + i);
     if (it.y != 0) continue;
     const int v = it.x;
@@ -944,7 +1064,7 @@ __device__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned rou
 // flow = excess(t) + sum of negative excess over v != s, t (per instance in
 // batched mode).
 template <int BLOCK>
-__device__ void ph_flow(const Params &p, typename BlockGroup<BLOCK>::Temp &btmp) {
+__device__ __forceinline__ void ph_flow(const Params &p, typename BlockGroup<BLOCK>::Temp &btmp) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   long long acc = 0;
   for (int v = gt; v < p.n; v += nt) {
@@ -986,7 +1106,7 @@ __device__ __forceinline__ bool pp_active(const Params &p, int v, long long ex) 
 }
 
 // Seeds (pp_bfs_init, code/dyn_pp.h:76-83): t, B's deficits and A's excess.
-__device__ void ph_pp_init(const Params &p, Slot *out) {
+__device__ __forceinline__ void ph_pp_init(const Params &p, Slot *out) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   Ctrl *c = p.ctrl;
   if (gt == 0) {
@@ -1035,12 +1155,12 @@ __device__ __forceinline__ void pp_td_range(const Params &p, Slot *out, int nxt,
 }
 
 template <int TILE>
-__device__ void ph_pp_bfs(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
+__device__ __forceinline__ void ph_pp_bfs(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
   const int cur = L & 1, nxt = cur ^ 1;
   const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
   VisitAcc acc;
   const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nh; i += nwarps) {
+  for (int i = spread_group<32>(); i < nh; i += nwarps) {
     const int2 it = __ldcg(p.fh[cur] + i);
     int beg, end;
     chunk_range(p, it, beg, end);
@@ -1055,7 +1175,7 @@ __device__ void ph_pp_bfs(const Params &p, const Slot *in, Slot *out, int L, LSt
 
 // Unlabelled vertices cannot reach a target within their side: inactive for
 // phase 1 (not dead: the general solve decides that).
-__device__ void ph_pp_finalize(const Params &p) {
+__device__ __forceinline__ void ph_pp_finalize(const Params &p) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   if (gt == 0) p.ctrl->pos_count = 0;  // read by every block before this phase
   for (int v = gt; v < p.n; v += nt)
@@ -1073,7 +1193,7 @@ __device__ __forceinline__ void pp_enqueue(const Params &p, int r, unsigned roun
 // the other residual arcs; a group prefix sum gives lane budgets; pass 2 moves
 // them.  A pull of d from w along w->v lowers res(w->v) and excess(w).
 template <class G>
-__device__ void pp_discharge(G &g, const Params &p, int v, int r, unsigned round_id, LStats &ls) {
+__device__ __forceinline__ void pp_discharge(G &g, const Params &p, int v, int r, unsigned round_id, LStats &ls) {
   long long e0 = 0;
   int hh = 0;
   if (g.rank() == 0) {
@@ -1156,7 +1276,7 @@ __device__ void pp_discharge(G &g, const Params &p, int v, int r, unsigned round
 }
 
 template <int TILE>
-__device__ void ph_pp_round(const Params &p, const Ctrl *sc, int r, unsigned round_id, LStats &ls) {
+__device__ __forceinline__ void ph_pp_round(const Params &p, const Ctrl *sc, int r, unsigned round_id, LStats &ls) {
   Ctrl *c = p.ctrl;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   if (gt == 0) c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
@@ -1164,14 +1284,14 @@ __device__ void ph_pp_round(const Params &p, const Ctrl *sc, int r, unsigned rou
   const int nn = r == 0 ? sc->act_q : sc->wtail[(r - 1) % 3];
   // small vertices by a lane, medium ones by a tile; hubs wait for phase 2
   const int nt = gridDim.x * blockDim.x;
-  for (int i = gt; i < nn; i += nt) {
+  for (int i = spread_thread(); i < nn; i += nt) {
     const int v = __ldcg(list + i);
     if (deg_of(p, v) > p.small_deg) continue;
     ThreadGroup th;
     pp_discharge(th, p, v, r, round_id, ls);
   }
   TileGroup<TILE> tg;
-  for (int i = gt / TILE; i < nn; i += nt / TILE) {
+  for (int i = spread_group<TILE>(); i < nn; i += nt / TILE) {
     int v = 0, d = 0;
     if (tg.rank() == 0) {
       v = __ldcg(list + i);
@@ -1185,7 +1305,7 @@ __device__ void ph_pp_round(const Params &p, const Ctrl *sc, int r, unsigned rou
 }
 
 template <int TILE, int BLOCK>
-__device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Temp &btmp, int *bci,
+__device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Temp &btmp, int *bci,
                     long long *bcl, Ctrl *sc) {
   // c: the control block in global memory (atomics, writes by the lead);
   // sc: this block's copy taken at the last barrier, for every read of a count
@@ -1203,7 +1323,9 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
                         ((unsigned long long)(hubitems & 0xffffff) << 40);
       p.trace[4 * ph + 1] = globaltimer();
       p.trace[4 * ph + 2] = ph > 0 ? ld_vol((const long long *)&c->probe[(ph + 1) & 1]) : 0;
+      p.trace[4 * ph + 3] = ph > 0 ? ld_vol((const long long *)&c->blk[(ph + 1) & 1]) : 0;
       c->probe[(ph + 1) & 1] = 0;
+      c->blk[(ph + 1) & 1] = 0;
     }
   };
   auto next = [&]() -> bool {
@@ -1212,8 +1334,11 @@ __device__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Tem
       const unsigned long long mx = cg::reduce(w, ls.probe, cg::greater<unsigned long long>());
       if (w.thread_rank() == 0 && mx) atomicMax(&c->probe[ph & 1], mx);
       ls.probe = 0;
+      __syncthreads();  // the block's work of this phase is done
+      if (threadIdx.x == 0 && ls.t_phase) atomicMax(&c->blk[ph & 1], globaltimer() - ls.t_phase);
     }
     if (!grid_barrier(c, sc)) return false;
+    if (p.probe && threadIdx.x == 0) ls.t_phase = globaltimer();
     ph++;
     record();
     if (lead) clear_slot(&c->slot[(ph + 1) % 3]);
@@ -2460,6 +2585,18 @@ int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs, 
     if (slow_ns) slow_ns[i] = (int64_t)(h[4 * i + 2] >> 32);
     if (slow_v) slow_v[i] = (int64_t)(h[4 * i + 2] & 0xffffffffull);
   }
+  return ok();
+}
+
+int dmf_trace_blocks(dmf_solver *sv, int32_t cap, int64_t *block_ns) {
+  if (!sv || cap < 0 || (cap > 0 && !block_ns)) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  const int len = std::min(std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap), cap);
+  if (len <= 0) return ok();
+  std::vector<unsigned long long> h(4 * (size_t)len);
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  CK(cudaMemcpyAsync(h.data(), sv->trace, 32 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
+  CK(cudaStreamSynchronize(sv->stream), "trace");
+  for (int i = 0; i < len; i++) block_ns[i] = (int64_t)h[4 * i + 3];
   return ok();
 }
 

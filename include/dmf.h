@@ -221,6 +221,10 @@ int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us,
  * longest single work item (slow_ns / slow_v may be NULL). */
 int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs,
                     int64_t *slow_ns, int64_t *slow_v);
+/* With DMF_FLAG_PROBE: block_ns[i] = the longest time any block spent on phase
+ * i's work (from leaving the previous grid barrier to arriving at the next);
+ * the phase's duration minus this is barrier and skew. */
+int dmf_trace_blocks(dmf_solver *sv, int32_t cap, int64_t *block_ns);
 /* Replaces the option set of a live solver (variant, cycles, interval, tile). */
 int dmf_solver_set_opts(dmf_solver *sv, const dmf_opts *opts);
 int dmf_solver_destroy(dmf_solver *sv);
