@@ -139,12 +139,26 @@ __device__ __forceinline__ bool grid_barrier(Ctrl *c, Ctrl *snap) {
 // instead of filling the first blocks, whose load/store units would serialise
 // its scattered accesses.  Loops over every vertex keep the contiguous
 // numbering, which keeps their per-vertex array accesses coalesced.
-__device__ __forceinline__ int spread_thread() { return threadIdx.x * gridDim.x + blockIdx.x; }
-// The same for groups of T consecutive threads (T divides the block size).
-template <int T>
-__device__ __forceinline__ int spread_group() {
-  return (int)(threadIdx.x / T) * gridDim.x + blockIdx.x;
+// `rot` rotates the order inside a block so that thread `rot` takes a block's
+// first item: the kinds of work of one phase (hub chunks, one-thread items,
+// tile items) start on different warps and run side by side when the lists are
+// short, instead of queueing on warp 0.
+__device__ __forceinline__ int spread_thread(int rot = 0) {
+  const int t = (int)threadIdx.x - rot;
+  return (t < 0 ? t + (int)blockDim.x : t) * gridDim.x + blockIdx.x;
 }
+// The same for groups of T consecutive threads (T divides the block size and
+// `rot`).
+template <int T>
+__device__ __forceinline__ int spread_group(int rot = 0) {
+  const int t = (int)threadIdx.x - rot;
+  return ((t < 0 ? t + (int)blockDim.x : t) / T) * gridDim.x + blockIdx.x;
+}
+// Rotations used by the phases: hub chunks from warp 0, tile items from the
+// first warp of the second quarter of the block, one-thread items from the
+// middle.
+__device__ __forceinline__ int rot_tiles() { return (int)blockDim.x / 4; }
+__device__ __forceinline__ int rot_threads() { return (int)blockDim.x / 2; }
 
 // ---- queue append (warp-aggregated) -----------------------------------------
 __device__ __forceinline__ void append(int *q, int *tail, int v) {

@@ -296,7 +296,7 @@ __device__ __forceinline__ void ph_cut_saturate(const Params &p) {
 template <int TILE, class F>
 __device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const int *list, int nn, F &&f) {
   const int nt = gridDim.x * blockDim.x;
-  const int gt = list ? spread_thread() : blockIdx.x * blockDim.x + threadIdx.x;
+  const int gt = list ? spread_thread(rot_threads()) : blockIdx.x * blockDim.x + threadIdx.x;
   for (int i = gt; i < nn; i += nt) {
     const int v = list ? __ldcg(list + i) : i;
     if (deg_of(p, v) > p.small_deg) continue;
@@ -306,7 +306,7 @@ __device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const in
     tm.done(ls, v);
   }
   TileGroup<TILE> tg;
-  const int gi = list ? spread_group<TILE>() : (int)((blockIdx.x * blockDim.x + threadIdx.x) / TILE);
+  const int gi = list ? spread_group<TILE>(rot_tiles()) : (int)((blockIdx.x * blockDim.x + threadIdx.x) / TILE);
   for (int i = gi; i < nn; i += nt / TILE) {
     int v = 0, d = 0;
     if (tg.rank() == 0) {
@@ -600,6 +600,9 @@ __device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, i
   if (enq && !is_term(p, w) && old + d > 0) enqueue(p, r, round_id, w);
 }
 
+// Arcs a lane handles together in a tile discharge.
+constexpr int kPushBatch = 4;
+
 // Reserves `cnt` consecutive slots behind *tail for this thread with one atomic
 // per group of threads that call it together.
 __device__ __forceinline__ int reserve(int *tail, int cnt) {
@@ -608,6 +611,65 @@ __device__ __forceinline__ int reserve(int *tail, int cnt) {
   int base = 0;
   if (g.thread_rank() == g.size() - 1) base = atomicAdd(tail, pre + cnt);
   return g.shfl(base, g.size() - 1) + pre;
+}
+
+// Queues the heads x[k] marked in `cand` for round r+1 (each at most once per
+// round, by its stamp): all stamp exchanges in flight together, then all degree
+// reads, then one reservation for the non-hub heads (hubs go to the chunk queue).
+template <int K>
+__device__ __forceinline__ void enqueue_batch(const Params &p, const int (&x)[K], unsigned cand, int r,
+                                              unsigned round_id) {
+  unsigned keep = 0;
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if ((cand >> k) & 1)
+      if (atomicExch(p.stamp + x[k], (int)round_id) != (int)round_id) keep |= 1u << k;
+  if (!keep) return;
+  int dg[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) dg[k] = ((keep >> k) & 1) ? deg_of(p, x[k]) : 0;
+  int cnt = 0;
+  unsigned small = 0;
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if ((keep >> k) & 1) {
+      if (dg[k] > p.hub_deg) {
+        append_hub(p, p.wh[r & 1], &p.ctrl->whtail[r % 3], x[k]);
+      } else {
+        small |= 1u << k;
+        cnt++;
+      }
+    }
+  if (!cnt) return;
+  int pos = reserve(&p.ctrl->wtail[r % 3], cnt);
+  int *q = p.wq[r & 1];
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if ((small >> k) & 1) q[pos++] = x[k];
+}
+
+// Pushes d[k] > 0 units over arcs a[k] into heads w[k] (one lane's batch): the
+// residual and excess atomics of all arcs are in flight together, then the
+// partner residuals; heads whose excess became positive are queued (enq).
+template <int K>
+__device__ __forceinline__ void push_batch(const Params &p, const int (&a)[K], const int (&w)[K], const int (&d)[K],
+                                           int r, unsigned round_id, bool enq, LStats &ls) {
+  long long old[K];
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if (d[k] > 0) {
+      atomicSub(p.res + a[k], d[k]);
+      old[k] = atomic_add_ll(p.excess + w[k], d[k]);
+    }
+  unsigned cand = 0;
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if (d[k] > 0) {
+      atomicAdd(p.res + __ldg(p.par + a[k]), d[k]);
+      ls.pushes++;
+      if (enq && !is_term(p, w[k]) && old[k] + d[k] > 0) cand |= 1u << k;
+    }
+  if (cand) enqueue_batch<K>(p, w, cand, r, round_id);
 }
 
 // Adjacency bound of the register-resident thread discharge below.
@@ -681,34 +743,11 @@ __device__ __forceinline__ void discharge_small(const Params &p, int v, int beg,
   if (ex0 != ex) atomic_add_ll(p.excess + v, ex - ex0);
   if (enq && ex > 0 && h < p.n) cand |= 1u << kSmallMax;
   if (!cand) return;
-  // stamps of all candidates in flight together, then their degrees
-  unsigned keep = 0;
+  int x[kSmallMax + 1];
 #pragma unroll
-  for (int k = 0; k <= kSmallMax; k++)
-    if ((cand >> k) & 1) {
-      const int x = k < kSmallMax ? w[k] : v;
-      if (atomicExch(p.stamp + x, (int)round_id) != (int)round_id) keep |= 1u << k;
-    }
-  if (!keep) return;
-  int cnt = 0;
-  unsigned small = 0;
-#pragma unroll
-  for (int k = 0; k <= kSmallMax; k++)
-    if ((keep >> k) & 1) {
-      const int x = k < kSmallMax ? w[k] : v;
-      if (deg_of(p, x) > p.hub_deg) {
-        append_hub(p, p.wh[r & 1], &p.ctrl->whtail[r % 3], x);
-      } else {
-        small |= 1u << k;
-        cnt++;
-      }
-    }
-  if (!cnt) return;
-  int pos = reserve(&p.ctrl->wtail[r % 3], cnt);
-  int *q = p.wq[r & 1];
-#pragma unroll
-  for (int k = 0; k <= kSmallMax; k++)
-    if ((small >> k) & 1) q[pos++] = k < kSmallMax ? w[k] : v;
+  for (int k = 0; k < kSmallMax; k++) x[k] = w[k];
+  x[kSmallMax] = v;
+  enqueue_batch<kSmallMax + 1>(p, x, cand, r, round_id);
 }
 
 // Discharge of a non-hub v by a lane or a tile: up to `cycles` rounds of
@@ -790,34 +829,56 @@ __device__ __forceinline__ void discharge(G &g, const Params &p, int v, int r, u
       }
       continue;
     }
-    // pass 1
+    // pass 1 (batches of kPushBatch arcs a lane: heads and residuals, then head
+    // heights, each batch's loads in flight together)
     long long tsum = 0;
     int tmin = INT_MAX;
-#pragma unroll 4
-    for (int a = beg + g.rank(); a < end; a += S) {
-      const int rr = __ldcg(p.res + a);
-      if (rr > 0) {
-        const int hw = __ldcg(p.height + __ldg(p.adj + a));
-        if (hw < h) tsum += rr;
-        else tmin = min(tmin, hw);
+    for (int a0 = beg + g.rank(); a0 < end; a0 += kPushBatch * S) {
+      int rr[kPushBatch], w[kPushBatch];
+#pragma unroll
+      for (int k = 0; k < kPushBatch; k++) {
+        const int a = a0 + k * S;
+        rr[k] = a < end ? __ldcg(p.res + a) : 0;
+        w[k] = a < end ? __ldg(p.adj + a) : 0;
       }
+#pragma unroll
+      for (int k = 0; k < kPushBatch; k++)
+        if (rr[k] > 0) {
+          const int hw = __ldcg(p.height + w[k]);
+          if (hw < h) tsum += rr[k];
+          else tmin = min(tmin, hw);
+        }
     }
     ls.arcs += (unsigned long long)((end - beg - g.rank() + S - 1) / S);
     long long tot;
     const long long pre = g.scan(tsum, tot);
-    // pass 2
+    // pass 2: heights reread (a concurrent relabel may have made an arc
+    // inadmissible), the lane's budget spread greedily, each batch's pushes in
+    // flight together
     long long budget = ex - pre;
     budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
     long long done = 0;
-    for (int a = beg + g.rank(); a < end && budget > 0; a += S) {
-      const int rr = __ldcg(p.res + a);
-      if (rr <= 0) continue;
-      const int w = __ldg(p.adj + a);
-      if (__ldcg(p.height + w) >= h) continue;
-      const int d = (int)(rr < budget ? rr : budget);
-      push_arc(p, a, w, d, r, round_id, enq, ls);
-      budget -= d;
-      done += d;
+    for (int a0 = beg + g.rank(); a0 < end && budget > 0; a0 += kPushBatch * S) {
+      int aa[kPushBatch], rr[kPushBatch], w[kPushBatch], dd[kPushBatch];
+#pragma unroll
+      for (int k = 0; k < kPushBatch; k++) {
+        aa[k] = a0 + k * S;
+        rr[k] = aa[k] < end ? __ldcg(p.res + aa[k]) : 0;
+        w[k] = aa[k] < end ? __ldg(p.adj + aa[k]) : 0;
+      }
+      int hw[kPushBatch];
+#pragma unroll
+      for (int k = 0; k < kPushBatch; k++) hw[k] = rr[k] > 0 ? __ldcg(p.height + w[k]) : INT_MAX;
+#pragma unroll
+      for (int k = 0; k < kPushBatch; k++) {
+        dd[k] = 0;
+        if (hw[k] < h && budget > 0) {
+          dd[k] = (int)(rr[k] < budget ? rr[k] : budget);
+          budget -= dd[k];
+          done += dd[k];
+        }
+      }
+      push_batch<kPushBatch>(p, aa, w, dd, r, round_id, enq, ls);
     }
     const long long moved = g.sum_all(done);
     ex -= moved;
@@ -1007,15 +1068,18 @@ __device__ __forceinline__ void ph_push2(const Params &p, const RoundIn &in, int
     budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
     long long done = 0;
     // residuals only grew since the loads (reverse pushes), so rr is a safe amount
+    int aa[kBatch], dd[kBatch];
 #pragma unroll
     for (int k = 0; k < kBatch; k++) {
+      aa[k] = beg + wg.rank() + 32 * k;
+      dd[k] = 0;
       if (adm[k] && budget > 0) {
-        const int d = (int)(rr[k] < budget ? rr[k] : budget);
-        push_arc(p, beg + wg.rank() + 32 * k, w[k], d, r, round_id, !topo, ls);
-        budget -= d;
-        done += d;
+        dd[k] = (int)(rr[k] < budget ? rr[k] : budget);
+        budget -= dd[k];
+        done += dd[k];
       }
     }
+    push_batch<kBatch>(p, aa, w, dd, r, round_id, !topo, ls);
     const long long moved = wg.sum_all(done);
     if (wg.rank() == 0) {
       if (moved) atomic_add_ll(p.hc_moved + base, moved);
@@ -1284,14 +1348,14 @@ __device__ __forceinline__ void ph_pp_round(const Params &p, const Ctrl *sc, int
   const int nn = r == 0 ? sc->act_q : sc->wtail[(r - 1) % 3];
   // small vertices by a lane, medium ones by a tile; hubs wait for phase 2
   const int nt = gridDim.x * blockDim.x;
-  for (int i = spread_thread(); i < nn; i += nt) {
+  for (int i = spread_thread(rot_threads()); i < nn; i += nt) {
     const int v = __ldcg(list + i);
     if (deg_of(p, v) > p.small_deg) continue;
     ThreadGroup th;
     pp_discharge(th, p, v, r, round_id, ls);
   }
   TileGroup<TILE> tg;
-  for (int i = spread_group<TILE>(); i < nn; i += nt / TILE) {
+  for (int i = spread_group<TILE>(rot_tiles()); i < nn; i += nt / TILE) {
     int v = 0, d = 0;
     if (tg.rank() == 0) {
       v = __ldcg(list + i);
