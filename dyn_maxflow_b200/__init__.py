@@ -21,7 +21,7 @@ import numpy as np
 __all__ = [
     "DmfError", "Graph", "Solver", "Stats", "load_updates", "save_updates", "gen_grid", "gen_rmat",
     "gen_batches", "recalculate_max_flow", "static_recalculate", "device_count", "VARIANTS", "lib_path",
-    "static_maxflow_noalloc", "MultiSolver", "Server",
+    "static_maxflow_noalloc", "MultiSolver", "Server", "Scheduler", "ACTIONS",
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -112,6 +112,25 @@ _sig("dmf_server_submit", C.c_int, VP, C.c_int32, C.c_int32, I32P, I32P, I32P, C
 _sig("dmf_server_wait", C.c_int, VP, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double))
 _sig("dmf_server_stats", C.c_int, VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_double))
 _sig("dmf_server_destroy", C.c_int, VP)
+F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+U16P = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
+_sig("dmf_sched_create", C.c_int, C.c_int32, C.c_uint64, PP)
+_sig("dmf_sched_destroy", C.c_int, VP)
+_sig("dmf_sched_set_weights", C.c_int, VP, U16P, F32P)
+_sig("dmf_sched_get_weights", C.c_int, VP, U16P, F32P)
+_sig("dmf_sched_train", C.c_int, VP, C.c_int32, F32P, F32P, C.c_int32, C.c_int32, C.c_float, C.c_uint64, F32P)
+_sig("dmf_sched_predict", C.c_int, VP, C.c_int32, F32P, F32P)
+_sig("dmf_solver_features", C.c_int, VP, C.c_int32, I32P, I32P, I32P, F32P)
+_sig("dmf_apply_updates_action", C.c_int, VP, C.c_int32, C.c_int32, I32P, I32P, I32P, C.POINTER(C.c_int64))
+_sig("dmf_apply_updates_scheduled", C.c_int, VP, VP, C.c_int32, I32P, I32P, I32P, C.POINTER(C.c_int64),
+     C.POINTER(C.c_int32))
+_sig("dmf_sched_records", C.c_int, VP, C.c_int32, F32P, I32P, F32P, I64P, C.POINTER(C.c_int32))
+_sig("dmf_solver_copy_state", C.c_int, VP, VP)
+
+# schedules the picker chooses from (DMF_ACTION_*); every one gives the same flow
+ACTIONS = ("plain", "short_interval", "warp_per_vertex", "recompute")
+N_FEATURES, N_HIDDEN, N_ACTIONS, N_WEIGHTS, N_BIASES = 12, 64, 4, 5120, 132
+
 _sig("dmf_static_maxflow_noalloc", C.c_int, C.c_int32, C.c_int32, VP, VP, VP, VP, C.c_int32, C.c_int32, VP,
      C.POINTER(C.c_int64), VP)
 
@@ -313,6 +332,45 @@ class Solver:
                                            C.byref(f)))
         return f.value
 
+    def features(self, src, dst, w) -> np.ndarray:
+        """The schedule picker's 12 features of a batch against the current state (nothing applied)."""
+        src, dst, w = _i32(src), _i32(dst), _i32(w)
+        out = np.zeros(N_FEATURES, np.float32)
+        _check(_L.dmf_solver_features(self._h, len(src), src, dst, w, out))
+        return out
+
+    def apply_updates_action(self, action: int, src, dst, w) -> int:
+        """Applies a batch under one schedule (index into ACTIONS); same flow for every action."""
+        src, dst, w = _i32(src), _i32(dst), _i32(w)
+        f = C.c_int64()
+        _check(_L.dmf_apply_updates_action(self._h, int(action), len(src), src, dst, w, C.byref(f)))
+        return f.value
+
+    def apply_updates_scheduled(self, sched, src, dst, w):
+        """Applies a batch under the schedule `sched` (a Scheduler, or None for the plain
+        one) picks; returns (flow, action)."""
+        src, dst, w = _i32(src), _i32(dst), _i32(w)
+        f, a = C.c_int64(), C.c_int32()
+        _check(_L.dmf_apply_updates_scheduled(self._h, None if sched is None else sched._h, len(src), src, dst, w,
+                                              C.byref(f), C.byref(a)))
+        return f.value, a.value
+
+    def sched_records(self, cap: int = 1 << 16):
+        """Drains the per-batch records of the scheduled/action calls:
+        (features[n,12], action[n], ms[n], flow[n])."""
+        feat = np.zeros((cap, N_FEATURES), np.float32)
+        act = np.zeros(cap, np.int32)
+        ms = np.zeros(cap, np.float32)
+        fl = np.zeros(cap, np.int64)
+        cnt = C.c_int32()
+        _check(_L.dmf_sched_records(self._h, cap, feat.reshape(-1), act, ms, fl, C.byref(cnt)))
+        n = cnt.value
+        return feat[:n], act[:n], ms[:n], fl[:n]
+
+    def copy_state_from(self, other: "Solver") -> None:
+        """Makes this solver's residual state an exact copy of `other`'s (same graph)."""
+        _check(_L.dmf_solver_copy_state(self._h, other._h))
+
     def recompute(self, src=(), dst=(), w=()) -> int:
         src, dst, w = _i32(src), _i32(dst), _i32(w)
         f = C.c_int64()
@@ -459,6 +517,66 @@ class MultiSolver(Solver):
         _check(_L.dmf_multi_run_batches(self._h, steps, ofs, C.c_void_p(d_src), C.c_void_p(d_dst), C.c_void_p(d_w),
                                         1 if use_graph else 0, out, C.byref(ms)))
         return out.reshape(steps, self.count), ms.value
+
+
+class Scheduler:
+    """The learned schedule picker (dmf_sched): MLP 12-64-64-4 with bf16 weights and fp32
+    accumulation; training and inference run in CUDA kernels on the device."""
+
+    def __init__(self, device: int = -1, seed: int = 0):
+        self._h = C.c_void_p()
+        _check(_L.dmf_sched_create(device, seed, C.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _L.dmf_sched_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def get_weights(self):
+        """(weights[5120] as bf16 bit patterns in uint16, biases[132] fp32)."""
+        w = np.zeros(N_WEIGHTS, np.uint16)
+        b = np.zeros(N_BIASES, np.float32)
+        _check(_L.dmf_sched_get_weights(self._h, w, b))
+        return w, b
+
+    def set_weights(self, weights, biases) -> None:
+        _check(_L.dmf_sched_set_weights(self._h, np.ascontiguousarray(weights, np.uint16),
+                                        np.ascontiguousarray(biases, np.float32)))
+
+    def train(self, X, Y, steps=2000, batch=64, lr=3e-3, seed=0) -> np.ndarray:
+        """Minibatch Adam on the device; returns the per-step minibatch MSE."""
+        X = np.ascontiguousarray(X, np.float32).reshape(-1)
+        Y = np.ascontiguousarray(Y, np.float32).reshape(-1)
+        n = len(Y) // N_ACTIONS
+        loss = np.zeros(max(steps, 1), np.float32)
+        _check(_L.dmf_sched_train(self._h, n, X, Y, steps, batch, lr, seed, loss))
+        return loss[:steps]
+
+    def predict(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32).reshape(-1)
+        n = len(X) // N_FEATURES
+        Y = np.zeros(n * N_ACTIONS, np.float32)
+        _check(_L.dmf_sched_predict(self._h, n, X, Y))
+        return Y.reshape(n, N_ACTIONS)
+
+    def save(self, path: str) -> None:
+        w, b = self.get_weights()
+        np.savez(path, weights=w, biases=b)
+
+    @classmethod
+    def load(cls, path: str, device: int = -1) -> "Scheduler":
+        d = np.load(path)
+        s = cls(device)
+        s.set_weights(d["weights"], d["biases"])
+        return s
 
 
 class Server:

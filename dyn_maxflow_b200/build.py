@@ -57,7 +57,7 @@ def build_lib(force: bool = False, verbose: bool = False, ptxas_info: bool = Fal
     if force or ptxas_info or _stale(LIB, deps):
         cmd = ["nvcc", *NVCC_FLAGS, "-shared", "-I", INCLUDE, "-I", CSRC,
                os.path.join(CSRC, "dmf_solver.cu"), os.path.join(CSRC, "dmf_host.cpp"),
-               os.path.join(CSRC, "dmf_server.cpp"),
+               os.path.join(CSRC, "dmf_server.cpp"), os.path.join(CSRC, "dmf_sched.cu"),
                "-o", LIB + ".tmp", "-lgomp"]
         if ptxas_info:
             cmd[1:1] = ["-Xptxas", "-v"]

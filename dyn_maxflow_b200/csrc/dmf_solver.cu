@@ -24,6 +24,7 @@
 
 #include "dmf_device.cuh"
 #include "dmf_internal.h"
+#include "dmf_sched_internal.h"
 
 using namespace dmfd;
 
@@ -194,6 +195,24 @@ __device__ __forceinline__ void ph_saturate(const Params &p) {
 
 // Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201) by binary search over the
 // per-vertex head-sorted index; also validates the batch.
+// Arc u->v by binary search over u's head-sorted arc index (the last arc among
+// equal heads, as OnAdd_kernel's linear scan keeps the last match), or -1.
+__device__ __forceinline__ int find_arc_dev(const int *__restrict__ off, const int *__restrict__ adj,
+                                            const int *__restrict__ sidx, int u, int v) {
+  const int first = __ldg(off + u);
+  int lo = first, hi = __ldg(off + u + 1);
+  while (lo < hi) {  // last position with head <= v
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(adj + __ldg(sidx + mid)) <= v) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo > first) {
+    const int cand = __ldg(sidx + lo - 1);
+    if (__ldg(adj + cand) == v) return cand;
+  }
+  return -1;
+}
+
 __device__ __forceinline__ void ph_lookup(const Params &p) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   for (int i = gt; i < p.k; i += nt) {
@@ -204,18 +223,7 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
       continue;
     }
     if (u == v) continue;  // ignored, as OnAdd_kernel does (code/dyn_data.h:194)
-    int lo = __ldg(p.off + u), hi = __ldg(p.off + u + 1);
-    // last position with head <= v
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (__ldg(p.adj + __ldg(p.sidx + mid)) <= v) lo = mid + 1;
-      else hi = mid;
-    }
-    int e = -1;
-    if (lo > __ldg(p.off + u)) {
-      int cand = __ldg(p.sidx + lo - 1);
-      if (__ldg(p.adj + cand) == v) e = cand;
-    }
+    const int e = find_arc_dev(p.off, p.adj, p.sidx, u, v);
     if (e < 0) {
       set_err(p.ctrl, ERR_UNKNOWN_ARC, i);
       continue;
@@ -1597,6 +1605,61 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_solve(Params p) {
   }
 }
 
+// Raw feature sums of an update batch against the current residual state, for
+// the schedule picker (nothing is modified).  Updates the solver would reject
+// (bad ids, unknown arcs) are skipped here; the solve reports them.
+__global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, const int *__restrict__ adj,
+                                                  const int *__restrict__ sidx, const int *cap, const int *res, int n,
+                                                  int k, const int *usrc, const int *udst, const int *uw,
+                                                  dmfs::FeatAcc *acc) {
+  unsigned long long valid = 0, dec = 0, satdec = 0, incsat = 0, ins = 0, del = 0, sdeg = 0, mdeg = 0;
+  long long exc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+    const int u = __ldg(usrc + i), v = __ldg(udst + i), w = __ldg(uw + i);
+    if (u < 0 || u >= n || v < 0 || v >= n || u == v) continue;
+    const int e = find_arc_dev(off, adj, sidx, u, v);
+    if (e < 0) continue;
+    valid++;
+    const int c0 = __ldcg(cap + e), r = __ldcg(res + e);
+    const long long flow = (long long)c0 - r;  // negative: the partner carries flow
+    const unsigned long long d = (unsigned long long)(__ldg(off + u + 1) - __ldg(off + u));
+    sdeg += d;
+    mdeg = d > mdeg ? d : mdeg;
+    if (w < c0) {
+      dec++;
+      if (flow > w) {
+        satdec++;
+        exc += flow - w;
+      }
+    } else if (w > c0 && r == 0) {
+      incsat++;
+    }
+    if (c0 == 0 && w > 0) ins++;
+    if (c0 > 0 && w == 0) del++;
+  }
+  cg::thread_block_tile<32> wp = cg::tiled_partition<32>(cg::this_thread_block());
+  valid = cg::reduce(wp, valid, cg::plus<unsigned long long>());
+  dec = cg::reduce(wp, dec, cg::plus<unsigned long long>());
+  satdec = cg::reduce(wp, satdec, cg::plus<unsigned long long>());
+  incsat = cg::reduce(wp, incsat, cg::plus<unsigned long long>());
+  ins = cg::reduce(wp, ins, cg::plus<unsigned long long>());
+  del = cg::reduce(wp, del, cg::plus<unsigned long long>());
+  sdeg = cg::reduce(wp, sdeg, cg::plus<unsigned long long>());
+  mdeg = cg::reduce(wp, mdeg, cg::greater<unsigned long long>());
+  exc = cg::reduce(wp, exc, cg::plus<long long>());
+  if (wp.thread_rank() == 0 && valid) {
+    atomicAdd(&acc->valid, valid);
+    atomicAdd(&acc->dec, dec);
+    atomicAdd(&acc->satdec, satdec);
+    atomicAdd(&acc->incsat, incsat);
+    atomicAdd(&acc->ins, ins);
+    atomicAdd(&acc->del, del);
+    atomicAdd(&acc->sum_deg, sdeg);
+    atomicMax(&acc->max_deg, mdeg);
+    atomic_add_ll(&acc->excess_created, exc);
+  }
+}
+
 using KernelFn = void (*)(Params);
 
 // minb = resident blocks per SM the register budget is sized for (1: up to 128
@@ -1675,6 +1738,15 @@ struct dmf_solver {
   int epoch = 0;
   bool solved = false, side_valid = false;
   dmf_stats st{};
+  // schedule picker: feature sums of the batch being scheduled, per-batch log
+  dmfs::FeatAcc *facc = nullptr;
+  struct SchedRecord {
+    float feat[DMF_SCHED_FEATURES];
+    int action;
+    float ms;
+    int64_t flow;
+  };
+  std::vector<SchedRecord> records;
   std::vector<void *> allocs;
 };
 
@@ -1954,11 +2026,10 @@ int check_updates_args(dmf_solver *sv, int32_t k, const void *a, const void *b, 
   return DMF_OK;
 }
 
-int host_updates(dmf_solver *sv, int mode, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
-                 int64_t *flow) {
-  int st = check_updates_args(sv, k, src, dst, w);
-  if (st) return st;
-  if (mode == MODE_DYNAMIC && !sv->solved) return fail(DMF_ERR_NOT_SOLVED, "apply_updates before a solve");
+// Copies a host batch into the device staging buffers through pinned memory,
+// after recording the solve's start event (the copies are part of its time).
+int stage_batch(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w) {
+  int st;
   CK(cudaSetDevice(sv->dev), "cudaSetDevice");
   if ((st = ensure_ubuf(sv, k)) || (st = ensure_host_ubuf(sv, k))) return st;
   const size_t K = (size_t)sv->kcap, HK = (size_t)sv->h_kcap;
@@ -1974,7 +2045,90 @@ int host_updates(dmf_solver *sv, int mode, int32_t k, const int32_t *src, const 
     CK(cudaMemcpyAsync(sv->ubuf + 2 * K, sv->h_ubuf + 2 * HK, 4 * (size_t)k, cudaMemcpyHostToDevice, sv->stream),
        "H2D w");
   }
+  return DMF_OK;
+}
+
+int host_updates(dmf_solver *sv, int mode, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
+                 int64_t *flow) {
+  int st = check_updates_args(sv, k, src, dst, w);
+  if (st) return st;
+  if (mode == MODE_DYNAMIC && !sv->solved) return fail(DMF_ERR_NOT_SOLVED, "apply_updates before a solve");
+  if ((st = stage_batch(sv, k, src, dst, w))) return st;
+  const size_t K = (size_t)sv->kcap;
   return run_mode(sv, mode, k, sv->ubuf, sv->ubuf + K, sv->ubuf + 2 * K, flow, true);
+}
+
+// Feature sums of the staged batch, then the picker's decision (sched = null:
+// features only, action 0).
+int batch_features(dmf_solver *sv, dmf_sched *sched, int k, float *feat, int *action) {
+  CK(cudaMemsetAsync(sv->facc, 0, sizeof(dmfs::FeatAcc), sv->stream), "memset features");
+  if (k > 0) {
+    const size_t K = (size_t)sv->kcap;
+    const int blocks = std::min((k + 255) / 256, 4 * 148);
+    k_features<<<blocks, 256, 0, sv->stream>>>(sv->off, sv->adj, sv->sidx, sv->cap, sv->res, sv->n, k, sv->ubuf,
+                                               sv->ubuf + K, sv->ubuf + 2 * K, sv->facc);
+    CK(cudaGetLastError(), "feature launch");
+  }
+  dmfs::FeatScalars sc;
+  sc.k = (float)k;
+  sc.m = (float)sv->m;
+  sc.n = (float)sv->n;
+  sc.last_flow = (float)sv->st.flow;
+  sc.last_levels = (float)sv->st.bfs_levels;
+  sc.last_outer = (float)sv->st.outer_iters;
+  return dmf_sched_decide(sched, sv->facc, sc, sv->stream, sv->dev, feat, nullptr, action);
+}
+
+// Runs the staged batch under one of the DMF_ACTION_* schedules; the solver's
+// own options are restored afterwards.
+int apply_action(dmf_solver *sv, int action, int k, int64_t *flow) {
+  const dmf_opts saved = sv->opts;
+  const int saved_small = sv->small_deg;
+  int mode = MODE_DYNAMIC;
+  switch (action) {
+    case DMF_ACTION_SHORT:
+      sv->opts.relabel_interval = 2;
+      sv->opts.flags |= DMF_FLAG_FIXED_INTERVAL;
+      break;
+    case DMF_ACTION_WARP:
+      sv->opts.relabel_interval = 12;
+      sv->opts.flags |= DMF_FLAG_FIXED_INTERVAL;
+      sv->small_deg = 0;
+      break;
+    case DMF_ACTION_RECOMPUTE:
+      mode = MODE_RECOMPUTE;
+      break;
+    default:
+      break;
+  }
+  const size_t K = (size_t)sv->kcap;
+  const int st = run_mode(sv, mode, k, sv->ubuf, sv->ubuf + K, sv->ubuf + 2 * K, flow, true);
+  sv->opts = saved;
+  sv->small_deg = saved_small;
+  return st;
+}
+
+// Shared body of dmf_apply_updates_action / _scheduled (action < 0: ask sched).
+int scheduled_updates(dmf_solver *sv, dmf_sched *sched, int action, int32_t k, const int32_t *src,
+                      const int32_t *dst, const int32_t *w, int64_t *flow, int32_t *chosen) {
+  int st = check_updates_args(sv, k, src, dst, w);
+  if (st) return st;
+  if (!sv->solved) return fail(DMF_ERR_NOT_SOLVED, "apply_updates before a solve");
+  if (action >= DMF_SCHED_ACTIONS) return fail(DMF_ERR_INVALID_ARG, "unknown action %d", action);
+  if ((st = stage_batch(sv, k, src, dst, w))) return st;
+  dmf_solver::SchedRecord rec{};
+  int picked = 0;
+  if ((st = batch_features(sv, action < 0 ? sched : nullptr, k, rec.feat, &picked))) return st;
+  if (action >= 0) picked = action;
+  int64_t f = 0;
+  if ((st = apply_action(sv, picked, k, &f))) return st;
+  rec.action = picked;
+  rec.ms = (float)sv->st.last_ms;
+  rec.flow = f;
+  if (sv->records.size() < (1u << 20)) sv->records.push_back(rec);
+  if (flow) *flow = f;
+  if (chosen) *chosen = picked;
+  return ok();
 }
 
 int device_updates(dmf_solver *sv, int mode, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
@@ -2272,6 +2426,7 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
   }
   sv->trace_cap = 1 << 16;
   if ((st = dalloc(sv, &sv->trace, 4 * (size_t)sv->trace_cap))) return bail(st);
+  if ((st = dalloc(sv, &sv->facc, 1))) return bail(st);
   *out = sv;
   return ok();
 }
@@ -2683,6 +2838,76 @@ int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us, int
 int dmf_stats_get(const dmf_solver *sv, dmf_stats *st) {
   if (!sv || !st) return fail(DMF_ERR_INVALID_ARG, "null argument");
   *st = sv->st;
+  return ok();
+}
+
+int dmf_solver_features(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
+                        float *feat) {
+  int st = check_updates_args(sv, k, src, dst, w);
+  if (st) return st;
+  if (!feat) return fail(DMF_ERR_INVALID_ARG, "null feature output");
+  if ((st = stage_batch(sv, k, src, dst, w))) return st;
+  int action = 0;
+  if ((st = batch_features(sv, nullptr, k, feat, &action))) return st;
+  return ok();
+}
+
+int dmf_apply_updates_action(dmf_solver *sv, int32_t action, int32_t k, const int32_t *src, const int32_t *dst,
+                             const int32_t *w, int64_t *flow) {
+  if (action < 0) return fail(DMF_ERR_INVALID_ARG, "unknown action %d", action);
+  return scheduled_updates(sv, nullptr, action, k, src, dst, w, flow, nullptr);
+}
+
+int dmf_apply_updates_scheduled(dmf_solver *sv, dmf_sched *sched, int32_t k, const int32_t *src, const int32_t *dst,
+                                const int32_t *w, int64_t *flow, int32_t *action) {
+  return scheduled_updates(sv, sched, -1, k, src, dst, w, flow, action);
+}
+
+int dmf_sched_records(dmf_solver *sv, int32_t cap, float *feat, int32_t *action, float *ms, int64_t *flow,
+                      int32_t *count) {
+  if (!sv || cap < 0 || !count) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+  const int n = (int)std::min<size_t>((size_t)cap, sv->records.size());
+  for (int i = 0; i < n; i++) {
+    const auto &r = sv->records[i];
+    if (feat) std::memcpy(feat + (size_t)i * DMF_SCHED_FEATURES, r.feat, sizeof(r.feat));
+    if (action) action[i] = r.action;
+    if (ms) ms[i] = r.ms;
+    if (flow) flow[i] = r.flow;
+  }
+  sv->records.erase(sv->records.begin(), sv->records.begin() + n);
+  *count = n;
+  return ok();
+}
+
+int dmf_solver_copy_state(dmf_solver *dst, const dmf_solver *src) {
+  if (!dst || !src) return fail(DMF_ERR_INVALID_ARG, "null solver");
+  if (dst == src) return ok();
+  if (dst->n != src->n || dst->m != src->m || dst->hub_deg != src->hub_deg || dst->nchunk != src->nchunk ||
+      dst->ninst != 1 || src->ninst != 1 || dst->dev != src->dev)
+    return fail(DMF_ERR_INVALID_ARG, "copy_state needs two single-instance solvers of the same graph, hub "
+                                     "threshold and device");
+  CK(cudaSetDevice(dst->dev), "cudaSetDevice");
+  CK(cudaStreamSynchronize(src->stream), "source solver");
+  const size_t N = (size_t)src->n + 1, M = (size_t)src->m, NC = (size_t)std::max(src->nchunk, 1);
+  cudaStream_t S = dst->stream;
+  CK(cudaMemcpyAsync(dst->cap, src->cap, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D cap");
+  CK(cudaMemcpyAsync(dst->res, src->res, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D res");
+  CK(cudaMemcpyAsync(dst->astamp, src->astamp, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D astamp");
+  CK(cudaMemcpyAsync(dst->excess, src->excess, 8 * N, cudaMemcpyDeviceToDevice, S), "D2D excess");
+  CK(cudaMemcpyAsync(dst->height, src->height, 4 * N, cudaMemcpyDeviceToDevice, S), "D2D height");
+  CK(cudaMemcpyAsync(dst->stamp, src->stamp, 4 * N, cudaMemcpyDeviceToDevice, S), "D2D stamp");
+  CK(cudaMemcpyAsync(dst->dead, src->dead, N, cudaMemcpyDeviceToDevice, S), "D2D dead");
+  CK(cudaMemcpyAsync(dst->side, src->side, N, cudaMemcpyDeviceToDevice, S), "D2D side");
+  CK(cudaMemcpyAsync(dst->chunk_mark, src->chunk_mark, 8 * NC, cudaMemcpyDeviceToDevice, S), "D2D marks");
+  CK(cudaMemcpyAsync(dst->chunk_tmin, src->chunk_tmin, 4 * NC, cudaMemcpyDeviceToDevice, S), "D2D marks");
+  CK(cudaStreamSynchronize(S), "copy state");
+  dst->round_base = src->round_base;
+  dst->relabel_base = src->relabel_base;
+  dst->epoch = src->epoch;
+  dst->solved = src->solved;
+  dst->side_valid = src->side_valid;
+  dst->st = src->st;
+  dst->flows = src->flows;
   return ok();
 }
 

@@ -291,6 +291,69 @@ int dmf_server_destroy(dmf_server *srv);
  * current capacities. */
 int dmf_autotune(dmf_solver *sv, int32_t repeats, dmf_opts *chosen);
 
+/* ---- learned schedule picker ----------------------------------------------- */
+/* No counterpart in the reference, whose schedule is fixed (one kernel_cycles
+ * value, a global relabel after every push, incremental repair; code/
+ * dyn_data_bench.cu:113-167).  Per update batch a small MLP picks one of
+ * DMF_SCHED_ACTIONS schedules from DMF_SCHED_FEATURES features of the batch
+ * measured against the live residual state.  Every action computes the same
+ * exact flow; only the time differs.  Action 0 is the plain schedule, used
+ * whenever no trained model is given. */
+#define DMF_SCHED_FEATURES 12
+#define DMF_SCHED_HIDDEN 64
+#define DMF_SCHED_ACTIONS 4
+#define DMF_SCHED_WEIGHTS 5120 /* bf16: W1[64][12], W2[64][64], W3[4][64] (row = output unit) */
+#define DMF_SCHED_BIASES 132   /* fp32: b1[64], b2[64], b3[4] */
+/* actions */
+#define DMF_ACTION_PLAIN 0       /* incremental repair, engine defaults */
+#define DMF_ACTION_SHORT 1       /* incremental, global relabel every 2 push rounds */
+#define DMF_ACTION_WARP 2        /* incremental, every non-hub vertex by a tile (no
+                                    thread-per-vertex tier), 12 rounds per relabel */
+#define DMF_ACTION_RECOMPUTE 3   /* set the capacities and solve from scratch */
+
+typedef struct dmf_sched dmf_sched; /* MLP 12-64-64-4, bf16 weights, fp32 accumulation */
+
+/* A model on `device` (-1 = current) with He-uniform weights from `seed`;
+ * untrained until dmf_sched_train or dmf_sched_set_weights. */
+int dmf_sched_create(int32_t device, uint64_t seed, dmf_sched **out);
+int dmf_sched_destroy(dmf_sched *sched);
+/* weights: DMF_SCHED_WEIGHTS bf16 bit patterns, biases: DMF_SCHED_BIASES. */
+int dmf_sched_set_weights(dmf_sched *sched, const uint16_t *weights, const float *biases);
+int dmf_sched_get_weights(dmf_sched *sched, uint16_t *weights, float *biases);
+/* Trains on n samples X[n][12] -> Y[n][4] (the targets are per-action costs,
+ * e.g. log2 of the time) by minibatch Adam on fp32 master weights with bf16
+ * weights in the forward pass, all on the device in one kernel: `steps`
+ * minibatches of `batch` (1..64) samples drawn from `seed`, learning rate `lr`.
+ * loss[steps] (may be NULL) receives the minibatch mean squared error. */
+int dmf_sched_train(dmf_sched *sched, int32_t n, const float *X, const float *Y, int32_t steps,
+                    int32_t batch, float lr, uint64_t seed, float *loss);
+/* Y[n][4] = model(X[n][12]) on the device. */
+int dmf_sched_predict(dmf_sched *sched, int32_t n, const float *X, float *Y);
+
+/* Features of a batch against the solver's current state (nothing applied):
+ * feat[12]; the names are listed in dyn_maxflow_b200/sched.py. */
+int dmf_solver_features(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst,
+                        const int32_t *w, float *feat);
+/* Applies a batch with a given action (0..3). */
+int dmf_apply_updates_action(dmf_solver *sv, int32_t action, int32_t k, const int32_t *src,
+                             const int32_t *dst, const int32_t *w, int64_t *flow);
+/* Applies a batch with the action `sched` picks (sched = NULL or untrained:
+ * the plain schedule); *action (may be NULL) receives it.  The time reported
+ * by dmf_stats_get includes the features and the decision. */
+int dmf_apply_updates_scheduled(dmf_solver *sv, dmf_sched *sched, int32_t k, const int32_t *src,
+                                const int32_t *dst, const int32_t *w, int64_t *flow,
+                                int32_t *action);
+/* Per-batch records the two calls above keep (the traces a model is trained
+ * on): feat[i*12..], action[i], ms[i] (solve time), flow[i]; up to `cap`
+ * oldest-first records are returned in *count and removed from the log.  Any
+ * output pointer may be NULL. */
+int dmf_sched_records(dmf_solver *sv, int32_t cap, float *feat, int32_t *action, float *ms,
+                      int64_t *flow, int32_t *count);
+/* Makes `dst` an exact copy of `src`'s residual state (same graph and
+ * options required), so that a batch can be timed under several actions from
+ * the same state. */
+int dmf_solver_copy_state(dmf_solver *dst, const dmf_solver *src);
+
 /* Static solve that allocates nothing, for callers that cannot allocate device
  * memory while they run (code inside a fixed memory pool or arena, or a host
  * that forbids cudaMalloc after start-up).  No counterpart in the reference.
