@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -52,9 +53,20 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-certify", action="store_true")
     ap.add_argument("--cpu-batches", type=int, default=3)
-    ap.add_argument("--workload", default="rmat20", choices=["rmat20", "batched"],
+    ap.add_argument("--workload", default="rmat20", choices=["rmat20", "batched", "learned", "serving"],
                     help="rmat20: the headline single-graph workload (scale from --scale); batched: 256 "
-                         "independent instances in one device state, 5 successive batches")
+                         "independent instances in one device state, 5 successive batches; learned: the "
+                         "learned schedule picker against the plain schedule on held-out R-MAT instances")
+    ap.add_argument("--learn-scale", type=int, default=22)
+    ap.add_argument("--learn-seeds", default="1000,1001")
+    ap.add_argument("--learn-fracs", default="0.01,0.01",
+                    help="batch fraction range lo,hi (log-uniform); 0.01,0.01 = the 1%% batches")
+    ap.add_argument("--serve-scale", type=int, default=24, help="scale of the large served R-MAT graph")
+    ap.add_argument("--serve-small", type=int, default=64, help="number of small (scale 16-18) served graphs")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson request rate (requests/s)")
+    ap.add_argument("--serve-seconds", type=float, default=15.0, help="length of the request stream")
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="HBM budget for admission (GiB)")
+    ap.add_argument("--sched-weights", default=os.path.join(ROOT, "dyn_maxflow_b200", "sched_weights.npz"))
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--autotune", action="store_true")
     return ap.parse_args()
@@ -388,6 +400,154 @@ def run_batched(args, rank: int, world: int):
     }
 
 
+def run_learned(args, rank: int, world: int):
+    """The learned schedule picker (weights trained on solver-recorded traces of
+    R-MAT scales 16-22) against the plain schedule on held-out seeds: both run
+    side by side from the same start and must give identical flows every batch;
+    every batch is also timed under all four schedules from the learned
+    solver's state for the regret.  Times are CUDA-event times of the host-array
+    entry point (batch staging, features and decision included)."""
+    import torch
+    import dyn_maxflow_b200 as D
+    from dyn_maxflow_b200 import sched as S
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if not os.path.exists(args.sched_weights):
+        return {"metric": METRIC + ", learned schedule", "error": f"no weights at {args.sched_weights}"}
+    sc = D.Scheduler.load(args.sched_weights)
+    seeds = [int(x) + 100 * rank for x in args.learn_seeds.split(",")]
+    lo, hi = (float(x) for x in args.learn_fracs.split(","))
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    t0 = time.time()
+    ev = S.evaluate(sc, [(args.learn_scale, sd) for sd in seeds], args.steps, lo, hi, oracle=True, verbose=False,
+                    warmup=max(3, args.warmup))
+    wall = time.time() - t0
+    clk = clocks.stop()
+    sc.close()
+    lp = ev["learned"]
+    n = 1 << args.learn_scale
+    k_mean = int(0.5 * (lo + hi) * (16 << args.learn_scale))
+    return {
+        "metric": METRIC + ", learned schedule", "value": round(lp["p50_ms"], 3), "unit": "ms", "n_gpus": world,
+        "steps": ev["batches"], "warmup": max(3, args.warmup), "ms_per_step": round(lp["total_ms"] / ev["batches"], 3),
+        "p99_ms": round(lp["p99_ms"], 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32 (int64 excess); scheduler bf16 weights, fp32 accumulation",
+        "data": "synthetic (seeded R-MAT, held-out seeds)",
+        "config": {"workload": f"learned-rmat{args.learn_scale}-heldout", "seeds": seeds,
+                   "vertices": n, "batches_per_seed": args.steps, "batch_fraction": [lo, hi],
+                   "l2": "inputs (67M-arc CSR) larger than L2"},
+        "plain": ev["plain"], "learned": lp, "best_total_ms": ev.get("best_total_ms"),
+        "speedup_vs_plain": round(ev["speedup_vs_plain"], 4),
+        "regret_vs_best": round(ev.get("regret_vs_best", 0.0), 4),
+        "plain_regret_vs_best": round(ev.get("plain_regret_vs_best", 0.0), 4),
+        "pick_hist": dict(zip(D.ACTIONS, ev["pick_hist"])), "exact_equal_flows": ev["exact_equal_flows"],
+        "e2e": {"value": round(lp["p50_ms"], 3), "unit": "ms", "h2d_bytes_per_step": 12 * k_mean,
+                "d2h_bytes_per_step": 8},
+        "clocks": clk, "wall_s": round(wall, 1),
+        "gpu_launches": 4 * ev["batches"],
+    }
+
+
+def run_serving(args, rank: int, world: int):
+    """Serving loop: one R-MAT graph of --serve-scale plus --serve-small graphs of
+    scales 16-18, device-resident, admitted by HBM budget; update-batch requests
+    arrive as a Poisson stream (--serve-rate per second, uniform over the graphs)
+    with sizes log-uniform in [1k, 1M] updates (at most half a graph's arcs),
+    mixed increases/decreases/inserts/deletes, drawn from a per-graph pool of
+    pre-generated batches (updates are absolute capacities, so any batch is valid
+    at any time).  Latency = submission to exact max-flow returned."""
+    import threading
+    import numpy as np
+    import torch
+    import dyn_maxflow_b200 as D
+    from dyn_maxflow_b200 import sched as S
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rng = np.random.default_rng(17 + rank)
+    t_gen = time.time()
+    specs = [(args.serve_scale, 3000 + rank)] + [(16 + i % 3, 4000 + 100 * rank + i) for i in range(args.serve_small)]
+    graphs, srcs, snks = [], [], []
+    for sc, sd in specs:
+        g, s_, t_ = S.rmat_instance(sc, sd)
+        graphs.append(g)
+        srcs.append(s_)
+        snks.append(t_)
+    pools = []
+    for gi, g in enumerate(graphs):
+        m = g.num_edges()
+        pool = []
+        for j in range(4):
+            size = int(min(math.exp(rng.uniform(math.log(1e3), math.log(1e6))), m // 2))
+            pool.append(S.next_batch(g, size / m, 5000 + 10 * gi + j))
+        pools.append(pool)
+    gen_s = time.time() - t_gen
+    srv = D.Server(graphs, srcs, snks, int(args.serve_budget_gb * (1 << 30)))
+    admitted = srv.admitted
+    # warm-up: one request per admitted graph
+    for gi in range(admitted):
+        srv.wait(srv.submit(gi, *pools[gi][0]))
+    # the Poisson stream
+    n_req = max(1, int(args.serve_rate * args.serve_seconds))
+    gaps = rng.exponential(1.0 / args.serve_rate, size=n_req)
+    choice = rng.integers(0, admitted, size=n_req)
+    pick = rng.integers(0, 4, size=n_req)
+    tickets = [None] * n_req
+    lat = [None] * n_req
+    flows = [None] * n_req
+    ready = threading.Semaphore(0)
+
+    def waiter():
+        for i in range(n_req):
+            ready.acquire()
+            flows[i], lat[i] = srv.wait(tickets[i])
+
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    th = threading.Thread(target=waiter)
+    th.start()
+    t0 = time.perf_counter()
+    due = t0
+    for i in range(n_req):
+        due += gaps[i]
+        now = time.perf_counter()
+        if due > now:
+            time.sleep(due - now)
+        tickets[i] = srv.submit(int(choice[i]), *pools[choice[i]][pick[i]])
+        ready.release()
+    th.join()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    st = srv.stats()
+    srv.close()
+    updates = int(sum(len(pools[choice[i]][pick[i]][0]) for i in range(n_req)))
+    # exactness: replay the requests of a few small graphs alone, in order, and
+    # compare every returned flow
+    exact = True
+    for gi in range(1, min(admitted, 5)):
+        idx = [i for i in range(n_req) if choice[i] == gi]
+        with D.Solver(graphs[gi], srcs[gi], snks[gi]) as sv:
+            sv.static_maxflow()
+            sv.apply_updates(*pools[gi][0])  # the warm-up request
+            for i in idx:
+                exact &= sv.apply_updates(*pools[gi][pick[i]]) == flows[i]
+    lat_ms = [x for x in lat if x is not None]
+    p50, p99 = pct(lat_ms, 0.5), pct(lat_ms, 0.99)
+    return {
+        "metric": "ms from request to exact maxflow, serving (p50)", "value": round(p50, 3), "unit": "ms",
+        "n_gpus": world, "steps": n_req, "warmup": admitted, "ms_per_step": round(float(np.mean(lat_ms)), 3),
+        "p99_ms": round(p99, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32 (int64 excess)", "data": "synthetic (seeded R-MAT graphs and update batches)",
+        "config": {"workload": f"serving-rmat{args.serve_scale}+{args.serve_small}x(16-18)",
+                   "graphs": len(graphs), "admitted": admitted, "device_bytes": srv.device_bytes,
+                   "big_graph": {"vertices": graphs[0].num_nodes(), "csr_arcs": graphs[0].num_edges()},
+                   "rate_req_s": args.serve_rate, "stream_s": args.serve_seconds,
+                   "request_sizes": "log-uniform [1e3, 1e6] updates, <= m/2",
+                   "l2": "device state (large graph) far larger than L2"},
+        "sustained_updates_per_s": round(updates / wall, 1), "requests_per_s": round(n_req / wall, 2),
+        "server": st, "exact_replay_check": bool(exact), "generation_s": round(gen_s, 1),
+        "e2e": {"value": round(p50, 3), "unit": "ms", "h2d_bytes_per_step": int(12 * updates / n_req),
+                "d2h_bytes_per_step": 8},
+        "clocks": clk, "gpu_launches": int(st["ticks"]),
+    }
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return None
@@ -427,6 +587,10 @@ def main():
             res = run_reference(args, rank)
         elif args.workload == "batched":
             res = run_batched(args, rank, world)
+        elif args.workload == "learned":
+            res = run_learned(args, rank, world)
+        elif args.workload == "serving":
+            res = run_serving(args, rank, world)
         else:
             res = run_ours(args, rank, world)
     finally:

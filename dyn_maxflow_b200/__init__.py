@@ -118,6 +118,7 @@ _sig("dmf_sched_create", C.c_int, C.c_int32, C.c_uint64, PP)
 _sig("dmf_sched_destroy", C.c_int, VP)
 _sig("dmf_sched_set_weights", C.c_int, VP, U16P, F32P)
 _sig("dmf_sched_get_weights", C.c_int, VP, U16P, F32P)
+_sig("dmf_sched_set_margin", C.c_int, VP, C.c_float)
 _sig("dmf_sched_train", C.c_int, VP, C.c_int32, F32P, F32P, C.c_int32, C.c_int32, C.c_float, C.c_uint64, F32P)
 _sig("dmf_sched_predict", C.c_int, VP, C.c_int32, F32P, F32P)
 _sig("dmf_solver_features", C.c_int, VP, C.c_int32, I32P, I32P, I32P, F32P)
@@ -539,6 +540,10 @@ class Scheduler:
 
     def __exit__(self, *exc):
         self.close()
+
+    def set_margin(self, margin: float) -> None:
+        """log2 units a non-plain action must be predicted to win by (default 0.1)."""
+        _check(_L.dmf_sched_set_margin(self._h, float(margin)))
 
     def get_weights(self):
         """(weights[5120] as bf16 bit patterns in uint16, biases[132] fp32)."""

@@ -90,9 +90,12 @@ __device__ void make_features(const FeatAcc &a, const FeatScalars &sc, float *x)
 }
 
 // Features, then (use_model) the forward pass and the argmin action.
+// Outputs are log2 of each action's time relative to the plain schedule; a
+// non-plain action is taken only when it is predicted to beat the plain one by
+// more than `margin` (log2 units), so that prediction noise falls back to plain.
 __global__ void __launch_bounds__(kHidden) k_decide(const __nv_bfloat16 *W, const float *b, const FeatAcc *acc,
-                                                    FeatScalars sc, int use_model, float *feat, float *pred,
-                                                    int *action) {
+                                                    FeatScalars sc, int use_model, float margin, float *feat,
+                                                    float *pred, int *action) {
   __shared__ float x[kFeatures], h1[kHidden], h2[kHidden], out[kActions];
   if (threadIdx.x == 0) make_features(*acc, sc, x);
   __syncthreads();
@@ -106,8 +109,12 @@ __global__ void __launch_bounds__(kHidden) k_decide(const __nv_bfloat16 *W, cons
   if (threadIdx.x < kActions) pred[threadIdx.x] = out[threadIdx.x];
   if (threadIdx.x == 0) {
     int best = 0;
+    float bestv = out[0] - margin;
     for (int a = 1; a < kActions; a++)
-      if (out[a] < out[best]) best = a;
+      if (out[a] < bestv) {
+        best = a;
+        bestv = out[a];
+      }
     *action = best;
   }
 }
@@ -269,6 +276,7 @@ struct dmf_sched {
   float *h_io = nullptr;  // pinned
   long long adam_t = 0;
   bool trained = false;
+  float margin = 0.1f;  // log2 units a non-plain action must win by
   std::mutex mu;  // one call at a time per model (training, prediction, decisions)
 };
 
@@ -373,6 +381,13 @@ int dmf_sched_set_weights(dmf_sched *s, const uint16_t *weights, const float *bi
   SCK(cudaStreamSynchronize(s->stream), "set weights");
   s->adam_t = 0;
   s->trained = true;
+  return ok();
+}
+
+int dmf_sched_set_margin(dmf_sched *s, float margin) {
+  if (!s || !(margin >= 0.f) || !std::isfinite(margin)) return fail(DMF_ERR_INVALID_ARG, "margin must be >= 0");
+  std::lock_guard<std::mutex> lock(s->mu);
+  s->margin = margin;
   return ok();
 }
 
@@ -482,7 +497,8 @@ int dmf_sched_decide(dmf_sched *s, const FeatAcc *d_acc, const FeatScalars &sc, 
     io = scratch[device];
     h_io = h_scratch[device];
   }
-  k_decide<<<1, kHidden, 0, stream>>>(W, b, d_acc, sc, use ? 1 : 0, io, io + kFeatures, (int *)(io + kFeatures + kActions));
+  k_decide<<<1, kHidden, 0, stream>>>(W, b, d_acc, sc, use ? 1 : 0, s ? s->margin : 0.f, io, io + kFeatures,
+                                      (int *)(io + kFeatures + kActions));
   SCK(cudaGetLastError(), "decision launch");
   SCK(cudaMemcpyAsync(h_io, io, sizeof(float) * (kFeatures + kActions + 1), cudaMemcpyDeviceToHost, stream), "D2H decision");
   SCK(cudaStreamSynchronize(stream), "decision");

@@ -107,12 +107,43 @@ def record(specs, batches: int, frac_lo: float, frac_hi: float, verbose=True):
     return np.array(X, np.float32), np.array(T, np.float32), meta
 
 
+MARGIN = 0.1  # log2 units a non-plain action must be predicted to win by (the model's default)
+
+
 def targets(T) -> np.ndarray:
-    return np.log2(np.maximum(np.asarray(T, np.float64), 1e-3)).astype(np.float32)
+    """log2 of each action's time over the plain schedule's (column 0 is 0): the
+    differences that decide the pick are the whole target, not a small part of
+    an absolute time that varies 100x across graph sizes."""
+    L = np.log2(np.maximum(np.asarray(T, np.float64), 1e-3))
+    return (L - L[:, :1]).astype(np.float32)
 
 
-def train(X, T, steps=4000, lr=3e-3, seed=0, device=-1):
-    """Trains a Scheduler on traces; returns (scheduler, loss curve)."""
+def balance(X, T, groups):
+    """Repeats samples so that every group (graph scale) weighs the same."""
+    groups = np.asarray(groups)
+    keys, counts = np.unique(groups, return_counts=True)
+    mx = counts.max()
+    idx = np.concatenate([np.repeat(np.where(groups == k)[0], int(math.ceil(mx / c))) for k, c in zip(keys, counts)])
+    return X[idx], T[idx]
+
+
+def pick_actions(pred, margin=MARGIN) -> np.ndarray:
+    """The decision rule of the device kernel (k_decide) on predictions."""
+    pred = np.asarray(pred)
+    best = np.zeros(len(pred), int)
+    bestv = pred[:, 0] - margin
+    for a in range(1, pred.shape[1]):
+        better = pred[:, a] < bestv
+        best[better] = a
+        bestv = np.where(better, pred[:, a], bestv)
+    return best
+
+
+def train(X, T, groups=None, steps=4000, lr=3e-3, seed=0, device=-1):
+    """Trains a Scheduler on traces (balanced over `groups` when given); returns
+    (scheduler, loss curve)."""
+    if groups is not None:
+        X, T = balance(np.asarray(X), np.asarray(T), groups)
     sched = D.Scheduler(device, seed)
     loss = sched.train(X, targets(T), steps=steps, batch=64, lr=lr, seed=seed)
     return sched, loss
@@ -121,7 +152,7 @@ def train(X, T, steps=4000, lr=3e-3, seed=0, device=-1):
 def choice_quality(sched, X, T) -> dict:
     """Offline quality on traces: time of the picked action vs plain and vs the best."""
     pred = sched.predict(X)
-    pick = pred.argmin(1)
+    pick = pick_actions(pred)
     T = np.asarray(T, np.float64)
     rows = np.arange(len(T))
     return {
@@ -134,11 +165,12 @@ def choice_quality(sched, X, T) -> dict:
     }
 
 
-def evaluate(sched, specs, batches: int, frac_lo: float, frac_hi: float, oracle=True, verbose=True):
+def evaluate(sched, specs, batches: int, frac_lo: float, frac_hi: float, oracle=True, verbose=True, warmup=1):
     """Runs the plain schedule and the learned one side by side on held-out
-    instances; both must give identical flows.  With `oracle`, every batch is
-    also timed under all actions from the learned solver's state (the best of
-    them is the regret's yardstick)."""
+    instances (`warmup` untimed batches of 0.1% first); both must give
+    identical flows.  With `oracle`, every batch is also timed under all actions
+    from the learned solver's state (the best of them is the regret's
+    yardstick)."""
     plain_ms, learned_ms, best_ms, picks, exact = [], [], [], [], True
     for scale, seed in specs:
         g, s, t = rmat_instance(scale, seed)
@@ -149,10 +181,11 @@ def evaluate(sched, specs, batches: int, frac_lo: float, frac_hi: float, oracle=
         L.static_maxflow()
         rng = np.random.default_rng(seed)
         fracs = batch_sizes(rng, batches, frac_lo, frac_hi)
-        bs, bd, bw = next_batch(g, 1e-3, seed * 7919 + 99991)  # warm-up batch, untimed
-        P.apply_updates_scheduled(None, bs, bd, bw)
-        L.apply_updates_scheduled(sched, bs, bd, bw)
-        g.set_caps(bs, bd, bw)
+        for wi in range(warmup):  # untimed
+            bs, bd, bw = next_batch(g, 1e-3, seed * 7919 + 99991 + wi)
+            P.apply_updates_scheduled(None, bs, bd, bw)
+            L.apply_updates_scheduled(sched, bs, bd, bw)
+            g.set_caps(bs, bd, bw)
         for b, frac in enumerate(fracs):
             bs, bd, bw = next_batch(g, frac, seed * 7919 + b)
             if O is not None:
@@ -184,6 +217,8 @@ def evaluate(sched, specs, batches: int, frac_lo: float, frac_hi: float, oracle=
         "learned": {"total_ms": float(np.sum(learned_ms)), "p50_ms": pct(learned_ms, 50),
                     "p99_ms": pct(learned_ms, 99)},
         "pick_hist": np.bincount(np.asarray(picks, int), minlength=D.N_ACTIONS).tolist(),
+        "per_batch": {"plain_ms": [round(x, 4) for x in plain_ms], "learned_ms": [round(x, 4) for x in learned_ms],
+                      "best_ms": [round(x, 4) for x in best_ms], "picks": [int(a) for a in picks]},
     }
     out["speedup_vs_plain"] = out["plain"]["total_ms"] / max(out["learned"]["total_ms"], 1e-9)
     if best_ms:
@@ -245,13 +280,14 @@ def main(argv=None):
         np.savez(a.out, X=X, T=T, meta=json.dumps(meta))
         print(f"{len(X)} records -> {a.out}")
     elif a.cmd == "train":
-        Xs, Ts = [], []
+        Xs, Ts, G = [], [], []
         for p in a.traces:
             d = np.load(p)
             Xs.append(d["X"])
             Ts.append(d["T"])
+            G += [m["scale"] for m in json.loads(str(d["meta"]))]
         X, T = np.concatenate(Xs), np.concatenate(Ts)
-        sched, loss = train(X, T, steps=a.steps, lr=a.lr)
+        sched, loss = train(X, T, groups=G, steps=a.steps, lr=a.lr)
         sched.save(a.out)
         q = choice_quality(sched, X, T)
         print(json.dumps({"loss_first": float(loss[:50].mean()), "loss_last": float(loss[-50:].mean()),

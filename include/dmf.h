@@ -320,8 +320,12 @@ int dmf_sched_destroy(dmf_sched *sched);
 /* weights: DMF_SCHED_WEIGHTS bf16 bit patterns, biases: DMF_SCHED_BIASES. */
 int dmf_sched_set_weights(dmf_sched *sched, const uint16_t *weights, const float *biases);
 int dmf_sched_get_weights(dmf_sched *sched, uint16_t *weights, float *biases);
+/* The model predicts, per action, log2 of its time relative to the plain
+ * schedule; a non-plain action is picked only when predicted to win by more
+ * than `margin` log2 units (default 0.1), else the plain schedule runs. */
+int dmf_sched_set_margin(dmf_sched *sched, float margin);
 /* Trains on n samples X[n][12] -> Y[n][4] (the targets are per-action costs,
- * e.g. log2 of the time) by minibatch Adam on fp32 master weights with bf16
+ * log2 of each action's time over the plain schedule's) by minibatch Adam on fp32 master weights with bf16
  * weights in the forward pass, all on the device in one kernel: `steps`
  * minibatches of `batch` (1..64) samples drawn from `seed`, learning rate `lr`.
  * loss[steps] (may be NULL) receives the minibatch mean squared error. */
