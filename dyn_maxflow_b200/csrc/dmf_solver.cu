@@ -314,11 +314,30 @@ __device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const in
     tm.done(ls, v);
   }
   TileGroup<TILE> tg;
-  const int gi = list ? spread_group<TILE>(rot_tiles()) : (int)((blockIdx.x * blockDim.x + threadIdx.x) / TILE);
+  if (!list) {
+    // Sweep over every vertex: a tile checks TILE consecutive vertices per step
+    // (one coalesced degree read, a ballot) and then works on the medium ones
+    // it found, instead of one serial degree read per vertex.
+    const int tiles = nt / TILE;
+    for (int base = (int)((blockIdx.x * blockDim.x + threadIdx.x) / TILE) * TILE; base < nn; base += tiles * TILE) {
+      const int v = base + tg.rank();
+      const int d = v < nn ? deg_of(p, v) : 0;
+      unsigned mask = tg.g.ballot(d > p.small_deg && d <= p.hub_deg);
+      while (mask) {  // tile-uniform
+        const int vv = base + __ffs(mask) - 1;
+        mask &= mask - 1;
+        ItemTimer tm(p);
+        f(tg, vv);
+        tm.done(ls, vv);
+      }
+    }
+    return;
+  }
+  const int gi = spread_group<TILE>(rot_tiles());
   for (int i = gi; i < nn; i += nt / TILE) {
     int v = 0, d = 0;
     if (tg.rank() == 0) {
-      v = list ? __ldcg(list + i) : i;
+      v = __ldcg(list + i);
       d = deg_of(p, v);
     }
     v = tg.g.shfl(v, 0);

@@ -60,3 +60,30 @@ def test_scheduler_needs_a_device(dmf):
         pytest.skip("a GPU is visible")
     with pytest.raises(dmf.DmfError):
         dmf.Scheduler()
+
+
+def test_committed_model_on_its_traces():
+    """The shipped weights, run through the numpy forward pass and the kernel's
+    decision rule on the recorded traces: never slower than the plain schedule
+    by more than 1% per scale, and faster overall."""
+    import glob
+    import json
+    from dyn_maxflow_b200 import sched
+    d = np.load(os.path.join(ROOT, "dyn_maxflow_b200", "sched_weights.npz"))
+    w, b = d["weights"], d["biases"]
+    assert w.dtype == np.uint16 and w.shape == (5120,) and b.dtype == np.float32 and b.shape == (132,)
+    assert np.isfinite(sched.bf16_to_f32(w)).all() and np.isfinite(b).all()
+    plain_all = learned_all = 0.0
+    for p in sorted(glob.glob(os.path.join(ROOT, "dyn_maxflow_b200", "sched_data", "traces_*.npz"))):
+        t = np.load(p)
+        X, T = t["X"], t["T"].astype(np.float64)
+        scale = np.array([m["scale"] for m in json.loads(str(t["meta"]))])
+        pick = sched.pick_actions(sched.forward_reference(w, b, X))
+        for s in np.unique(scale):
+            i = scale == s
+            plain = T[i, 0].sum()
+            learned = T[i][np.arange(i.sum()), pick[i]].sum()
+            assert learned <= 1.01 * plain, (p, s, plain, learned)
+            plain_all += plain
+            learned_all += learned
+    assert plain_all > 0 and learned_all < 0.97 * plain_all
