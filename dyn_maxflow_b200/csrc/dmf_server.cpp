@@ -14,6 +14,8 @@
 // result of the same request sequence served alone.  No counterpart in the
 // reference (a one-shot bench).
 #include <algorithm>
+#include <climits>
+#include <parallel/algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -170,27 +172,46 @@ int dmf_server_submit(dmf_server *S, int32_t graph, int32_t k, const int32_t *sr
   if (!S || !ticket || k < 0 || (k > 0 && (!src || !dst || !w))) return dmf::fail(DMF_ERR_INVALID_ARG, "bad arguments");
   if (graph < 0 || graph >= (int32_t)S->graphs.size())
     return dmf::fail(DMF_ERR_INVALID_ARG, "graph %d was not admitted", graph);
+  const auto t_arrival = Clock::now();  // latency counts from here, validation included
   const dmf_graph *g = S->graphs[graph];
-  // requests are checked on their own, so one bad request never fails a tick
-  std::vector<int64_t> arcs;
+  // Requests are checked on their own, so one bad request never fails a tick:
+  // every update's arc is looked up (in parallel for large requests), then the
+  // arc ids are sorted to find repeats.  The first bad update is reported.
+  std::vector<int64_t> arcs((size_t)k);
+  int32_t bad_range = INT32_MAX, bad_cap = INT32_MAX, bad_arc = INT32_MAX;
+#pragma omp parallel for schedule(static) reduction(min : bad_range, bad_cap, bad_arc) if (k >= 16384)
   for (int32_t i = 0; i < k; i++) {
-    if (src[i] < 0 || dst[i] < 0 || src[i] >= g->n || dst[i] >= g->n)
-      return dmf::fail(DMF_ERR_INVALID_ARG, "update %d: vertex out of range", i);
-    if (w[i] < 0 || w[i] > (1 << 30) - 1) return dmf::fail(DMF_ERR_INVALID_ARG, "update %d: capacity out of range", i);
+    arcs[i] = -1;
+    if (src[i] < 0 || dst[i] < 0 || src[i] >= g->n || dst[i] >= g->n) {
+      bad_range = std::min(bad_range, i);
+      continue;
+    }
+    if (w[i] < 0 || w[i] > (1 << 30) - 1) {
+      bad_cap = std::min(bad_cap, i);
+      continue;
+    }
     if (src[i] == dst[i]) continue;
-    const int64_t e = dmf::find_arc(*g, src[i], dst[i]);
-    if (e < 0) return dmf::fail(DMF_ERR_UNKNOWN_ARC, "update %d: arc %d->%d not in graph %d", i, src[i], dst[i], graph);
-    arcs.push_back(e);
+    arcs[i] = dmf::find_arc(*g, src[i], dst[i]);
+    if (arcs[i] < 0) bad_arc = std::min(bad_arc, i);
   }
-  std::sort(arcs.begin(), arcs.end());
-  if (std::adjacent_find(arcs.begin(), arcs.end()) != arcs.end())
+  const int32_t first_bad = std::min(bad_range, std::min(bad_cap, bad_arc));
+  if (first_bad != INT32_MAX) {
+    const int32_t i = first_bad;
+    if (i == bad_range) return dmf::fail(DMF_ERR_INVALID_ARG, "update %d: vertex out of range", i);
+    if (i == bad_cap) return dmf::fail(DMF_ERR_INVALID_ARG, "update %d: capacity out of range", i);
+    return dmf::fail(DMF_ERR_UNKNOWN_ARC, "update %d: arc %d->%d not in graph %d", i, src[i], dst[i], graph);
+  }
+  if (k >= 16384) __gnu_parallel::sort(arcs.begin(), arcs.end());
+  else std::sort(arcs.begin(), arcs.end());
+  const auto first_arc = std::upper_bound(arcs.begin(), arcs.end(), (int64_t)-1);  // skip ignored self-loops
+  if (std::adjacent_find(first_arc, arcs.end()) != arcs.end())
     return dmf::fail(DMF_ERR_DUP_ARC, "an arc repeats within the request");
   auto *r = new Request();
   r->graph = graph;
   r->src.assign(src, src + k);
   r->dst.assign(dst, dst + k);
   r->w.assign(w, w + k);
-  r->t_submit = Clock::now();
+  r->t_submit = t_arrival;
   {
     std::lock_guard<std::mutex> lk(S->mu);
     r->ticket = S->next_ticket++;

@@ -64,7 +64,9 @@ struct Params {
   // per hub-chunk scratch of a push round, indexed by list position: tsum/tmin
   // per chunk; ex/alloc/moved/min at the hub's first chunk
   long long *hc_tsum, *hc_ex, *hc_moved, *hc_alloc;
-  int *hc_tmin, *hc_min;
+  int *hc_tmin;
+  int *hc_min;  // per hub (indexed by hub_base): minimum non-admissible head height of the round
+  int *hpush;   // list positions of the round's hub chunks with admissible residual
   // Exhausted hub chunks: a chunk with no admissible arc at hub height h stays
   // so until the hub's height changes or the next global relabel (heights only
   // rise in between, and a reverse residual only opens from a higher head).
@@ -301,13 +303,17 @@ __device__ __forceinline__ void ph_cut_saturate(const Params &p) {
 // vertices of degree <= small_deg one per thread over the whole grid, then the
 // larger ones (up to hub_deg; hubs are split into arc chunks and done by warps)
 // one per tile.  `f(group, v)` does the work for one vertex.
-template <int TILE, class F>
-__device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const int *list, int nn, F &&f) {
+// `pre(v)` is a per-vertex filter evaluated by one lane together with the degree
+// read (a vertex it rejects costs one round of independent loads); it must not
+// depend on writes of the current phase by other vertices' work.
+template <int TILE, class F, class Pre>
+__device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const int *list, int nn, F &&f, Pre &&pre) {
   const int nt = gridDim.x * blockDim.x;
   const int gt = list ? spread_thread(rot_threads()) : blockIdx.x * blockDim.x + threadIdx.x;
   for (int i = gt; i < nn; i += nt) {
     const int v = list ? __ldcg(list + i) : i;
-    if (deg_of(p, v) > p.small_deg) continue;
+    const bool keep = pre(v);
+    if (deg_of(p, v) > p.small_deg || !keep) continue;
     ThreadGroup th;
     ItemTimer tm(p);
     f(th, v);
@@ -322,7 +328,8 @@ __device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const in
     for (int base = (int)((blockIdx.x * blockDim.x + threadIdx.x) / TILE) * TILE; base < nn; base += tiles * TILE) {
       const int v = base + tg.rank();
       const int d = v < nn ? deg_of(p, v) : 0;
-      unsigned mask = tg.g.ballot(d > p.small_deg && d <= p.hub_deg);
+      const bool keep = v < nn && pre(v);
+      unsigned mask = tg.g.ballot(keep && d > p.small_deg && d <= p.hub_deg);
       while (mask) {  // tile-uniform
         const int vv = base + __ffs(mask) - 1;
         mask &= mask - 1;
@@ -347,6 +354,11 @@ __device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const in
     f(tg, v);
     tm.done(ls, v);
   }
+}
+
+template <int TILE, class F>
+__device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const int *list, int nn, F &&f) {
+  for_tiered<TILE>(p, ls, list, nn, f, [](int) { return true; });
 }
 
 // A hub (degree > hub_deg) enters a queue as ceil(deg / kChunk) consecutive
@@ -379,7 +391,7 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
   if (gt == 0) {
     c->act_q = 0;
     c->act_hq = 0;
-    c->wtail[0] = c->whtail[0] = c->seen[0] = 0;  // written by push round 0
+    c->wtail[0] = c->whtail[0] = c->seen[0] = c->hptail[0] = 0;  // written by push round 0
   }
   int pos = 0;
   long long unexpl = 0, seed_arcs = 0;
@@ -398,6 +410,7 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
     }
     long long ex = __ldcg(p.excess + v);
     int d = deg_of(p, v);
+    if (d > p.hub_deg) p.hc_min[__ldg(p.hub_base + v)] = INT_MAX;  // clean before the first push round
     if (is_snk(p, v) || (!is_src(p, v) && ex < 0)) {
       p.height[v] = 0;
       if (d > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
@@ -581,7 +594,7 @@ __device__ __forceinline__ void ph_bfs_bu(const Params &p, Slot *out, int L, LSt
       p.height[v] = L + 1;
       bfs_visit(p, out, nxt, v, acc);
     }
-  });
+  }, [&](int v) { return __ldcg(p.height + v) == UNV; });
   flush_visits(p, out, acc);
 }
 
@@ -967,7 +980,7 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
       c->pos_count = 0;
       c->unexplored = 0;
     }
-    c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
+    c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = c->hptail[(r + 1) % 3] = 0;
   }
   {
     TileGroup<32> wg;
@@ -983,7 +996,6 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
           p.hc_ex[i] = __ldcg(p.excess + v);
           p.hc_alloc[i] = 0;
           p.hc_moved[i] = 0;
-          p.hc_min[i] = INT_MAX;
         }
       }
       const int h = wg.g.shfl(hh, 0);
@@ -1027,14 +1039,20 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
       if (wg.rank() == 0) {
         p.hc_tsum[i] = ts;
         p.hc_tmin[i] = tm;
+        // the hub's relabel height needs every chunk; the pushes only the chunks
+        // with admissible residual, which phase 2 gets as a compact list
+        if (tm != INT_MAX) atomicMin(p.hc_min + (cidx - it.y), tm);
+        if (ts > 0) p.hpush[atomicAdd(&c->hptail[r % 3], 1)] = i;
       }
       tmr.done(ls, v);
     }
   }
   int seen = 0;
-  for_tiered<TILE>(p, ls, in.nlist, in.nn, [&](auto &g, int v) {
-    discharge(g, p, v, r, round_id, !topo, ls, topo ? &seen : nullptr);
-  });
+  // topology rounds sweep every vertex: only those with excess need a look
+  for_tiered<TILE>(
+      p, ls, in.nlist, in.nn,
+      [&](auto &g, int v) { discharge(g, p, v, r, round_id, !topo, ls, topo ? &seen : nullptr); },
+      [&](int v) { return !topo || __ldcg(p.excess + v) > 0; });
   if (topo) agg_add_int(&c->seen[r % 3], seen);
 }
 
@@ -1045,12 +1063,14 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
 // arcs: lane budgets from a warp prefix sum, then a greedy pass.  The same
 // atomics leave the hub's total admissible residual, minimum non-admissible
 // height and moved amount at its first chunk.
-__device__ __forceinline__ void ph_push2(const Params &p, const RoundIn &in, int r, unsigned round_id, unsigned gepoch,
-                         LStats &ls) {
+__device__ __forceinline__ void ph_push2(const Params &p, const Ctrl *sc, const RoundIn &in, int r, unsigned round_id,
+                                         unsigned gepoch, LStats &ls) {
   const bool topo = p.variant == DMF_VARIANT_TOPO;
   TileGroup<32> wg;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = spread_group<32>(); i < in.nh; i += nwarps) {
+  const int np = sc->hptail[r % 3];
+  for (int j = spread_group<32>(); j < np; j += nwarps) {
+    const int i = __ldcg(p.hpush + j);
     const int2 it = __ldcg(in.hlist + i);
     const int v = it.x, base = i - it.y;
     long long e0 = 0, old = 0, mine = 0;
@@ -1061,8 +1081,6 @@ __device__ __forceinline__ void ph_push2(const Params &p, const RoundIn &in, int
       if (e0 > 0 && hh < p.n && !is_term(p, v)) {
         mine = __ldcg(p.hc_tsum + i);
         old = atomic_add_ll(p.hc_alloc + base, mine);
-        const int tm = __ldcg(p.hc_tmin + i);
-        if (tm != INT_MAX) atomicMin(p.hc_min + base, tm);
       }
     }
     const int h = wg.g.shfl(hh, 0);
@@ -1131,13 +1149,15 @@ __device__ __forceinline__ void ph_push3(const Params &p, const RoundIn &in, int
     const int2 it = __ldcg(in.hlist + i);
     if (it.y != 0) continue;
     const int v = it.x;
+    const int hid = __ldg(p.hub_base + v);
+    const int mh = __ldcg(p.hc_min + hid);
+    p.hc_min[hid] = INT_MAX;  // clean for the next round
     const long long ex0 = __ldcg(p.hc_ex + i);
     int h = __ldcg(p.height + v);
     if (!(ex0 > 0 && h < p.n) || is_term(p, v)) continue;
     seen++;
     ls.visits++;
     const long long tot = __ldcg(p.hc_alloc + i);
-    const int mh = __ldcg(p.hc_min + i);
     const long long moved = __ldcg(p.hc_moved + i);
     const long long ex = ex0 - moved;
     if (moved) atomic_add_ll(p.excess + v, -moved);
@@ -1203,7 +1223,7 @@ __device__ __forceinline__ void ph_pp_init(const Params &p, Slot *out) {
   if (gt == 0) {
     c->act_q = 0;
     c->act_hq = 0;
-    c->wtail[0] = c->whtail[0] = c->seen[0] = 0;
+    c->wtail[0] = c->whtail[0] = c->seen[0] = c->hptail[0] = 0;
   }
   int pos = 0;
   for (int v = gt; v < p.n; v += nt) {
@@ -1581,7 +1601,7 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
       if (!next()) return;
       if (in.nh > 0) {
         kind = TR_PUSH_HUB;
-        ph_push2(p, in, r, round_id, p.relabel_base + it, ls);
+        ph_push2(p, sc, in, r, round_id, p.relabel_base + it, ls);
         if (!next()) return;
         kind = TR_PUSH_HUB_FINISH;
         ph_push3(p, in, r, round_id, ls);
@@ -1723,7 +1743,7 @@ struct dmf_solver {
   int2 *hch = nullptr;    // every hub's chunks
   int nchunk = 0;         // total hub chunks = capacity of each hub-chunk queue
   long long *hc_tsum = nullptr, *hc_ex = nullptr, *hc_moved = nullptr, *hc_alloc = nullptr;
-  int *hc_tmin = nullptr, *hc_min = nullptr;
+  int *hc_tmin = nullptr, *hc_min = nullptr, *hpush = nullptr;
   int *hub_base = nullptr;
   unsigned long long *chunk_mark = nullptr;
   int *chunk_tmin = nullptr;
@@ -1915,6 +1935,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.hc_tmin = sv->hc_tmin;
   p.hc_alloc = sv->hc_alloc;
   p.hc_min = sv->hc_min;
+  p.hpush = sv->hpush;
   p.hub_base = sv->hub_base;
   p.role = sv->role;
   p.inst = sv->inst;
@@ -2261,7 +2282,7 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
   p.hch = hub_dummy;
   p.nhch = 0;
   p.hc_tsum = p.hc_ex = p.hc_moved = p.hc_alloc = ll_dummy;
-  p.hc_tmin = p.hc_min = int_dummy;
+  p.hc_tmin = p.hc_min = p.hpush = int_dummy;
   p.hub_base = int_dummy;
   p.chunk_mark = mark_dummy;
   p.chunk_tmin = int_dummy;
@@ -2386,6 +2407,7 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
       (st = dalloc(sv, &sv->hc_tsum, NC)) || (st = dalloc(sv, &sv->hc_ex, NC)) ||
       (st = dalloc(sv, &sv->hc_moved, NC)) || (st = dalloc(sv, &sv->hc_tmin, NC)) ||
       (st = dalloc(sv, &sv->hc_alloc, NC)) || (st = dalloc(sv, &sv->hc_min, NC)) ||
+      (st = dalloc(sv, &sv->hpush, NC)) ||
       (st = dalloc(sv, &sv->hub_base, N)) || (st = dalloc(sv, &sv->chunk_mark, NC)) ||
       (st = dalloc(sv, &sv->chunk_tmin, NC)))
     return bail(st);

@@ -269,7 +269,8 @@ int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs,
  * next.  Batches of one graph apply in submission order.  submit() validates a
  * request on the host (vertex ranges, existing arcs, no repeats) and copies it;
  * wait() blocks until it is served and returns the graph's exact max-flow after
- * it and its latency from submission.  No counterpart in the reference. */
+ * it and its latency from the start of its submit() call (validation
+ * included).  No counterpart in the reference. */
 typedef struct dmf_server dmf_server;
 int dmf_server_create(int32_t count, const dmf_graph *const *graphs,
                       const int32_t *s, const int32_t *t, int64_t hbm_budget,
