@@ -694,6 +694,9 @@ __device__ __forceinline__ void enqueue_batch(const Params &p, const int (&x)[K]
 template <int K>
 __device__ __forceinline__ void push_batch(const Params &p, const int (&a)[K], const int (&w)[K], const int (&d)[K],
                                            int r, unsigned round_id, bool enq, LStats &ls) {
+  int pk[K];  // partner arcs, loaded while the atomics below are in flight
+#pragma unroll
+  for (int k = 0; k < K; k++) pk[k] = d[k] > 0 ? __ldg(p.par + a[k]) : 0;
   long long old[K];
 #pragma unroll
   for (int k = 0; k < K; k++)
@@ -705,7 +708,7 @@ __device__ __forceinline__ void push_batch(const Params &p, const int (&a)[K], c
 #pragma unroll
   for (int k = 0; k < K; k++)
     if (d[k] > 0) {
-      atomicAdd(p.res + __ldg(p.par + a[k]), d[k]);
+      atomicAdd(p.res + pk[k], d[k]);
       ls.pushes++;
       if (enq && !is_term(p, w[k]) && old[k] + d[k] > 0) cand |= 1u << k;
     }
@@ -754,6 +757,9 @@ __device__ __forceinline__ void discharge_small(const Params &p, int v, int beg,
         left -= dd[k];
       }
     }
+    int pk[kSmallMax];  // partner arcs, loaded while the atomics below are in flight
+#pragma unroll
+    for (int k = 0; k < kSmallMax; k++) pk[k] = dd[k] > 0 ? __ldg(p.par + beg + k) : 0;
     long long old[kSmallMax];
 #pragma unroll
     for (int k = 0; k < kSmallMax; k++)
@@ -764,7 +770,7 @@ __device__ __forceinline__ void discharge_small(const Params &p, int v, int beg,
 #pragma unroll
     for (int k = 0; k < kSmallMax; k++)
       if (dd[k] > 0) {
-        atomicAdd(p.res + __ldg(p.par + beg + k), dd[k]);
+        atomicAdd(p.res + pk[k], dd[k]);
         rr[k] -= dd[k];
         ls.pushes++;
         if (enq && !is_term(p, w[k]) && old[k] + dd[k] > 0) cand |= 1u << k;
