@@ -53,7 +53,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-certify", action="store_true")
     ap.add_argument("--cpu-batches", type=int, default=3)
-    ap.add_argument("--workload", default="rmat20", choices=["rmat20", "batched", "learned", "serving"],
+    ap.add_argument("--workload", default="rmat20", choices=["rmat20", "grid256", "batched", "learned", "serving"],
                     help="rmat20: the headline single-graph workload (scale from --scale); batched: 256 "
                          "independent instances in one device state, 5 successive batches; learned: the "
                          "learned schedule picker against the plain schedule on held-out R-MAT instances")
@@ -400,6 +400,74 @@ def run_batched(args, rank: int, world: int):
     }
 
 
+def run_grid(args, rank: int, world: int):
+    """The plain-method small configuration: 4-neighbour 256x256 grid (caps
+    U[1,100] from seed 0, s = (0,0) joined to column 0 and t = (255,255) fed from
+    column 255 by capacity-1000 arcs), static max-flow, then one batch touching
+    1% of the arcs (half +U[1,50], half max(0, c - U[1,50])).  Each step applies
+    the batch to a copy of the post-static state (device pointers, CUDA events);
+    the static solve is timed once per step as well."""
+    import numpy as np
+    import torch
+    import dyn_maxflow_b200 as D
+    from oracle import oracle as O
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import make_config
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    g, s, t, (batch,) = make_config("grid256")
+    stream = torch.cuda.Stream()
+    trunk = D.Solver(g, s, t, stream=stream)
+    work = D.Solver(g, s, t, stream=stream)
+    dS, dD, dW = (torch.as_tensor(np.ascontiguousarray(a, np.int32), device="cuda") for a in batch)
+    k = len(batch[0])
+    static_ms, batch_ms, flows = [], [], set()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    for step in range(args.warmup + args.steps):
+        f0 = trunk.static_maxflow()
+        st_ms = trunk.stats()["last_ms"]
+        work.copy_state_from(trunk)
+        torch.cuda.synchronize()
+        f1 = work.apply_updates_device(dS.data_ptr(), dD.data_ptr(), dW.data_ptr(), k)
+        if step >= args.warmup:
+            static_ms.append(st_ms)
+            batch_ms.append(work.stats()["last_ms"])
+            flows.add((f0, f1))
+    clk = clocks.stop()
+    # end to end through the host-array entry point
+    e2e = []
+    for step in range(args.steps):
+        work.copy_state_from(trunk)
+        t0 = time.perf_counter()
+        work.apply_updates(*batch)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    off, adj, w, par = g.arrays()
+    cur = w.copy()
+    for a, b, c in zip(*batch):
+        if a != b:
+            cur[g.find_arc(int(a), int(b))] = c
+    want = (O.dinic(g.num_nodes(), off, adj, w, par, s, t), O.dinic(g.num_nodes(), off, adj, cur, par, s, t))
+    exact = flows == {want}
+    ref = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_flows.json")))["grid256"]["runs"]["data/sm100a"]
+    ref_dyn = [x["dyn_ms"] for x in ref[0]["runs"]]
+    ref_static = [x["recompute_ms"] for x in ref[0]["runs"]]
+    trunk.close()
+    work.close()
+    p50 = pct(batch_ms, 0.5)
+    return {
+        "metric": METRIC + ", 256x256 grid", "value": round(p50, 3), "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(float(np.mean(batch_ms)), 3),
+        "p99_ms": round(pct(batch_ms, 0.99), 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32 (int64 excess)", "data": "synthetic (seeded grid and batch)",
+        "config": {"workload": "grid256-static+1pct", "vertices": g.num_nodes(), "csr_arcs": g.num_edges(),
+                   "batch_updates": k, "l2": "graph (3 MB) is L2-resident; latency-bound phases"},
+        "static_ms_p50": round(pct(static_ms, 0.5), 3), "flows": list(want), "exact": bool(exact),
+        "reference_data_bench_ms": {"dyn_per_batch": ref_dyn, "static_update": ref_static,
+                                    "source": "tests/golden/reference_flows.json (reference CUDA binary, same B200 type)"},
+        "e2e": {"value": round(pct(e2e, 0.5), 3), "unit": "ms", "h2d_bytes_per_step": 12 * k, "d2h_bytes_per_step": 8},
+        "clocks": clk, "gpu_launches": 2 * (args.warmup + args.steps),
+    }
+
+
 def run_learned(args, rank: int, world: int):
     """The learned schedule picker (weights trained on solver-recorded traces of
     R-MAT scales 16-22) against the plain schedule on held-out seeds: both run
@@ -587,6 +655,8 @@ def main():
             res = run_reference(args, rank)
         elif args.workload == "batched":
             res = run_batched(args, rank, world)
+        elif args.workload == "grid256":
+            res = run_grid(args, rank, world)
         elif args.workload == "learned":
             res = run_learned(args, rank, world)
         elif args.workload == "serving":
