@@ -57,7 +57,6 @@ struct Ctrl {
   int trace_len;              // entries written to the optional timeline
   // push-round worklist tails and topology-driven active counts, round r uses [r % 3]
   int wtail[3], whtail[3], seen[3];
-  int hptail[3];              // hub chunks with admissible residual in round r (compact list)
   int pad1;
   unsigned long long probe[2];  // longest work item of a phase, (ns << 32) | vertex
   unsigned long long blk[2];    // longest block work of a phase (ns), barrier exit to arrival

@@ -61,12 +61,10 @@ struct Params {
   int2 *fh[2], *wh[2], *ah;    // hub chunk queues
   const int2 *hch;             // every hub's chunks (bottom-up BFS, topology-driven rounds)
   int nhch;
-  // per hub-chunk scratch of a push round, indexed by list position: tsum/tmin
-  // per chunk; ex/alloc/moved/min at the hub's first chunk
-  long long *hc_tsum, *hc_ex, *hc_moved, *hc_alloc;
-  int *hc_tmin;
-  int *hc_min;  // per hub (indexed by hub_base): minimum non-admissible head height of the round
-  int *hpush;   // list positions of the round's hub chunks with admissible residual
+  // per hub (indexed by hub_base), totals of the current push round:
+  long long *hc_alloc;  // admissible residual claimed by the hub's chunks
+  long long *hc_moved;  // excess pushed by them
+  int *hc_min;          // minimum non-admissible head height
   // Exhausted hub chunks: a chunk with no admissible arc at hub height h stays
   // so until the hub's height changes or the next global relabel (heights only
   // rise in between, and a reverse residual only opens from a higher head).
@@ -391,7 +389,7 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
   if (gt == 0) {
     c->act_q = 0;
     c->act_hq = 0;
-    c->wtail[0] = c->whtail[0] = c->seen[0] = c->hptail[0] = 0;  // written by push round 0
+    c->wtail[0] = c->whtail[0] = c->seen[0] = 0;  // written by push round 0
   }
   int pos = 0;
   long long unexpl = 0, seed_arcs = 0;
@@ -410,7 +408,12 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
     }
     long long ex = __ldcg(p.excess + v);
     int d = deg_of(p, v);
-    if (d > p.hub_deg) p.hc_min[__ldg(p.hub_base + v)] = INT_MAX;  // clean before the first push round
+    if (d > p.hub_deg) {  // the hub's round totals start clean
+      const int hid = __ldg(p.hub_base + v);
+      p.hc_min[hid] = INT_MAX;
+      p.hc_alloc[hid] = 0;
+      p.hc_moved[hid] = 0;
+    }
     if (is_snk(p, v) || (!is_src(p, v) && ex < 0)) {
       p.height[v] = 0;
       if (d > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
@@ -973,8 +976,8 @@ __device__ __forceinline__ RoundIn round_inputs(const Params &p, const Ctrl *c, 
 }
 
 // Push round, phase 1: non-hub vertices are discharged completely; every hub
-// chunk computes its admissible residual sum and its minimum non-admissible
-// height (chunk 0 also snapshots the hub's excess and clears its totals).
+// chunk sums its admissible residual, adds its minimum non-admissible head
+// height to the hub's, and pushes its share of the hub's excess.
 template <int TILE, int BLOCK>
 __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned round_id, unsigned gepoch, LStats &ls,
                          typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
@@ -986,9 +989,15 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
       c->pos_count = 0;
       c->unexplored = 0;
     }
-    c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = c->hptail[(r + 1) % 3] = 0;
+    c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
   }
   {
+    // Hub chunks: scan, then claim a share of the hub's excess and push it from
+    // the scan's registers, in one phase.  A hub's excess only grows during the
+    // phase (its own pushes leave it in phase 2), so each chunk's read of it is
+    // at most the hub's excess at the end of the phase, and the shares claimed
+    // in arc-chunk order by the atomic on the hub's allocation never add up to
+    // more than that.
     TileGroup<32> wg;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int i = spread_group<32>(); i < in.nh; i += nwarps) {
@@ -996,59 +1005,79 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
       const int v = it.x;
       ItemTimer tmr(p);
       int hh = 0;
-      if (wg.rank() == 0) {
-        hh = __ldcg(p.height + v);
-        if (it.y == 0) {
-          p.hc_ex[i] = __ldcg(p.excess + v);
-          p.hc_alloc[i] = 0;
-          p.hc_moved[i] = 0;
-        }
-      }
+      if (wg.rank() == 0) hh = __ldcg(p.height + v);
       const int h = wg.g.shfl(hh, 0);
-      const int cidx = __ldg(p.hub_base + v) + it.y;
+      const int hid = __ldg(p.hub_base + v), cidx = hid + it.y;
       const unsigned long long key = ((unsigned long long)gepoch << 32) | (unsigned)h;
       unsigned long long mk = 0;
       if (wg.rank() == 0) mk = __ldcg(p.chunk_mark + cidx);
       mk = wg.g.shfl(mk, 0);
-      long long ts = 0;
-      int tm = INT_MAX;
       if (mk == key) {  // exhausted at this height: only its minimum head height matters
-        if (wg.rank() == 0) tm = __ldcg(p.chunk_tmin + cidx);
+        if (wg.rank() == 0) {
+          const int tm = __ldcg(p.chunk_tmin + cidx);
+          if (tm != INT_MAX) atomicMin(p.hc_min + hid, tm);
+        }
       } else if (h < p.n && !is_term(p, v)) {
         int beg, end;
         chunk_range(p, it, beg, end);
-        int rr[kBatch], w[kBatch];
+        int aa[kBatch], rr[kBatch], w[kBatch], hw[kBatch];
 #pragma unroll
         for (int k = 0; k < kBatch; k++) {
-          const int a = beg + wg.rank() + 32 * k;
-          rr[k] = a < end ? __ldcg(p.res + a) : 0;
-          w[k] = a < end ? __ldg(p.adj + a) : 0;
+          aa[k] = beg + wg.rank() + 32 * k;
+          rr[k] = aa[k] < end ? __ldcg(p.res + aa[k]) : 0;
+          w[k] = aa[k] < end ? __ldg(p.adj + aa[k]) : 0;
         }
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) hw[k] = rr[k] > 0 ? __ldcg(p.height + w[k]) : INT_MAX;
         long long tsum = 0;
         int tmin = INT_MAX;
 #pragma unroll
         for (int k = 0; k < kBatch; k++) {
           if (rr[k] > 0) {
-            const int hw = __ldcg(p.height + w[k]);
-            if (hw < h) tsum += rr[k];
-            else tmin = min(tmin, hw);
+            if (hw[k] < h) tsum += rr[k];
+            else tmin = min(tmin, hw[k]);
           }
         }
         ls.arcs += kBatch;
-        ts = wg.sum_all(tsum);
-        tm = wg.min_all(tmin);
-        if (ts == 0 && wg.rank() == 0) {
+        long long ts;
+        const long long pre = wg.scan(tsum, ts);
+        const int tm = wg.min_all(tmin);
+        long long cb = 0;  // this chunk's share of the hub's excess
+        if (wg.rank() == 0) {
+          if (tm != INT_MAX) atomicMin(p.hc_min + hid, tm);
+          if (ts > 0) {
+            const long long exr = __ldcg(p.excess + v);
+            const long long old = atomic_add_ll(p.hc_alloc + hid, ts);
+            cb = exr - old;
+            cb = cb < 0 ? 0 : (cb > ts ? ts : cb);
+          }
+        }
+        cb = wg.g.shfl(cb, 0);
+        long long moved = 0;
+        if (cb > 0) {  // warp-uniform
+          long long budget = cb - pre;
+          budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
+          long long done = 0;
+          int dd[kBatch];
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) {
+            dd[k] = 0;
+            if (rr[k] > 0 && hw[k] < h && budget > 0) {
+              dd[k] = (int)(rr[k] < budget ? rr[k] : budget);
+              budget -= dd[k];
+              done += dd[k];
+            }
+          }
+          push_batch<kBatch>(p, aa, w, dd, r, round_id, !topo, ls);
+          moved = wg.sum_all(done);
+          if (wg.rank() == 0 && moved) atomic_add_ll(p.hc_moved + hid, moved);
+        }
+        // no admissible arc left in the chunk at this height: skip it until the
+        // hub's height or the relabel epoch changes
+        if (wg.rank() == 0 && moved == ts) {
           p.chunk_mark[cidx] = key;
           p.chunk_tmin[cidx] = tm;
         }
-      }
-      if (wg.rank() == 0) {
-        p.hc_tsum[i] = ts;
-        p.hc_tmin[i] = tm;
-        // the hub's relabel height needs every chunk; the pushes only the chunks
-        // with admissible residual, which phase 2 gets as a compact list
-        if (tm != INT_MAX) atomicMin(p.hc_min + (cidx - it.y), tm);
-        if (ts > 0) p.hpush[atomicAdd(&c->hptail[r % 3], 1)] = i;
       }
       tmr.done(ls, v);
     }
@@ -1062,91 +1091,10 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
   if (topo) agg_add_int(&c->seen[r % 3], seen);
 }
 
-// Push round, phase 2: each hub chunk takes its share of the hub's excess by an
-// atomic prefix over the chunks' admissible residual sums (the order of the
-// atomics decides which chunk pushes first; the sum pushed is exactly
-// min(excess, total admissible residual)), then pushes it over its admissible
-// arcs: lane budgets from a warp prefix sum, then a greedy pass.  The same
-// atomics leave the hub's total admissible residual, minimum non-admissible
-// height and moved amount at its first chunk.
-__device__ __forceinline__ void ph_push2(const Params &p, const Ctrl *sc, const RoundIn &in, int r, unsigned round_id,
-                                         unsigned gepoch, LStats &ls) {
-  const bool topo = p.variant == DMF_VARIANT_TOPO;
-  TileGroup<32> wg;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int np = sc->hptail[r % 3];
-  for (int j = spread_group<32>(); j < np; j += nwarps) {
-    const int i = __ldcg(p.hpush + j);
-    const int2 it = __ldcg(in.hlist + i);
-    const int v = it.x, base = i - it.y;
-    long long e0 = 0, old = 0, mine = 0;
-    int hh = 0;
-    if (wg.rank() == 0) {
-      hh = __ldcg(p.height + v);
-      e0 = __ldcg(p.hc_ex + base);
-      if (e0 > 0 && hh < p.n && !is_term(p, v)) {
-        mine = __ldcg(p.hc_tsum + i);
-        old = atomic_add_ll(p.hc_alloc + base, mine);
-      }
-    }
-    const int h = wg.g.shfl(hh, 0);
-    const long long ex0 = wg.g.shfl(e0, 0);
-    if (!(ex0 > 0 && h < p.n) || is_term(p, v)) continue;
-    old = wg.g.shfl(old, 0);
-    mine = wg.g.shfl(mine, 0);
-    long long cb = ex0 - old;
-    cb = cb < 0 ? 0 : (cb > mine ? mine : cb);
-    if (cb == 0) continue;  // warp-uniform
-    int beg, end;
-    chunk_range(p, it, beg, end);
-    int rr[kBatch], w[kBatch];
-    bool adm[kBatch];
-    long long tsum = 0;
-#pragma unroll
-    for (int k = 0; k < kBatch; k++) {
-      const int a = beg + wg.rank() + 32 * k;
-      rr[k] = a < end ? __ldcg(p.res + a) : 0;
-      w[k] = a < end ? __ldg(p.adj + a) : 0;
-    }
-#pragma unroll
-    for (int k = 0; k < kBatch; k++) {
-      adm[k] = rr[k] > 0 && __ldcg(p.height + w[k]) < h;
-      if (adm[k]) tsum += rr[k];
-    }
-    long long tot;
-    const long long pre = wg.scan(tsum, tot);
-    long long budget = cb - pre;
-    budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
-    long long done = 0;
-    // residuals only grew since the loads (reverse pushes), so rr is a safe amount
-    int aa[kBatch], dd[kBatch];
-#pragma unroll
-    for (int k = 0; k < kBatch; k++) {
-      aa[k] = beg + wg.rank() + 32 * k;
-      dd[k] = 0;
-      if (adm[k] && budget > 0) {
-        dd[k] = (int)(rr[k] < budget ? rr[k] : budget);
-        budget -= dd[k];
-        done += dd[k];
-      }
-    }
-    push_batch<kBatch>(p, aa, w, dd, r, round_id, !topo, ls);
-    const long long moved = wg.sum_all(done);
-    if (wg.rank() == 0) {
-      if (moved) atomic_add_ll(p.hc_moved + base, moved);
-      if (moved == mine && cb == mine) {  // every admissible arc of the chunk saturated
-        const int cidx = __ldg(p.hub_base + v) + it.y;
-        p.chunk_mark[cidx] = ((unsigned long long)gepoch << 32) | (unsigned)h;
-        p.chunk_tmin[cidx] = __ldcg(p.hc_tmin + i);
-      }
-    }
-  }
-}
-
-// Push round, phase 3: per hub (its first chunk), the moved total leaves its
-// excess; when all of the hub's admissible residual was pushed and excess is
+// Push round, phase 2 (hubs): per hub (its first chunk), the moved total leaves
+// its excess; when all of the hub's admissible residual was pushed and excess is
 // left, the hub is relabelled to 1 + the minimum non-admissible height; a hub
-// with excess left is queued for the next round.
+// with excess left is queued for the next round.  The hub's totals are reset.
 __device__ __forceinline__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls) {
   const int nt = gridDim.x * blockDim.x;
   const bool topo = p.variant == DMF_VARIANT_TOPO;
@@ -1156,18 +1104,20 @@ __device__ __forceinline__ void ph_push3(const Params &p, const RoundIn &in, int
     if (it.y != 0) continue;
     const int v = it.x;
     const int hid = __ldg(p.hub_base + v);
+    const long long tot = __ldcg(p.hc_alloc + hid), moved = __ldcg(p.hc_moved + hid);
     const int mh = __ldcg(p.hc_min + hid);
-    p.hc_min[hid] = INT_MAX;  // clean for the next round
-    const long long ex0 = __ldcg(p.hc_ex + i);
+    const long long ex0 = __ldcg(p.excess + v);
     int h = __ldcg(p.height + v);
+    // clean for the next round
+    p.hc_alloc[hid] = 0;
+    p.hc_moved[hid] = 0;
+    p.hc_min[hid] = INT_MAX;
     if (!(ex0 > 0 && h < p.n) || is_term(p, v)) continue;
     seen++;
     ls.visits++;
-    const long long tot = __ldcg(p.hc_alloc + i);
-    const long long moved = __ldcg(p.hc_moved + i);
     const long long ex = ex0 - moved;
     if (moved) atomic_add_ll(p.excess + v, -moved);
-    if (ex > 0 && moved == tot) {
+    if (ex > 0 && moved == tot) {  // every admissible arc saturated: relabel
       h = mh >= p.n ? p.n : mh + 1;
       p.height[v] = h;
       ls.relabels++;
@@ -1229,7 +1179,7 @@ __device__ __forceinline__ void ph_pp_init(const Params &p, Slot *out) {
   if (gt == 0) {
     c->act_q = 0;
     c->act_hq = 0;
-    c->wtail[0] = c->whtail[0] = c->seen[0] = c->hptail[0] = 0;
+    c->wtail[0] = c->whtail[0] = c->seen[0] = 0;
   }
   int pos = 0;
   for (int v = gt; v < p.n; v += nt) {
@@ -1606,9 +1556,6 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
       ph_push1<TILE, BLOCK>(p, in, r, round_id, p.relabel_base + it, ls, btmp, bci, bcl);
       if (!next()) return;
       if (in.nh > 0) {
-        kind = TR_PUSH_HUB;
-        ph_push2(p, sc, in, r, round_id, p.relabel_base + it, ls);
-        if (!next()) return;
         kind = TR_PUSH_HUB_FINISH;
         ph_push3(p, in, r, round_id, ls);
         if (!next()) return;
@@ -1748,8 +1695,8 @@ struct dmf_solver {
   int2 *hqbuf = nullptr;  // 5 hub-chunk queues, same roles
   int2 *hch = nullptr;    // every hub's chunks
   int nchunk = 0;         // total hub chunks = capacity of each hub-chunk queue
-  long long *hc_tsum = nullptr, *hc_ex = nullptr, *hc_moved = nullptr, *hc_alloc = nullptr;
-  int *hc_tmin = nullptr, *hc_min = nullptr, *hpush = nullptr;
+  long long *hc_moved = nullptr, *hc_alloc = nullptr;  // per hub, push-round totals
+  int *hc_min = nullptr;
   int *hub_base = nullptr;
   unsigned long long *chunk_mark = nullptr;
   int *chunk_tmin = nullptr;
@@ -1935,13 +1882,9 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.ah = sv->hqbuf + 4 * NC;
   p.hch = sv->hch;
   p.nhch = sv->nchunk;
-  p.hc_tsum = sv->hc_tsum;
-  p.hc_ex = sv->hc_ex;
   p.hc_moved = sv->hc_moved;
-  p.hc_tmin = sv->hc_tmin;
   p.hc_alloc = sv->hc_alloc;
   p.hc_min = sv->hc_min;
-  p.hpush = sv->hpush;
   p.hub_base = sv->hub_base;
   p.role = sv->role;
   p.inst = sv->inst;
@@ -2287,8 +2230,8 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
   p.fh[0] = p.fh[1] = p.wh[0] = p.wh[1] = p.ah = hub_dummy;
   p.hch = hub_dummy;
   p.nhch = 0;
-  p.hc_tsum = p.hc_ex = p.hc_moved = p.hc_alloc = ll_dummy;
-  p.hc_tmin = p.hc_min = p.hpush = int_dummy;
+  p.hc_moved = p.hc_alloc = ll_dummy;
+  p.hc_min = int_dummy;
   p.hub_base = int_dummy;
   p.chunk_mark = mark_dummy;
   p.chunk_tmin = int_dummy;
@@ -2410,10 +2353,8 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
   sv->nchunk = (int)hub_chunks.size();
   const size_t NC = (size_t)std::max(sv->nchunk, 1);
   if ((st = dalloc(sv, &sv->hqbuf, 5 * NC)) || (st = dalloc(sv, &sv->hch, NC)) ||
-      (st = dalloc(sv, &sv->hc_tsum, NC)) || (st = dalloc(sv, &sv->hc_ex, NC)) ||
-      (st = dalloc(sv, &sv->hc_moved, NC)) || (st = dalloc(sv, &sv->hc_tmin, NC)) ||
-      (st = dalloc(sv, &sv->hc_alloc, NC)) || (st = dalloc(sv, &sv->hc_min, NC)) ||
-      (st = dalloc(sv, &sv->hpush, NC)) ||
+      (st = dalloc(sv, &sv->hc_moved, NC)) || (st = dalloc(sv, &sv->hc_alloc, NC)) ||
+      (st = dalloc(sv, &sv->hc_min, NC)) ||
       (st = dalloc(sv, &sv->hub_base, N)) || (st = dalloc(sv, &sv->chunk_mark, NC)) ||
       (st = dalloc(sv, &sv->chunk_tmin, NC)))
     return bail(st);
