@@ -473,8 +473,10 @@ def run_learned(args, rank: int, world: int):
     R-MAT scales 16-22) against the plain schedule on held-out seeds: both run
     side by side from the same start and must give identical flows every batch;
     every batch is also timed under all four schedules from the learned
-    solver's state for the regret.  Times are CUDA-event times of the host-array
-    entry point (batch staging, features and decision included)."""
+    solver's state, and the learned and plain times of a batch are those of the
+    picked action and of the plain one from that same state (paired timing).
+    Times are CUDA-event times of the host-array entry point (batch staging,
+    features and decision included)."""
     import torch
     import dyn_maxflow_b200 as D
     from dyn_maxflow_b200 import sched as S
@@ -503,7 +505,8 @@ def run_learned(args, rank: int, world: int):
         "config": {"workload": f"learned-rmat{args.learn_scale}-heldout", "seeds": seeds,
                    "vertices": n, "batches_per_seed": args.steps, "batch_fraction": [lo, hi],
                    "l2": "inputs (67M-arc CSR) larger than L2"},
-        "plain": ev["plain"], "learned": lp, "best_total_ms": ev.get("best_total_ms"),
+        "plain": ev["plain"], "learned": lp, "best_total_ms": ev.get("best_total_ms"), "timing": ev["timing"],
+        "live_solvers": ev["live_solvers"],
         "speedup_vs_plain": round(ev["speedup_vs_plain"], 4),
         "regret_vs_best": round(ev.get("regret_vs_best", 0.0), 4),
         "plain_regret_vs_best": round(ev.get("plain_regret_vs_best", 0.0), 4),

@@ -994,10 +994,10 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
   {
     // Hub chunks: scan, then claim a share of the hub's excess and push it from
     // the scan's registers, in one phase.  A hub's excess only grows during the
-    // phase (its own pushes leave it in phase 2), so each chunk's read of it is
-    // at most the hub's excess at the end of the phase, and the shares claimed
-    // in arc-chunk order by the atomic on the hub's allocation never add up to
-    // more than that.
+    // phase (its own pushes leave it in phase 2), so each chunk's read of it at
+    // the start of its item is at most the hub's excess at the end of the
+    // phase, and the shares claimed in arc-chunk order by the atomic on the
+    // hub's allocation never add up to more than that.
     TileGroup<32> wg;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int i = spread_group<32>(); i < in.nh; i += nwarps) {
@@ -1005,7 +1005,11 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
       const int v = it.x;
       ItemTimer tmr(p);
       int hh = 0;
-      if (wg.rank() == 0) hh = __ldcg(p.height + v);
+      long long ex_start = 0;  // the hub's excess as the phase found it
+      if (wg.rank() == 0) {
+        hh = __ldcg(p.height + v);
+        ex_start = __ldcg(p.excess + v);
+      }
       const int h = wg.g.shfl(hh, 0);
       const int hid = __ldg(p.hub_base + v), cidx = hid + it.y;
       const unsigned long long key = ((unsigned long long)gepoch << 32) | (unsigned)h;
@@ -1045,10 +1049,9 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
         long long cb = 0;  // this chunk's share of the hub's excess
         if (wg.rank() == 0) {
           if (tm != INT_MAX) atomicMin(p.hc_min + hid, tm);
-          if (ts > 0) {
-            const long long exr = __ldcg(p.excess + v);
+          if (ts > 0 && ex_start > 0) {  // (topology rounds also sweep hubs without excess)
             const long long old = atomic_add_ll(p.hc_alloc + hid, ts);
-            cb = exr - old;
+            cb = ex_start - old;
             cb = cb < 0 ? 0 : (cb > ts ? ts : cb);
           }
         }

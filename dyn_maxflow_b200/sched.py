@@ -166,12 +166,21 @@ def choice_quality(sched, X, T) -> dict:
 
 
 def evaluate(sched, specs, batches: int, frac_lo: float, frac_hi: float, oracle=True, verbose=True, warmup=1):
-    """Runs the plain schedule and the learned one side by side on held-out
-    instances (`warmup` untimed batches of 0.1% first); both must give
-    identical flows.  With `oracle`, every batch is also timed under all actions
-    from the learned solver's state (the best of them is the regret's
-    yardstick)."""
+    """The learned schedule against the plain one on held-out instances
+    (`warmup` untimed batches of 0.1% first).
+
+    Paired timing (oracle=True): before the learned solver applies a batch, the
+    batch is solved under every action from a copy of the learned solver's
+    state; the learned time of the batch is the time of the action it picks,
+    the plain time that of action 0, both from the same state.  (Two solvers
+    that apply the same batches independently hold different residual flows --
+    push-relabel's atomics make the flow decomposition vary -- so their times
+    differ by several per cent even under the same schedule.)  A plain solver
+    also runs its own trajectory; every flow of every action and of both
+    solvers must be identical.  With oracle=False only the two live solvers
+    are timed."""
     plain_ms, learned_ms, best_ms, picks, exact = [], [], [], [], True
+    live_plain, live_learned = [], []
     for scale, seed in specs:
         g, s, t = rmat_instance(scale, seed)
         P = D.Solver(g, s, t)
@@ -185,22 +194,32 @@ def evaluate(sched, specs, batches: int, frac_lo: float, frac_hi: float, oracle=
             bs, bd, bw = next_batch(g, 1e-3, seed * 7919 + 99991 + wi)
             P.apply_updates_scheduled(None, bs, bd, bw)
             L.apply_updates_scheduled(sched, bs, bd, bw)
-            g.set_caps(bs, bd, bw)
-        for b, frac in enumerate(fracs):
-            bs, bd, bw = next_batch(g, frac, seed * 7919 + b)
             if O is not None:
-                t_all = []
                 for a in range(D.N_ACTIONS):
                     O.copy_state_from(L)
                     O.apply_updates_action(a, bs, bd, bw)
+            g.set_caps(bs, bd, bw)
+        for b, frac in enumerate(fracs):
+            bs, bd, bw = next_batch(g, frac, seed * 7919 + b)
+            t_all, f_all = [], []
+            if O is not None:
+                for a in range(D.N_ACTIONS):
+                    O.copy_state_from(L)
+                    f_all.append(O.apply_updates_action(a, bs, bd, bw))
                     t_all.append(O.stats()["last_ms"])
-                best_ms.append(min(t_all))
             fp, _ = P.apply_updates_scheduled(None, bs, bd, bw)
-            plain_ms.append(P.stats()["last_ms"])
+            live_plain.append(P.stats()["last_ms"])
             fl, a = L.apply_updates_scheduled(sched, bs, bd, bw)
-            learned_ms.append(L.stats()["last_ms"])
+            live_learned.append(L.stats()["last_ms"])
             picks.append(a)
-            exact &= fp == fl
+            exact &= fp == fl and all(f == fl for f in f_all)
+            if t_all:
+                plain_ms.append(t_all[0])
+                learned_ms.append(t_all[a])
+                best_ms.append(min(t_all))
+            else:
+                plain_ms.append(live_plain[-1])
+                learned_ms.append(live_learned[-1])
             g.set_caps(bs, bd, bw)
         for x in (P, L, O):
             if x is not None:
@@ -211,11 +230,13 @@ def evaluate(sched, specs, batches: int, frac_lo: float, frac_hi: float, oracle=
     def pct(v, q):
         return float(np.percentile(np.asarray(v), q)) if v else None
 
+    def summary(v):
+        return {"total_ms": float(np.sum(v)), "p50_ms": pct(v, 50), "p99_ms": pct(v, 99)}
+
     out = {
-        "batches": len(plain_ms), "exact_equal_flows": bool(exact),
-        "plain": {"total_ms": float(np.sum(plain_ms)), "p50_ms": pct(plain_ms, 50), "p99_ms": pct(plain_ms, 99)},
-        "learned": {"total_ms": float(np.sum(learned_ms)), "p50_ms": pct(learned_ms, 50),
-                    "p99_ms": pct(learned_ms, 99)},
+        "batches": len(plain_ms), "exact_equal_flows": bool(exact), "timing": "paired" if best_ms else "live",
+        "plain": summary(plain_ms), "learned": summary(learned_ms),
+        "live_solvers": {"plain": summary(live_plain), "learned": summary(live_learned)},
         "pick_hist": np.bincount(np.asarray(picks, int), minlength=D.N_ACTIONS).tolist(),
         "per_batch": {"plain_ms": [round(x, 4) for x in plain_ms], "learned_ms": [round(x, 4) for x in learned_ms],
                       "best_ms": [round(x, 4) for x in best_ms], "picks": [int(a) for a in picks]},
