@@ -82,3 +82,52 @@ def test_bad_requests_are_rejected_alone(dmf):
         with dmf.Solver(g, s, t) as sv:
             sv.static_maxflow()
             assert f == sv.apply_updates(*batches[0])
+
+
+def test_large_requests_validated_in_parallel(dmf, oracle):
+    """Requests of 16k+ updates take the parallel validation path: a repeated
+    arc, an unknown arc, an out-of-range vertex and an out-of-range capacity
+    are each rejected with their status, and nothing of a rejected request is
+    applied; a valid large request is served with the exact flow."""
+    g, s, t, (b,) = make_config_rmat14_one()
+    k = len(b[0])
+    assert k >= 16384
+    off, adj, w, par = g.arrays()
+    n = g.num_nodes()
+    with dmf.Server([g], [s], [t], 1 << 31) as srv:
+        src, dst, cap = (x.copy() for x in b)
+        dup = (np.concatenate([src, src[:1]]), np.concatenate([dst, dst[:1]]), np.concatenate([cap, cap[:1]]))
+        with pytest.raises(dmf.DmfError) as ei:
+            srv.submit(0, *dup)
+        assert ei.value.status == 4  # DMF_ERR_DUP_ARC
+        missing = next((a, c) for a in range(n) for c in range(n) if a != c and g.find_arc(a, c) < 0)
+        unk = (src.copy(), dst.copy(), cap.copy())
+        unk[0][k // 2], unk[1][k // 2] = missing
+        with pytest.raises(dmf.DmfError) as ei:
+            srv.submit(0, *unk)
+        assert ei.value.status == 3  # DMF_ERR_UNKNOWN_ARC
+        oor = (src.copy(), dst.copy(), cap.copy())
+        oor[1][k - 1] = n
+        with pytest.raises(dmf.DmfError) as ei:
+            srv.submit(0, *oor)
+        assert ei.value.status == 1
+        big = (src.copy(), dst.copy(), cap.copy())
+        big[2][7] = 1 << 30
+        with pytest.raises(dmf.DmfError) as ei:
+            srv.submit(0, *big)
+        assert ei.value.status == 1
+        f, _ = srv.wait(srv.submit(0, src, dst, cap))
+    cur = w.copy()
+    for a, c, x in zip(src, dst, cap):
+        if a != c:
+            cur[g.find_arc(int(a), int(c))] = x
+    assert f == oracle.dinic(n, off, adj, cur, par, s, t)
+
+
+def make_config_rmat14_one():
+    """R-MAT 14 with one batch of 8% of its arcs (about 40k updates)."""
+    import dyn_maxflow_b200 as D
+    narcs = 16 << 14
+    g, s, t = D.gen_rmat(14, narcs, 0.57, 0.19, 0.19, seed=0, cap_lo=1, cap_hi=1000, reserve=narcs // 50)
+    b = D.gen_batches(g, 1, frac=0.08, p_inc=0.4, p_dec=0.4, p_ins=0.1, delta_hi=500, ins_lo=1, ins_hi=1000, seed=3)
+    return g, s, t, b
