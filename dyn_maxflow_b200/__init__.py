@@ -442,12 +442,13 @@ class Solver:
         _check(_L.dmf_autotune(self._h, repeats, C.byref(o)))
         return {k: getattr(o, k) for k, _ in Opts._fields_}
 
-    def set_opts(self, variant=None, kernel_cycles=None, relabel_interval=None, tile=None, max_iters=None):
+    def set_opts(self, variant=None, kernel_cycles=None, relabel_interval=None, tile=None, max_iters=None,
+                 small_deg=None):
         o = Opts()
         _L.dmf_opts_default(C.byref(o))
         cur = getattr(self, "_opts", {})
         vals = dict(variant=variant, kernel_cycles=kernel_cycles, relabel_interval=relabel_interval, tile=tile,
-                    max_iters=max_iters)
+                    max_iters=max_iters, small_deg=small_deg)
         for k_, v_ in vals.items():
             if v_ is None:
                 v_ = cur.get(k_, 0 if k_ != "variant" else 0)

@@ -65,6 +65,7 @@ struct Params {
   long long *hc_alloc;  // admissible residual claimed by the hub's chunks
   long long *hc_moved;  // excess pushed by them
   int *hc_min;          // minimum non-admissible head height
+  int *hc_done;         // chunks that contributed to hc_min
   // Exhausted hub chunks: a chunk with no admissible arc at hub height h stays
   // so until the hub's height changes or the next global relabel (heights only
   // rise in between, and a reverse residual only opens from a higher head).
@@ -413,6 +414,7 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
       p.hc_min[hid] = INT_MAX;
       p.hc_alloc[hid] = 0;
       p.hc_moved[hid] = 0;
+      p.hc_done[hid] = 0;
     }
     if (is_snk(p, v) || (!is_src(p, v) && ex < 0)) {
       p.height[v] = 0;
@@ -1011,17 +1013,23 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
         ex_start = __ldcg(p.excess + v);
       }
       const int h = wg.g.shfl(hh, 0);
+      const bool has_ex = wg.g.shfl(ex_start, 0) > 0;
       const int hid = __ldg(p.hub_base + v), cidx = hid + it.y;
       const unsigned long long key = ((unsigned long long)gepoch << 32) | (unsigned)h;
       unsigned long long mk = 0;
       if (wg.rank() == 0) mk = __ldcg(p.chunk_mark + cidx);
       mk = wg.g.shfl(mk, 0);
-      if (mk == key) {  // exhausted at this height: only its minimum head height matters
+      // A hub without excess (topology rounds sweep every hub) needs nothing.
+      // Every chunk that does look counts itself: the hub is relabelled only
+      // when all its chunks contributed to the minimum head height.
+      if (!has_ex || h >= p.n || is_term(p, v)) {
+      } else if (mk == key) {  // exhausted at this height: only its minimum head height matters
         if (wg.rank() == 0) {
           const int tm = __ldcg(p.chunk_tmin + cidx);
           if (tm != INT_MAX) atomicMin(p.hc_min + hid, tm);
+          atomicAdd(p.hc_done + hid, 1);
         }
-      } else if (h < p.n && !is_term(p, v)) {
+      } else {
         int beg, end;
         chunk_range(p, it, beg, end);
         int aa[kBatch], rr[kBatch], w[kBatch], hw[kBatch];
@@ -1049,7 +1057,8 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
         long long cb = 0;  // this chunk's share of the hub's excess
         if (wg.rank() == 0) {
           if (tm != INT_MAX) atomicMin(p.hc_min + hid, tm);
-          if (ts > 0 && ex_start > 0) {  // (topology rounds also sweep hubs without excess)
+          atomicAdd(p.hc_done + hid, 1);
+          if (ts > 0) {
             const long long old = atomic_add_ll(p.hc_alloc + hid, ts);
             cb = ex_start - old;
             cb = cb < 0 ? 0 : (cb > ts ? ts : cb);
@@ -1108,19 +1117,21 @@ __device__ __forceinline__ void ph_push3(const Params &p, const RoundIn &in, int
     const int v = it.x;
     const int hid = __ldg(p.hub_base + v);
     const long long tot = __ldcg(p.hc_alloc + hid), moved = __ldcg(p.hc_moved + hid);
-    const int mh = __ldcg(p.hc_min + hid);
+    const int mh = __ldcg(p.hc_min + hid), looked = __ldcg(p.hc_done + hid);
     const long long ex0 = __ldcg(p.excess + v);
     int h = __ldcg(p.height + v);
+    const bool complete = looked == nchunks(deg_of(p, v));  // every chunk gave its minimum
     // clean for the next round
     p.hc_alloc[hid] = 0;
     p.hc_moved[hid] = 0;
     p.hc_min[hid] = INT_MAX;
+    p.hc_done[hid] = 0;
     if (!(ex0 > 0 && h < p.n) || is_term(p, v)) continue;
     seen++;
     ls.visits++;
     const long long ex = ex0 - moved;
     if (moved) atomic_add_ll(p.excess + v, -moved);
-    if (ex > 0 && moved == tot) {  // every admissible arc saturated: relabel
+    if (ex > 0 && moved == tot && complete) {  // every admissible arc saturated: relabel
       h = mh >= p.n ? p.n : mh + 1;
       p.height[v] = h;
       ls.relabels++;
@@ -1699,7 +1710,7 @@ struct dmf_solver {
   int2 *hch = nullptr;    // every hub's chunks
   int nchunk = 0;         // total hub chunks = capacity of each hub-chunk queue
   long long *hc_moved = nullptr, *hc_alloc = nullptr;  // per hub, push-round totals
-  int *hc_min = nullptr;
+  int *hc_min = nullptr, *hc_done = nullptr;
   int *hub_base = nullptr;
   unsigned long long *chunk_mark = nullptr;
   int *chunk_tmin = nullptr;
@@ -1888,6 +1899,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.hc_moved = sv->hc_moved;
   p.hc_alloc = sv->hc_alloc;
   p.hc_min = sv->hc_min;
+  p.hc_done = sv->hc_done;
   p.hub_base = sv->hub_base;
   p.role = sv->role;
   p.inst = sv->inst;
@@ -2234,7 +2246,7 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
   p.hch = hub_dummy;
   p.nhch = 0;
   p.hc_moved = p.hc_alloc = ll_dummy;
-  p.hc_min = int_dummy;
+  p.hc_min = p.hc_done = int_dummy;
   p.hub_base = int_dummy;
   p.chunk_mark = mark_dummy;
   p.chunk_tmin = int_dummy;
@@ -2357,7 +2369,7 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
   const size_t NC = (size_t)std::max(sv->nchunk, 1);
   if ((st = dalloc(sv, &sv->hqbuf, 5 * NC)) || (st = dalloc(sv, &sv->hch, NC)) ||
       (st = dalloc(sv, &sv->hc_moved, NC)) || (st = dalloc(sv, &sv->hc_alloc, NC)) ||
-      (st = dalloc(sv, &sv->hc_min, NC)) ||
+      (st = dalloc(sv, &sv->hc_min, NC)) || (st = dalloc(sv, &sv->hc_done, NC)) ||
       (st = dalloc(sv, &sv->hub_base, N)) || (st = dalloc(sv, &sv->chunk_mark, NC)) ||
       (st = dalloc(sv, &sv->chunk_tmin, NC)))
     return bail(st);
@@ -2375,6 +2387,9 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
   up(sv->hub_base, hub_base.data(), 4 * (size_t)g->n);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->chunk_mark, 0, 8 * NC, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->astamp, 0, 4 * M, S);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->hc_done, 0, 4 * NC, S);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->hc_alloc, 0, 8 * NC, S);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->hc_moved, 0, 8 * NC, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->stamp, 0, 4 * N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->dead, 0, N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->side, 0, N, S);

@@ -85,3 +85,28 @@ def test_autotune_keeps_the_flow(dmf, oracle):
             for a, c, x in zip(*b):
                 cur[g.find_arc(int(a), int(c))] = x
             assert sv.apply_updates(*b) == oracle.dinic(g.num_nodes(), off, adj, cur, par, s, t)
+
+
+def test_every_autotune_configuration_is_exact(dmf, oracle):
+    """Every launch configuration the autotuner can choose (tile width, per-thread
+    degree bound, relabel interval, cycles), set on a live solver as the
+    autotuner sets it: a recompute and three successive batches must equal
+    Dinic.  The autotuner picks by timing, so this covers deterministically what
+    its choices could be."""
+    import itertools
+    g, s, t, batches = make_config("rmat12")
+    off, adj, w, par = g.arrays()
+    n = g.num_nodes()
+    want = [oracle.dinic(n, off, adj, w, par, s, t)]
+    cur = w.copy()
+    for b in batches[:3]:
+        for a, c, x in zip(*b):
+            if a != c:
+                cur[g.find_arc(int(a), int(c))] = x
+        want.append(oracle.dinic(n, off, adj, cur, par, s, t))
+    for tile, sd, iv, cyc in itertools.product([4, 8, 16, 32], [-1, 4, 8, 16, 32], [2, 3, 6, 12], [1, 2, 4]):
+        with dmf.Solver(g, s, t) as sv:
+            sv.static_maxflow()
+            sv.set_opts(variant=0, kernel_cycles=cyc, relabel_interval=iv, tile=tile, small_deg=sd)
+            got = [sv.recompute()] + [sv.apply_updates(*b) for b in batches[:3]]
+            assert got == want, dict(tile=tile, small_deg=sd, interval=iv, cycles=cyc)
