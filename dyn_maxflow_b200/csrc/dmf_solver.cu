@@ -442,6 +442,16 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
   agg_add_ll(&out->arcs, seed_arcs);
 }
 
+// Reserves `cnt` consecutive slots behind *tail for this thread with one atomic
+// per group of threads that call it together.
+__device__ __forceinline__ int reserve(int *tail, int cnt) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  const int pre = cg::exclusive_scan(g, cnt, cg::plus<int>());
+  int base = 0;
+  if (g.thread_rank() == g.size() - 1) base = atomicAdd(tail, pre + cnt);
+  return g.shfl(base, g.size() - 1) + pre;
+}
+
 struct VisitAcc {
   long long arcs = 0;
   int reached = 0;
@@ -470,18 +480,6 @@ __device__ __forceinline__ void flush_visits(const Params &p, Slot *out, VisitAc
 // Top-down level (staticMaxFlow_kernel_11, code/dyn_data.h:72-87, run over the
 // frontier queue instead of all V): x at level L labels w when arc w->x has
 // residual, i.e. res[par[e]] > 0 for e = x->w.
-__device__ __forceinline__ void visit_claimed(const Params &p, Slot *out, int nxt, int w, int d, long long ex,
-                                              VisitAcc &acc) {
-  const bool hub = d > p.hub_deg;
-  if (hub) append_hub(p, p.fh[nxt], &out->hq, w);
-  else append(p.fq[nxt], &out->q, w);
-  acc.arcs += d;
-  if (!is_term(p, w) && ex > 0) {
-    if (hub) append_hub(p, p.ah, &p.ctrl->act_hq, w);
-    else append(p.aq, &p.ctrl->act_q, w);
-    acc.reached++;
-  }
-}
 
 // Arcs first, first+stride, ... < end of a frontier vertex, in register
 // batches of kBatch so that the gathers of a batch are in flight together:
@@ -515,10 +513,42 @@ __device__ __forceinline__ void td_range(const Params &p, Slot *out, int nxt, in
         d[k] = deg_of(p, w[k]);
         ex[k] = __ldcg(p.excess + w[k]);
       }
+    // the batch's claimed heads go to the next frontier and, when active, to
+    // the active list, with one reservation per list for the whole batch (a
+    // large level claims hundreds of thousands of vertices: appends per arc
+    // would serialise on the lists' tail counters)
+    int nq = 0, na = 0;
+    unsigned qmask = 0, amask = 0;
 #pragma unroll
     for (int k = 0; k < kTdBatch; k++) {
       if (w[k] >= 0) ls.arcs++;
-      if (c[k]) visit_claimed(p, out, nxt, w[k], d[k], ex[k], acc);
+      if (!c[k]) continue;
+      acc.arcs += d[k];
+      const bool act = !is_term(p, w[k]) && ex[k] > 0;
+      if (act) acc.reached++;
+      if (d[k] > p.hub_deg) {
+        append_hub(p, p.fh[nxt], &out->hq, w[k]);
+        if (act) append_hub(p, p.ah, &p.ctrl->act_hq, w[k]);
+      } else {
+        qmask |= 1u << k;
+        nq++;
+        if (act) {
+          amask |= 1u << k;
+          na++;
+        }
+      }
+    }
+    if (nq) {
+      int pos = reserve(&out->q, nq);
+#pragma unroll
+      for (int k = 0; k < kTdBatch; k++)
+        if ((qmask >> k) & 1) p.fq[nxt][pos++] = w[k];
+    }
+    if (na) {
+      int pos = reserve(&p.ctrl->act_q, na);
+#pragma unroll
+      for (int k = 0; k < kTdBatch; k++)
+        if ((amask >> k) & 1) p.aq[pos++] = w[k];
     }
   }
 }
@@ -648,15 +678,6 @@ __device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, i
 // Arcs a lane handles together in a tile discharge.
 constexpr int kPushBatch = 4;
 
-// Reserves `cnt` consecutive slots behind *tail for this thread with one atomic
-// per group of threads that call it together.
-__device__ __forceinline__ int reserve(int *tail, int cnt) {
-  cg::coalesced_group g = cg::coalesced_threads();
-  const int pre = cg::exclusive_scan(g, cnt, cg::plus<int>());
-  int base = 0;
-  if (g.thread_rank() == g.size() - 1) base = atomicAdd(tail, pre + cnt);
-  return g.shfl(base, g.size() - 1) + pre;
-}
 
 // Queues the heads x[k] marked in `cand` for round r+1 (each at most once per
 // round, by its stamp): all stamp exchanges in flight together, then all degree
