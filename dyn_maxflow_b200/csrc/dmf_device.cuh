@@ -181,6 +181,34 @@ __device__ __forceinline__ void agg_add_int(int *p, int v) {
   if (g.thread_rank() == 0 && s) atomicAdd(p, s);
 }
 
+// Block-wide sum added with one global atomic: for counters that every warp of
+// the grid contributes to at the end of a phase (thousands of same-address
+// atomics otherwise serialise at one L2 slice).  Every thread of the block must
+// call it (uniform control flow: it contains block barriers).
+__device__ __forceinline__ void block_add_ll(long long *p, long long v) {
+  __shared__ long long s_acc;
+  if (threadIdx.x == 0) s_acc = 0;
+  __syncthreads();
+  cg::thread_block_tile<32> w = cg::tiled_partition<32>(cg::this_thread_block());
+  const long long sw = cg::reduce(w, v, cg::plus<long long>());
+  if (w.thread_rank() == 0 && sw) atomicAdd((unsigned long long *)&s_acc, (unsigned long long)sw);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_acc) atomic_add_ll(p, s_acc);
+  __syncthreads();
+}
+
+__device__ __forceinline__ void block_add_int(int *p, int v) {
+  __shared__ int s_acc;
+  if (threadIdx.x == 0) s_acc = 0;
+  __syncthreads();
+  cg::thread_block_tile<32> w = cg::tiled_partition<32>(cg::this_thread_block());
+  const int sw = cg::reduce(w, v, cg::plus<int>());
+  if (w.thread_rank() == 0 && sw) atomicAdd(&s_acc, sw);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_acc) atomicAdd(p, s_acc);
+  __syncthreads();
+}
+
 // ---- groups: one thread, T lanes of a warp, or the whole block ----------------
 struct ThreadGroup {
   __device__ __forceinline__ int rank() const { return 0; }

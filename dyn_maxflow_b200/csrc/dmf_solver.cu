@@ -437,9 +437,9 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
     }
     if (!is_term(p, v) && ex > 0) pos++;
   }
-  agg_add_int(&c->pos_count, pos);
-  agg_add_ll(&c->unexplored, unexpl);
-  agg_add_ll(&out->arcs, seed_arcs);
+  block_add_int(&c->pos_count, pos);
+  block_add_ll(&c->unexplored, unexpl);
+  block_add_ll(&out->arcs, seed_arcs);
 }
 
 // Reserves `cnt` consecutive slots behind *tail for this thread with one atomic
@@ -473,8 +473,8 @@ __device__ __forceinline__ void bfs_visit(const Params &p, Slot *out, int nxt, i
 // Counts go to the phase's own slot: a cross-phase counter would be read by a
 // slow block after a fast block already added to it in the next phase.
 __device__ __forceinline__ void flush_visits(const Params &p, Slot *out, VisitAcc &acc) {
-  agg_add_ll(&out->arcs, acc.arcs);
-  agg_add_int(&out->cnt, acc.reached);
+  block_add_ll(&out->arcs, acc.arcs);
+  block_add_int(&out->cnt, acc.reached);
 }
 
 // Top-down level (staticMaxFlow_kernel_11, code/dyn_data.h:72-87, run over the
@@ -652,7 +652,7 @@ __device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int 
     }
     if (write_side && (!p.inst_active || p.inst_active[__ldg(p.inst + v)])) p.side[v] = h < p.n ? 1 : 0;
   }
-  agg_add_ll((long long *)&p.ctrl->st_dead, nd);
+  block_add_ll((long long *)&p.ctrl->st_dead, nd);
 }
 
 // ---- push rounds ---------------------------------------------------------------
