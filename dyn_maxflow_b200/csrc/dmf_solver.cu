@@ -105,6 +105,7 @@ struct LStats {
   unsigned long long pushes = 0, relabels = 0, arcs = 0, visits = 0;
   unsigned long long probe = 0;  // (longest single item in ns << 32) | vertex, this phase
   unsigned long long t_phase = 0;  // thread 0: when this block left the last barrier
+  long long to_sink = 0;  // flow pushed into the sink this push phase, not yet added
 };
 
 // Optional probe (DMF_FLAG_PROBE): times every work item and keeps the longest.
@@ -666,11 +667,31 @@ __device__ __forceinline__ void enqueue(const Params &p, int r, unsigned round_i
   else append(p.wq[r & 1], &p.ctrl->wtail[r % 3], v);
 }
 
+// Adds d to the head's excess and returns the old value.  Pushes into the one
+// sink of a single-instance solve are summed per thread instead and added once
+// per block when the push phase ends (sink_flush): a high in-degree sink takes
+// thousands of pushes a round, which would serialise on its excess word, and a
+// terminal is never queued, so its old value is not needed.
+__device__ __forceinline__ long long push_excess(const Params &p, int w, int d, LStats &ls) {
+  if (!p.role && w == p.t) {
+    ls.to_sink += d;
+    return 0;
+  }
+  return atomic_add_ll(p.excess + w, d);
+}
+
+// Every thread of the block calls it at the end of the push phase.
+__device__ __forceinline__ void sink_flush(const Params &p, LStats &ls) {
+  if (p.role) return;  // uniform
+  block_add_ll(p.excess + p.t, ls.to_sink);
+  ls.to_sink = 0;
+}
+
 __device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, int r, unsigned round_id, bool enq,
                                          LStats &ls) {
   atomicSub(p.res + a, d);
   atomicAdd(p.res + __ldg(p.par + a), d);
-  long long old = atomic_add_ll(p.excess + w, d);
+  long long old = push_excess(p, w, d, ls);
   ls.pushes++;
   if (enq && !is_term(p, w) && old + d > 0) enqueue(p, r, round_id, w);
 }
@@ -728,7 +749,7 @@ __device__ __forceinline__ void push_batch(const Params &p, const int (&a)[K], c
   for (int k = 0; k < K; k++)
     if (d[k] > 0) {
       atomicSub(p.res + a[k], d[k]);
-      old[k] = atomic_add_ll(p.excess + w[k], d[k]);
+      old[k] = push_excess(p, w[k], d[k], ls);
     }
   unsigned cand = 0;
 #pragma unroll
@@ -791,7 +812,7 @@ __device__ __forceinline__ void discharge_small(const Params &p, int v, int beg,
     for (int k = 0; k < kSmallMax; k++)
       if (dd[k] > 0) {
         atomicSub(p.res + beg + k, dd[k]);
-        old[k] = atomic_add_ll(p.excess + w[k], dd[k]);
+        old[k] = push_excess(p, w[k], dd[k], ls);
       }
 #pragma unroll
     for (int k = 0; k < kSmallMax; k++)
@@ -1122,6 +1143,7 @@ __device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int
       [&](auto &g, int v) { discharge(g, p, v, r, round_id, !topo, ls, topo ? &seen : nullptr); },
       [&](int v) { return !topo || __ldcg(p.excess + v) > 0; });
   if (topo) agg_add_int(&c->seen[r % 3], seen);
+  sink_flush(p, ls);
 }
 
 // Push round, phase 2 (hubs): per hub (its first chunk), the moved total leaves
