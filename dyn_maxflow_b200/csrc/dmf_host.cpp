@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <numeric>
 #include <unordered_set>
 
@@ -30,7 +31,11 @@ int fail(int status, const char *fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(buf, sizeof buf, fmt, ap);
   va_end(ap);
-  g_err = buf;
+  try {
+    g_err = buf;
+  } catch (...) {
+    // no room for the message: the status alone still reaches the caller
+  }
   return status;
 }
 
@@ -49,9 +54,10 @@ int validate(const dmf_graph &g) {
     return fail(DMF_ERR_BAD_FILE, "offsets must start at 0 and end at m (got %d, %d)", g.off[0], g.off[n]);
   for (int32_t v = 0; v < n; v++)
     if (g.off[v] > g.off[v + 1]) return fail(DMF_ERR_BAD_FILE, "offsets decrease at vertex %d", v);
-  int bad = 0;
-  int64_t bad_e = -1;
-#pragma omp parallel for schedule(static) reduction(max : bad)
+  // (code << 32) | (INT32_MAX - arc): the most severe defect, at its lowest arc,
+  // whatever the thread count
+  int64_t worst = 0;
+#pragma omp parallel for schedule(static) reduction(max : worst)
   for (int32_t v = 0; v < n; v++) {
     for (int32_t e = g.off[v]; e < g.off[v + 1]; e++) {
       int32_t h = g.adj[e], p = g.par[e];
@@ -62,13 +68,11 @@ int validate(const dmf_graph &g) {
       else if (g.par[p] != e || g.adj[p] != v || p < g.off[h] || p >= g.off[h + 1]) code = 4;
       else if (g.w[e] < 0) code = 5;
       else if ((int64_t)g.w[e] + g.w[p] > INT32_MAX) code = 6;
-      if (code > bad) {
-        bad = code;
-#pragma omp critical
-        bad_e = e;
-      }
+      if (code) worst = std::max(worst, ((int64_t)code << 32) | (int64_t)(INT32_MAX - e));
     }
   }
+  const int bad = (int)(worst >> 32);
+  const int64_t bad_e = INT32_MAX - (worst & 0xffffffffll);
   switch (bad) {
     case 0: return DMF_OK;
     case 1: return fail(DMF_ERR_BAD_FILE, "arc %lld: head out of range", (long long)bad_e);
@@ -137,14 +141,23 @@ int build_from_edges(int64_t k, const int32_t *u, const int32_t *v, const int32_
   }
   // per tail: unique heads in first-event order, weights summed
   std::vector<int32_t> ucount(n, 0);
-  int overflow = 0;
+  int overflow = 0, nomem = 0;
 #pragma omp parallel
   {
+    // an exception may not leave the parallel region: a failed allocation
+    // is flagged and reported after it
     std::vector<int64_t> ord;
-#pragma omp for schedule(dynamic, 256) reduction(| : overflow)
+    std::vector<Ev> tmp;
+#pragma omp for schedule(dynamic, 256) reduction(| : overflow, nomem)
     for (int32_t x = 0; x < n; x++) {
       int64_t b = bofs[x], e = bofs[x + 1], len = e - b;
-      ord.resize(len);
+      try {
+        ord.resize(len);
+        tmp.resize(len);
+      } catch (...) {
+        nomem = 1;
+        continue;
+      }
       std::iota(ord.begin(), ord.end(), b);
       std::stable_sort(ord.begin(), ord.end(), [&](int64_t p, int64_t q) { return ev[p].head < ev[q].head; });
       // merge equal heads into the first occurrence (smallest position)
@@ -162,17 +175,17 @@ int build_from_edges(int64_t k, const int32_t *u, const int32_t *v, const int32_
       ord.resize(nu);
       std::sort(ord.begin(), ord.end());  // first-touch order
       // compact unique arcs to the front of the bucket, in order
-      std::vector<Ev> tmp(nu);
       for (int64_t i = 0; i < nu; i++) tmp[i] = ev[ord[i]];
       for (int64_t i = 0; i < nu; i++) ev[b + i] = tmp[i];
       ucount[x] = (int32_t)nu;
     }
   }
+  if (nomem) return fail(DMF_ERR_OOM, "host allocation failed");
   if (overflow) return fail(DMF_ERR_OVERFLOW, "summed duplicate capacity exceeds int32");
   int64_t m64 = 0;
   for (int32_t x = 0; x < n; x++) m64 += ucount[x];
   if (m64 > INT32_MAX) return fail(DMF_ERR_INVALID_ARG, "too many arcs (%lld) for int32 indices", (long long)m64);
-  auto *g = new dmf_graph();
+  std::unique_ptr<dmf_graph> g(new dmf_graph());
   g->n = n;
   g->m = (int32_t)m64;
   g->off.resize((size_t)n + 1);
@@ -193,7 +206,7 @@ int build_from_edges(int64_t k, const int32_t *u, const int32_t *v, const int32_
   for (int32_t x = 0; x < n; x++)
     for (int32_t e = g->off[x]; e < g->off[x + 1]; e++)
       g->par[e] = (int32_t)find_arc(*g, g->adj[e], x);
-  *out = g;
+  *out = g.release();
   return ok();
 }
 
@@ -256,6 +269,7 @@ const char *dmf_status_string(int st) {
     case DMF_ERR_TIMEOUT: return "device wait timed out";
     case DMF_ERR_OVERFLOW: return "capacity overflow";
     case DMF_ERR_NOT_SOLVED: return "not solved";
+    case DMF_ERR_HOST: return "host runtime error";
     default: return "unknown status";
   }
 }
@@ -271,74 +285,66 @@ void dmf_free(void *p) { std::free(p); }
 
 int dmf_graph_load(const char *path, dmf_graph **out) {
   if (!path || !out) return fail(DMF_ERR_INVALID_ARG, "null argument");
-  FILE *f = std::fopen(path, "rb");
-  if (!f) return fail(DMF_ERR_BAD_FILE, "cannot open %s", path);
-  std::fseek(f, 0, SEEK_END);
-  long long size = std::ftell(f);
-  std::fseek(f, 0, SEEK_SET);
-  int32_t hdr[2] = {0, 0};
-  if (std::fread(hdr, 4, 2, f) != 2) {
-    std::fclose(f);
-    return fail(DMF_ERR_BAD_FILE, "%s: shorter than the 8-byte header", path);
-  }
-  long long want = 8 + 4LL * ((long long)hdr[0] + 1) + 12LL * hdr[1];
-  if (hdr[0] < 0 || hdr[1] < 0 || size != want) {
-    std::fclose(f);
-    return fail(DMF_ERR_BAD_FILE, "%s: size %lld does not match n=%d m=%d (expected %lld)", path, size,
-                hdr[0], hdr[1], want);
-  }
-  auto *g = new dmf_graph();
-  g->n = hdr[0];
-  g->m = hdr[1];
-  g->off.resize((size_t)g->n + 1);
-  g->adj.resize(g->m);
-  g->w.resize(g->m);
-  g->par.resize(g->m);
-  bool okr = std::fread(g->off.data(), 4, g->off.size(), f) == g->off.size() &&
-             std::fread(g->adj.data(), 4, g->m, f) == (size_t)g->m &&
-             std::fread(g->w.data(), 4, g->m, f) == (size_t)g->m &&
-             std::fread(g->par.data(), 4, g->m, f) == (size_t)g->m;
-  std::fclose(f);
-  if (!okr) {
-    delete g;
-    return fail(DMF_ERR_BAD_FILE, "%s: short read", path);
-  }
-  int st = validate(*g);
-  if (st) {
-    std::string msg = std::string(path) + ": " + g_err;
-    delete g;
-    return fail(st, "%s", msg.c_str());
-  }
-  build_sorted_index(*g);
-  *out = g;
-  return ok();
+  return guarded([&]() -> int {
+    std::unique_ptr<FILE, int (*)(FILE *)> f(std::fopen(path, "rb"), &std::fclose);
+    if (!f) return fail(DMF_ERR_BAD_FILE, "cannot open %s", path);
+    std::fseek(f.get(), 0, SEEK_END);
+    long long size = std::ftell(f.get());
+    std::fseek(f.get(), 0, SEEK_SET);
+    int32_t hdr[2] = {0, 0};
+    if (std::fread(hdr, 4, 2, f.get()) != 2) return fail(DMF_ERR_BAD_FILE, "%s: shorter than the 8-byte header", path);
+    long long want = 8 + 4LL * ((long long)hdr[0] + 1) + 12LL * hdr[1];
+    if (hdr[0] < 0 || hdr[1] < 0 || size != want)
+      return fail(DMF_ERR_BAD_FILE, "%s: size %lld does not match n=%d m=%d (expected %lld)", path, size, hdr[0],
+                  hdr[1], want);
+    std::unique_ptr<dmf_graph> g(new dmf_graph());
+    g->n = hdr[0];
+    g->m = hdr[1];
+    g->off.resize((size_t)g->n + 1);
+    g->adj.resize(g->m);
+    g->w.resize(g->m);
+    g->par.resize(g->m);
+    bool okr = std::fread(g->off.data(), 4, g->off.size(), f.get()) == g->off.size() &&
+               std::fread(g->adj.data(), 4, g->m, f.get()) == (size_t)g->m &&
+               std::fread(g->w.data(), 4, g->m, f.get()) == (size_t)g->m &&
+               std::fread(g->par.data(), 4, g->m, f.get()) == (size_t)g->m;
+    f.reset();
+    if (!okr) return fail(DMF_ERR_BAD_FILE, "%s: short read", path);
+    int st = validate(*g);
+    if (st) {
+      std::string msg = std::string(path) + ": " + g_err;
+      return fail(st, "%s", msg.c_str());
+    }
+    build_sorted_index(*g);
+    *out = g.release();
+    return ok();
+  });
 }
 
 int dmf_graph_from_csr(int32_t n, int32_t m, const int32_t *index, const int32_t *adj,
                        const int32_t *w, const int32_t *par, dmf_graph **out) {
   if (!out || n < 0 || m < 0 || !index || (m > 0 && (!adj || !w || !par)))
     return fail(DMF_ERR_INVALID_ARG, "bad CSR arguments");
-  auto *g = new dmf_graph();
-  g->n = n;
-  g->m = m;
-  g->off.assign(index, index + (size_t)n + 1);
-  g->adj.assign(adj, adj + m);
-  g->w.assign(w, w + m);
-  g->par.assign(par, par + m);
-  int st = validate(*g);
-  if (st) {
-    delete g;
-    return st;
-  }
-  build_sorted_index(*g);
-  *out = g;
-  return ok();
+  return guarded([&]() -> int {
+    std::unique_ptr<dmf_graph> g(new dmf_graph());
+    g->n = n;
+    g->m = m;
+    g->off.assign(index, index + (size_t)n + 1);
+    g->adj.assign(adj, adj + m);
+    g->w.assign(w, w + m);
+    g->par.assign(par, par + m);
+    int st = validate(*g);
+    if (st) return st;
+    build_sorted_index(*g);
+    *out = g.release();
+    return ok();
+  });
 }
 
 int dmf_graph_from_edges(int64_t k, const int32_t *u, const int32_t *v, const int32_t *w,
                          dmf_graph **out) {
   if (!out) return fail(DMF_ERR_INVALID_ARG, "null out");
-  return build_from_edges(k, u, v, w, out);
+  return guarded([&] { return build_from_edges(k, u, v, w, out); });
 }
 
 int dmf_graph_save(const dmf_graph *g, const char *path) {
@@ -440,31 +446,33 @@ int dmf_gen_grid(int32_t rows, int32_t cols, uint64_t seed, int32_t cap_lo, int3
   if (!out || rows < 1 || cols < 1 || (int64_t)rows * cols < 2 || (int64_t)rows * cols > INT32_MAX ||
       cap_lo < 0 || cap_hi < cap_lo || st_cap < 0)
     return fail(DMF_ERR_INVALID_ARG, "bad grid parameters");
-  Rng rng(seed);
-  std::vector<int32_t> U, V, W;
-  int64_t nv = (int64_t)rows * cols;
-  U.reserve(4 * nv + rows * 2);
-  auto emit = [&](int32_t a, int32_t b, int32_t c) { U.push_back(a); V.push_back(b); W.push_back(c); };
-  for (int32_t r = 0; r < rows; r++)
-    for (int32_t c = 0; c < cols; c++) {
-      int32_t x = r * cols + c;
-      if (c + 1 < cols) {
-        emit(x, x + 1, (int32_t)rng.uniform(cap_lo, cap_hi));
-        emit(x + 1, x, (int32_t)rng.uniform(cap_lo, cap_hi));
+  return guarded([&]() -> int {
+    Rng rng(seed);
+    std::vector<int32_t> U, V, W;
+    int64_t nv = (int64_t)rows * cols;
+    U.reserve(4 * nv + rows * 2);
+    auto emit = [&](int32_t a, int32_t b, int32_t c) { U.push_back(a); V.push_back(b); W.push_back(c); };
+    for (int32_t r = 0; r < rows; r++)
+      for (int32_t c = 0; c < cols; c++) {
+        int32_t x = r * cols + c;
+        if (c + 1 < cols) {
+          emit(x, x + 1, (int32_t)rng.uniform(cap_lo, cap_hi));
+          emit(x + 1, x, (int32_t)rng.uniform(cap_lo, cap_hi));
+        }
+        if (r + 1 < rows) {
+          emit(x, x + cols, (int32_t)rng.uniform(cap_lo, cap_hi));
+          emit(x + cols, x, (int32_t)rng.uniform(cap_lo, cap_hi));
+        }
       }
-      if (r + 1 < rows) {
-        emit(x, x + cols, (int32_t)rng.uniform(cap_lo, cap_hi));
-        emit(x + cols, x, (int32_t)rng.uniform(cap_lo, cap_hi));
-      }
-    }
-  int32_t src = 0, snk = (int32_t)(nv - 1);
-  for (int32_t r = 1; r < rows; r++) emit(src, r * cols, st_cap);
-  for (int32_t r = 0; r + 1 < rows; r++) emit(r * cols + cols - 1, snk, st_cap);
-  int st = build_from_edges((int64_t)U.size(), U.data(), V.data(), W.data(), out);
-  if (st) return st;
-  if (s) *s = src;
-  if (t) *t = snk;
-  return ok();
+    int32_t src = 0, snk = (int32_t)(nv - 1);
+    for (int32_t r = 1; r < rows; r++) emit(src, r * cols, st_cap);
+    for (int32_t r = 0; r + 1 < rows; r++) emit(r * cols + cols - 1, snk, st_cap);
+    int st = build_from_edges((int64_t)U.size(), U.data(), V.data(), W.data(), out);
+    if (st) return st;
+    if (s) *s = src;
+    if (t) *t = snk;
+    return ok();
+  });
 }
 
 int dmf_gen_rmat(int32_t scale, int64_t narcs, double a, double b, double c, uint64_t seed,
@@ -473,79 +481,80 @@ int dmf_gen_rmat(int32_t scale, int64_t narcs, double a, double b, double c, uin
   if (!out || scale < 1 || scale > 30 || narcs < 1 || a < 0 || b < 0 || c < 0 || a + b + c > 1.0 ||
       cap_lo < 0 || cap_hi < cap_lo || reserve < 0)
     return fail(DMF_ERR_INVALID_ARG, "bad R-MAT parameters");
-  const double ab = a + b, abc = a + b + c;
-  // arc i draws from its own counter-derived stream, so the output does not
-  // depend on the thread count
-  auto sample = [&](uint64_t idx, uint64_t salt) -> uint64_t {
-    Rng r(seed ^ (salt * 0xD1B54A32D192ED03ull) ^ (idx * 0x9E3779B97F4A7C15ull));
-    uint64_t uu = 0, vv = 0;
-    for (int32_t l = 0; l < scale; l++) {
-      double p = r.unit();
-      uint64_t bu = p >= ab, bv = (p >= a && p < ab) || p >= abc;
-      uu = (uu << 1) | bu;
-      vv = (vv << 1) | bv;
+  return guarded([&]() -> int {
+    const double ab = a + b, abc = a + b + c;
+    // arc i draws from its own counter-derived stream, so the output does not
+    // depend on the thread count
+    auto sample = [&](uint64_t idx, uint64_t salt) -> uint64_t {
+      Rng r(seed ^ (salt * 0xD1B54A32D192ED03ull) ^ (idx * 0x9E3779B97F4A7C15ull));
+      uint64_t uu = 0, vv = 0;
+      for (int32_t l = 0; l < scale; l++) {
+        double p = r.unit();
+        uint64_t bu = p >= ab, bv = (p >= a && p < ab) || p >= abc;
+        uu = (uu << 1) | bu;
+        vv = (vv << 1) | bv;
+      }
+      return (uu << 32) | vv;
+    };
+    std::vector<uint64_t> keys((size_t)narcs);
+  #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < narcs; i++) keys[i] = sample((uint64_t)i, 1);
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    keys.erase(std::remove_if(keys.begin(), keys.end(), [](uint64_t k) { return (k >> 32) == (k & 0xffffffffu); }),
+               keys.end());
+    const int32_t nv = 1 << scale;
+    // source / sink on the sampled arcs
+    std::vector<int64_t> outd(nv, 0), ind(nv, 0);
+    for (uint64_t k : keys) { outd[k >> 32]++; ind[k & 0xffffffffu]++; }
+    int32_t src = 0, snk = -1;
+    for (int32_t x = 0; x < nv; x++) if (outd[x] > outd[src]) src = x;
+    for (int32_t x = 0; x < nv; x++)
+      if (x != src && (snk < 0 || ind[x] > ind[snk])) snk = x;
+    // reserved insert slots: further R-MAT samples that are not arcs in either direction
+    std::vector<uint64_t> extra;
+    if (reserve > 0) {
+      std::unordered_set<uint64_t> taken;
+      uint64_t idx = 0;
+      while ((int64_t)extra.size() < reserve && idx < (uint64_t)reserve * 64 + 1024) {
+        uint64_t k = sample(idx++, 2);
+        uint64_t rk = (k << 32) | (k >> 32);
+        if ((k >> 32) == (k & 0xffffffffu)) continue;
+        if (std::binary_search(keys.begin(), keys.end(), k) || std::binary_search(keys.begin(), keys.end(), rk))
+          continue;
+        if (taken.count(k) || taken.count(rk)) continue;
+        taken.insert(k);
+        extra.push_back(k);
+      }
     }
-    return (uu << 32) | vv;
-  };
-  std::vector<uint64_t> keys((size_t)narcs);
-#pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < narcs; i++) keys[i] = sample((uint64_t)i, 1);
-  std::sort(keys.begin(), keys.end());
-  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
-  keys.erase(std::remove_if(keys.begin(), keys.end(), [](uint64_t k) { return (k >> 32) == (k & 0xffffffffu); }),
-             keys.end());
-  const int32_t nv = 1 << scale;
-  // source / sink on the sampled arcs
-  std::vector<int64_t> outd(nv, 0), ind(nv, 0);
-  for (uint64_t k : keys) { outd[k >> 32]++; ind[k & 0xffffffffu]++; }
-  int32_t src = 0, snk = -1;
-  for (int32_t x = 0; x < nv; x++) if (outd[x] > outd[src]) src = x;
-  for (int32_t x = 0; x < nv; x++)
-    if (x != src && (snk < 0 || ind[x] > ind[snk])) snk = x;
-  // reserved insert slots: further R-MAT samples that are not arcs in either direction
-  std::vector<uint64_t> extra;
-  if (reserve > 0) {
-    std::unordered_set<uint64_t> taken;
-    uint64_t idx = 0;
-    while ((int64_t)extra.size() < reserve && idx < (uint64_t)reserve * 64 + 1024) {
-      uint64_t k = sample(idx++, 2);
-      uint64_t rk = (k << 32) | (k >> 32);
-      if ((k >> 32) == (k & 0xffffffffu)) continue;
-      if (std::binary_search(keys.begin(), keys.end(), k) || std::binary_search(keys.begin(), keys.end(), rk))
-        continue;
-      if (taken.count(k) || taken.count(rk)) continue;
-      taken.insert(k);
-      extra.push_back(k);
+    const size_t na = keys.size(), ne = extra.size();
+    std::vector<int32_t> U(na + ne), V(na + ne), W(na + ne);
+    Rng caps(seed ^ 0xC0FFEEull);
+    for (size_t i = 0; i < na; i++) {
+      U[i] = (int32_t)(keys[i] >> 32);
+      V[i] = (int32_t)(keys[i] & 0xffffffffu);
+      W[i] = (int32_t)caps.uniform(cap_lo, cap_hi);
     }
-  }
-  const size_t na = keys.size(), ne = extra.size();
-  std::vector<int32_t> U(na + ne), V(na + ne), W(na + ne);
-  Rng caps(seed ^ 0xC0FFEEull);
-  for (size_t i = 0; i < na; i++) {
-    U[i] = (int32_t)(keys[i] >> 32);
-    V[i] = (int32_t)(keys[i] & 0xffffffffu);
-    W[i] = (int32_t)caps.uniform(cap_lo, cap_hi);
-  }
-  for (size_t i = 0; i < ne; i++) {
-    U[na + i] = (int32_t)(extra[i] >> 32);
-    V[na + i] = (int32_t)(extra[i] & 0xffffffffu);
-    W[na + i] = 0;
-  }
-  std::vector<uint64_t>().swap(keys);
-  // keep all 2^scale vertices even if the highest ids are isolated
-  dmf_graph *g = nullptr;
-  int st = build_from_edges((int64_t)U.size(), U.data(), V.data(), W.data(), &g);
-  if (st) return st;
-  if (g->n < nv) {
-    int32_t old = g->n;
-    g->off.resize((size_t)nv + 1, g->m);
-    g->n = nv;
-    (void)old;
-  }
-  *out = g;
-  if (s) *s = src;
-  if (t) *t = snk;
-  return ok();
+    for (size_t i = 0; i < ne; i++) {
+      U[na + i] = (int32_t)(extra[i] >> 32);
+      V[na + i] = (int32_t)(extra[i] & 0xffffffffu);
+      W[na + i] = 0;
+    }
+    std::vector<uint64_t>().swap(keys);
+    // keep all 2^scale vertices even if the highest ids are isolated
+    dmf_graph *built = nullptr;
+    int st = build_from_edges((int64_t)U.size(), U.data(), V.data(), W.data(), &built);
+    if (st) return st;
+    std::unique_ptr<dmf_graph> g(built);
+    if (g->n < nv) {
+      g->off.resize((size_t)nv + 1, g->m);
+      g->n = nv;
+    }
+    *out = g.release();
+    if (s) *s = src;
+    if (t) *t = snk;
+    return ok();
+  });
 }
 
 int dmf_gen_batches(const dmf_graph *g, int32_t nb, double frac, double p_inc, double p_dec, double p_ins,
@@ -555,73 +564,82 @@ int dmf_gen_batches(const dmf_graph *g, int32_t nb, double frac, double p_inc, d
       p_inc + p_dec + p_ins > 1.0 + 1e-9 || delta_hi < 1 || ins_lo < 0 || ins_hi < ins_lo || !ofs || !src ||
       !dst || !w)
     return fail(DMF_ERR_INVALID_ARG, "bad batch parameters");
-  const int32_t m = g->m;
-  std::vector<int32_t> cap(g->w);
-  std::vector<int32_t> tail(m);
-  for (int32_t x = 0; x < g->n; x++)
-    for (int32_t e = g->off[x]; e < g->off[x + 1]; e++) tail[e] = x;
-  Rng rng(seed);
-  std::vector<int64_t> O(1, 0);
-  std::vector<int32_t> S, D, Wn;
-  std::vector<uint8_t> chosen(m, 0);
-  for (int32_t bi = 0; bi < nb; bi++) {
-    std::vector<int32_t> pos, absent;
-    for (int32_t e = 0; e < m; e++) {
-      if (cap[e] > 0) pos.push_back(e);
-      else if (cap[g->par[e]] == 0) absent.push_back(e);
+  return guarded([&]() -> int {
+    const int32_t m = g->m;
+    std::vector<int32_t> cap(g->w);
+    std::vector<int32_t> tail(m);
+    for (int32_t x = 0; x < g->n; x++)
+      for (int32_t e = g->off[x]; e < g->off[x + 1]; e++) tail[e] = x;
+    Rng rng(seed);
+    std::vector<int64_t> O(1, 0);
+    std::vector<int32_t> S, D, Wn;
+    std::vector<uint8_t> chosen(m, 0);
+    for (int32_t bi = 0; bi < nb; bi++) {
+      std::vector<int32_t> pos, absent;
+      for (int32_t e = 0; e < m; e++) {
+        if (cap[e] > 0) pos.push_back(e);
+        else if (cap[g->par[e]] == 0) absent.push_back(e);
+      }
+      int64_t K = std::max<int64_t>(1, (int64_t)std::llround(frac * (double)pos.size()));
+      int64_t n_ins = absent.empty() ? 0 : std::min<int64_t>((int64_t)absent.size(), std::llround(p_ins * K));
+      int64_t n_inc = std::llround(p_inc * K), n_dec = std::llround(p_dec * K);
+      int64_t n_del = std::max<int64_t>(0, K - n_inc - n_dec - n_ins);
+      int64_t need = std::min<int64_t>((int64_t)pos.size(), n_inc + n_dec + n_del);
+      std::vector<int32_t> picks;
+      while ((int64_t)picks.size() < need) {
+        int32_t e = pos[rng.uniform(0, (int64_t)pos.size() - 1)];
+        if (chosen[e]) continue;
+        chosen[e] = 1;
+        picks.push_back(e);
+      }
+      std::vector<int32_t> ins;
+      while ((int64_t)ins.size() < n_ins) {
+        int32_t e = absent[rng.uniform(0, (int64_t)absent.size() - 1)];
+        if (chosen[e]) continue;
+        chosen[e] = 1;
+        ins.push_back(e);
+      }
+      int64_t i = 0;
+      for (int32_t e : picks) {
+        int32_t nc;
+        if (i < n_inc) nc = (int32_t)std::min<int64_t>((int64_t)cap[e] + rng.uniform(1, delta_hi),
+                                                      (int64_t)INT32_MAX - cap[g->par[e]]);
+        else if (i < n_inc + n_dec) nc = (int32_t)std::max<int64_t>(0, (int64_t)cap[e] - rng.uniform(1, delta_hi));
+        else nc = 0;
+        i++;
+        S.push_back(tail[e]); D.push_back(g->adj[e]); Wn.push_back(nc);
+        cap[e] = nc;
+        chosen[e] = 0;
+      }
+      for (int32_t e : ins) {
+        int32_t nc = (int32_t)rng.uniform(ins_lo, ins_hi);
+        S.push_back(tail[e]); D.push_back(g->adj[e]); Wn.push_back(nc);
+        cap[e] = nc;
+        chosen[e] = 0;
+      }
+      O.push_back((int64_t)S.size());
     }
-    int64_t K = std::max<int64_t>(1, (int64_t)std::llround(frac * (double)pos.size()));
-    int64_t n_ins = absent.empty() ? 0 : std::min<int64_t>((int64_t)absent.size(), std::llround(p_ins * K));
-    int64_t n_inc = std::llround(p_inc * K), n_dec = std::llround(p_dec * K);
-    int64_t n_del = std::max<int64_t>(0, K - n_inc - n_dec - n_ins);
-    int64_t need = std::min<int64_t>((int64_t)pos.size(), n_inc + n_dec + n_del);
-    std::vector<int32_t> picks;
-    while ((int64_t)picks.size() < need) {
-      int32_t e = pos[rng.uniform(0, (int64_t)pos.size() - 1)];
-      if (chosen[e]) continue;
-      chosen[e] = 1;
-      picks.push_back(e);
+    size_t kk = S.size();
+    auto *o_ofs = (int64_t *)std::malloc(sizeof(int64_t) * O.size());
+    auto *o_src = (int32_t *)std::malloc(sizeof(int32_t) * (kk + 1));
+    auto *o_dst = (int32_t *)std::malloc(sizeof(int32_t) * (kk + 1));
+    auto *o_w = (int32_t *)std::malloc(sizeof(int32_t) * (kk + 1));
+    if (!o_ofs || !o_src || !o_dst || !o_w) {
+      std::free(o_ofs); std::free(o_src); std::free(o_dst); std::free(o_w);
+      return fail(DMF_ERR_OOM, "host allocation failed");
     }
-    std::vector<int32_t> ins;
-    while ((int64_t)ins.size() < n_ins) {
-      int32_t e = absent[rng.uniform(0, (int64_t)absent.size() - 1)];
-      if (chosen[e]) continue;
-      chosen[e] = 1;
-      ins.push_back(e);
+    std::memcpy(o_ofs, O.data(), sizeof(int64_t) * O.size());
+    if (kk) {
+      std::memcpy(o_src, S.data(), 4 * kk);
+      std::memcpy(o_dst, D.data(), 4 * kk);
+      std::memcpy(o_w, Wn.data(), 4 * kk);
     }
-    int64_t i = 0;
-    for (int32_t e : picks) {
-      int32_t nc;
-      if (i < n_inc) nc = (int32_t)std::min<int64_t>((int64_t)cap[e] + rng.uniform(1, delta_hi),
-                                                    (int64_t)INT32_MAX - cap[g->par[e]]);
-      else if (i < n_inc + n_dec) nc = (int32_t)std::max<int64_t>(0, (int64_t)cap[e] - rng.uniform(1, delta_hi));
-      else nc = 0;
-      i++;
-      S.push_back(tail[e]); D.push_back(g->adj[e]); Wn.push_back(nc);
-      cap[e] = nc;
-      chosen[e] = 0;
-    }
-    for (int32_t e : ins) {
-      int32_t nc = (int32_t)rng.uniform(ins_lo, ins_hi);
-      S.push_back(tail[e]); D.push_back(g->adj[e]); Wn.push_back(nc);
-      cap[e] = nc;
-      chosen[e] = 0;
-    }
-    O.push_back((int64_t)S.size());
-  }
-  size_t kk = S.size();
-  *ofs = (int64_t *)std::malloc(sizeof(int64_t) * O.size());
-  *src = (int32_t *)std::malloc(sizeof(int32_t) * (kk + 1));
-  *dst = (int32_t *)std::malloc(sizeof(int32_t) * (kk + 1));
-  *w = (int32_t *)std::malloc(sizeof(int32_t) * (kk + 1));
-  if (!*ofs || !*src || !*dst || !*w) return fail(DMF_ERR_OOM, "host allocation failed");
-  std::memcpy(*ofs, O.data(), sizeof(int64_t) * O.size());
-  if (kk) {
-    std::memcpy(*src, S.data(), 4 * kk);
-    std::memcpy(*dst, D.data(), 4 * kk);
-    std::memcpy(*w, Wn.data(), 4 * kk);
-  }
-  return ok();
+    *ofs = o_ofs;
+    *src = o_src;
+    *dst = o_dst;
+    *w = o_w;
+    return ok();
+  });
 }
 
 }  // extern "C"

@@ -3,6 +3,9 @@
 #pragma once
 
 #include <cstdint>
+#include <exception>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -19,10 +22,28 @@ struct dmf_graph {
 
 namespace dmf {
 
-// Records a thread-local error message and returns `status`.
+// Records a thread-local error message and returns `status`.  Never throws.
 int fail(int status, const char *fmt, ...);
 // Clears the thread-local message, returns DMF_OK.
 int ok();
+
+// Runs `body` (which returns a status) and turns a C++ exception into a
+// status, so that none unwinds through the C ABI: std::bad_alloc and
+// std::length_error become DMF_ERR_OOM, anything else DMF_ERR_HOST.
+template <class F>
+int guarded(F &&body) noexcept {
+  try {
+    return body();
+  } catch (const std::bad_alloc &) {
+    return fail(DMF_ERR_OOM, "host allocation failed");
+  } catch (const std::length_error &x) {
+    return fail(DMF_ERR_OOM, "host allocation too large (%s)", x.what());
+  } catch (const std::exception &x) {
+    return fail(DMF_ERR_HOST, "%s", x.what());
+  } catch (...) {
+    return fail(DMF_ERR_HOST, "unknown C++ exception");
+  }
+}
 
 // Validates CSR structure: offsets, ids, partner involution, capacities.
 int validate(const dmf_graph &g);

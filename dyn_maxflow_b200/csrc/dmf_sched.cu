@@ -24,6 +24,7 @@
 using namespace dmfs;
 using dmf::fail;
 using dmf::ok;
+using dmf::guarded;
 
 namespace {
 
@@ -317,30 +318,38 @@ int init_masters(dmf_sched *s, uint64_t seed) {
 extern "C" {
 
 int dmf_sched_create(int32_t device, uint64_t seed, dmf_sched **out) {
-  if (!out) return fail(DMF_ERR_INVALID_ARG, "null output");
-  *out = nullptr;
-  int dev = device;
-  if (dev < 0) SCK(cudaGetDevice(&dev), "cudaGetDevice");
-  SCK(cudaSetDevice(dev), "cudaSetDevice");
-  dmf_sched *s = new dmf_sched();
-  s->dev = dev;
-  auto bail = [&](int st) {
-    dmf_sched_destroy(s);
-    return st;
-  };
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&s->W, sizeof(__nv_bfloat16) * kNumW) != cudaSuccess ||
-      cudaMalloc(&s->b, sizeof(float) * kNumB) != cudaSuccess ||
-      cudaMalloc(&s->master, sizeof(float) * kNumP) != cudaSuccess ||
-      cudaMalloc(&s->mom, sizeof(float) * kNumP) != cudaSuccess ||
-      cudaMalloc(&s->vel, sizeof(float) * kNumP) != cudaSuccess ||
-      cudaMalloc(&s->io, sizeof(float) * 32) != cudaSuccess ||
-      cudaMallocHost(&s->h_io, sizeof(float) * 32) != cudaSuccess)
-    return bail(fail(DMF_ERR_OOM, "scheduler allocation: %s", cudaGetErrorString(cudaGetLastError())));
-  int st = init_masters(s, seed);
-  if (st) return bail(st);
-  *out = s;
-  return ok();
+  return guarded([&]() -> int {
+    if (!out) return fail(DMF_ERR_INVALID_ARG, "null output");
+    *out = nullptr;
+    int dev = device;
+    if (dev < 0) SCK(cudaGetDevice(&dev), "cudaGetDevice");
+    SCK(cudaSetDevice(dev), "cudaSetDevice");
+    dmf_sched *s = new dmf_sched();
+    s->dev = dev;
+    auto bail = [&](int st) {
+      dmf_sched_destroy(s);
+      return st;
+    };
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&s->W, sizeof(__nv_bfloat16) * kNumW) != cudaSuccess ||
+        cudaMalloc(&s->b, sizeof(float) * kNumB) != cudaSuccess ||
+        cudaMalloc(&s->master, sizeof(float) * kNumP) != cudaSuccess ||
+        cudaMalloc(&s->mom, sizeof(float) * kNumP) != cudaSuccess ||
+        cudaMalloc(&s->vel, sizeof(float) * kNumP) != cudaSuccess ||
+        cudaMalloc(&s->io, sizeof(float) * 32) != cudaSuccess ||
+        cudaMallocHost(&s->h_io, sizeof(float) * 32) != cudaSuccess)
+      return bail(fail(DMF_ERR_OOM, "scheduler allocation: %s", cudaGetErrorString(cudaGetLastError())));
+    int st;
+    try {
+      st = init_masters(s, seed);
+    } catch (...) {
+      dmf_sched_destroy(s);
+      throw;
+    }
+    if (st) return bail(st);
+    *out = s;
+    return ok();
+  });
 }
 
 int dmf_sched_destroy(dmf_sched *s) {
@@ -360,28 +369,30 @@ int dmf_sched_destroy(dmf_sched *s) {
 }
 
 int dmf_sched_set_weights(dmf_sched *s, const uint16_t *weights, const float *biases) {
-  if (!s || !weights || !biases) return fail(DMF_ERR_INVALID_ARG, "null argument");
-  std::lock_guard<std::mutex> lock(s->mu);
-  SCK(cudaSetDevice(s->dev), "cudaSetDevice");
-  std::vector<float> h(kNumP);
-  for (int i = 0; i < kNumW; i++) {
-    const uint32_t bits = (uint32_t)weights[i] << 16;
-    std::memcpy(&h[i], &bits, 4);
-    if (!std::isfinite(h[i])) return fail(DMF_ERR_INVALID_ARG, "weight %d is not finite", i);
-  }
-  for (int i = 0; i < kNumB; i++) {
-    if (!std::isfinite(biases[i])) return fail(DMF_ERR_INVALID_ARG, "bias %d is not finite", i);
-    h[kNumW + i] = biases[i];
-  }
-  SCK(cudaMemcpyAsync(s->master, h.data(), sizeof(float) * kNumP, cudaMemcpyHostToDevice, s->stream), "H2D weights");
-  SCK(cudaMemsetAsync(s->mom, 0, sizeof(float) * kNumP, s->stream), "memset");
-  SCK(cudaMemsetAsync(s->vel, 0, sizeof(float) * kNumP, s->stream), "memset");
-  k_publish<<<(kNumP + 255) / 256, 256, 0, s->stream>>>(s->master, s->W, s->b);
-  SCK(cudaGetLastError(), "publish");
-  SCK(cudaStreamSynchronize(s->stream), "set weights");
-  s->adam_t = 0;
-  s->trained = true;
-  return ok();
+  return guarded([&]() -> int {
+    if (!s || !weights || !biases) return fail(DMF_ERR_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    SCK(cudaSetDevice(s->dev), "cudaSetDevice");
+    std::vector<float> h(kNumP);
+    for (int i = 0; i < kNumW; i++) {
+      const uint32_t bits = (uint32_t)weights[i] << 16;
+      std::memcpy(&h[i], &bits, 4);
+      if (!std::isfinite(h[i])) return fail(DMF_ERR_INVALID_ARG, "weight %d is not finite", i);
+    }
+    for (int i = 0; i < kNumB; i++) {
+      if (!std::isfinite(biases[i])) return fail(DMF_ERR_INVALID_ARG, "bias %d is not finite", i);
+      h[kNumW + i] = biases[i];
+    }
+    SCK(cudaMemcpyAsync(s->master, h.data(), sizeof(float) * kNumP, cudaMemcpyHostToDevice, s->stream), "H2D weights");
+    SCK(cudaMemsetAsync(s->mom, 0, sizeof(float) * kNumP, s->stream), "memset");
+    SCK(cudaMemsetAsync(s->vel, 0, sizeof(float) * kNumP, s->stream), "memset");
+    k_publish<<<(kNumP + 255) / 256, 256, 0, s->stream>>>(s->master, s->W, s->b);
+    SCK(cudaGetLastError(), "publish");
+    SCK(cudaStreamSynchronize(s->stream), "set weights");
+    s->adam_t = 0;
+    s->trained = true;
+    return ok();
+  });
 }
 
 int dmf_sched_set_margin(dmf_sched *s, float margin) {
@@ -403,70 +414,74 @@ int dmf_sched_get_weights(dmf_sched *s, uint16_t *weights, float *biases) {
 
 int dmf_sched_train(dmf_sched *s, int32_t n, const float *X, const float *Y, int32_t steps, int32_t batch, float lr,
                     uint64_t seed, float *loss) {
-  if (!s || n <= 0 || !X || !Y || steps < 0 || batch < 1 || batch > kMaxBatch || !(lr > 0.f) || !std::isfinite(lr))
-    return fail(DMF_ERR_INVALID_ARG, "bad training arguments (n > 0, 1 <= batch <= %d, lr > 0)", kMaxBatch);
-  std::lock_guard<std::mutex> lock(s->mu);
-  for (size_t i = 0; i < (size_t)n * kFeatures; i++)
-    if (!std::isfinite(X[i])) return fail(DMF_ERR_INVALID_ARG, "feature value %zu is not finite", i);
-  for (size_t i = 0; i < (size_t)n * kActions; i++)
-    if (!std::isfinite(Y[i])) return fail(DMF_ERR_INVALID_ARG, "target value %zu is not finite", i);
-  SCK(cudaSetDevice(s->dev), "cudaSetDevice");
-  float *dX = nullptr, *dY = nullptr, *dL = nullptr;
-  auto cleanup = [&]() {
-    cudaFree(dX);
-    cudaFree(dY);
-    cudaFree(dL);
-  };
-  if (cudaMalloc(&dX, sizeof(float) * kFeatures * (size_t)n) != cudaSuccess ||
-      cudaMalloc(&dY, sizeof(float) * kActions * (size_t)n) != cudaSuccess ||
-      cudaMalloc(&dL, sizeof(float) * std::max(steps, 1)) != cudaSuccess) {
+  return guarded([&]() -> int {
+    if (!s || n <= 0 || !X || !Y || steps < 0 || batch < 1 || batch > kMaxBatch || !(lr > 0.f) || !std::isfinite(lr))
+      return fail(DMF_ERR_INVALID_ARG, "bad training arguments (n > 0, 1 <= batch <= %d, lr > 0)", kMaxBatch);
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (size_t i = 0; i < (size_t)n * kFeatures; i++)
+      if (!std::isfinite(X[i])) return fail(DMF_ERR_INVALID_ARG, "feature value %zu is not finite", i);
+    for (size_t i = 0; i < (size_t)n * kActions; i++)
+      if (!std::isfinite(Y[i])) return fail(DMF_ERR_INVALID_ARG, "target value %zu is not finite", i);
+    SCK(cudaSetDevice(s->dev), "cudaSetDevice");
+    float *dX = nullptr, *dY = nullptr, *dL = nullptr;
+    auto cleanup = [&]() {
+      cudaFree(dX);
+      cudaFree(dY);
+      cudaFree(dL);
+    };
+    if (cudaMalloc(&dX, sizeof(float) * kFeatures * (size_t)n) != cudaSuccess ||
+        cudaMalloc(&dY, sizeof(float) * kActions * (size_t)n) != cudaSuccess ||
+        cudaMalloc(&dL, sizeof(float) * std::max(steps, 1)) != cudaSuccess) {
+      cleanup();
+      return fail(DMF_ERR_OOM, "training buffers");
+    }
+    cudaError_t e = cudaMemcpyAsync(dX, X, sizeof(float) * kFeatures * (size_t)n, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(dY, Y, sizeof(float) * kActions * (size_t)n, cudaMemcpyHostToDevice, s->stream);
+    const int smem = (int)sizeof(TrainSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess && steps > 0) {
+      k_train<<<1, kTrainThreads, smem, s->stream>>>(s->W, s->b, s->master, s->mom, s->vel, dX, dY, n, steps, batch, lr,
+                                                      seed, s->adam_t, dL);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && loss && steps > 0)
+      e = cudaMemcpyAsync(loss, dL, sizeof(float) * steps, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     cleanup();
-    return fail(DMF_ERR_OOM, "training buffers");
-  }
-  cudaError_t e = cudaMemcpyAsync(dX, X, sizeof(float) * kFeatures * (size_t)n, cudaMemcpyHostToDevice, s->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(dY, Y, sizeof(float) * kActions * (size_t)n, cudaMemcpyHostToDevice, s->stream);
-  const int smem = (int)sizeof(TrainSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess && steps > 0) {
-    k_train<<<1, kTrainThreads, smem, s->stream>>>(s->W, s->b, s->master, s->mom, s->vel, dX, dY, n, steps, batch, lr,
-                                                    seed, s->adam_t, dL);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess && loss && steps > 0)
-    e = cudaMemcpyAsync(loss, dL, sizeof(float) * steps, cudaMemcpyDeviceToHost, s->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-  cleanup();
-  if (e != cudaSuccess) return fail(DMF_ERR_CUDA, "training: %s", cudaGetErrorString(e));
-  s->adam_t += steps;
-  s->trained = true;
-  return ok();
+    if (e != cudaSuccess) return fail(DMF_ERR_CUDA, "training: %s", cudaGetErrorString(e));
+    s->adam_t += steps;
+    s->trained = true;
+    return ok();
+  });
 }
 
 int dmf_sched_predict(dmf_sched *s, int32_t n, const float *X, float *Y) {
-  if (!s || n < 0 || (n > 0 && (!X || !Y))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
-  std::lock_guard<std::mutex> lock(s->mu);
-  if (n == 0) return ok();
-  SCK(cudaSetDevice(s->dev), "cudaSetDevice");
-  float *dX = nullptr, *dY = nullptr;
-  if (cudaMalloc(&dX, sizeof(float) * kFeatures * (size_t)n) != cudaSuccess ||
-      cudaMalloc(&dY, sizeof(float) * kActions * (size_t)n) != cudaSuccess) {
+  return guarded([&]() -> int {
+    if (!s || n < 0 || (n > 0 && (!X || !Y))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (n == 0) return ok();
+    SCK(cudaSetDevice(s->dev), "cudaSetDevice");
+    float *dX = nullptr, *dY = nullptr;
+    if (cudaMalloc(&dX, sizeof(float) * kFeatures * (size_t)n) != cudaSuccess ||
+        cudaMalloc(&dY, sizeof(float) * kActions * (size_t)n) != cudaSuccess) {
+      cudaFree(dX);
+      cudaFree(dY);
+      return fail(DMF_ERR_OOM, "prediction buffers");
+    }
+    cudaError_t e = cudaMemcpyAsync(dX, X, sizeof(float) * kFeatures * (size_t)n, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) {
+      k_predict<<<std::min(n, 4096), kHidden, 0, s->stream>>>(s->W, s->b, dX, n, dY);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(Y, dY, sizeof(float) * kActions * (size_t)n, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     cudaFree(dX);
     cudaFree(dY);
-    return fail(DMF_ERR_OOM, "prediction buffers");
-  }
-  cudaError_t e = cudaMemcpyAsync(dX, X, sizeof(float) * kFeatures * (size_t)n, cudaMemcpyHostToDevice, s->stream);
-  if (e == cudaSuccess) {
-    k_predict<<<std::min(n, 4096), kHidden, 0, s->stream>>>(s->W, s->b, dX, n, dY);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(Y, dY, sizeof(float) * kActions * (size_t)n, cudaMemcpyDeviceToHost, s->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-  cudaFree(dX);
-  cudaFree(dY);
-  if (e != cudaSuccess) return fail(DMF_ERR_CUDA, "prediction: %s", cudaGetErrorString(e));
-  return ok();
+    if (e != cudaSuccess) return fail(DMF_ERR_CUDA, "prediction: %s", cudaGetErrorString(e));
+    return ok();
+  });
 }
 
 }  // extern "C"

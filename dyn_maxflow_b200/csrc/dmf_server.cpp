@@ -18,14 +18,18 @@
 #include <parallel/algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
 
 #include "dmf_internal.h"
+
+using dmf::guarded;
 
 namespace {
 
@@ -36,6 +40,7 @@ struct Request {
   int32_t graph;
   std::vector<int32_t> src, dst, w;
   Clock::time_point t_submit;
+  bool claimed = false;  // a wait() holds it
   bool done = false;
   int status = DMF_OK;
   std::string error;
@@ -55,9 +60,13 @@ struct dmf_server {
   std::vector<std::deque<Request *>> pending;  // per graph, FIFO
   std::map<int64_t, Request *> all;
   int64_t next_ticket = 1;
-  bool stop = false;
+  bool stop = false;  // destroy(): serve what is pending, then end the worker
+  int waiters = 0;    // threads inside wait()
   std::thread worker;
   int64_t ticks = 0, served = 0, batched_sum = 0;
+  // worker-owned staging, sized at create so a tick's selection never allocates
+  std::vector<Request *> batch;
+  std::vector<int64_t> flows;
 };
 
 static int64_t footprint(const dmf_graph *g) {
@@ -67,9 +76,9 @@ static int64_t footprint(const dmf_graph *g) {
 
 static void tick_loop(dmf_server *S) {
   const int G = (int)S->graphs.size();
-  std::vector<int64_t> flows(G);
+  std::vector<Request *> &batch = S->batch;
   for (;;) {
-    std::vector<Request *> batch;
+    batch.clear();  // capacity G: the selection below never allocates
     {
       std::unique_lock<std::mutex> lk(S->mu);
       S->cv_work.wait(lk, [&] {
@@ -78,7 +87,6 @@ static void tick_loop(dmf_server *S) {
           if (!q.empty()) return true;
         return false;
       });
-      if (S->stop) return;
       int64_t bytes = 0;
       for (int g = 0; g < G; g++) {
         if (S->pending[g].empty()) continue;
@@ -89,23 +97,33 @@ static void tick_loop(dmf_server *S) {
         S->pending[g].pop_front();
         batch.push_back(r);
       }
+      if (batch.empty()) return;  // stopping, and every submitted request is served
     }
-    std::vector<int32_t> I, A, B, W;
-    for (Request *r : batch) {
-      I.insert(I.end(), r->src.size(), r->graph);
-      A.insert(A.end(), r->src.begin(), r->src.end());
-      B.insert(B.end(), r->dst.begin(), r->dst.end());
-      W.insert(W.end(), r->w.begin(), r->w.end());
-    }
-    int st = dmf_multi_apply_updates(S->sv, (int32_t)A.size(), I.data(), A.data(), B.data(), W.data(), flows.data());
-    std::string err = st ? dmf_last_error() : "";
+    // a failure here (staging allocation included) fails this tick's requests
+    // and leaves the worker running
+    int st = guarded([&]() -> int {
+      std::vector<int32_t> I, A, B, W;
+      for (Request *r : batch) {
+        I.insert(I.end(), r->src.size(), r->graph);
+        A.insert(A.end(), r->src.begin(), r->src.end());
+        B.insert(B.end(), r->dst.begin(), r->dst.end());
+        W.insert(W.end(), r->w.begin(), r->w.end());
+      }
+      return dmf_multi_apply_updates(S->sv, (int32_t)A.size(), I.data(), A.data(), B.data(), W.data(),
+                                     S->flows.data());
+    });
+    const char *err = st ? dmf_last_error() : "";
     const auto now = Clock::now();
     {
       std::lock_guard<std::mutex> lk(S->mu);
       for (Request *r : batch) {
         r->status = st;
-        r->error = err;
-        r->flow = flows[r->graph];
+        try {
+          r->error = err;
+        } catch (...) {
+          // the status alone reaches the waiter
+        }
+        r->flow = S->flows[r->graph];
         r->latency_ms = std::chrono::duration<double, std::milli>(now - r->t_submit).count();
         r->done = true;
       }
@@ -123,39 +141,43 @@ int dmf_server_create(int32_t count, const dmf_graph *const *graphs, const int32
                       int64_t hbm_budget, const dmf_opts *opts, dmf_server **out) {
   if (count < 1 || !graphs || !s || !t || !out || hbm_budget <= 0)
     return dmf::fail(DMF_ERR_INVALID_ARG, "bad arguments");
-  auto *S = new dmf_server();
-  S->budget = hbm_budget;
-  for (int i = 0; i < count; i++) {
-    if (!graphs[i]) {
-      delete S;
-      return dmf::fail(DMF_ERR_INVALID_ARG, "graph %d is null", i);
+  for (int i = 0; i < count; i++)
+    if (!graphs[i]) return dmf::fail(DMF_ERR_INVALID_ARG, "graph %d is null", i);
+  dmf_server *S = nullptr;
+  int st = guarded([&]() -> int {
+    S = new dmf_server();
+    S->budget = hbm_budget;
+    for (int i = 0; i < count; i++) {
+      const int64_t f = footprint(graphs[i]);
+      if (S->device_bytes + f > hbm_budget) continue;  // not admitted
+      S->device_bytes += f;
+      S->graphs.push_back(graphs[i]);
+      S->s.push_back(s[i]);
+      S->t.push_back(t[i]);
     }
-    const int64_t f = footprint(graphs[i]);
-    if (S->device_bytes + f > hbm_budget) continue;  // not admitted
-    S->device_bytes += f;
-    S->graphs.push_back(graphs[i]);
-    S->s.push_back(s[i]);
-    S->t.push_back(t[i]);
-  }
-  if (S->graphs.empty()) {
-    delete S;
-    return dmf::fail(DMF_ERR_OOM, "no graph fits the HBM budget of %lld bytes", (long long)hbm_budget);
-  }
-  S->stage_budget = std::max<int64_t>(hbm_budget - S->device_bytes, 16LL << 20);
-  int st = dmf_multi_create((int32_t)S->graphs.size(), S->graphs.data(), S->s.data(), S->t.data(), opts, nullptr,
-                            &S->sv);
+    if (S->graphs.empty())
+      return dmf::fail(DMF_ERR_OOM, "no graph fits the HBM budget of %lld bytes", (long long)hbm_budget);
+    S->stage_budget = std::max<int64_t>(hbm_budget - S->device_bytes, 16LL << 20);
+    const size_t G = S->graphs.size();
+    S->pending.resize(G);
+    S->batch.reserve(G);
+    S->flows.resize(G);
+    int rc = dmf_multi_create((int32_t)G, S->graphs.data(), S->s.data(), S->t.data(), opts, nullptr, &S->sv);
+    if (rc) return rc;
+    if ((rc = dmf_multi_static_maxflow(S->sv, S->flows.data()))) return rc;
+    S->worker = std::thread(tick_loop, S);
+    return dmf::ok();
+  });
   if (st) {
-    delete S;
+    if (S) {
+      char msg[1024];
+      std::snprintf(msg, sizeof msg, "%s", dmf_last_error());
+      dmf_solver_destroy(S->sv);
+      delete S;
+      dmf::fail(st, "%s", msg);
+    }
     return st;
   }
-  std::vector<int64_t> f(S->graphs.size());
-  if ((st = dmf_multi_static_maxflow(S->sv, f.data()))) {
-    dmf_solver_destroy(S->sv);
-    delete S;
-    return st;
-  }
-  S->pending.resize(S->graphs.size());
-  S->worker = std::thread(tick_loop, S);
   *out = S;
   return dmf::ok();
 }
@@ -206,21 +228,31 @@ int dmf_server_submit(dmf_server *S, int32_t graph, int32_t k, const int32_t *sr
   const auto first_arc = std::upper_bound(arcs.begin(), arcs.end(), (int64_t)-1);  // skip ignored self-loops
   if (std::adjacent_find(first_arc, arcs.end()) != arcs.end())
     return dmf::fail(DMF_ERR_DUP_ARC, "an arc repeats within the request");
-  auto *r = new Request();
-  r->graph = graph;
-  r->src.assign(src, src + k);
-  r->dst.assign(dst, dst + k);
-  r->w.assign(w, w + k);
-  r->t_submit = t_arrival;
-  {
-    std::lock_guard<std::mutex> lk(S->mu);
-    r->ticket = S->next_ticket++;
-    S->all[r->ticket] = r;
-    S->pending[graph].push_back(r);
-  }
-  S->cv_work.notify_one();
-  *ticket = r->ticket;
-  return dmf::ok();
+  return guarded([&]() -> int {
+    std::unique_ptr<Request> r(new Request());
+    r->graph = graph;
+    r->src.assign(src, src + k);
+    r->dst.assign(dst, dst + k);
+    r->w.assign(w, w + k);
+    r->t_submit = t_arrival;
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      const int64_t tk = S->next_ticket;
+      auto ins = S->all.emplace(tk, r.get());
+      try {
+        S->pending[graph].push_back(r.get());
+      } catch (...) {
+        S->all.erase(ins.first);
+        throw;
+      }
+      S->next_ticket++;
+      r->ticket = tk;
+      *ticket = tk;
+      r.release();  // owned by the server until its wait() returns
+    }
+    S->cv_work.notify_one();
+    return dmf::ok();
+  });
 }
 
 int dmf_server_wait(dmf_server *S, int64_t ticket, int64_t *flow, double *latency_ms) {
@@ -229,15 +261,20 @@ int dmf_server_wait(dmf_server *S, int64_t ticket, int64_t *flow, double *latenc
   auto it = S->all.find(ticket);
   if (it == S->all.end()) return dmf::fail(DMF_ERR_INVALID_ARG, "unknown ticket %lld", (long long)ticket);
   Request *r = it->second;
+  if (r->claimed) return dmf::fail(DMF_ERR_INVALID_ARG, "ticket %lld is already being waited on", (long long)ticket);
+  r->claimed = true;
+  S->waiters++;
   S->cv_done.wait(lk, [&] { return r->done; });
-  S->all.erase(it);
+  S->waiters--;
+  S->all.erase(ticket);
+  std::unique_ptr<Request> own(r);
   const int st = r->status;
-  const std::string err = r->error;
   if (flow) *flow = r->flow;
   if (latency_ms) *latency_ms = r->latency_ms;
-  delete r;
+  if (st) dmf::fail(st, "%s", r->error.c_str());
   lk.unlock();
-  return st ? dmf::fail(st, "%s", err.c_str()) : dmf::ok();
+  S->cv_done.notify_all();  // destroy() may be waiting for the last waiter
+  return st ? st : dmf::ok();
 }
 
 int dmf_server_stats(const dmf_server *S, int64_t *ticks, int64_t *served, double *mean_per_tick) {
@@ -257,8 +294,14 @@ int dmf_server_destroy(dmf_server *S) {
     S->stop = true;
   }
   S->cv_work.notify_all();
+  // the worker serves every request already submitted before it ends, so a
+  // thread blocked in wait() gets its result; no call may start after this one
   if (S->worker.joinable()) S->worker.join();
-  for (auto &kv : S->all) delete kv.second;
+  {
+    std::unique_lock<std::mutex> lk(S->mu);
+    S->cv_done.wait(lk, [&] { return S->waiters == 0; });
+  }
+  for (auto &kv : S->all) delete kv.second;  // served, never waited on
   dmf_solver_destroy(S->sv);
   delete S;
   return dmf::ok();

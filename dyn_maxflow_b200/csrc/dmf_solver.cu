@@ -1737,6 +1737,7 @@ KernelFn pick_kernel(int tile, int minb) {
 // ============================================================================
 using dmf::fail;
 using dmf::ok;
+using dmf::guarded;
 
 struct dmf_solver {
   int dev = 0;
@@ -1814,6 +1815,7 @@ int cuda_fail(cudaError_t e, const char *what) {
 template <class T>
 int dalloc(dmf_solver *sv, T **p, size_t count) {
   void *q = nullptr;
+  sv->allocs.reserve(sv->allocs.size() + 1);  // may throw; the push below then cannot
   cudaError_t e = cudaMalloc(&q, sizeof(T) * std::max<size_t>(count, 1));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
   sv->allocs.push_back(q);
@@ -2361,6 +2363,9 @@ struct MultiSpec {
   std::vector<int> inst;
 };
 
+int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, void *stream,
+                 const MultiSpec *ms);
+
 int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, void *stream, const MultiSpec *ms,
                 dmf_solver **out) {
   if (!g || !out) return fail(DMF_ERR_INVALID_ARG, "null argument");
@@ -2369,36 +2374,50 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
   if ((int64_t)g->sidx.size() != g->m) return fail(DMF_ERR_INVALID_ARG, "graph has no arc index");
   int ndev = dmf_device_count();
   if (ndev == 0) return fail(DMF_ERR_CUDA, "no CUDA device is visible; the solver runs only on the GPU");
-  auto *sv = new dmf_solver();
+  if (opts && (opts->variant < 0 || opts->variant > 2))
+    return fail(DMF_ERR_INVALID_ARG, "unknown variant %d", opts->variant);
+  dmf_solver *sv = nullptr;
+  const int st = guarded([&]() -> int {
+    sv = new dmf_solver();
+    return setup_solver(sv, g, s, t, opts, stream, ms);
+  });
+  if (st) {
+    if (sv) {
+      char msg[1024];
+      std::snprintf(msg, sizeof msg, "%s", dmf_last_error());
+      free_all(sv);
+      delete sv;
+      fail(st, "%s", msg);
+    }
+    return st;
+  }
+  *out = sv;
+  return ok();
+}
+
+// Fills a new solver: device arrays, hub chunks, sources.  On failure the
+// caller frees what was allocated (free_all).
+int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, void *stream,
+                 const MultiSpec *ms) {
   if (opts) sv->opts = *opts;
   else dmf_opts_default(&sv->opts);
-  if (sv->opts.variant < 0 || sv->opts.variant > 2) {
-    delete sv;
-    return fail(DMF_ERR_INVALID_ARG, "unknown variant %d", sv->opts.variant);
-  }
   sv->n = g->n;
   sv->m = g->m;
   sv->s = s;
   sv->t = t;
   sv->stream = (cudaStream_t)stream;
   int st = DMF_OK;
-  auto bail = [&](int code) {
-    std::string msg = dmf_last_error();
-    free_all(sv);
-    delete sv;
-    return fail(code, "%s", msg.c_str());
-  };
   if (sv->opts.device >= 0) sv->dev = sv->opts.device;
-  else if (cudaGetDevice(&sv->dev) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "cudaGetDevice"));
-  if (cudaSetDevice(sv->dev) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "cudaSetDevice"));
-  if ((st = configure(sv))) return bail(st);
+  else if (cudaGetDevice(&sv->dev) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaGetDevice");
+  if (cudaSetDevice(sv->dev) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaSetDevice");
+  if ((st = configure(sv))) return st;
   const size_t N = (size_t)g->n + 1, M = (size_t)g->m;
   if ((st = dalloc(sv, &sv->off, N)) || (st = dalloc(sv, &sv->adj, M)) || (st = dalloc(sv, &sv->par, M)) ||
       (st = dalloc(sv, &sv->sidx, M)) || (st = dalloc(sv, &sv->cap, M)) || (st = dalloc(sv, &sv->res, M)) ||
       (st = dalloc(sv, &sv->astamp, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
       (st = dalloc(sv, &sv->excess, N)) || (st = dalloc(sv, &sv->dead, N)) || (st = dalloc(sv, &sv->side, N)) ||
       (st = dalloc(sv, &sv->qbuf, 5 * N)) || (st = dalloc(sv, &sv->ctrl, 1)))
-    return bail(st);
+    return st;
   std::vector<int2> hub_chunks;
   std::vector<int> hub_base(g->n, -1);
   for (int v = 0; v < g->n; v++) {
@@ -2415,7 +2434,7 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
       (st = dalloc(sv, &sv->hc_min, NC)) || (st = dalloc(sv, &sv->hc_done, NC)) ||
       (st = dalloc(sv, &sv->hub_base, N)) || (st = dalloc(sv, &sv->chunk_mark, NC)) ||
       (st = dalloc(sv, &sv->chunk_tmin, NC)))
-    return bail(st);
+    return st;
   cudaStream_t S = sv->stream;
   cudaError_t e = cudaSuccess;
   auto up = [&](void *d, const void *h, size_t bytes) {
@@ -2441,8 +2460,8 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
   if (e == cudaSuccess) e = cudaEventCreate(&sv->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&sv->ev1);
   if (e == cudaSuccess) e = cudaStreamSynchronize(S);
-  if (e != cudaSuccess) return bail(cuda_fail(e, "solver upload"));
-  if ((st = ensure_ubuf(sv, 1024))) return bail(st);
+  if (e != cudaSuccess) return cuda_fail(e, "solver upload");
+  if ((st = ensure_ubuf(sv, 1024))) return st;
   // sources (and, for batched instances, roles, instance ids, per-instance flows)
   {
     const std::vector<int> one(1, s);
@@ -2452,31 +2471,30 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
     std::vector<int> so(sl.size() + 1, 0);
     for (size_t i = 0; i < sl.size(); i++) {
       const long long nx = (long long)so[i] + g->off[sl[i] + 1] - g->off[sl[i]];
-      if (nx > INT_MAX) return bail(fail(DMF_ERR_INVALID_ARG, "sources have more than 2^31 arcs in total"));
+      if (nx > INT_MAX) return fail(DMF_ERR_INVALID_ARG, "sources have more than 2^31 arcs in total");
       so[i + 1] = (int)nx;
     }
-    if ((st = dalloc(sv, &sv->srcs, sl.size())) || (st = dalloc(sv, &sv->src_off, so.size()))) return bail(st);
+    if ((st = dalloc(sv, &sv->srcs, sl.size())) || (st = dalloc(sv, &sv->src_off, so.size()))) return st;
     if (cudaMemcpy(sv->srcs, sl.data(), 4 * sl.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(sv->src_off, so.data(), 4 * so.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-      return bail(cuda_fail(cudaGetLastError(), "H2D sources"));
+      return cuda_fail(cudaGetLastError(), "H2D sources");
     if (ms) {
       sv->vbase = ms->vbase;
       if ((st = dalloc(sv, &sv->role, N)) || (st = dalloc(sv, &sv->inst, N)) ||
           (st = dalloc(sv, &sv->inst_flow, (size_t)ms->count)) ||
           (st = dalloc(sv, &sv->inst_active, (size_t)ms->count)))
-        return bail(st);
+        return st;
       if (cudaMallocHost(&sv->h_inst_active, (size_t)ms->count) != cudaSuccess)
-        return bail(cuda_fail(cudaGetLastError(), "pinned mask"));
+        return cuda_fail(cudaGetLastError(), "pinned mask");
       if (cudaMemcpy(sv->role, ms->role.data(), ms->role.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
           cudaMemcpy(sv->inst, ms->inst.data(), 4 * ms->inst.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
           cudaMallocHost(&sv->h_inst_flow, 8 * (size_t)ms->count) != cudaSuccess)
-        return bail(cuda_fail(cudaGetLastError(), "batched-instance upload"));
+        return cuda_fail(cudaGetLastError(), "batched-instance upload");
     }
   }
   sv->trace_cap = 1 << 16;
-  if ((st = dalloc(sv, &sv->trace, 4 * (size_t)sv->trace_cap))) return bail(st);
-  if ((st = dalloc(sv, &sv->facc, 1))) return bail(st);
-  *out = sv;
+  if ((st = dalloc(sv, &sv->trace, 4 * (size_t)sv->trace_cap))) return st;
+  if ((st = dalloc(sv, &sv->facc, 1))) return st;
   return ok();
 }
 
@@ -2502,51 +2520,53 @@ int dmf_multi_create(int32_t count, const dmf_graph *const *graphs, const int32_
     M += g->m;
   }
   if (N >= INT32_MAX || M >= INT32_MAX) return fail(DMF_ERR_INVALID_ARG, "union too large for int32 ids");
-  dmf_graph U;
-  U.n = (int32_t)N;
-  U.m = (int32_t)M;
-  U.off.resize((size_t)N + 1);
-  U.adj.resize((size_t)M);
-  U.w.resize((size_t)M);
-  U.par.resize((size_t)M);
-  U.sidx.resize((size_t)M);
-  MultiSpec ms;
-  ms.count = count;
-  ms.vbase.resize((size_t)count + 1);
-  ms.srcs.resize(count);
-  ms.role.assign((size_t)N + 1, 0);
-  ms.inst.resize((size_t)N + 1);
-  std::vector<int64_t> abase((size_t)count + 1, 0);
-  int64_t vb = 0;
-  for (int i = 0; i < count; i++) {
-    ms.vbase[i] = (int)vb;
-    abase[i + 1] = abase[i] + graphs[i]->m;
-    vb += graphs[i]->n;
-  }
-  ms.vbase[count] = (int)vb;
+  return guarded([&]() -> int {
+    dmf_graph U;
+    U.n = (int32_t)N;
+    U.m = (int32_t)M;
+    U.off.resize((size_t)N + 1);
+    U.adj.resize((size_t)M);
+    U.w.resize((size_t)M);
+    U.par.resize((size_t)M);
+    U.sidx.resize((size_t)M);
+    MultiSpec ms;
+    ms.count = count;
+    ms.vbase.resize((size_t)count + 1);
+    ms.srcs.resize(count);
+    ms.role.assign((size_t)N + 1, 0);
+    ms.inst.resize((size_t)N + 1);
+    std::vector<int64_t> abase((size_t)count + 1, 0);
+    int64_t vb = 0;
+    for (int i = 0; i < count; i++) {
+      ms.vbase[i] = (int)vb;
+      abase[i + 1] = abase[i] + graphs[i]->m;
+      vb += graphs[i]->n;
+    }
+    ms.vbase[count] = (int)vb;
 #pragma omp parallel for schedule(dynamic, 1)
-  for (int i = 0; i < count; i++) {
-    const dmf_graph &g = *graphs[i];
-    const int vb_i = ms.vbase[i];
-    const int ab = (int)abase[i];
-    for (int v = 0; v < g.n; v++) {
-      U.off[vb_i + v] = ab + g.off[v];
-      ms.inst[vb_i + v] = i;
+    for (int i = 0; i < count; i++) {
+      const dmf_graph &g = *graphs[i];
+      const int vb_i = ms.vbase[i];
+      const int ab = (int)abase[i];
+      for (int v = 0; v < g.n; v++) {
+        U.off[vb_i + v] = ab + g.off[v];
+        ms.inst[vb_i + v] = i;
+      }
+      for (int e = 0; e < g.m; e++) {
+        U.adj[ab + e] = vb_i + g.adj[e];
+        U.w[ab + e] = g.w[e];
+        U.par[ab + e] = ab + g.par[e];
+        U.sidx[ab + e] = ab + g.sidx[e];
+      }
     }
-    for (int e = 0; e < g.m; e++) {
-      U.adj[ab + e] = vb_i + g.adj[e];
-      U.w[ab + e] = g.w[e];
-      U.par[ab + e] = ab + g.par[e];
-      U.sidx[ab + e] = ab + g.sidx[e];
+    U.off[N] = (int32_t)M;
+    for (int i = 0; i < count; i++) {
+      ms.srcs[i] = ms.vbase[i] + s[i];
+      ms.role[ms.vbase[i] + s[i]] |= 1;
+      ms.role[ms.vbase[i] + t[i]] |= 2;
     }
-  }
-  U.off[N] = (int32_t)M;
-  for (int i = 0; i < count; i++) {
-    ms.srcs[i] = ms.vbase[i] + s[i];
-    ms.role[ms.vbase[i] + s[i]] |= 1;
-    ms.role[ms.vbase[i] + t[i]] |= 2;
-  }
-  return create_impl(&U, ms.srcs[0], ms.vbase[0] + t[0], opts, stream, &ms, out);
+    return create_impl(&U, ms.srcs[0], ms.vbase[0] + t[0], opts, stream, &ms, out);
+  });
 }
 
 int dmf_multi_info(const dmf_solver *sv, int32_t *count, int32_t *vertex_base) {
@@ -2569,236 +2589,254 @@ int dmf_multi_static_maxflow(dmf_solver *sv, int64_t *flows) {
 
 int dmf_multi_apply_updates(dmf_solver *sv, int32_t k, const int32_t *inst, const int32_t *src, const int32_t *dst,
                             const int32_t *w, int64_t *flows) {
-  if (!sv || !flows || k < 0 || (k > 0 && (!inst || !src || !dst || !w)))
-    return fail(DMF_ERR_INVALID_ARG, "bad arguments");
-  std::vector<int32_t> gs(k), gd(k);
-  for (int32_t i = 0; i < k; i++) {
-    const int in = inst[i];
-    if (in < 0 || in >= sv->ninst) return fail(DMF_ERR_INVALID_ARG, "update %d: instance %d out of range", i, in);
-    const int b = sv->vbase.empty() ? 0 : sv->vbase[in];
-    const int nloc = sv->vbase.empty() ? sv->n : sv->vbase[in + 1] - b;
-    if (src[i] < 0 || dst[i] < 0 || src[i] >= nloc || dst[i] >= nloc)
-      return fail(DMF_ERR_INVALID_ARG, "update %d: vertex out of range for instance %d", i, in);
-    gs[i] = b + src[i];
-    gd[i] = b + dst[i];
-  }
-  // only the instances this batch touches are relabelled, pushed and read out
-  if (sv->inst_active && (int)sv->flows.size() == sv->ninst && sv->solved) {
-    std::memset(sv->h_inst_active, 0, (size_t)sv->ninst);
-    for (int32_t i = 0; i < k; i++) sv->h_inst_active[inst[i]] = 1;
-    CK(cudaMemcpyAsync(sv->inst_active, sv->h_inst_active, (size_t)sv->ninst, cudaMemcpyHostToDevice, sv->stream),
-       "H2D mask");
-    sv->use_active = true;
-  }
-  int st = host_updates(sv, MODE_DYNAMIC, k, gs.data(), gd.data(), w, nullptr);
-  sv->use_active = false;
-  if (st) return st;
-  for (int i = 0; i < sv->ninst; i++) flows[i] = sv->flows[i];
-  return ok();
+  return guarded([&]() -> int {
+    if (!sv || !flows || k < 0 || (k > 0 && (!inst || !src || !dst || !w)))
+      return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+    std::vector<int32_t> gs(k), gd(k);
+    for (int32_t i = 0; i < k; i++) {
+      const int in = inst[i];
+      if (in < 0 || in >= sv->ninst) return fail(DMF_ERR_INVALID_ARG, "update %d: instance %d out of range", i, in);
+      const int b = sv->vbase.empty() ? 0 : sv->vbase[in];
+      const int nloc = sv->vbase.empty() ? sv->n : sv->vbase[in + 1] - b;
+      if (src[i] < 0 || dst[i] < 0 || src[i] >= nloc || dst[i] >= nloc)
+        return fail(DMF_ERR_INVALID_ARG, "update %d: vertex out of range for instance %d", i, in);
+      gs[i] = b + src[i];
+      gd[i] = b + dst[i];
+    }
+    // only the instances this batch touches are relabelled, pushed and read out
+    if (sv->inst_active && (int)sv->flows.size() == sv->ninst && sv->solved) {
+      std::memset(sv->h_inst_active, 0, (size_t)sv->ninst);
+      for (int32_t i = 0; i < k; i++) sv->h_inst_active[inst[i]] = 1;
+      CK(cudaMemcpyAsync(sv->inst_active, sv->h_inst_active, (size_t)sv->ninst, cudaMemcpyHostToDevice, sv->stream),
+         "H2D mask");
+      sv->use_active = true;
+    }
+    int st = host_updates(sv, MODE_DYNAMIC, k, gs.data(), gd.data(), w, nullptr);
+    sv->use_active = false;
+    if (st) return st;
+    for (int i = 0; i < sv->ninst; i++) flows[i] = sv->flows[i];
+    return ok();
+  });
 }
 
 int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs, const int32_t *d_src,
                           const int32_t *d_dst, const int32_t *d_w, int32_t use_graph, int64_t *flows, double *ms) {
-  if (!sv || steps < 1 || !ofs || !flows || !d_src || !d_dst || !d_w) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
-  if (!sv->solved) return fail(DMF_ERR_NOT_SOLVED, "run_batches before a solve");
-  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
-  int64_t kmax = 0;
-  for (int b = 0; b < steps; b++) {
-    if (ofs[b + 1] < ofs[b]) return fail(DMF_ERR_INVALID_ARG, "offsets decrease at step %d", b);
-    kmax = std::max(kmax, ofs[b + 1] - ofs[b]);
-  }
-  if (kmax > INT32_MAX) return fail(DMF_ERR_INVALID_ARG, "batch too large");
-  int st = ensure_ubuf(sv, (int)kmax);
-  if (st) return st;
-  cudaStream_t S = sv->stream;
-  if (use_graph && !S) {  // the legacy default stream cannot be captured
-    if (!sv->own_stream) CK(cudaStreamCreateWithFlags(&sv->own_stream, cudaStreamNonBlocking), "stream create");
-    CK(cudaStreamSynchronize(nullptr), "sync");
-    S = sv->own_stream;
-  }
-  const int cnt = sv->ninst;
-  Ctrl *h_ctrl = nullptr;
-  long long *h_fl = nullptr;
-  CK(cudaMallocHost(&h_ctrl, sizeof(Ctrl) * (size_t)steps), "pinned control");
-  if (cudaMallocHost(&h_fl, 8 * (size_t)steps * cnt) != cudaSuccess) {
-    cudaFreeHost(h_ctrl);
-    return fail(DMF_ERR_OOM, "pinned flows");
-  }
-  // step b uses its own range of round ids, relabel epochs and batch stamp
-  constexpr unsigned kRoundStride = 1u << 20, kRelabelStride = 1u << 18;
-  KernelFn fn = pick_kernel(sv->tile, sv->minb);
-  auto enqueue_steps = [&]() -> cudaError_t {
+  return guarded([&]() -> int {
+    if (!sv || steps < 1 || !ofs || !flows || !d_src || !d_dst || !d_w) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+    if (!sv->solved) return fail(DMF_ERR_NOT_SOLVED, "run_batches before a solve");
+    CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+    int64_t kmax = 0;
     for (int b = 0; b < steps; b++) {
-      Params p = make_params(sv, MODE_DYNAMIC, (int)(ofs[b + 1] - ofs[b]), d_src + ofs[b], d_dst + ofs[b],
-                             d_w + ofs[b]);
-      p.round_base = sv->round_base + (unsigned)b * kRoundStride;
-      p.relabel_base = sv->relabel_base + (unsigned)b * kRelabelStride;
-      p.trace = nullptr;
-      p.probe = 0;
-      cudaError_t e = cudaMemsetAsync(sv->ctrl, 0, sizeof(Ctrl), S);
-      if (e == cudaSuccess && sv->inst_flow) e = cudaMemsetAsync(sv->inst_flow, 0, 8 * (size_t)cnt, S);
-      if (e != cudaSuccess) return e;
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(sv->grid);
-      cfg.blockDim = dim3(sv->block);
-      cfg.dynamicSmemBytes = 0;
-      cfg.stream = S;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeCooperative;
-      attr[0].val.cooperative = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      e = cudaLaunchKernelEx(&cfg, fn, p);
-      if (e != cudaSuccess) return e;
-      e = cudaMemcpyAsync(h_ctrl + b, sv->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, S);
-      if (e == cudaSuccess) {
-        if (sv->inst_flow)
-          e = cudaMemcpyAsync(h_fl + (size_t)b * cnt, sv->inst_flow, 8 * (size_t)cnt, cudaMemcpyDeviceToHost, S);
-        else
-          e = cudaMemcpyAsync(h_fl + b, &sv->ctrl->flow, 8, cudaMemcpyDeviceToHost, S);
+      if (ofs[b + 1] < ofs[b]) return fail(DMF_ERR_INVALID_ARG, "offsets decrease at step %d", b);
+      kmax = std::max(kmax, ofs[b + 1] - ofs[b]);
+    }
+    if (kmax > INT32_MAX) return fail(DMF_ERR_INVALID_ARG, "batch too large");
+    int st = ensure_ubuf(sv, (int)kmax);
+    if (st) return st;
+    cudaStream_t S = sv->stream;
+    if (use_graph && !S) {  // the legacy default stream cannot be captured
+      if (!sv->own_stream) CK(cudaStreamCreateWithFlags(&sv->own_stream, cudaStreamNonBlocking), "stream create");
+      CK(cudaStreamSynchronize(nullptr), "sync");
+      S = sv->own_stream;
+    }
+    const int cnt = sv->ninst;
+    Ctrl *h_ctrl = nullptr;
+    long long *h_fl = nullptr;
+    CK(cudaMallocHost(&h_ctrl, sizeof(Ctrl) * (size_t)steps), "pinned control");
+    if (cudaMallocHost(&h_fl, 8 * (size_t)steps * cnt) != cudaSuccess) {
+      cudaFreeHost(h_ctrl);
+      return fail(DMF_ERR_OOM, "pinned flows");
+    }
+    // step b uses its own range of round ids, relabel epochs and batch stamp
+    constexpr unsigned kRoundStride = 1u << 20, kRelabelStride = 1u << 18;
+    KernelFn fn = pick_kernel(sv->tile, sv->minb);
+    auto enqueue_steps = [&]() -> cudaError_t {
+      for (int b = 0; b < steps; b++) {
+        Params p = make_params(sv, MODE_DYNAMIC, (int)(ofs[b + 1] - ofs[b]), d_src + ofs[b], d_dst + ofs[b],
+                               d_w + ofs[b]);
+        p.round_base = sv->round_base + (unsigned)b * kRoundStride;
+        p.relabel_base = sv->relabel_base + (unsigned)b * kRelabelStride;
+        p.trace = nullptr;
+        p.probe = 0;
+        cudaError_t e = cudaMemsetAsync(sv->ctrl, 0, sizeof(Ctrl), S);
+        if (e == cudaSuccess && sv->inst_flow) e = cudaMemsetAsync(sv->inst_flow, 0, 8 * (size_t)cnt, S);
+        if (e != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(sv->grid);
+        cfg.blockDim = dim3(sv->block);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = S;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, fn, p);
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpyAsync(h_ctrl + b, sv->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, S);
+        if (e == cudaSuccess) {
+          if (sv->inst_flow)
+            e = cudaMemcpyAsync(h_fl + (size_t)b * cnt, sv->inst_flow, 8 * (size_t)cnt, cudaMemcpyDeviceToHost, S);
+          else
+            e = cudaMemcpyAsync(h_fl + b, &sv->ctrl->flow, 8, cudaMemcpyDeviceToHost, S);
+        }
+        if (e != cudaSuccess) return e;
       }
-      if (e != cudaSuccess) return e;
+      return cudaSuccess;
+    };
+    cudaError_t e = cudaSuccess;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (use_graph) {
+      e = cudaStreamBeginCapture(S, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        cudaError_t e2 = enqueue_steps();
+        e = cudaStreamEndCapture(S, &graph);
+        if (e2 != cudaSuccess) e = e2;
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     }
-    return cudaSuccess;
-  };
-  cudaError_t e = cudaSuccess;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  if (use_graph) {
-    e = cudaStreamBeginCapture(S, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-      cudaError_t e2 = enqueue_steps();
-      e = cudaStreamEndCapture(S, &graph);
-      if (e2 != cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaEventRecord(sv->ev0, S);
+    if (e == cudaSuccess) e = use_graph ? cudaGraphLaunch(exec, S) : enqueue_steps();
+    if (e == cudaSuccess) e = cudaEventRecord(sv->ev1, S);
+    if (e == cudaSuccess) e = cudaEventSynchronize(sv->ev1);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      cudaFreeHost(h_ctrl);
+      cudaFreeHost(h_fl);
+      return cuda_fail(e, use_graph ? "graph-captured batch loop" : "batch loop");
     }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-  }
-  if (e == cudaSuccess) e = cudaEventRecord(sv->ev0, S);
-  if (e == cudaSuccess) e = use_graph ? cudaGraphLaunch(exec, S) : enqueue_steps();
-  if (e == cudaSuccess) e = cudaEventRecord(sv->ev1, S);
-  if (e == cudaSuccess) e = cudaEventSynchronize(sv->ev1);
-  if (exec) cudaGraphExecDestroy(exec);
-  if (graph) cudaGraphDestroy(graph);
-  if (e != cudaSuccess) {
+    float t_ms = 0;
+    cudaEventElapsedTime(&t_ms, sv->ev0, sv->ev1);
+    if (ms) *ms = t_ms;
+    int rc = DMF_OK;
+    unsigned outer = 0;
+    for (int b = 0; b < steps && !rc; b++) {
+      const Ctrl &c = h_ctrl[b];
+      outer += (unsigned)c.st_outer;
+      if (c.err) rc = fail(c.err & ERR_TIMEOUT ? DMF_ERR_TIMEOUT
+                           : c.err & ERR_NO_CONV ? DMF_ERR_NO_CONVERGENCE
+                           : c.err & (ERR_UNKNOWN_ARC | ERR_DUP_ARC | ERR_BAD_UPDATE) ? DMF_ERR_INVALID_ARG
+                                                                                      : DMF_ERR_CUDA,
+                           "step %d: device error flags 0x%x (update %d)", b, c.err, c.err_info);
+    }
+    for (size_t i = 0; i < (size_t)steps * cnt; i++) flows[i] = h_fl[i];
+    sv->round_base += (unsigned)steps * kRoundStride;
+    sv->relabel_base += (unsigned)steps * kRelabelStride;
+    if (!rc) {
+      sv->flows.assign(h_fl + (size_t)(steps - 1) * cnt, h_fl + (size_t)steps * cnt);
+      int64_t tot = 0;
+      for (int64_t f : sv->flows) tot += f;
+      sv->st.flow = tot;
+      sv->st.last_ms = t_ms;
+      sv->st.outer_iters = outer;
+      sv->side_valid = false;
+    } else {
+      sv->solved = false;
+    }
     cudaFreeHost(h_ctrl);
     cudaFreeHost(h_fl);
-    return cuda_fail(e, use_graph ? "graph-captured batch loop" : "batch loop");
-  }
-  float t_ms = 0;
-  cudaEventElapsedTime(&t_ms, sv->ev0, sv->ev1);
-  if (ms) *ms = t_ms;
-  int rc = DMF_OK;
-  unsigned outer = 0;
-  for (int b = 0; b < steps && !rc; b++) {
-    const Ctrl &c = h_ctrl[b];
-    outer += (unsigned)c.st_outer;
-    if (c.err) rc = fail(c.err & ERR_TIMEOUT ? DMF_ERR_TIMEOUT
-                         : c.err & ERR_NO_CONV ? DMF_ERR_NO_CONVERGENCE
-                         : c.err & (ERR_UNKNOWN_ARC | ERR_DUP_ARC | ERR_BAD_UPDATE) ? DMF_ERR_INVALID_ARG
-                                                                                    : DMF_ERR_CUDA,
-                         "step %d: device error flags 0x%x (update %d)", b, c.err, c.err_info);
-  }
-  for (size_t i = 0; i < (size_t)steps * cnt; i++) flows[i] = h_fl[i];
-  sv->round_base += (unsigned)steps * kRoundStride;
-  sv->relabel_base += (unsigned)steps * kRelabelStride;
-  if (!rc) {
-    sv->flows.assign(h_fl + (size_t)(steps - 1) * cnt, h_fl + (size_t)steps * cnt);
-    int64_t tot = 0;
-    for (int64_t f : sv->flows) tot += f;
-    sv->st.flow = tot;
-    sv->st.last_ms = t_ms;
-    sv->st.outer_iters = outer;
-    sv->side_valid = false;
-  } else {
-    sv->solved = false;
-  }
-  cudaFreeHost(h_ctrl);
-  cudaFreeHost(h_fl);
-  return rc ? rc : ok();
+    return rc ? rc : ok();
+  });
 }
 
 int dmf_autotune(dmf_solver *sv, int32_t repeats, dmf_opts *chosen) {
-  if (!sv) return fail(DMF_ERR_INVALID_ARG, "null solver");
-  if (repeats < 1) repeats = 1;
-  dmf_opts best = sv->opts;
-  auto cost = [&](const dmf_opts &o, double *out) -> int {
-    sv->opts = o;
-    int st = configure(sv);
-    if (st) return st;
-    double b = 1e30;
-    for (int r = 0; r < repeats; r++) {
-      st = host_updates(sv, MODE_RECOMPUTE, 0, nullptr, nullptr, nullptr, nullptr);
+  return guarded([&]() -> int {
+    if (!sv) return fail(DMF_ERR_INVALID_ARG, "null solver");
+    if (repeats < 1) repeats = 1;
+    dmf_opts best = sv->opts;
+    auto cost = [&](const dmf_opts &o, double *out) -> int {
+      sv->opts = o;
+      int st = configure(sv);
       if (st) return st;
-      b = std::min(b, sv->st.last_ms);
-    }
-    *out = b;
-    return DMF_OK;
-  };
-  double best_ms = 0;
-  int st = cost(best, &best_ms);
-  if (st) return st;
-  auto try_dim = [&](int32_t dmf_opts::*field, std::initializer_list<int32_t> vals) -> int {
-    for (int32_t v : vals) {
-      dmf_opts o = best;
-      if (o.*field == v) continue;
-      o.*field = v;
-      double ms = 0;
-      int s2 = cost(o, &ms);
-      if (s2) return s2;
-      if (ms < best_ms) {
-        best_ms = ms;
-        best = o;
+      double b = 1e30;
+      for (int r = 0; r < repeats; r++) {
+        st = host_updates(sv, MODE_RECOMPUTE, 0, nullptr, nullptr, nullptr, nullptr);
+        if (st) return st;
+        b = std::min(b, sv->st.last_ms);
       }
-    }
-    return DMF_OK;
-  };
-  if ((st = try_dim(&dmf_opts::tile, {4, 8, 16, 32})) || (st = try_dim(&dmf_opts::small_deg, {-1, 4, 8, 16, 32})) ||
-      (st = try_dim(&dmf_opts::relabel_interval, {2, 3, 6, 12})) || (st = try_dim(&dmf_opts::kernel_cycles, {1, 2, 4})))
-    return st;
-  sv->opts = best;
-  if ((st = configure(sv))) return st;
-  st = host_updates(sv, MODE_RECOMPUTE, 0, nullptr, nullptr, nullptr, nullptr);  // leave a solved state
-  if (st) return st;
-  if (chosen) *chosen = best;
-  return ok();
+      *out = b;
+      return DMF_OK;
+    };
+    double best_ms = 0;
+    int st = cost(best, &best_ms);
+    if (st) return st;
+    auto try_dim = [&](int32_t dmf_opts::*field, std::initializer_list<int32_t> vals) -> int {
+      for (int32_t v : vals) {
+        dmf_opts o = best;
+        if (o.*field == v) continue;
+        o.*field = v;
+        double ms = 0;
+        int s2 = cost(o, &ms);
+        if (s2) return s2;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = o;
+        }
+      }
+      return DMF_OK;
+    };
+    if ((st = try_dim(&dmf_opts::tile, {4, 8, 16, 32})) || (st = try_dim(&dmf_opts::small_deg, {-1, 4, 8, 16, 32})) ||
+        (st = try_dim(&dmf_opts::relabel_interval, {2, 3, 6, 12})) || (st = try_dim(&dmf_opts::kernel_cycles, {1, 2, 4})))
+      return st;
+    sv->opts = best;
+    if ((st = configure(sv))) return st;
+    st = host_updates(sv, MODE_RECOMPUTE, 0, nullptr, nullptr, nullptr, nullptr);  // leave a solved state
+    if (st) return st;
+    if (chosen) *chosen = best;
+    return ok();
+  });
 }
 
 int dmf_solver_set_opts(dmf_solver *sv, const dmf_opts *opts) {
-  if (!sv || !opts) return fail(DMF_ERR_INVALID_ARG, "null argument");
-  if (opts->variant < 0 || opts->variant > 2) return fail(DMF_ERR_INVALID_ARG, "unknown variant");
-  bool variant_changed = opts->variant != sv->opts.variant;
-  sv->opts = *opts;
-  if (cudaSetDevice(sv->dev) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaSetDevice");
-  int st = configure(sv);
-  if (st) return st;
-  if (variant_changed) sv->side_valid = false;
-  return ok();
+  return guarded([&]() -> int {
+    if (!sv || !opts) return fail(DMF_ERR_INVALID_ARG, "null argument");
+    if (opts->variant < 0 || opts->variant > 2) return fail(DMF_ERR_INVALID_ARG, "unknown variant");
+    bool variant_changed = opts->variant != sv->opts.variant;
+    sv->opts = *opts;
+    if (cudaSetDevice(sv->dev) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaSetDevice");
+    int st = configure(sv);
+    if (st) return st;
+    if (variant_changed) sv->side_valid = false;
+    return ok();
+  });
 }
 
 int dmf_static_maxflow(dmf_solver *sv, int64_t *flow) {
-  if (!sv) return fail(DMF_ERR_INVALID_ARG, "null solver");
-  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
-  return run_mode(sv, MODE_STATIC, 0, nullptr, nullptr, nullptr, flow, false);
+  return guarded([&]() -> int {
+    if (!sv) return fail(DMF_ERR_INVALID_ARG, "null solver");
+    CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+    return run_mode(sv, MODE_STATIC, 0, nullptr, nullptr, nullptr, flow, false);
+  });
 }
 
 int dmf_apply_updates(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
                       int64_t *flow) {
-  return host_updates(sv, MODE_DYNAMIC, k, src, dst, w, flow);
+  return guarded([&]() -> int {
+    return host_updates(sv, MODE_DYNAMIC, k, src, dst, w, flow);
+  });
 }
 
 int dmf_apply_updates_device(dmf_solver *sv, int32_t k, const int32_t *d_src, const int32_t *d_dst,
                              const int32_t *d_w, int64_t *flow) {
-  return device_updates(sv, MODE_DYNAMIC, k, d_src, d_dst, d_w, flow);
+  return guarded([&]() -> int {
+    return device_updates(sv, MODE_DYNAMIC, k, d_src, d_dst, d_w, flow);
+  });
 }
 
 int dmf_recompute(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
                   int64_t *flow) {
-  return host_updates(sv, MODE_RECOMPUTE, k, src, dst, w, flow);
+  return guarded([&]() -> int {
+    return host_updates(sv, MODE_RECOMPUTE, k, src, dst, w, flow);
+  });
 }
 
 int dmf_recompute_device(dmf_solver *sv, int32_t k, const int32_t *d_src, const int32_t *d_dst,
                          const int32_t *d_w, int64_t *flow) {
-  return device_updates(sv, MODE_RECOMPUTE, k, d_src, d_dst, d_w, flow);
+  return guarded([&]() -> int {
+    return device_updates(sv, MODE_RECOMPUTE, k, d_src, d_dst, d_w, flow);
+  });
 }
 
 int dmf_flow_value(const dmf_solver *sv, int64_t *flow) {
@@ -2809,21 +2847,23 @@ int dmf_flow_value(const dmf_solver *sv, int64_t *flow) {
 }
 
 int dmf_get_cut(dmf_solver *sv, uint8_t *sink_side) {
-  if (!sv || !sink_side) return fail(DMF_ERR_INVALID_ARG, "null argument");
-  if (!sv->solved) return fail(DMF_ERR_NOT_SOLVED, "no solve yet");
-  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
-  if (!sv->side_valid) {
-    int64_t f = sv->st.flow;
-    dmf_stats keep = sv->st;
-    int st = run_mode(sv, MODE_CUT, 0, nullptr, nullptr, nullptr, nullptr, false);
-    if (st) return st;
-    sv->st = keep;
-    sv->st.flow = f;
-    sv->side_valid = true;
-  }
-  CK(cudaMemcpyAsync(sink_side, sv->side, (size_t)sv->n, cudaMemcpyDeviceToHost, sv->stream), "D2H cut");
-  CK(cudaStreamSynchronize(sv->stream), "cut");
-  return ok();
+  return guarded([&]() -> int {
+    if (!sv || !sink_side) return fail(DMF_ERR_INVALID_ARG, "null argument");
+    if (!sv->solved) return fail(DMF_ERR_NOT_SOLVED, "no solve yet");
+    CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+    if (!sv->side_valid) {
+      int64_t f = sv->st.flow;
+      dmf_stats keep = sv->st;
+      int st = run_mode(sv, MODE_CUT, 0, nullptr, nullptr, nullptr, nullptr, false);
+      if (st) return st;
+      sv->st = keep;
+      sv->st.flow = f;
+      sv->side_valid = true;
+    }
+    CK(cudaMemcpyAsync(sink_side, sv->side, (size_t)sv->n, cudaMemcpyDeviceToHost, sv->stream), "D2H cut");
+    CK(cudaStreamSynchronize(sv->stream), "cut");
+    return ok();
+  });
 }
 
 int dmf_get_state(dmf_solver *sv, int32_t *cap, int32_t *res, int64_t *excess, int32_t *height) {
@@ -2840,48 +2880,54 @@ int dmf_get_state(dmf_solver *sv, int32_t *cap, int32_t *res, int64_t *excess, i
 
 int dmf_trace_items(dmf_solver *sv, int32_t cap, int64_t *items, int64_t *hubs, int64_t *slow_ns,
                     int64_t *slow_v) {
-  if (!sv || cap < 0 || (cap > 0 && (!items || !hubs))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
-  const int len = std::min(std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap), cap);
-  if (len <= 0) return ok();
-  std::vector<unsigned long long> h(4 * (size_t)len);
-  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
-  CK(cudaMemcpyAsync(h.data(), sv->trace, 32 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
-  CK(cudaStreamSynchronize(sv->stream), "trace");
-  for (int i = 0; i < len; i++) {
-    items[i] = (int64_t)((h[4 * i] >> 8) & 0xffffffffull);
-    hubs[i] = (int64_t)(h[4 * i] >> 40);
-    if (slow_ns) slow_ns[i] = (int64_t)(h[4 * i + 2] >> 32);
-    if (slow_v) slow_v[i] = (int64_t)(h[4 * i + 2] & 0xffffffffull);
-  }
-  return ok();
+  return guarded([&]() -> int {
+    if (!sv || cap < 0 || (cap > 0 && (!items || !hubs))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+    const int len = std::min(std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap), cap);
+    if (len <= 0) return ok();
+    std::vector<unsigned long long> h(4 * (size_t)len);
+    CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+    CK(cudaMemcpyAsync(h.data(), sv->trace, 32 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
+    CK(cudaStreamSynchronize(sv->stream), "trace");
+    for (int i = 0; i < len; i++) {
+      items[i] = (int64_t)((h[4 * i] >> 8) & 0xffffffffull);
+      hubs[i] = (int64_t)(h[4 * i] >> 40);
+      if (slow_ns) slow_ns[i] = (int64_t)(h[4 * i + 2] >> 32);
+      if (slow_v) slow_v[i] = (int64_t)(h[4 * i + 2] & 0xffffffffull);
+    }
+    return ok();
+  });
 }
 
 int dmf_trace_blocks(dmf_solver *sv, int32_t cap, int64_t *block_ns) {
-  if (!sv || cap < 0 || (cap > 0 && !block_ns)) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
-  const int len = std::min(std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap), cap);
-  if (len <= 0) return ok();
-  std::vector<unsigned long long> h(4 * (size_t)len);
-  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
-  CK(cudaMemcpyAsync(h.data(), sv->trace, 32 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
-  CK(cudaStreamSynchronize(sv->stream), "trace");
-  for (int i = 0; i < len; i++) block_ns[i] = (int64_t)h[4 * i + 3];
-  return ok();
+  return guarded([&]() -> int {
+    if (!sv || cap < 0 || (cap > 0 && !block_ns)) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+    const int len = std::min(std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap), cap);
+    if (len <= 0) return ok();
+    std::vector<unsigned long long> h(4 * (size_t)len);
+    CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+    CK(cudaMemcpyAsync(h.data(), sv->trace, 32 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
+    CK(cudaStreamSynchronize(sv->stream), "trace");
+    for (int i = 0; i < len; i++) block_ns[i] = (int64_t)h[4 * i + 3];
+    return ok();
+  });
 }
 
 int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us, int32_t *count) {
-  if (!sv || !count || cap < 0 || (cap > 0 && (!kinds || !t_us))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
-  const int len = std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap);
-  *count = len;
-  if (len == 0 || cap == 0) return ok();
-  std::vector<unsigned long long> h(4 * (size_t)len);
-  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
-  CK(cudaMemcpyAsync(h.data(), sv->trace, 32 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
-  CK(cudaStreamSynchronize(sv->stream), "trace");
-  for (int i = 0; i < std::min(len, cap); i++) {
-    kinds[i] = (int32_t)(h[4 * i] & 0xff);
-    t_us[i] = (double)(h[4 * i + 1] - h[1]) * 1e-3;
-  }
-  return ok();
+  return guarded([&]() -> int {
+    if (!sv || !count || cap < 0 || (cap > 0 && (!kinds || !t_us))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+    const int len = std::min(sv->h_ctrl ? sv->h_ctrl->trace_len : 0, sv->trace_cap);
+    *count = len;
+    if (len == 0 || cap == 0) return ok();
+    std::vector<unsigned long long> h(4 * (size_t)len);
+    CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+    CK(cudaMemcpyAsync(h.data(), sv->trace, 32 * (size_t)len, cudaMemcpyDeviceToHost, sv->stream), "D2H trace");
+    CK(cudaStreamSynchronize(sv->stream), "trace");
+    for (int i = 0; i < std::min(len, cap); i++) {
+      kinds[i] = (int32_t)(h[4 * i] & 0xff);
+      t_us[i] = (double)(h[4 * i + 1] - h[1]) * 1e-3;
+    }
+    return ok();
+  });
 }
 
 int dmf_stats_get(const dmf_solver *sv, dmf_stats *st) {
@@ -2892,24 +2938,30 @@ int dmf_stats_get(const dmf_solver *sv, dmf_stats *st) {
 
 int dmf_solver_features(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w,
                         float *feat) {
-  int st = check_updates_args(sv, k, src, dst, w);
-  if (st) return st;
-  if (!feat) return fail(DMF_ERR_INVALID_ARG, "null feature output");
-  if ((st = stage_batch(sv, k, src, dst, w))) return st;
-  int action = 0;
-  if ((st = batch_features(sv, nullptr, k, feat, &action))) return st;
-  return ok();
+  return guarded([&]() -> int {
+    int st = check_updates_args(sv, k, src, dst, w);
+    if (st) return st;
+    if (!feat) return fail(DMF_ERR_INVALID_ARG, "null feature output");
+    if ((st = stage_batch(sv, k, src, dst, w))) return st;
+    int action = 0;
+    if ((st = batch_features(sv, nullptr, k, feat, &action))) return st;
+    return ok();
+  });
 }
 
 int dmf_apply_updates_action(dmf_solver *sv, int32_t action, int32_t k, const int32_t *src, const int32_t *dst,
                              const int32_t *w, int64_t *flow) {
-  if (action < 0) return fail(DMF_ERR_INVALID_ARG, "unknown action %d", action);
-  return scheduled_updates(sv, nullptr, action, k, src, dst, w, flow, nullptr);
+  return guarded([&]() -> int {
+    if (action < 0) return fail(DMF_ERR_INVALID_ARG, "unknown action %d", action);
+    return scheduled_updates(sv, nullptr, action, k, src, dst, w, flow, nullptr);
+  });
 }
 
 int dmf_apply_updates_scheduled(dmf_solver *sv, dmf_sched *sched, int32_t k, const int32_t *src, const int32_t *dst,
                                 const int32_t *w, int64_t *flow, int32_t *action) {
-  return scheduled_updates(sv, sched, -1, k, src, dst, w, flow, action);
+  return guarded([&]() -> int {
+    return scheduled_updates(sv, sched, -1, k, src, dst, w, flow, action);
+  });
 }
 
 int dmf_sched_records(dmf_solver *sv, int32_t cap, float *feat, int32_t *action, float *ms, int64_t *flow,
@@ -2929,35 +2981,37 @@ int dmf_sched_records(dmf_solver *sv, int32_t cap, float *feat, int32_t *action,
 }
 
 int dmf_solver_copy_state(dmf_solver *dst, const dmf_solver *src) {
-  if (!dst || !src) return fail(DMF_ERR_INVALID_ARG, "null solver");
-  if (dst == src) return ok();
-  if (dst->n != src->n || dst->m != src->m || dst->hub_deg != src->hub_deg || dst->nchunk != src->nchunk ||
-      dst->ninst != 1 || src->ninst != 1 || dst->dev != src->dev)
-    return fail(DMF_ERR_INVALID_ARG, "copy_state needs two single-instance solvers of the same graph, hub "
-                                     "threshold and device");
-  CK(cudaSetDevice(dst->dev), "cudaSetDevice");
-  CK(cudaStreamSynchronize(src->stream), "source solver");
-  const size_t N = (size_t)src->n + 1, M = (size_t)src->m, NC = (size_t)std::max(src->nchunk, 1);
-  cudaStream_t S = dst->stream;
-  CK(cudaMemcpyAsync(dst->cap, src->cap, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D cap");
-  CK(cudaMemcpyAsync(dst->res, src->res, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D res");
-  CK(cudaMemcpyAsync(dst->astamp, src->astamp, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D astamp");
-  CK(cudaMemcpyAsync(dst->excess, src->excess, 8 * N, cudaMemcpyDeviceToDevice, S), "D2D excess");
-  CK(cudaMemcpyAsync(dst->height, src->height, 4 * N, cudaMemcpyDeviceToDevice, S), "D2D height");
-  CK(cudaMemcpyAsync(dst->stamp, src->stamp, 4 * N, cudaMemcpyDeviceToDevice, S), "D2D stamp");
-  CK(cudaMemcpyAsync(dst->dead, src->dead, N, cudaMemcpyDeviceToDevice, S), "D2D dead");
-  CK(cudaMemcpyAsync(dst->side, src->side, N, cudaMemcpyDeviceToDevice, S), "D2D side");
-  CK(cudaMemcpyAsync(dst->chunk_mark, src->chunk_mark, 8 * NC, cudaMemcpyDeviceToDevice, S), "D2D marks");
-  CK(cudaMemcpyAsync(dst->chunk_tmin, src->chunk_tmin, 4 * NC, cudaMemcpyDeviceToDevice, S), "D2D marks");
-  CK(cudaStreamSynchronize(S), "copy state");
-  dst->round_base = src->round_base;
-  dst->relabel_base = src->relabel_base;
-  dst->epoch = src->epoch;
-  dst->solved = src->solved;
-  dst->side_valid = src->side_valid;
-  dst->st = src->st;
-  dst->flows = src->flows;
-  return ok();
+  return guarded([&]() -> int {
+    if (!dst || !src) return fail(DMF_ERR_INVALID_ARG, "null solver");
+    if (dst == src) return ok();
+    if (dst->n != src->n || dst->m != src->m || dst->hub_deg != src->hub_deg || dst->nchunk != src->nchunk ||
+        dst->ninst != 1 || src->ninst != 1 || dst->dev != src->dev)
+      return fail(DMF_ERR_INVALID_ARG, "copy_state needs two single-instance solvers of the same graph, hub "
+                                       "threshold and device");
+    CK(cudaSetDevice(dst->dev), "cudaSetDevice");
+    CK(cudaStreamSynchronize(src->stream), "source solver");
+    const size_t N = (size_t)src->n + 1, M = (size_t)src->m, NC = (size_t)std::max(src->nchunk, 1);
+    cudaStream_t S = dst->stream;
+    CK(cudaMemcpyAsync(dst->cap, src->cap, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D cap");
+    CK(cudaMemcpyAsync(dst->res, src->res, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D res");
+    CK(cudaMemcpyAsync(dst->astamp, src->astamp, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D astamp");
+    CK(cudaMemcpyAsync(dst->excess, src->excess, 8 * N, cudaMemcpyDeviceToDevice, S), "D2D excess");
+    CK(cudaMemcpyAsync(dst->height, src->height, 4 * N, cudaMemcpyDeviceToDevice, S), "D2D height");
+    CK(cudaMemcpyAsync(dst->stamp, src->stamp, 4 * N, cudaMemcpyDeviceToDevice, S), "D2D stamp");
+    CK(cudaMemcpyAsync(dst->dead, src->dead, N, cudaMemcpyDeviceToDevice, S), "D2D dead");
+    CK(cudaMemcpyAsync(dst->side, src->side, N, cudaMemcpyDeviceToDevice, S), "D2D side");
+    CK(cudaMemcpyAsync(dst->chunk_mark, src->chunk_mark, 8 * NC, cudaMemcpyDeviceToDevice, S), "D2D marks");
+    CK(cudaMemcpyAsync(dst->chunk_tmin, src->chunk_tmin, 4 * NC, cudaMemcpyDeviceToDevice, S), "D2D marks");
+    CK(cudaStreamSynchronize(S), "copy state");
+    dst->round_base = src->round_base;
+    dst->relabel_base = src->relabel_base;
+    dst->epoch = src->epoch;
+    dst->solved = src->solved;
+    dst->side_valid = src->side_valid;
+    dst->st = src->st;
+    dst->flows = src->flows;
+    return ok();
+  });
 }
 
 int dmf_solver_destroy(dmf_solver *sv) {

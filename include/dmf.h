@@ -11,7 +11,9 @@
  * Conventions
  *   - Every function returns a dmf_status (0 = DMF_OK).  dmf_last_error()
  *     returns a message for the last failure on the calling thread.  The
- *     library never calls exit().
+ *     library never calls exit(), and no C++ exception leaves an entry point:
+ *     a failed host allocation returns DMF_ERR_OOM, any other host runtime
+ *     failure DMF_ERR_HOST.
  *   - Host arrays passed in are copied during the call; the caller keeps them.
  *     Arrays returned through out-pointers are owned by the library and freed
  *     with dmf_free() / dmf_graph_free().
@@ -45,7 +47,8 @@ typedef enum {
   DMF_ERR_CUDA = 7,          /* CUDA runtime error, or no usable device */
   DMF_ERR_TIMEOUT = 8,       /* a bounded device-side wait gave up */
   DMF_ERR_OVERFLOW = 9,      /* cap(e) + cap(partner) exceeds int32 */
-  DMF_ERR_NOT_SOLVED = 10    /* update or query before the first solve */
+  DMF_ERR_NOT_SOLVED = 10,   /* update or query before the first solve */
+  DMF_ERR_HOST = 11          /* host runtime failure other than allocation (thread, lock) */
 } dmf_status;
 
 /* Algorithm variants: the three reference entry points. */
@@ -270,7 +273,11 @@ int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs,
  * request on the host (vertex ranges, existing arcs, no repeats) and copies it;
  * wait() blocks until it is served and returns the graph's exact max-flow after
  * it and its latency from the start of its submit() call (validation
- * included).  No counterpart in the reference. */
+ * included); a ticket has one waiter, and a second wait() on it returns
+ * DMF_ERR_INVALID_ARG.  destroy() serves every request already submitted,
+ * lets threads blocked in wait() return their results, then frees the server;
+ * no call on the server may start once destroy() has.  No counterpart in the
+ * reference. */
 typedef struct dmf_server dmf_server;
 int dmf_server_create(int32_t count, const dmf_graph *const *graphs,
                       const int32_t *s, const int32_t *t, int64_t hbm_budget,

@@ -44,6 +44,19 @@ def test_status_strings_and_defaults(dmf):
     assert o.variant == 0 and o.device == -1
 
 
+def test_host_failure_is_a_status(dmf):
+    """No C++ exception leaves the C ABI: an R-MAT request for 2^62 arcs cannot
+    be allocated and returns DMF_ERR_OOM instead of ending the process."""
+    with pytest.raises(dmf.DmfError) as ei:
+        dmf.gen_rmat(scale=10, narcs=1 << 62)
+    assert ei.value.status == 5 and "allocation" in str(ei.value)
+    L = ctypes.CDLL(dmf.lib_path)
+    L.dmf_status_string.restype = ctypes.c_char_p
+    assert L.dmf_status_string(11) == b"host runtime error"
+    g, _, _ = dmf.gen_rmat(scale=6, seed=1)  # the library still works
+    assert g.num_edges() > 0
+
+
 def test_solver_requires_gpu_and_validates_args(dmf, golden_dir):
     g = dmf.Graph.load(os.path.join(golden_dir, "johnson8-2-4.bin"))
     with pytest.raises(dmf.DmfError) as ei:

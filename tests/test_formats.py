@@ -94,6 +94,19 @@ def test_load_rejects_bad_files(dmf, golden_dir, tmp_path):
     assert dmf.Graph.load(str(tmp_path / "ok.bin")).num_edges() == 2
 
 
+def test_validation_names_the_lowest_bad_arc(dmf, golden_dir):
+    """With several defects of one kind, the message names the lowest arc,
+    whatever the number of host threads that checked them."""
+    g = dmf.Graph.load(os.path.join(golden_dir, "johnson8-2-4.bin"))
+    off, adj, w, par = g.arrays()
+    bad = w.copy()
+    bad[[7, 40, g.num_edges() - 1]] = -1
+    for _ in range(5):
+        with pytest.raises(dmf.DmfError) as ei:
+            dmf.Graph.from_csr(off, adj, bad, par)
+        assert ei.value.status == 2 and "arc 7: negative capacity" in str(ei.value)
+
+
 def test_updates_roundtrip_and_errors(dmf, tmp_path, oracle):
     p = str(tmp_path / "u.bin")
     dmf.save_updates(p, [1, 2, 3], [4, 5, 6], [7, 8, 9])

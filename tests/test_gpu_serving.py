@@ -1,6 +1,7 @@
 """Serving loop: graphs admitted by HBM budget, continuous batching of
 update-batch requests; each result is the same alone and in the mix."""
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -82,6 +83,60 @@ def test_bad_requests_are_rejected_alone(dmf):
         with dmf.Solver(g, s, t) as sv:
             sv.static_maxflow()
             assert f == sv.apply_updates(*batches[0])
+
+
+def test_one_waiter_per_ticket(dmf):
+    """Two threads waiting on one ticket: one gets the flow, the other an
+    invalid-argument error (the ticket is taken, or already gone)."""
+    inst = _graphs(dmf)
+    g, s, t, batches = inst[0]
+    with dmf.Solver(g, s, t) as sv:
+        sv.static_maxflow()
+        want = sv.apply_updates(*batches[0])
+    with dmf.Server([g], [s], [t], 1 << 30) as srv:
+        for _ in range(3):
+            tk = srv.submit(0, *batches[0])
+            out = []
+
+            def waiter():
+                try:
+                    out.append(("flow", srv.wait(tk)[0]))
+                except dmf.DmfError as e:
+                    out.append(("error", e.status))
+
+            th = [threading.Thread(target=waiter) for _ in range(2)]
+            for x in th:
+                x.start()
+            for x in th:
+                x.join()
+            # updates set capacities, so the same batch again gives the same flow
+            assert sorted(out) == [("error", 1), ("flow", want)]
+
+
+def test_destroy_serves_pending_and_blocked_waiters(dmf):
+    """close() serves every submitted request; a thread blocked in wait() gets
+    its exact result, and tickets nobody waits for are freed."""
+    inst = _graphs(dmf)
+    alone = []
+    for g, s, t, batches in inst:
+        with dmf.Solver(g, s, t) as sv:
+            sv.static_maxflow()
+            alone.append([sv.apply_updates(*b) for b in batches])
+    srv = dmf.Server([x[0] for x in inst], [x[1] for x in inst], [x[2] for x in inst], 1 << 34)
+    tickets = [[srv.submit(i, *b) for b in x[3]] for i, x in enumerate(inst)]
+    got, entered = [], threading.Event()
+
+    def waiter():
+        entered.set()
+        got.append(srv.wait(tickets[0][-1])[0])
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    entered.wait()
+    time.sleep(0.3)  # the waiter is inside wait() before close() starts
+    srv.close()
+    th.join(timeout=60)
+    assert not th.is_alive() and got == [alone[0][-1]]
 
 
 def test_large_requests_validated_in_parallel(dmf, oracle):
