@@ -158,7 +158,17 @@ def _check(st: int) -> None:
 
 
 def _i32(a) -> np.ndarray:
-    return np.ascontiguousarray(np.asarray(a), dtype=np.int32)
+    """Contiguous int32 view or copy; values that int32 cannot hold exactly
+    (out of range, fractional) raise instead of wrapping to another id."""
+    a = np.asarray(a)
+    if a.dtype != np.int32 and a.size:
+        if a.dtype.kind not in "biuf":
+            raise TypeError(f"expected integers, got {a.dtype}")
+        if a.dtype.kind == "f" and not np.array_equal(a, np.trunc(a)):
+            raise ValueError("expected integers, got fractional values")
+        if a.min() < -2**31 or a.max() > 2**31 - 1:
+            raise OverflowError("value outside the int32 range")
+    return np.ascontiguousarray(a, dtype=np.int32)
 
 
 def _take_i32(ptr: C.c_void_p, count: int) -> np.ndarray:

@@ -94,6 +94,22 @@ def test_load_rejects_bad_files(dmf, golden_dir, tmp_path):
     assert dmf.Graph.load(str(tmp_path / "ok.bin")).num_edges() == 2
 
 
+def test_int32_arguments_never_wrap(dmf, golden_dir):
+    """Host arrays are converted to int32 only when every value fits exactly."""
+    g = dmf.Graph.load(os.path.join(golden_dir, "johnson8-2-4.bin"))
+    with pytest.raises(OverflowError):
+        g.set_caps(np.array([2**32 + 1], np.int64), [2], [5])
+    with pytest.raises(ValueError):
+        g.set_caps([1.5], [2], [5])
+    with pytest.raises(TypeError):
+        g.set_caps(["a"], [2], [5])
+    off, adj, _, _ = g.arrays()
+    u = int(np.argmax(np.diff(off) > 0))  # a vertex with an out-arc
+    v = int(adj[off[u]])
+    g.set_caps(np.array([u], np.int64), np.array([v], np.uint8), np.array([7.0]))  # exact: accepted
+    assert g.arrays()[2][g.find_arc(u, v)] == 7
+
+
 def test_validation_names_the_lowest_bad_arc(dmf, golden_dir):
     """With several defects of one kind, the message names the lowest arc,
     whatever the number of host threads that checked them."""
