@@ -16,6 +16,10 @@
 #include <unordered_set>
 
 #ifdef _OPENMP
+#include <parallel/algorithm>
+#endif
+
+#ifdef _OPENMP
 #include <omp.h>
 #endif
 
@@ -110,34 +114,107 @@ int64_t find_arc(const dmf_graph &g, int32_t src, int32_t dst) {
 // events 2j = arc (u_j, v_j) with weight w_j, 2j+1 = arc (v_j, u_j) weight 0,
 // bucketed by tail in event order; per tail, duplicates merged (weights summed)
 // and unique arcs kept in order of their first event.
+//
+// The bucketing runs in parallel and keeps event order: the tails are cut into
+// ranges of about equal event counts; each thread scatters a contiguous slice
+// of the edges into the ranges (so every range receives its events in edge
+// order), then each range is bucketed by tail on its own.
 int build_from_edges(int64_t k, const int32_t *u, const int32_t *v, const int32_t *w,
                      dmf_graph **out) {
   if (k < 0 || (k > 0 && (!u || !v || !w))) return fail(DMF_ERR_INVALID_ARG, "bad edge arrays");
   int32_t maxnode = -1;
-  int64_t kept = 0;
+  int64_t kept = 0, first_bad = INT64_MAX;
+#pragma omp parallel for schedule(static) reduction(max : maxnode) reduction(+ : kept) reduction(min : first_bad)
   for (int64_t i = 0; i < k; i++) {
-    if (u[i] < 0 || v[i] < 0) return fail(DMF_ERR_INVALID_ARG, "negative vertex id at edge %lld", (long long)i);
+    if (u[i] < 0 || v[i] < 0) {
+      first_bad = std::min(first_bad, i);
+      continue;
+    }
     if (u[i] == v[i]) continue;
     maxnode = std::max(maxnode, std::max(u[i], v[i]));
     kept++;
   }
+  if (first_bad != INT64_MAX)
+    return fail(DMF_ERR_INVALID_ARG, "negative vertex id at edge %lld", (long long)first_bad);
   const int32_t n = maxnode + 1;
   std::vector<int64_t> bofs((size_t)n + 1, 0);
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < k; i++) {
     if (u[i] == v[i]) continue;
+#pragma omp atomic
     bofs[u[i] + 1]++;
+#pragma omp atomic
     bofs[v[i] + 1]++;
   }
   for (int32_t x = 0; x < n; x++) bofs[x + 1] += bofs[x];
   struct Ev { int32_t head; int32_t wt; };
   std::vector<Ev> ev((size_t)(2 * kept));
   {
-    std::vector<int64_t> fill(bofs.begin(), bofs.end() - 1);
-    for (int64_t i = 0; i < k; i++) {
-      if (u[i] == v[i]) continue;
-      ev[fill[u[i]]++] = {v[i], w[i]};
-      ev[fill[v[i]]++] = {u[i], 0};
+    int nth = 1;
+#ifdef _OPENMP
+    nth = omp_get_max_threads();
+#endif
+    // tail ranges [vb[r], vb[r+1]) of about equal event counts
+    const int R = std::max(1, std::min(std::min(8 * nth, 65535), n > 0 ? n : 1));
+    std::vector<int32_t> vb((size_t)R + 1, n);
+    vb[0] = 0;
+    for (int r = 1; r < R; r++) {
+      const int64_t want = (int64_t)((__int128)2 * kept * r / R);
+      vb[r] = (int32_t)(std::lower_bound(bofs.begin(), bofs.begin() + n, want) - bofs.begin());
+      vb[r] = std::max(vb[r], vb[r - 1]);
     }
+    std::vector<uint16_t> rng_of(n > 0 ? (size_t)n : 1);
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < R; r++)
+      for (int32_t x = vb[r]; x < vb[r + 1]; x++) rng_of[x] = (uint16_t)r;
+    // edge slices: slice t counts its events per range, then scatters them
+    const int T = nth;
+    std::vector<int64_t> cnt((size_t)T * R, 0);
+    struct TEv { int32_t tail; int32_t head; int32_t wt; };
+    std::vector<TEv> staged((size_t)(2 * kept));
+#pragma omp parallel num_threads(T)
+    {
+      int t = 0;
+#ifdef _OPENMP
+      t = omp_get_thread_num();
+      const int tt = omp_get_num_threads();
+#else
+      const int tt = 1;
+#endif
+      const int64_t b = (int64_t)((__int128)k * t / tt), e = (int64_t)((__int128)k * (t + 1) / tt);
+      int64_t *c = cnt.data() + (size_t)t * R;
+      for (int64_t i = b; i < e; i++) {
+        if (u[i] == v[i]) continue;
+        c[rng_of[u[i]]]++;
+        c[rng_of[v[i]]]++;
+      }
+#pragma omp barrier
+#pragma omp single
+      {
+        for (int r = 0; r < R; r++) {
+          int64_t pos = bofs[vb[r]];
+          for (int q = 0; q < tt; q++) {
+            const int64_t x = cnt[(size_t)q * R + r];
+            cnt[(size_t)q * R + r] = pos;
+            pos += x;
+          }
+        }
+      }
+      for (int64_t i = b; i < e; i++) {
+        if (u[i] == v[i]) continue;
+        staged[c[rng_of[u[i]]]++] = {u[i], v[i], w[i]};
+        staged[c[rng_of[v[i]]]++] = {v[i], u[i], 0};
+      }
+    }
+    std::vector<uint16_t>().swap(rng_of);
+    // per range: events into their tails' buckets, in order
+    std::vector<int64_t> fill(bofs.begin(), bofs.end() - 1);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int r = 0; r < R; r++)
+      for (int64_t j = bofs[vb[r]]; j < bofs[vb[r + 1]]; j++) {
+        const TEv &s = staged[j];
+        ev[fill[s.tail]++] = {s.head, s.wt};
+      }
   }
   // per tail: unique heads in first-event order, weights summed
   std::vector<int32_t> ucount(n, 0);
@@ -202,10 +279,25 @@ int build_from_edges(int64_t k, const int32_t *u, const int32_t *v, const int32_
     }
   std::vector<Ev>().swap(ev);
   build_sorted_index(*g);
+  // Partners: every arc x->h has exactly one reverse arc h->x (heads are unique
+  // per tail after the merge).  The pair is resolved once, from its smaller
+  // endpoint, by a binary search over h's heads laid out in sorted order.
+  {
+    std::vector<int32_t> sh((size_t)g->m);
 #pragma omp parallel for schedule(dynamic, 1024)
-  for (int32_t x = 0; x < n; x++)
-    for (int32_t e = g->off[x]; e < g->off[x + 1]; e++)
-      g->par[e] = (int32_t)find_arc(*g, g->adj[e], x);
+    for (int32_t x = 0; x < n; x++)
+      for (int32_t i = g->off[x]; i < g->off[x + 1]; i++) sh[i] = g->adj[g->sidx[i]];
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int32_t x = 0; x < n; x++)
+      for (int32_t e = g->off[x]; e < g->off[x + 1]; e++) {
+        const int32_t h = g->adj[e];
+        if (h < x) continue;
+        const int32_t *b = sh.data() + g->off[h], *end = sh.data() + g->off[h + 1];
+        const int32_t p = g->sidx[g->off[h] + (int32_t)(std::lower_bound(b, end, x) - b)];
+        g->par[e] = p;
+        g->par[p] = e;
+      }
+  }
   *out = g.release();
   return ok();
 }
@@ -499,42 +591,71 @@ int dmf_gen_rmat(int32_t scale, int64_t narcs, double a, double b, double c, uin
     std::vector<uint64_t> keys((size_t)narcs);
   #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < narcs; i++) keys[i] = sample((uint64_t)i, 1);
+#ifdef _OPENMP
+    __gnu_parallel::sort(keys.begin(), keys.end());
+#else
     std::sort(keys.begin(), keys.end());
+#endif
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
     keys.erase(std::remove_if(keys.begin(), keys.end(), [](uint64_t k) { return (k >> 32) == (k & 0xffffffffu); }),
                keys.end());
     const int32_t nv = 1 << scale;
     // source / sink on the sampled arcs
     std::vector<int64_t> outd(nv, 0), ind(nv, 0);
-    for (uint64_t k : keys) { outd[k >> 32]++; ind[k & 0xffffffffu]++; }
+    const int64_t nk = (int64_t)keys.size();
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nk; i++) {
+      const uint64_t k = keys[i];
+#pragma omp atomic
+      outd[k >> 32]++;
+#pragma omp atomic
+      ind[k & 0xffffffffu]++;
+    }
     int32_t src = 0, snk = -1;
     for (int32_t x = 0; x < nv; x++) if (outd[x] > outd[src]) src = x;
     for (int32_t x = 0; x < nv; x++)
       if (x != src && (snk < 0 || ind[x] > ind[snk])) snk = x;
-    // reserved insert slots: further R-MAT samples that are not arcs in either direction
+    // reserved insert slots: further R-MAT samples, in sample order, that are
+    // not arcs in either direction and not taken already in either direction.
+    // The candidates of a window are drawn and checked against the arcs in
+    // parallel; only the survivors go through the sequential taken-set check.
     std::vector<uint64_t> extra;
     if (reserve > 0) {
       std::unordered_set<uint64_t> taken;
-      uint64_t idx = 0;
-      while ((int64_t)extra.size() < reserve && idx < (uint64_t)reserve * 64 + 1024) {
-        uint64_t k = sample(idx++, 2);
-        uint64_t rk = (k << 32) | (k >> 32);
-        if ((k >> 32) == (k & 0xffffffffu)) continue;
-        if (std::binary_search(keys.begin(), keys.end(), k) || std::binary_search(keys.begin(), keys.end(), rk))
-          continue;
-        if (taken.count(k) || taken.count(rk)) continue;
-        taken.insert(k);
-        extra.push_back(k);
+      const uint64_t limit = (uint64_t)reserve * 64 + 1024;
+      const uint64_t win = std::max<uint64_t>(1 << 16, 2 * (uint64_t)reserve);
+      std::vector<uint64_t> cand;
+      std::vector<uint8_t> okc;
+      for (uint64_t base = 0; base < limit && (int64_t)extra.size() < reserve; base += win) {
+        const uint64_t cnt = std::min(win, limit - base);
+        cand.resize(cnt);
+        okc.resize(cnt);
+#pragma omp parallel for schedule(static)
+        for (int64_t j = 0; j < (int64_t)cnt; j++) {
+          const uint64_t k = sample(base + (uint64_t)j, 2);
+          const uint64_t rk = (k << 32) | (k >> 32);
+          cand[j] = k;
+          okc[j] = (k >> 32) != (k & 0xffffffffu) && !std::binary_search(keys.begin(), keys.end(), k) &&
+                   !std::binary_search(keys.begin(), keys.end(), rk);
+        }
+        for (uint64_t j = 0; j < cnt && (int64_t)extra.size() < reserve; j++) {
+          if (!okc[j]) continue;
+          const uint64_t k = cand[j], rk = (k << 32) | (k >> 32);
+          if (taken.count(k) || taken.count(rk)) continue;
+          taken.insert(k);
+          extra.push_back(k);
+        }
       }
     }
     const size_t na = keys.size(), ne = extra.size();
     std::vector<int32_t> U(na + ne), V(na + ne), W(na + ne);
-    Rng caps(seed ^ 0xC0FFEEull);
-    for (size_t i = 0; i < na; i++) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)na; i++) {
       U[i] = (int32_t)(keys[i] >> 32);
       V[i] = (int32_t)(keys[i] & 0xffffffffu);
-      W[i] = (int32_t)caps.uniform(cap_lo, cap_hi);
     }
+    Rng caps(seed ^ 0xC0FFEEull);
+    for (size_t i = 0; i < na; i++) W[i] = (int32_t)caps.uniform(cap_lo, cap_hi);
     for (size_t i = 0; i < ne; i++) {
       U[na + i] = (int32_t)(extra[i] >> 32);
       V[na + i] = (int32_t)(extra[i] & 0xffffffffu);
@@ -568,18 +689,82 @@ int dmf_gen_batches(const dmf_graph *g, int32_t nb, double frac, double p_inc, d
     const int32_t m = g->m;
     std::vector<int32_t> cap(g->w);
     std::vector<int32_t> tail(m);
+#pragma omp parallel for schedule(dynamic, 1024)
     for (int32_t x = 0; x < g->n; x++)
       for (int32_t e = g->off[x]; e < g->off[x + 1]; e++) tail[e] = x;
+    // Candidate lists, in arc order: `pos` = arcs with capacity > 0, `absent` =
+    // arcs whose pair has capacity 0 both ways.  Built once, then updated after
+    // each batch from the arcs it touched (and their partners), which is all
+    // that can change membership.
+    auto is_pos = [&](int32_t e) { return cap[e] > 0; };
+    auto is_absent = [&](int32_t e) { return cap[e] == 0 && cap[g->par[e]] == 0; };
+    std::vector<int32_t> pos, absent;
+    {
+      int nth = 1;
+#ifdef _OPENMP
+      nth = omp_get_max_threads();
+#endif
+      std::vector<int64_t> cp((size_t)nth + 1, 0), ca((size_t)nth + 1, 0);
+#pragma omp parallel num_threads(nth)
+      {
+        int t = 0, tt = 1;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+        tt = omp_get_num_threads();
+#endif
+        const int32_t b = (int32_t)((int64_t)m * t / tt), e = (int32_t)((int64_t)m * (t + 1) / tt);
+        int64_t np = 0, na = 0;
+        for (int32_t x = b; x < e; x++) {
+          np += is_pos(x);
+          na += is_absent(x);
+        }
+        cp[t + 1] = np;
+        ca[t + 1] = na;
+#pragma omp barrier
+#pragma omp single
+        {
+          for (int q = 0; q < tt; q++) {
+            cp[q + 1] += cp[q];
+            ca[q + 1] += ca[q];
+          }
+          pos.resize(cp[tt]);
+          absent.resize(ca[tt]);
+        }
+        int64_t ip = cp[t], ia = ca[t];
+        for (int32_t x = b; x < e; x++) {
+          if (is_pos(x)) pos[ip++] = x;
+          if (is_absent(x)) absent[ia++] = x;
+        }
+      }
+    }
+    // list := (list without `drop`) merged with `add` (all sorted, drop within list)
+    auto refresh = [](std::vector<int32_t> &list, const std::vector<int32_t> &drop, const std::vector<int32_t> &add) {
+      if (drop.empty() && add.empty()) return;
+      std::vector<int32_t> out;
+      out.reserve(list.size() - drop.size() + add.size());
+      size_t i = 0, d = 0, a = 0;
+      while (i < list.size()) {
+        const int32_t x = list[i];
+        if (d < drop.size() && drop[d] == x) {
+          d++;
+          i++;
+          continue;
+        }
+        if (a < add.size() && add[a] < x) {
+          out.push_back(add[a++]);
+          continue;
+        }
+        out.push_back(x);
+        i++;
+      }
+      while (a < add.size()) out.push_back(add[a++]);
+      list.swap(out);
+    };
     Rng rng(seed);
     std::vector<int64_t> O(1, 0);
     std::vector<int32_t> S, D, Wn;
     std::vector<uint8_t> chosen(m, 0);
     for (int32_t bi = 0; bi < nb; bi++) {
-      std::vector<int32_t> pos, absent;
-      for (int32_t e = 0; e < m; e++) {
-        if (cap[e] > 0) pos.push_back(e);
-        else if (cap[g->par[e]] == 0) absent.push_back(e);
-      }
       int64_t K = std::max<int64_t>(1, (int64_t)std::llround(frac * (double)pos.size()));
       int64_t n_ins = absent.empty() ? 0 : std::min<int64_t>((int64_t)absent.size(), std::llround(p_ins * K));
       int64_t n_inc = std::llround(p_inc * K), n_dec = std::llround(p_dec * K);
@@ -599,6 +784,17 @@ int dmf_gen_batches(const dmf_graph *g, int32_t nb, double frac, double p_inc, d
         chosen[e] = 1;
         ins.push_back(e);
       }
+      // arcs whose membership may change: the touched ones and their partners
+      std::vector<int32_t> touched;
+      touched.reserve(2 * (picks.size() + ins.size()));
+      for (int32_t e : picks) { touched.push_back(e); touched.push_back(g->par[e]); }
+      for (int32_t e : ins) { touched.push_back(e); touched.push_back(g->par[e]); }
+      std::sort(touched.begin(), touched.end());
+      touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+      std::vector<uint8_t> was((size_t)touched.size());
+#pragma omp parallel for schedule(static)
+      for (int64_t j = 0; j < (int64_t)touched.size(); j++)
+        was[j] = (uint8_t)(is_pos(touched[j]) | (is_absent(touched[j]) << 1));
       int64_t i = 0;
       for (int32_t e : picks) {
         int32_t nc;
@@ -618,6 +814,22 @@ int dmf_gen_batches(const dmf_graph *g, int32_t nb, double frac, double p_inc, d
         chosen[e] = 0;
       }
       O.push_back((int64_t)S.size());
+      std::vector<int32_t> pdrop, padd, adrop, aadd;
+#pragma omp parallel for schedule(static)
+      for (int64_t j = 0; j < (int64_t)touched.size(); j++)
+        was[j] |= (uint8_t)((is_pos(touched[j]) << 2) | (is_absent(touched[j]) << 3));
+      for (size_t j = 0; j < touched.size(); j++) {
+        const int32_t e = touched[j];
+        const bool p0 = was[j] & 1, a0 = (was[j] >> 1) & 1, p1 = (was[j] >> 2) & 1, a1 = (was[j] >> 3) & 1;
+        if (p0 && !p1) pdrop.push_back(e);
+        if (!p0 && p1) padd.push_back(e);
+        if (a0 && !a1) adrop.push_back(e);
+        if (!a0 && a1) aadd.push_back(e);
+      }
+      if (bi + 1 < nb) {
+        refresh(pos, pdrop, padd);
+        refresh(absent, adrop, aadd);
+      }
     }
     size_t kk = S.size();
     auto *o_ofs = (int64_t *)std::malloc(sizeof(int64_t) * O.size());

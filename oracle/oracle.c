@@ -945,7 +945,9 @@ int orc_ref_run_successive(int variant, int32_t n, int32_t m, const int32_t *off
                            int32_t nb, const int64_t *bofs, const int32_t *us,
                            const int32_t *ud, const int32_t *uw, int nthreads,
                            int64_t max_iters, int64_t *static_flow,
-                           int64_t *flows, double *batch_ms) {
+                           int64_t *flows, double *batch_ms, double budget_ms,
+                           int32_t *done) {
+  if (done) *done = 0;
   if (!args_ok(n, s, t)) return -2;
   st_t S;
   st_alloc(&S, n, m, off, adj, w0, par, s, t, kc, nthreads, max_iters);
@@ -956,7 +958,9 @@ int orc_ref_run_successive(int variant, int32_t n, int32_t m, const int32_t *off
       if (S.excess[v] < 0 && v != s) f += S.excess[v];
     *static_flow = f;
   }
+  double spent = 0;
   for (int32_t b = 0; b < nb && !rc; b++) {
+    if (budget_ms > 0 && spent > budget_ms) break;
     double t0 = now_ms();
     int64_t lo = bofs[b], hi = bofs[b + 1];
     if (k_onadd(&S, (int32_t)(hi - lo), us + lo, ud + lo, uw + lo)) { rc = -3; break; }
@@ -968,7 +972,10 @@ int orc_ref_run_successive(int variant, int32_t n, int32_t m, const int32_t *off
     for (int32_t v = 0; v < n; v++)
       if (S.excess[v] < 0 && v != s) f += S.excess[v];
     if (flows) flows[b] = f;
-    if (batch_ms) batch_ms[b] = now_ms() - t0;
+    const double dt = now_ms() - t0;
+    if (batch_ms) batch_ms[b] = dt;
+    spent += dt;
+    if (done) *done = b + 1;
   }
   st_free(&S);
   return rc;

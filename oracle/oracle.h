@@ -92,7 +92,9 @@ int orc_ref_run(int variant, int32_t n, int32_t m, const int32_t *off,
 /* Successive batches on one resident state (the state is never rebuilt between
  * batches): static solve, then for each batch b the reference's OnAdd +
  * Incremental + kernel_39 readout.  flows[b] receives the flow after batch b.
- * Batch b holds updates [bofs[b], bofs[b+1]). */
+ * Batch b holds updates [bofs[b], bofs[b+1]).  With budget_ms > 0 the run
+ * stops after the batch that brings the batches' total time over the budget;
+ * *done (if not NULL) receives the number of batches run. */
 int orc_ref_run_successive(int variant, int32_t n, int32_t m, const int32_t *off,
                            const int32_t *adj, const int32_t *w0,
                            const int32_t *par, int32_t s, int32_t t,
@@ -100,7 +102,8 @@ int orc_ref_run_successive(int variant, int32_t n, int32_t m, const int32_t *off
                            const int64_t *bofs, const int32_t *usrc,
                            const int32_t *udst, const int32_t *uw, int nthreads,
                            int64_t max_iters, int64_t *static_flow,
-                           int64_t *flows, double *batch_ms);
+                           int64_t *flows, double *batch_ms, double budget_ms,
+                           int32_t *done);
 
 #ifdef __cplusplus
 }

@@ -41,7 +41,8 @@ def lib():
         L.orc_ref_run_successive.restype = C.c_int
         L.orc_ref_run_successive.argtypes = [C.c_int, C.c_int32, C.c_int32, I32P, I32P, I32P, I32P, C.c_int32,
                                              C.c_int32, C.c_int32, C.c_int32, I64P, I32P, I32P, I32P, C.c_int,
-                                             C.c_int64, C.POINTER(C.c_int64), I64P, F64P]
+                                             C.c_int64, C.POINTER(C.c_int64), I64P, F64P, C.c_double,
+                                             C.POINTER(C.c_int32)]
         L.orc_build_csr.restype = C.c_int
         L.orc_build_csr.argtypes = [C.c_int64, I32P, I32P, I32P, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                     C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
@@ -128,8 +129,10 @@ def ref_run(variant, n, off, adj, w, par, s, t, kernel_cycles, src, dst, wt, nth
 
 
 def ref_run_successive(variant, n, off, adj, w, par, s, t, kernel_cycles, batches, nthreads=1,
-                       max_iters=10_000_000):
-    """Successive batches on one resident state -> (static_flow, flows[], batch_ms[])."""
+                       max_iters=10_000_000, budget_ms=0.0):
+    """Successive batches on one resident state -> (static_flow, flows[], batch_ms[]);
+    with budget_ms > 0 the run stops once the batches' total time passes it (the
+    lists then cover the batches that ran)."""
     off, adj, w, par = _i32(off), _i32(adj), _i32(w), _i32(par)
     bofs = np.zeros(len(batches) + 1, dtype=np.int64)
     for i, (bs, _, _) in enumerate(batches):
@@ -139,9 +142,10 @@ def ref_run_successive(variant, n, off, adj, w, par, s, t, kernel_cycles, batche
     flows = np.zeros(max(len(batches), 1), dtype=np.int64)
     ms = np.zeros(max(len(batches), 1), dtype=np.float64)
     sf = C.c_int64()
+    done = C.c_int32()
     rc = lib().orc_ref_run_successive(VARIANTS.get(variant, variant), n, len(adj), off, adj, w, par, s, t,
                                       kernel_cycles, len(batches), bofs, src, dst, wt, nthreads, max_iters,
-                                      C.byref(sf), flows, ms)
+                                      C.byref(sf), flows, ms, float(budget_ms), C.byref(done))
     if rc:
         raise RuntimeError(f"oracle ref_run_successive failed rc={rc}")
-    return sf.value, flows[:len(batches)], ms[:len(batches)]
+    return sf.value, flows[:done.value], ms[:done.value]
