@@ -49,10 +49,11 @@ class Stats(C.Structure):
                 ("push_rounds", C.c_int64), ("pushes", C.c_int64), ("relabels", C.c_int64),
                 ("arcs_scanned", C.c_int64), ("vertices_visited", C.c_int64), ("dead_vertices", C.c_int64),
                 ("last_ms", C.c_double), ("grid_blocks", C.c_int32), ("block_threads", C.c_int32),
-                ("tile", C.c_int32), ("pad", C.c_int32)]
+                ("tile", C.c_int32), ("pad", C.c_int32), ("bfs_arcs", C.c_int64), ("dead_deficits", C.c_int64),
+                ("dead_kept", C.c_int32), ("pad2", C.c_int32)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("pad")}
 
 
 def _sig(name, res, *args):
@@ -129,7 +130,7 @@ _sig("dmf_sched_records", C.c_int, VP, C.c_int32, F32P, I32P, F32P, I64P, C.POIN
 _sig("dmf_solver_copy_state", C.c_int, VP, VP)
 
 # schedules the picker chooses from (DMF_ACTION_*); every one gives the same flow
-ACTIONS = ("plain", "short_interval", "warp_per_vertex", "recompute")
+ACTIONS = ("plain", "short_interval", "revive_dead", "recompute")
 N_FEATURES, N_HIDDEN, N_ACTIONS, N_WEIGHTS, N_BIASES = 12, 64, 4, 5120, 132
 
 _sig("dmf_static_maxflow_noalloc", C.c_int, C.c_int32, C.c_int32, VP, VP, VP, VP, C.c_int32, C.c_int32, VP,
@@ -299,13 +300,15 @@ class Solver:
     """Device-resident residual state of one graph on one GPU (dmf_solver)."""
 
     def __init__(self, g: Graph, source: int, sink: int, variant="data", kernel_cycles=0, relabel_interval=0,
-                 tile=0, max_iters=0, device=-1, stream=None, trace=False, probe=False, fixed_interval=False):
+                 tile=0, max_iters=0, device=-1, stream=None, trace=False, probe=False, fixed_interval=False,
+                 revive_dead=False, test_barrier_timeout=False):
         o = Opts()
         _L.dmf_opts_default(C.byref(o))
         o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
         o.kernel_cycles, o.relabel_interval, o.tile, o.max_iters, o.device = (
             kernel_cycles, relabel_interval, tile, max_iters, device)
-        o.flags = (1 if trace or probe else 0) | (2 if probe else 0) | (4 if fixed_interval else 0)
+        o.flags = ((1 if trace or probe else 0) | (2 if probe else 0) | (4 if fixed_interval else 0)
+                   | (8 if revive_dead else 0) | (16 if test_barrier_timeout else 0))
         self._h = C.c_void_p()
         self.n, self.m = g.num_nodes(), g.num_edges()
         stream_ptr = None if stream is None else C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
@@ -418,7 +421,8 @@ class Solver:
     TRACE_KINDS = {0: "start", 1: "init_res", 2: "saturate", 3: "lookup", 4: "apply", 5: "repair",
                    6: "cut_saturate", 7: "bfs_init", 8: "bfs_td", 9: "bfs_bu", 10: "bfs_finalize", 11: "push",
                    12: "flow", 13: "push_hub", 14: "push_hub_finish", 15: "pp_init", 16: "pp_bfs",
-                   17: "pp_finalize", 18: "pp_round"}
+                   17: "pp_finalize", 18: "pp_round", 19: "reopen", 20: "dead_seed", 21: "dead_bfs",
+                   22: "dead_push", 23: "dead_check"}
 
     def trace(self):
         """[(phase kind, end time in us since kernel start)] of the last solve (trace=True)."""
@@ -453,12 +457,14 @@ class Solver:
         return {k: getattr(o, k) for k, _ in Opts._fields_}
 
     def set_opts(self, variant=None, kernel_cycles=None, relabel_interval=None, tile=None, max_iters=None,
-                 small_deg=None):
+                 small_deg=None, flags=None):
+        """Replaces the solver's options (dmf_solver_set_opts); a field left None keeps the
+        value a previous set_opts call gave it, else the library default."""
         o = Opts()
         _L.dmf_opts_default(C.byref(o))
         cur = getattr(self, "_opts", {})
         vals = dict(variant=variant, kernel_cycles=kernel_cycles, relabel_interval=relabel_interval, tile=tile,
-                    max_iters=max_iters, small_deg=small_deg)
+                    max_iters=max_iters, small_deg=small_deg, flags=flags)
         for k_, v_ in vals.items():
             if v_ is None:
                 v_ = cur.get(k_, 0 if k_ != "variant" else 0)

@@ -1,8 +1,11 @@
 """Build of the native parts of dyn_maxflow_b200 (in-tree).
 
-* ``libdmf.so``  -- the C-ABI library: csrc/dmf_solver.cu (sm_100a kernels and
-  the solver) + csrc/dmf_host.cpp (formats, builder, generators), compiled by
-  nvcc for ``-gencode arch=compute_100a,code=sm_100a`` only.
+* ``libdmf.so``  -- the C-ABI library: csrc/dmf_solver.cu (the solver's host
+  side), csrc/dmf_kernel_t*.cu (the sm_100a solve kernel, csrc/dmf_kernel.cuh,
+  one file per tile width), csrc/dmf_sched.cu (schedule picker),
+  csrc/dmf_host.cpp (formats, builder, generators) and csrc/dmf_server.cpp
+  (serving loop), compiled by nvcc for ``-gencode arch=compute_100a,code=sm_100a``
+  only.
 * ``bin/dyn_data_bench``, ``bin/dyn_topo_bench``, ``bin/dyn_pp_bench`` and the
   ``*_large`` forms -- the drop-in command-line entry points (csrc/dmf_cli.cpp),
   linked against libdmf.so.
@@ -52,19 +55,32 @@ def _run(cmd: list[str], verbose: bool = False) -> str:
     return r.stdout + r.stderr
 
 
+LIB_SOURCES = ["dmf_solver.cu", "dmf_kernel_t4.cu", "dmf_kernel_t8.cu", "dmf_kernel_t16.cu", "dmf_kernel_t32.cu",
+               "dmf_sched.cu", "dmf_host.cpp", "dmf_server.cpp"]
+OBJ_DIR = os.path.join(PKG, "_build")
+
+
 def build_lib(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Compiles every source of libdmf.so to an object file (in parallel: the
+    solve kernel's instantiations sit in one file per tile width) and links."""
+    from concurrent.futures import ThreadPoolExecutor
     deps = _sources()
-    if force or ptxas_info or _stale(LIB, deps):
-        cmd = ["nvcc", *NVCC_FLAGS, "-shared", "-I", INCLUDE, "-I", CSRC,
-               os.path.join(CSRC, "dmf_solver.cu"), os.path.join(CSRC, "dmf_host.cpp"),
-               os.path.join(CSRC, "dmf_server.cpp"), os.path.join(CSRC, "dmf_sched.cu"),
-               "-o", LIB + ".tmp", "-lgomp"]
-        if ptxas_info:
+    if not (force or ptxas_info or _stale(LIB, deps)):
+        return LIB
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    jobs = []
+    for src in LIB_SOURCES:
+        obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+        cmd = ["nvcc", *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
+        if ptxas_info and src.endswith(".cu"):
             cmd[1:1] = ["-Xptxas", "-v"]
-        out = _run(cmd, verbose)
-        os.replace(LIB + ".tmp", LIB)
-        if ptxas_info:
-            print(out)
+        jobs.append((cmd, obj))
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        outs = list(ex.map(lambda j: _run(j[0], verbose), jobs))
+    _run(["nvcc", *NVCC_FLAGS, "-shared", *[o for _, o in jobs], "-o", LIB + ".tmp", "-lgomp"], verbose)
+    os.replace(LIB + ".tmp", LIB)
+    if ptxas_info:
+        print("\n".join(outs))
     return LIB
 
 

@@ -27,6 +27,8 @@ enum : int {
 // Barrier wait limit: 4 s of %globaltimer.  Any single phase of a solve is
 // orders of magnitude shorter; hitting it means a block never arrived.
 constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;
+// The limit under the failure-injection test hook (DMF_FLAG_TEST_BARRIER_TIMEOUT).
+constexpr unsigned long long kTestBarrierTimeoutNs = 20000000ull;
 
 // Per-phase counters, triple-buffered: phase k appends into slot k%3, reads
 // slot (k-1)%3, and block 0 clears slot (k+1)%3.
@@ -36,6 +38,7 @@ struct Slot {
   long long arcs;    // sum of degrees of appended vertices
   int cnt;           // generic counter (BFS: active vertices labelled; topo push: active seen)
   int pad;
+  long long exsum;   // BFS inside the dead set: excess of the active vertices labelled
 };
 
 // Control block of one solver (device memory, cleared before every launch).
@@ -60,6 +63,16 @@ struct Ctrl {
   int pad1;
   unsigned long long probe[2];  // longest work item of a phase, (ns << 32) | vertex
   unsigned long long blk[2];    // longest block work of a phase (ns), barrier exit to arrival
+  // kept dead set (dynamic batches): vertices of the dead set whose excess a batch
+  // lowered (candidates for deficits), the deficits found among them, and those
+  // left after the local repair inside the dead set
+  int dcand;
+  int dseeds;
+  long long dneed;
+  int dleft;
+  int dkept;                    // 1: the dead set was kept for the global relabels
+  unsigned long long st_barcs;  // adjacency entries read by global-relabel BFS levels
+  unsigned long long st_dseeds; // deficits inside the kept dead set (first local pass)
 };
 
 // ---- memory helpers ---------------------------------------------------------
@@ -87,15 +100,15 @@ __device__ __forceinline__ long long atomic_add_ll(long long *p, long long v) {
 // where they were: nothing has to be reset between barriers).  A waiter polls
 // until the top bit differs from the value its own arrival saw; a block that
 // is already in the next barrier cannot flip it back, because that flip needs
-// every block, the waiter included.  Polls check the error word and a 4 s
-// %globaltimer limit every 64 iterations.
+// every block, the waiter included.  Polls check the error word and the
+// %globaltimer limit (`limit_ns`, normally kBarrierTimeoutNs) every 64 iterations.
 //
 // After the wait, warp 0 copies the whole control block into `snap` (shared
 // memory): the phase that follows reads the counters the previous phase
 // produced from there, so a phase costs G control-block reads instead of one
 // per warp on a single L2 line.  Returns false (uniformly per block) when an
 // error is set.
-__device__ __forceinline__ bool grid_barrier(Ctrl *c, Ctrl *snap) {
+__device__ __forceinline__ bool grid_barrier(Ctrl *c, Ctrl *snap, unsigned long long limit_ns) {
   __shared__ int s_err;
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -112,7 +125,7 @@ __device__ __forceinline__ bool grid_barrier(Ctrl *c, Ctrl *snap) {
           const unsigned long long now = globaltimer();
           if (!t0) {
             t0 = now;
-          } else if (now - t0 > kBarrierTimeoutNs) {
+          } else if (now - t0 > limit_ns) {
             atomicOr(&c->err, ERR_TIMEOUT);
             break;
           }

@@ -1,1663 +1,26 @@
-// dmf_solver.cu -- device half of libdmf.so: the persistent push-relabel
-// solver for sm_100a and the solver entry points of the C ABI.
-//
-// One cooperative launch runs a whole solve: the update prologue (arc lookup,
-// capacity apply, over-capacity repair, source saturation), then rounds of
-//   global relabel: direction-optimising reverse BFS from t and the deficit
-//                   vertices over residual arcs, which also builds the active
-//                   worklist and proves unreachable vertices dead;
-//   push rounds:    discharge of every active vertex by a warp tile (or a whole
-//                   block for hubs), multi-arc pushes per adjacency scan, with
-//                   warp-aggregated worklist appends;
-// until a global relabel finds no active vertex, then the flow readout
-// excess(t) + sum of deficits (recalculate_max_flow_kernel_39,
-// code/dyn_data.h:208-215).  Phases are separated by a bounded grid barrier, so
-// no host round trip happens inside a solve (the reference syncs and copies a
-// flag per BFS level, code/dyn_data_bench.cu:39-47).
+// dmf_solver.cu -- host side of the solver in libdmf.so: device state, launch
+// of the persistent sm_100a kernel (dmf_kernel.cuh), the batch feature kernel
+// of the schedule picker, and the solver entry points of the C ABI.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <climits>
 #include <cstdlib>
 #include <cstring>
-#include <mutex>
 
-#include "dmf_device.cuh"
+#include "dmf_kernel.cuh"
 #include "dmf_internal.h"
 #include "dmf_sched_internal.h"
 
 using namespace dmfd;
+using namespace dmfk;
 
 namespace {
-
-constexpr int kBlock = 512;
-constexpr int kChunk = 256;  // arcs per hub chunk: one warp item, 8 arcs per lane
-constexpr int kPPIters = 1;  // push-pull phase-1 relabel rounds before the general solve
-
-enum Mode : int { MODE_STATIC = 0, MODE_DYNAMIC = 1, MODE_RECOMPUTE = 2, MODE_CUT = 3 };
-
-// Phase kinds of the optional timeline (dmf_trace_get); values are part of the ABI.
-enum TraceKind : int {
-  TR_START = 0, TR_INIT_RES = 1, TR_SATURATE = 2, TR_LOOKUP = 3, TR_APPLY = 4, TR_REPAIR = 5,
-  TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
-  TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14, TR_PP_INIT = 15, TR_PP_BFS = 16, TR_PP_FINALIZE = 17,
-  TR_PP_ROUND = 18
-};
-
-// Largest capacity an update may set: keeps cap(e) + cap(partner) < 2^31 when
-// both arcs of a pair change in one batch.
-constexpr int kMaxUpdateCap = (1 << 30) - 1;
-
-struct Params {
-  int n, m, s, t;
-  const int *__restrict__ off;
-  const int *__restrict__ adj;
-  const int *__restrict__ par;
-  const int *__restrict__ sidx;
-  int *cap, *res, *height, *stamp, *astamp, *uarc;
-  long long *excess;
-  unsigned char *dead, *side;
-  int *fq[2], *wq[2], *aq;     // non-hub vertex queues
-  int2 *fh[2], *wh[2], *ah;    // hub chunk queues
-  const int2 *hch;             // every hub's chunks (bottom-up BFS, topology-driven rounds)
-  int nhch;
-  // per hub (indexed by hub_base), totals of the current push round:
-  long long *hc_alloc;  // admissible residual claimed by the hub's chunks
-  long long *hc_moved;  // excess pushed by them
-  int *hc_min;          // minimum non-admissible head height
-  int *hc_done;         // chunks that contributed to hc_min
-  // Exhausted hub chunks: a chunk with no admissible arc at hub height h stays
-  // so until the hub's height changes or the next global relabel (heights only
-  // rise in between, and a reverse residual only opens from a higher head).
-  // mark = (relabel epoch << 32) | h, indexed by hub_base[v] + chunk.
-  const int *hub_base;
-  unsigned long long *chunk_mark;
-  int *chunk_tmin;
-  unsigned relabel_base;
-  const int *usrc, *udst, *uw;
-  int k;
-  // Several independent instances in one residual graph (batched mode): role
-  // bit 0 = a source, bit 1 = a sink, inst = instance of each vertex, flows per
-  // instance.  Single instance: role == nullptr, s and t above.
-  const unsigned char *role;
-  const int *inst;
-  long long *inst_flow;
-  const int *srcs;  // every source vertex (just s for one instance)
-  // prefix sums of the sources' degrees (nsrc + 1 entries), or null: the
-  // saturation then walks the sources one after the other
-  const int *src_off;
-  int nsrc;
-  // instances a batched call works on (nullptr: all); the others are left as they
-  // are: not seeded, not saturated, not read out
-  const unsigned char *inst_active;
-  Ctrl *ctrl;
-  int mode, variant, cycles, interval, max_iters, hub_deg, small_deg, need_cut;
-  int bu_alpha;  // bottom-up when frontier arcs * bu_alpha > unexplored arcs (0: never)
-  int adaptive;  // push rounds per relabel at least the depth of the last relabel BFS
-  unsigned round_base;
-  int epoch;
-  unsigned long long *trace;  // optional phase timeline: 4 words per entry
-  int trace_cap;
-  int probe;                  // time work items (DMF_FLAG_PROBE)
-};
-
-struct LStats {
-  unsigned long long pushes = 0, relabels = 0, arcs = 0, visits = 0;
-  unsigned long long probe = 0;  // (longest single item in ns << 32) | vertex, this phase
-  unsigned long long t_phase = 0;  // thread 0: when this block left the last barrier
-  long long to_sink = 0;  // flow pushed into the sink this push phase, not yet added
-};
-
-// Optional probe (DMF_FLAG_PROBE): times every work item and keeps the longest.
-struct ItemTimer {
-  unsigned long long t0;
-  bool on;
-  __device__ __forceinline__ ItemTimer(const Params &p) : t0(0), on(p.probe) {
-    if (on) t0 = globaltimer();
-  }
-  __device__ __forceinline__ void done(LStats &ls, int v) {
-    if (!on) return;
-    unsigned long long dt = globaltimer() - t0;
-    if (dt > 0xffffffffull) dt = 0xffffffffull;
-    const unsigned long long key = (dt << 32) | (unsigned)v;
-    if (key > ls.probe) ls.probe = key;
-  }
-};
-
-__device__ __forceinline__ int deg_of(const Params &p, int v) { return __ldg(p.off + v + 1) - __ldg(p.off + v); }
-
-__device__ __forceinline__ bool is_src(const Params &p, int v) { return p.role ? (p.role[v] & 1) : v == p.s; }
-__device__ __forceinline__ bool is_snk(const Params &p, int v) { return p.role ? (p.role[v] & 2) : v == p.t; }
-__device__ __forceinline__ bool is_term(const Params &p, int v) { return p.role ? p.role[v] != 0 : (v == p.s || v == p.t); }
-
-__device__ __forceinline__ void set_err(Ctrl *c, int bit, int info) {
-  if (atomicOr(&c->err, bit) == 0) c->err_info = info;
-}
-
-// ---- prologue phases ----------------------------------------------------------
-
-// staticMaxFlow_kernel_1 (code/dyn_data.h:25-35): residual = capacity, excess 0.
-__device__ __forceinline__ void ph_init_res(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  for (int e = gt; e < p.m; e += nt) p.res[e] = __ldcg(p.cap + e);
-  for (int v = gt; v < p.n; v += nt) p.excess[v] = 0;
-}
-
-// staticMaxFlow_kernel_7 (code/dyn_data.h:39-56) made parallel: every residual
-// arc out of every source is saturated.  The arcs of all sources form one index
-// space (src_off) walked grid-stride, so one source of very high degree (R-MAT's
-// s) is spread over the whole grid and many small sources cost one pass.
-__device__ __forceinline__ long long saturate_arc(const Params &p, int a) {
-  const int r = __ldcg(p.res + a);
-  if (r <= 0) return 0;
-  p.res[a] = 0;
-  atomicAdd(p.res + __ldg(p.par + a), r);
-  atomic_add_ll(p.excess + __ldg(p.adj + a), r);
-  return r;
-}
-
-__device__ __forceinline__ void ph_saturate(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!p.src_off) {
-    for (int i = 0; i < p.nsrc; i++) {
-      if (p.inst_active && !p.inst_active[i]) continue;  // source i belongs to instance i
-      const int s = __ldg(p.srcs + i);
-      const int beg = __ldg(p.off + s), end = __ldg(p.off + s + 1);
-      long long sum = 0;
-      for (int a = beg + gt; a < end; a += nt) sum += saturate_arc(p, a);
-      agg_add_ll(p.excess + s, -sum);
-    }
-    return;
-  }
-  const int total = __ldg(p.src_off + p.nsrc);
-  int cur = -1;  // source whose arcs this thread is summing
-  long long sum = 0;
-  for (int j = gt; j < total; j += nt) {
-    int lo = 0, hi = p.nsrc;  // last i with src_off[i] <= j
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (__ldg(p.src_off + mid) <= j) lo = mid;
-      else hi = mid;
-    }
-    if (p.inst_active && !p.inst_active[lo]) continue;
-    if (lo != cur) {
-      if (sum) atomic_add_ll(p.excess + __ldg(p.srcs + cur), -sum);
-      cur = lo;
-      sum = 0;
-    }
-    const int s = __ldg(p.srcs + lo);
-    sum += saturate_arc(p, __ldg(p.off + s) + (j - __ldg(p.src_off + lo)));
-  }
-  // threads of a warp that ended on the same source add once
-  cg::coalesced_group g = cg::coalesced_threads();
-  cg::coalesced_group same = cg::labeled_partition(g, cur);
-  sum = cg::reduce(same, sum, cg::plus<long long>());
-  if (same.thread_rank() == 0 && cur >= 0 && sum) atomic_add_ll(p.excess + __ldg(p.srcs + cur), -sum);
-}
-
-// Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201) by binary search over the
-// per-vertex head-sorted index; also validates the batch.
-// Arc u->v by binary search over u's head-sorted arc index (the last arc among
-// equal heads, as OnAdd_kernel's linear scan keeps the last match), or -1.
-__device__ __forceinline__ int find_arc_dev(const int *__restrict__ off, const int *__restrict__ adj,
-                                            const int *__restrict__ sidx, int u, int v) {
-  const int first = __ldg(off + u);
-  int lo = first, hi = __ldg(off + u + 1);
-  while (lo < hi) {  // last position with head <= v
-    const int mid = (lo + hi) >> 1;
-    if (__ldg(adj + __ldg(sidx + mid)) <= v) lo = mid + 1;
-    else hi = mid;
-  }
-  if (lo > first) {
-    const int cand = __ldg(sidx + lo - 1);
-    if (__ldg(adj + cand) == v) return cand;
-  }
-  return -1;
-}
-
-__device__ __forceinline__ void ph_lookup(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
-  for (int i = gt; i < p.k; i += nt) {
-    int u = __ldg(p.usrc + i), v = __ldg(p.udst + i), w = __ldg(p.uw + i);
-    p.uarc[i] = -1;
-    if (u < 0 || u >= p.n || v < 0 || v >= p.n || w < 0 || w > kMaxUpdateCap) {
-      set_err(p.ctrl, ERR_BAD_UPDATE, i);
-      continue;
-    }
-    if (u == v) continue;  // ignored, as OnAdd_kernel does (code/dyn_data.h:194)
-    const int e = find_arc_dev(p.off, p.adj, p.sidx, u, v);
-    if (e < 0) {
-      set_err(p.ctrl, ERR_UNKNOWN_ARC, i);
-      continue;
-    }
-    if (atomicExch(p.astamp + e, p.epoch) == p.epoch) {
-      set_err(p.ctrl, ERR_DUP_ARC, i);
-      continue;
-    }
-    if ((long long)w + __ldcg(p.cap + __ldg(p.par + e)) > INT_MAX) {
-      set_err(p.ctrl, ERR_BAD_UPDATE, i);
-      continue;
-    }
-    p.uarc[i] = e;
-  }
-}
-
-// Capacity apply of OnAdd_kernel (code/dyn_data.h:202-205); in recompute mode
-// only the capacity is set (update_kernel, code/dyn_data_bench.cu:300-322).
-__device__ __forceinline__ void ph_apply(const Params &p, bool residual) {
-  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
-  for (int i = gt; i < p.k; i += nt) {
-    int e = __ldcg(p.uarc + i);
-    if (e < 0) continue;
-    int w = __ldg(p.uw + i);
-    int delta = w - __ldcg(p.cap + e);
-    p.cap[e] = w;
-    if (residual && delta) atomicAdd(p.res + e, delta);
-  }
-}
-
-// Over-capacity repair driven by the batch: replaces the O(m) sweeps
-// incremental_kernel_20 / _22 (code/dyn_data.h:157-183).  An arc whose residual
-// went negative carries more flow than its new capacity; the excess is returned
-// to its tail and taken from its head.  At most one arc of a pair can be
-// negative because res(e) + res(partner) = cap(e) + cap(partner) >= 0.
-__device__ __forceinline__ void ph_repair(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
-  for (int i = gt; i < p.k; i += nt) {
-    int e = __ldcg(p.uarc + i);
-    if (e < 0) continue;
-    int r = __ldcg(p.res + e);
-    if (r < 0) {
-      p.res[e] = 0;
-      atomicAdd(p.res + __ldg(p.par + e), r);
-      atomic_add_ll(p.excess + __ldg(p.usrc + i), -(long long)r);
-      atomic_add_ll(p.excess + __ldg(p.adj + e), (long long)r);
-    }
-  }
-}
-
-// Push-pull: an updated arc that now has residual from the source side A into
-// the sink side B of the kept cut is saturated (the cut part of the fused
-// incremental_kernel_20, code/dyn_pp.h:422-432, limited to touched arcs).
-__device__ __forceinline__ void ph_cut_saturate(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
-  for (int i = gt; i < p.k; i += nt) {
-    int e = __ldcg(p.uarc + i);
-    if (e < 0) continue;
-    int u = __ldg(p.usrc + i), v = __ldg(p.adj + e);
-    if (is_term(p, u) || is_term(p, v)) continue;
-    if (p.side[u] == 0 && p.side[v] == 1) {
-      int r = __ldcg(p.res + e);
-      if (r > 0) {
-        p.res[e] = 0;
-        atomicAdd(p.res + __ldg(p.par + e), r);
-        atomic_add_ll(p.excess + u, -(long long)r);
-        atomic_add_ll(p.excess + v, (long long)r);
-      }
-    }
-  }
-}
-
-// ---- degree tiers ------------------------------------------------------------------
-// Items of a vertex list (or all vertices when list == nullptr) in two passes:
-// vertices of degree <= small_deg one per thread over the whole grid, then the
-// larger ones (up to hub_deg; hubs are split into arc chunks and done by warps)
-// one per tile.  `f(group, v)` does the work for one vertex.
-// `pre(v)` is a per-vertex filter evaluated by one lane together with the degree
-// read (a vertex it rejects costs one round of independent loads); it must not
-// depend on writes of the current phase by other vertices' work.
-template <int TILE, class F, class Pre>
-__device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const int *list, int nn, F &&f, Pre &&pre) {
-  const int nt = gridDim.x * blockDim.x;
-  const int gt = list ? spread_thread(rot_threads()) : blockIdx.x * blockDim.x + threadIdx.x;
-  for (int i = gt; i < nn; i += nt) {
-    const int v = list ? __ldcg(list + i) : i;
-    const bool keep = pre(v);
-    if (deg_of(p, v) > p.small_deg || !keep) continue;
-    ThreadGroup th;
-    ItemTimer tm(p);
-    f(th, v);
-    tm.done(ls, v);
-  }
-  TileGroup<TILE> tg;
-  if (!list) {
-    // Sweep over every vertex: a tile checks TILE consecutive vertices per step
-    // (one coalesced degree read, a ballot) and then works on the medium ones
-    // it found, instead of one serial degree read per vertex.
-    const int tiles = nt / TILE;
-    for (int base = (int)((blockIdx.x * blockDim.x + threadIdx.x) / TILE) * TILE; base < nn; base += tiles * TILE) {
-      const int v = base + tg.rank();
-      const int d = v < nn ? deg_of(p, v) : 0;
-      const bool keep = v < nn && pre(v);
-      unsigned mask = tg.g.ballot(keep && d > p.small_deg && d <= p.hub_deg);
-      while (mask) {  // tile-uniform
-        const int vv = base + __ffs(mask) - 1;
-        mask &= mask - 1;
-        ItemTimer tm(p);
-        f(tg, vv);
-        tm.done(ls, vv);
-      }
-    }
-    return;
-  }
-  const int gi = spread_group<TILE>(rot_tiles());
-  for (int i = gi; i < nn; i += nt / TILE) {
-    int v = 0, d = 0;
-    if (tg.rank() == 0) {
-      v = __ldcg(list + i);
-      d = deg_of(p, v);
-    }
-    v = tg.g.shfl(v, 0);
-    d = tg.g.shfl(d, 0);
-    if (d <= p.small_deg || d > p.hub_deg) continue;  // tile-uniform
-    ItemTimer tm(p);
-    f(tg, v);
-    tm.done(ls, v);
-  }
-}
-
-template <int TILE, class F>
-__device__ __forceinline__ void for_tiered(const Params &p, LStats &ls, const int *list, int nn, F &&f) {
-  for_tiered<TILE>(p, ls, list, nn, f, [](int) { return true; });
-}
-
-// A hub (degree > hub_deg) enters a queue as ceil(deg / kChunk) consecutive
-// items (v, c), chunk c covering arcs [off[v] + c*kChunk, +kChunk).  Every item
-// is one warp's work, so a hub's adjacency is spread over many warps and no
-// block-wide synchronisation is needed.
-__device__ __forceinline__ int nchunks(int d) { return (d + kChunk - 1) / kChunk; }
-
-__device__ __forceinline__ void append_hub(const Params &p, int2 *q, int *tail, int v) {
-  const int k = nchunks(deg_of(p, v));
-  const int base = atomicAdd(tail, k);
-  for (int c = 0; c < k; c++) q[base + c] = make_int2(v, c);
-}
-
-__device__ __forceinline__ void chunk_range(const Params &p, int2 it, int &beg, int &end) {
-  const int b0 = __ldg(p.off + it.x), e0 = __ldg(p.off + it.x + 1);
-  beg = b0 + it.y * kChunk;
-  end = min(e0, beg + kChunk);
-}
-
-// ---- global relabel ---------------------------------------------------------------
-
-#define UNV (p.n + 1)
-
-// Seeds (my_init_1, code/dyn_data.h:60-67): t and every deficit vertex other
-// than s get height 0; all other live vertices become unvisited.
-__device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  Ctrl *c = p.ctrl;
-  if (gt == 0) {
-    c->act_q = 0;
-    c->act_hq = 0;
-    c->wtail[0] = c->whtail[0] = c->seen[0] = 0;  // written by push round 0
-  }
-  int pos = 0;
-  long long unexpl = 0, seed_arcs = 0;
-  for (int v = gt; v < p.n; v += nt) {
-    if (p.inst_active && !p.inst_active[__ldg(p.inst + v)]) {
-      if (reset_dead) {
-        p.dead[v] = 1;
-        p.height[v] = p.n;
-      }
-      continue;
-    }
-    if (reset_dead) {
-      if (__ldcg(p.dead + v)) p.dead[v] = 0;
-    } else if (__ldcg(p.dead + v)) {
-      continue;
-    }
-    long long ex = __ldcg(p.excess + v);
-    int d = deg_of(p, v);
-    if (d > p.hub_deg) {  // the hub's round totals start clean
-      const int hid = __ldg(p.hub_base + v);
-      p.hc_min[hid] = INT_MAX;
-      p.hc_alloc[hid] = 0;
-      p.hc_moved[hid] = 0;
-      p.hc_done[hid] = 0;
-    }
-    if (is_snk(p, v) || (!is_src(p, v) && ex < 0)) {
-      p.height[v] = 0;
-      if (d > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
-      else append(p.fq[0], &out->q, v);
-      seed_arcs += d;
-    } else if (is_src(p, v)) {
-      // Sources stay at height V and are never labelled: with a finite label
-      // (the reference's BFS gives s its distance) a run of local relabels can
-      // lift vertices above s while t is still reachable, excess drains back
-      // into s, and the solve ends with an augmenting path open.  Excess that
-      // cannot reach a sink or a deficit is parked on dead vertices instead,
-      // so nothing ever has to return to s.
-      p.height[v] = p.n;
-    } else {
-      p.height[v] = UNV;
-      // a bottom-up level scans the arcs of every unvisited vertex, so the
-      // direction heuristic weighs the frontier against all of them
-      unexpl += d;
-    }
-    if (!is_term(p, v) && ex > 0) pos++;
-  }
-  block_add_int(&c->pos_count, pos);
-  block_add_ll(&c->unexplored, unexpl);
-  block_add_ll(&out->arcs, seed_arcs);
-}
-
-// Reserves `cnt` consecutive slots behind *tail for this thread with one atomic
-// per group of threads that call it together.
-__device__ __forceinline__ int reserve(int *tail, int cnt) {
-  cg::coalesced_group g = cg::coalesced_threads();
-  const int pre = cg::exclusive_scan(g, cnt, cg::plus<int>());
-  int base = 0;
-  if (g.thread_rank() == g.size() - 1) base = atomicAdd(tail, pre + cnt);
-  return g.shfl(base, g.size() - 1) + pre;
-}
-
-struct VisitAcc {
-  long long arcs = 0;
-  int reached = 0;
-};
-
-__device__ __forceinline__ void bfs_visit(const Params &p, Slot *out, int nxt, int w, VisitAcc &acc) {
-  int d = deg_of(p, w);
-  const bool hub = d > p.hub_deg;
-  if (hub) append_hub(p, p.fh[nxt], &out->hq, w);
-  else append(p.fq[nxt], &out->q, w);
-  acc.arcs += d;
-  if (!is_term(p, w) && __ldcg(p.excess + w) > 0) {
-    if (hub) append_hub(p, p.ah, &p.ctrl->act_hq, w);
-    else append(p.aq, &p.ctrl->act_q, w);
-    acc.reached++;
-  }
-}
-
-// Counts go to the phase's own slot: a cross-phase counter would be read by a
-// slow block after a fast block already added to it in the next phase.
-__device__ __forceinline__ void flush_visits(const Params &p, Slot *out, VisitAcc &acc) {
-  block_add_ll(&out->arcs, acc.arcs);
-  block_add_int(&out->cnt, acc.reached);
-}
-
-// Top-down level (staticMaxFlow_kernel_11, code/dyn_data.h:72-87, run over the
-// frontier queue instead of all V): x at level L labels w when arc w->x has
-// residual, i.e. res[par[e]] > 0 for e = x->w.
-
-// Arcs first, first+stride, ... < end of a frontier vertex, in register
-// batches of kBatch so that the gathers of a batch are in flight together:
-// heads, then head labels, then the reverse residuals, then the claims, then
-// the claimed heads' degree and excess.
-constexpr int kBatch = 8;   // arcs per lane per batch (a hub chunk is one batch)
-constexpr int kTdBatch = 4;  // smaller for top-down, which keeps more state per arc
-__device__ __forceinline__ void td_range(const Params &p, Slot *out, int nxt, int first, int end, int stride, int L,
-                                         LStats &ls, VisitAcc &acc) {
-  for (int a0 = first; a0 < end; a0 += kTdBatch * stride) {
-    int w[kTdBatch];
-    bool c[kTdBatch];
-#pragma unroll
-    for (int k = 0; k < kTdBatch; k++) {
-      const int a = a0 + k * stride;
-      w[k] = a < end ? __ldg(p.adj + a) : -1;
-    }
-#pragma unroll
-    for (int k = 0; k < kTdBatch; k++) c[k] = w[k] >= 0 && __ldcg(p.height + w[k]) == UNV;
-#pragma unroll
-    for (int k = 0; k < kTdBatch; k++)
-      if (c[k]) c[k] = __ldcg(p.res + __ldg(p.par + a0 + k * stride)) > 0;
-#pragma unroll
-    for (int k = 0; k < kTdBatch; k++)
-      if (c[k]) c[k] = atomicCAS(p.height + w[k], UNV, L + 1) == UNV;
-    int d[kTdBatch];
-    long long ex[kTdBatch];
-#pragma unroll
-    for (int k = 0; k < kTdBatch; k++)
-      if (c[k]) {
-        d[k] = deg_of(p, w[k]);
-        ex[k] = __ldcg(p.excess + w[k]);
-      }
-    // the batch's claimed heads go to the next frontier and, when active, to
-    // the active list, with one reservation per list for the whole batch (a
-    // large level claims hundreds of thousands of vertices: appends per arc
-    // would serialise on the lists' tail counters)
-    int nq = 0, na = 0;
-    unsigned qmask = 0, amask = 0;
-#pragma unroll
-    for (int k = 0; k < kTdBatch; k++) {
-      if (w[k] >= 0) ls.arcs++;
-      if (!c[k]) continue;
-      acc.arcs += d[k];
-      const bool act = !is_term(p, w[k]) && ex[k] > 0;
-      if (act) acc.reached++;
-      if (d[k] > p.hub_deg) {
-        append_hub(p, p.fh[nxt], &out->hq, w[k]);
-        if (act) append_hub(p, p.ah, &p.ctrl->act_hq, w[k]);
-      } else {
-        qmask |= 1u << k;
-        nq++;
-        if (act) {
-          amask |= 1u << k;
-          na++;
-        }
-      }
-    }
-    if (nq) {
-      int pos = reserve(&out->q, nq);
-#pragma unroll
-      for (int k = 0; k < kTdBatch; k++)
-        if ((qmask >> k) & 1) p.fq[nxt][pos++] = w[k];
-    }
-    if (na) {
-      int pos = reserve(&p.ctrl->act_q, na);
-#pragma unroll
-      for (int k = 0; k < kTdBatch; k++)
-        if ((amask >> k) & 1) p.aq[pos++] = w[k];
-    }
-  }
-}
-
-template <int TILE>
-__device__ __forceinline__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
-  const int cur = L & 1, nxt = cur ^ 1;
-  const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
-  VisitAcc acc;
-  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = spread_group<32>(); i < nh; i += nwarps) {
-    int beg, end;
-    const int2 it = __ldcg(p.fh[cur] + i);
-    ItemTimer tm(p);
-    chunk_range(p, it, beg, end);
-    td_range(p, out, nxt, beg + lane, end, 32, L, ls, acc);
-    tm.done(ls, it.x);
-  }
-  for_tiered<TILE>(p, ls, p.fq[cur], nn, [&](auto &g, int x) {
-    const int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
-    td_range(p, out, nxt, beg + g.rank(), end, g.size(), L, ls, acc);
-  });
-  flush_visits(p, out, acc);
-}
-
-// Whether one of the arcs first, first+stride, ... < end (at most kBatch of them)
-// has residual into a vertex labelled L; loads batched as in td_range.
-__device__ __forceinline__ bool bu_batch(const Params &p, int first, int end, int stride, int L, LStats &ls) {
-  int r[kBatch], w[kBatch];
-#pragma unroll
-  for (int k = 0; k < kBatch; k++) {
-    const int a = first + k * stride;
-    r[k] = a < end ? __ldcg(p.res + a) : 0;
-    w[k] = a < end ? __ldg(p.adj + a) : -1;
-  }
-  bool hit = false;
-#pragma unroll
-  for (int k = 0; k < kBatch; k++) {
-    if (w[k] >= 0) ls.arcs++;
-    hit |= r[k] > 0 && __ldcg(p.height + w[k]) == L;
-  }
-  return hit;
-}
-
-// Bottom-up level: every unvisited vertex looks for a residual arc into level
-// L and stops at the first one.  Hub chunks are searched by warps (the first
-// chunk of a hub to succeed labels it); other vertices by a lane or a tile.
-template <int TILE>
-__device__ __forceinline__ void ph_bfs_bu(const Params &p, Slot *out, int L, LStats &ls) {
-  const int nxt = (L & 1) ^ 1;
-  VisitAcc acc;
-  {
-    TileGroup<32> wg;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = spread_group<32>(); i < p.nhch; i += nwarps) {
-      const int2 it = __ldg(p.hch + i);
-      int hv = 0;
-      if (wg.rank() == 0) hv = __ldcg(p.height + it.x);
-      if (wg.g.shfl(hv, 0) != UNV) continue;  // labelled already (possibly by another chunk)
-      int beg, end;
-      chunk_range(p, it, beg, end);
-      const bool hit = bu_batch(p, beg + wg.rank(), end, 32, L, ls);  // 256 arcs = one batch
-      if (wg.any(hit) && wg.rank() == 0 && atomicCAS(p.height + it.x, UNV, L + 1) == UNV)
-        bfs_visit(p, out, nxt, it.x, acc);
-    }
-  }
-  for_tiered<TILE>(p, ls, nullptr, p.n, [&](auto &g, int v) {
-    if (__ldcg(p.height + v) != UNV) return;  // only v's group writes it in this phase
-    const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
-    bool found = false;
-    for (int base = beg; base < end; base += kBatch * g.size()) {
-      if (g.any(bu_batch(p, base + g.rank(), end, g.size(), L, ls))) {
-        found = true;
-        break;
-      }
-    }
-    if (found && g.rank() == 0) {
-      p.height[v] = L + 1;
-      bfs_visit(p, out, nxt, v, acc);
-    }
-  }, [&](int v) { return __ldcg(p.height + v) == UNV; });
-  flush_visits(p, out, acc);
-}
-
-// After the BFS: a complete BFS proves every unvisited vertex unreachable
-// (dead for the rest of this solve; the reference gives them height V); an
-// early-stopped BFS gives them the valid lower bound `floor`.
-__device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int floor_h, bool write_side) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  int nd = 0;
-  for (int v = gt; v < p.n; v += nt) {
-    int h = __ldcg(p.height + v);
-    if (h == UNV) {
-      if (full) {
-        p.dead[v] = 1;
-        p.height[v] = p.n;
-        nd++;
-      } else {
-        p.height[v] = floor_h;
-      }
-    }
-    if (write_side && (!p.inst_active || p.inst_active[__ldg(p.inst + v)])) p.side[v] = h < p.n ? 1 : 0;
-  }
-  block_add_ll((long long *)&p.ctrl->st_dead, nd);
-}
-
-// ---- push rounds ---------------------------------------------------------------
-// Round r reads the worklists of round r-1 (the BFS active lists for r = 0) and
-// appends to buffers r&1 with tails wtail/whtail[r%3]; tails are triple-buffered
-// for the same reason as the phase slots.
-
-__device__ __forceinline__ void enqueue(const Params &p, int r, unsigned round_id, int v) {
-  if (atomicExch(p.stamp + v, (int)round_id) == (int)round_id) return;
-  if (deg_of(p, v) > p.hub_deg) append_hub(p, p.wh[r & 1], &p.ctrl->whtail[r % 3], v);
-  else append(p.wq[r & 1], &p.ctrl->wtail[r % 3], v);
-}
-
-// Adds d to the head's excess and returns the old value.  Pushes into the one
-// sink of a single-instance solve are summed per thread instead and added once
-// per block when the push phase ends (sink_flush): a high in-degree sink takes
-// thousands of pushes a round, which would serialise on its excess word, and a
-// terminal is never queued, so its old value is not needed.
-__device__ __forceinline__ long long push_excess(const Params &p, int w, int d, LStats &ls) {
-  if (!p.role && w == p.t) {
-    ls.to_sink += d;
-    return 0;
-  }
-  return atomic_add_ll(p.excess + w, d);
-}
-
-// Every thread of the block calls it at the end of the push phase.
-__device__ __forceinline__ void sink_flush(const Params &p, LStats &ls) {
-  if (p.role) return;  // uniform
-  block_add_ll(p.excess + p.t, ls.to_sink);
-  ls.to_sink = 0;
-}
-
-__device__ __forceinline__ void push_arc(const Params &p, int a, int w, int d, int r, unsigned round_id, bool enq,
-                                         LStats &ls) {
-  atomicSub(p.res + a, d);
-  atomicAdd(p.res + __ldg(p.par + a), d);
-  long long old = push_excess(p, w, d, ls);
-  ls.pushes++;
-  if (enq && !is_term(p, w) && old + d > 0) enqueue(p, r, round_id, w);
-}
-
-// Arcs a lane handles together in a tile discharge.
-constexpr int kPushBatch = 4;
-
-
-// Queues the heads x[k] marked in `cand` for round r+1 (each at most once per
-// round, by its stamp): all stamp exchanges in flight together, then all degree
-// reads, then one reservation for the non-hub heads (hubs go to the chunk queue).
-template <int K>
-__device__ __forceinline__ void enqueue_batch(const Params &p, const int (&x)[K], unsigned cand, int r,
-                                              unsigned round_id) {
-  unsigned keep = 0;
-#pragma unroll
-  for (int k = 0; k < K; k++)
-    if ((cand >> k) & 1)
-      if (atomicExch(p.stamp + x[k], (int)round_id) != (int)round_id) keep |= 1u << k;
-  if (!keep) return;
-  int dg[K];
-#pragma unroll
-  for (int k = 0; k < K; k++) dg[k] = ((keep >> k) & 1) ? deg_of(p, x[k]) : 0;
-  int cnt = 0;
-  unsigned small = 0;
-#pragma unroll
-  for (int k = 0; k < K; k++)
-    if ((keep >> k) & 1) {
-      if (dg[k] > p.hub_deg) {
-        append_hub(p, p.wh[r & 1], &p.ctrl->whtail[r % 3], x[k]);
-      } else {
-        small |= 1u << k;
-        cnt++;
-      }
-    }
-  if (!cnt) return;
-  int pos = reserve(&p.ctrl->wtail[r % 3], cnt);
-  int *q = p.wq[r & 1];
-#pragma unroll
-  for (int k = 0; k < K; k++)
-    if ((small >> k) & 1) q[pos++] = x[k];
-}
-
-// Pushes d[k] > 0 units over arcs a[k] into heads w[k] (one lane's batch): the
-// residual and excess atomics of all arcs are in flight together, then the
-// partner residuals; heads whose excess became positive are queued (enq).
-template <int K>
-__device__ __forceinline__ void push_batch(const Params &p, const int (&a)[K], const int (&w)[K], const int (&d)[K],
-                                           int r, unsigned round_id, bool enq, LStats &ls) {
-  int pk[K];  // partner arcs, loaded while the atomics below are in flight
-#pragma unroll
-  for (int k = 0; k < K; k++) pk[k] = d[k] > 0 ? __ldg(p.par + a[k]) : 0;
-  long long old[K];
-#pragma unroll
-  for (int k = 0; k < K; k++)
-    if (d[k] > 0) {
-      atomicSub(p.res + a[k], d[k]);
-      old[k] = push_excess(p, w[k], d[k], ls);
-    }
-  unsigned cand = 0;
-#pragma unroll
-  for (int k = 0; k < K; k++)
-    if (d[k] > 0) {
-      atomicAdd(p.res + pk[k], d[k]);
-      ls.pushes++;
-      if (enq && !is_term(p, w[k]) && old[k] + d[k] > 0) cand |= 1u << k;
-    }
-  if (cand) enqueue_batch<K>(p, w, cand, r, round_id);
-}
-
-// Adjacency bound of the register-resident thread discharge below.
-constexpr int kSmallMax = 8;
-
-// Discharge of a vertex of degree <= kSmallMax by one thread, with the same
-// push/relabel rule as discharge() but laid out for latency: per cycle the
-// residuals and head heights of all arcs are loaded together, the pushes are
-// decided in registers (excess spread over the admissible arcs in arc order),
-// and every atomic of the cycle is in flight before any result is used; the
-// heads that became active are deduplicated by their stamps together and
-// appended with one reservation.  A head height may be one load old when it is
-// used (a concurrent relabel only raises it), which can leave a label above
-// the exact distance for a while; labels only steer the pushes -- dead
-// vertices and termination are decided by the exact BFS of each relabel.
-__device__ __forceinline__ void discharge_small(const Params &p, int v, int beg, int deg, long long ex0, int h, int r,
-                                unsigned round_id, bool enq, LStats &ls) {
-  int rr[kSmallMax], w[kSmallMax], hw[kSmallMax];
-#pragma unroll
-  for (int k = 0; k < kSmallMax; k++) {
-    rr[k] = k < deg ? __ldcg(p.res + beg + k) : 0;
-    w[k] = k < deg ? __ldg(p.adj + beg + k) : 0;
-  }
-  unsigned cand = 0;  // bit k: head k may have become active; bit kSmallMax: v itself
-  long long ex = ex0;
-  for (int cyc = 0; cyc < p.cycles && ex > 0 && h < p.n; cyc++) {
-    if (cyc > 0) {
-#pragma unroll
-      for (int k = 0; k < kSmallMax; k++)
-        if (k < deg) rr[k] = __ldcg(p.res + beg + k);
-    }
-#pragma unroll
-    for (int k = 0; k < kSmallMax; k++) hw[k] = k < deg ? __ldcg(p.height + w[k]) : INT_MAX;
-    ls.arcs += deg;
-    int dd[kSmallMax];
-    long long left = ex;
-#pragma unroll
-    for (int k = 0; k < kSmallMax; k++) {
-      dd[k] = 0;
-      if (rr[k] > 0 && hw[k] < h && left > 0) {
-        dd[k] = (int)(rr[k] < left ? rr[k] : left);
-        left -= dd[k];
-      }
-    }
-    int pk[kSmallMax];  // partner arcs, loaded while the atomics below are in flight
-#pragma unroll
-    for (int k = 0; k < kSmallMax; k++) pk[k] = dd[k] > 0 ? __ldg(p.par + beg + k) : 0;
-    long long old[kSmallMax];
-#pragma unroll
-    for (int k = 0; k < kSmallMax; k++)
-      if (dd[k] > 0) {
-        atomicSub(p.res + beg + k, dd[k]);
-        old[k] = push_excess(p, w[k], dd[k], ls);
-      }
-#pragma unroll
-    for (int k = 0; k < kSmallMax; k++)
-      if (dd[k] > 0) {
-        atomicAdd(p.res + pk[k], dd[k]);
-        rr[k] -= dd[k];
-        ls.pushes++;
-        if (enq && !is_term(p, w[k]) && old[k] + dd[k] > 0) cand |= 1u << k;
-      }
-    ex = left;
-    if (ex > 0) {  // every admissible arc is saturated: relabel
-      int mh = INT_MAX;
-#pragma unroll
-      for (int k = 0; k < kSmallMax; k++)
-        if (rr[k] > 0) mh = min(mh, hw[k]);
-      h = mh >= p.n ? p.n : mh + 1;
-      p.height[v] = h;
-      ls.relabels++;
-    }
-  }
-  if (ex0 != ex) atomic_add_ll(p.excess + v, ex - ex0);
-  if (enq && ex > 0 && h < p.n) cand |= 1u << kSmallMax;
-  if (!cand) return;
-  int x[kSmallMax + 1];
-#pragma unroll
-  for (int k = 0; k < kSmallMax; k++) x[k] = w[k];
-  x[kSmallMax] = v;
-  enqueue_batch<kSmallMax + 1>(p, x, cand, r, round_id);
-}
-
-// Discharge of a non-hub v by a lane or a tile: up to `cycles` rounds of
-// push-then-relabel, the push/relabel of staticMaxFlow_kernel_14
-// (code/dyn_data.h:89-131) with every admissible arc (head below h) used per
-// round instead of only the lowest one.
-//  * adjacency within the group width: one load per lane, the excess is split
-//    over the admissible arcs in arc order by a group prefix sum;
-//  * longer adjacency: pass 1 has every lane sum the admissible residual and the
-//    minimum non-admissible height over its strided arcs (independent loads); a
-//    group prefix sum turns the sums into per-lane budgets; pass 2 pushes each
-//    lane's budget greedily.
-// When every admissible arc was saturated and excess is left, h becomes
-// 1 + the minimum height over the arcs still residual.  Concurrent relabels only
-// raise heights, so a pass-2 arc that lost admissibility is skipped and the
-// round is retried instead of relabelled.
-template <class G>
-__device__ __forceinline__ void discharge(G &g, const Params &p, int v, int r, unsigned round_id, bool enq, LStats &ls,
-                          int *seen) {
-  long long ex0;
-  int h;
-  // one read, broadcast: concurrent pushes may change excess[v] meanwhile
-  if constexpr (G::size() == 1) {
-    ex0 = __ldcg(p.excess + v);
-    h = __ldcg(p.height + v);
-  } else {
-    long long e = 0;
-    int hh = 0;
-    if (g.rank() == 0) {
-      e = __ldcg(p.excess + v);
-      hh = __ldcg(p.height + v);
-    }
-    ex0 = g.g.shfl(e, 0);
-    h = g.g.shfl(hh, 0);
-  }
-  if (!(ex0 > 0 && h < p.n) || is_term(p, v)) return;
-  if (g.rank() == 0) {
-    ls.visits++;
-    if (seen) (*seen)++;
-  }
-  long long ex = ex0;
-  const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
-  constexpr int S = G::size();
-  if constexpr (S == 1) {
-    if (end - beg <= kSmallMax) {
-      discharge_small(p, v, beg, end - beg, ex0, h, r, round_id, enq, ls);
-      return;
-    }
-  }
-  for (int cyc = 0; cyc < p.cycles && ex > 0 && h < p.n; cyc++) {
-    if (end - beg <= S) {
-      const int a = beg + g.rank();
-      int rr = 0, w = -1, hw = INT_MAX;
-      if (a < end) {
-        rr = __ldcg(p.res + a);
-        if (rr > 0) {
-          w = __ldg(p.adj + a);
-          hw = __ldcg(p.height + w);
-        }
-        ls.arcs++;
-      }
-      const bool adm = rr > 0 && hw < h;
-      long long tot;
-      const long long pre = g.scan(adm ? (long long)rr : 0ll, tot);
-      int d = 0;
-      if (adm) {
-        long long left = ex - pre;
-        d = left <= 0 ? 0 : (left < rr ? (int)left : rr);
-      }
-      if (d > 0) push_arc(p, a, w, d, r, round_id, enq, ls);
-      ex -= (tot < ex ? tot : ex);
-      if (ex > 0) {
-        const int mh = g.min_all(rr > 0 && !(adm && d == rr) ? hw : INT_MAX);
-        h = mh >= p.n ? p.n : mh + 1;
-        if (g.rank() == 0) {
-          p.height[v] = h;
-          ls.relabels++;
-        }
-      }
-      continue;
-    }
-    // pass 1 (batches of kPushBatch arcs a lane: heads and residuals, then head
-    // heights, each batch's loads in flight together)
-    long long tsum = 0;
-    int tmin = INT_MAX;
-    for (int a0 = beg + g.rank(); a0 < end; a0 += kPushBatch * S) {
-      int rr[kPushBatch], w[kPushBatch];
-#pragma unroll
-      for (int k = 0; k < kPushBatch; k++) {
-        const int a = a0 + k * S;
-        rr[k] = a < end ? __ldcg(p.res + a) : 0;
-        w[k] = a < end ? __ldg(p.adj + a) : 0;
-      }
-#pragma unroll
-      for (int k = 0; k < kPushBatch; k++)
-        if (rr[k] > 0) {
-          const int hw = __ldcg(p.height + w[k]);
-          if (hw < h) tsum += rr[k];
-          else tmin = min(tmin, hw);
-        }
-    }
-    ls.arcs += (unsigned long long)((end - beg - g.rank() + S - 1) / S);
-    long long tot;
-    const long long pre = g.scan(tsum, tot);
-    // pass 2: heights reread (a concurrent relabel may have made an arc
-    // inadmissible), the lane's budget spread greedily, each batch's pushes in
-    // flight together
-    long long budget = ex - pre;
-    budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
-    long long done = 0;
-    for (int a0 = beg + g.rank(); a0 < end && budget > 0; a0 += kPushBatch * S) {
-      int aa[kPushBatch], rr[kPushBatch], w[kPushBatch], dd[kPushBatch];
-#pragma unroll
-      for (int k = 0; k < kPushBatch; k++) {
-        aa[k] = a0 + k * S;
-        rr[k] = aa[k] < end ? __ldcg(p.res + aa[k]) : 0;
-        w[k] = aa[k] < end ? __ldg(p.adj + aa[k]) : 0;
-      }
-      int hw[kPushBatch];
-#pragma unroll
-      for (int k = 0; k < kPushBatch; k++) hw[k] = rr[k] > 0 ? __ldcg(p.height + w[k]) : INT_MAX;
-#pragma unroll
-      for (int k = 0; k < kPushBatch; k++) {
-        dd[k] = 0;
-        if (hw[k] < h && budget > 0) {
-          dd[k] = (int)(rr[k] < budget ? rr[k] : budget);
-          budget -= dd[k];
-          done += dd[k];
-        }
-      }
-      push_batch<kPushBatch>(p, aa, w, dd, r, round_id, enq, ls);
-    }
-    const long long moved = g.sum_all(done);
-    ex -= moved;
-    if (ex > 0 && moved == tot) {  // all admissible arcs saturated: relabel
-      const int mh = g.min_all(tmin);
-      h = mh >= p.n ? p.n : mh + 1;
-      if (g.rank() == 0) {
-        p.height[v] = h;
-        ls.relabels++;
-      }
-    }
-  }
-  if (g.rank() == 0) {
-    if (ex0 != ex) atomic_add_ll(p.excess + v, ex - ex0);
-    if (enq && ex > 0 && h < p.n) enqueue(p, r, round_id, v);
-  }
-}
-
-// Inputs of push round r: non-hub vertices and hub chunks.
-struct RoundIn {
-  const int *nlist;
-  int nn;
-  const int2 *hlist;
-  int nh;
-};
-
-__device__ __forceinline__ RoundIn round_inputs(const Params &p, const Ctrl *c, int r) {
-  RoundIn in;
-  if (p.variant == DMF_VARIANT_TOPO) {
-    in.nlist = nullptr;
-    in.nn = p.n;
-    in.hlist = p.hch;
-    in.nh = p.nhch;
-  } else if (r == 0) {
-    in.nlist = p.aq;
-    in.nn = ld_vol(&c->act_q);
-    in.hlist = p.ah;
-    in.nh = ld_vol(&c->act_hq);
-  } else {
-    in.nlist = p.wq[(r - 1) & 1];
-    in.nn = ld_vol(&c->wtail[(r - 1) % 3]);
-    in.hlist = p.wh[(r - 1) & 1];
-    in.nh = ld_vol(&c->whtail[(r - 1) % 3]);
-  }
-  return in;
-}
-
-// Push round, phase 1: non-hub vertices are discharged completely; every hub
-// chunk sums its admissible residual, adds its minimum non-admissible head
-// height to the hub's, and pushes its share of the hub's excess.
-template <int TILE, int BLOCK>
-__device__ __forceinline__ void ph_push1(const Params &p, const RoundIn &in, int r, unsigned round_id, unsigned gepoch, LStats &ls,
-                         typename BlockGroup<BLOCK>::Temp &btmp, int *bci, long long *bcl) {
-  Ctrl *c = p.ctrl;
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool topo = p.variant == DMF_VARIANT_TOPO;
-  if (gt == 0) {
-    if (r == 0) {  // read during the BFS just finished; cleared for the next one
-      c->pos_count = 0;
-      c->unexplored = 0;
-    }
-    c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
-  }
-  {
-    // Hub chunks: scan, then claim a share of the hub's excess and push it from
-    // the scan's registers, in one phase.  A hub's excess only grows during the
-    // phase (its own pushes leave it in phase 2), so each chunk's read of it at
-    // the start of its item is at most the hub's excess at the end of the
-    // phase, and the shares claimed in arc-chunk order by the atomic on the
-    // hub's allocation never add up to more than that.
-    TileGroup<32> wg;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = spread_group<32>(); i < in.nh; i += nwarps) {
-      const int2 it = __ldcg(in.hlist + i);
-      const int v = it.x;
-      ItemTimer tmr(p);
-      int hh = 0;
-      long long ex_start = 0;  // the hub's excess as the phase found it
-      if (wg.rank() == 0) {
-        hh = __ldcg(p.height + v);
-        ex_start = __ldcg(p.excess + v);
-      }
-      const int h = wg.g.shfl(hh, 0);
-      const bool has_ex = wg.g.shfl(ex_start, 0) > 0;
-      const int hid = __ldg(p.hub_base + v), cidx = hid + it.y;
-      const unsigned long long key = ((unsigned long long)gepoch << 32) | (unsigned)h;
-      unsigned long long mk = 0;
-      if (wg.rank() == 0) mk = __ldcg(p.chunk_mark + cidx);
-      mk = wg.g.shfl(mk, 0);
-      // A hub without excess (topology rounds sweep every hub) needs nothing.
-      // Every chunk that does look counts itself: the hub is relabelled only
-      // when all its chunks contributed to the minimum head height.
-      if (!has_ex || h >= p.n || is_term(p, v)) {
-      } else if (mk == key) {  // exhausted at this height: only its minimum head height matters
-        if (wg.rank() == 0) {
-          const int tm = __ldcg(p.chunk_tmin + cidx);
-          if (tm != INT_MAX) atomicMin(p.hc_min + hid, tm);
-          atomicAdd(p.hc_done + hid, 1);
-        }
-      } else {
-        int beg, end;
-        chunk_range(p, it, beg, end);
-        int aa[kBatch], rr[kBatch], w[kBatch], hw[kBatch];
-#pragma unroll
-        for (int k = 0; k < kBatch; k++) {
-          aa[k] = beg + wg.rank() + 32 * k;
-          rr[k] = aa[k] < end ? __ldcg(p.res + aa[k]) : 0;
-          w[k] = aa[k] < end ? __ldg(p.adj + aa[k]) : 0;
-        }
-#pragma unroll
-        for (int k = 0; k < kBatch; k++) hw[k] = rr[k] > 0 ? __ldcg(p.height + w[k]) : INT_MAX;
-        long long tsum = 0;
-        int tmin = INT_MAX;
-#pragma unroll
-        for (int k = 0; k < kBatch; k++) {
-          if (rr[k] > 0) {
-            if (hw[k] < h) tsum += rr[k];
-            else tmin = min(tmin, hw[k]);
-          }
-        }
-        ls.arcs += kBatch;
-        long long ts;
-        const long long pre = wg.scan(tsum, ts);
-        const int tm = wg.min_all(tmin);
-        long long cb = 0;  // this chunk's share of the hub's excess
-        if (wg.rank() == 0) {
-          if (tm != INT_MAX) atomicMin(p.hc_min + hid, tm);
-          atomicAdd(p.hc_done + hid, 1);
-          if (ts > 0) {
-            const long long old = atomic_add_ll(p.hc_alloc + hid, ts);
-            cb = ex_start - old;
-            cb = cb < 0 ? 0 : (cb > ts ? ts : cb);
-          }
-        }
-        cb = wg.g.shfl(cb, 0);
-        long long moved = 0;
-        if (cb > 0) {  // warp-uniform
-          long long budget = cb - pre;
-          budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
-          long long done = 0;
-          int dd[kBatch];
-#pragma unroll
-          for (int k = 0; k < kBatch; k++) {
-            dd[k] = 0;
-            if (rr[k] > 0 && hw[k] < h && budget > 0) {
-              dd[k] = (int)(rr[k] < budget ? rr[k] : budget);
-              budget -= dd[k];
-              done += dd[k];
-            }
-          }
-          push_batch<kBatch>(p, aa, w, dd, r, round_id, !topo, ls);
-          moved = wg.sum_all(done);
-          if (wg.rank() == 0 && moved) atomic_add_ll(p.hc_moved + hid, moved);
-        }
-        // no admissible arc left in the chunk at this height: skip it until the
-        // hub's height or the relabel epoch changes
-        if (wg.rank() == 0 && moved == ts) {
-          p.chunk_mark[cidx] = key;
-          p.chunk_tmin[cidx] = tm;
-        }
-      }
-      tmr.done(ls, v);
-    }
-  }
-  int seen = 0;
-  // topology rounds sweep every vertex: only those with excess need a look
-  for_tiered<TILE>(
-      p, ls, in.nlist, in.nn,
-      [&](auto &g, int v) { discharge(g, p, v, r, round_id, !topo, ls, topo ? &seen : nullptr); },
-      [&](int v) { return !topo || __ldcg(p.excess + v) > 0; });
-  if (topo) agg_add_int(&c->seen[r % 3], seen);
-  sink_flush(p, ls);
-}
-
-// Push round, phase 2 (hubs): per hub (its first chunk), the moved total leaves
-// its excess; when all of the hub's admissible residual was pushed and excess is
-// left, the hub is relabelled to 1 + the minimum non-admissible height; a hub
-// with excess left is queued for the next round.  The hub's totals are reset.
-__device__ __forceinline__ void ph_push3(const Params &p, const RoundIn &in, int r, unsigned round_id, LStats &ls) {
-  const int nt = gridDim.x * blockDim.x;
-  const bool topo = p.variant == DMF_VARIANT_TOPO;
-  int seen = 0;
-  for (int i = spread_thread(); i < in.nh; i += nt) {
-    const int2 it = __ldcg(in.hlist + i);
-    if (it.y != 0) continue;
-    const int v = it.x;
-    const int hid = __ldg(p.hub_base + v);
-    const long long tot = __ldcg(p.hc_alloc + hid), moved = __ldcg(p.hc_moved + hid);
-    const int mh = __ldcg(p.hc_min + hid), looked = __ldcg(p.hc_done + hid);
-    const long long ex0 = __ldcg(p.excess + v);
-    int h = __ldcg(p.height + v);
-    const bool complete = looked == nchunks(deg_of(p, v));  // every chunk gave its minimum
-    // clean for the next round
-    p.hc_alloc[hid] = 0;
-    p.hc_moved[hid] = 0;
-    p.hc_min[hid] = INT_MAX;
-    p.hc_done[hid] = 0;
-    if (!(ex0 > 0 && h < p.n) || is_term(p, v)) continue;
-    seen++;
-    ls.visits++;
-    const long long ex = ex0 - moved;
-    if (moved) atomic_add_ll(p.excess + v, -moved);
-    if (ex > 0 && moved == tot && complete) {  // every admissible arc saturated: relabel
-      h = mh >= p.n ? p.n : mh + 1;
-      p.height[v] = h;
-      ls.relabels++;
-    }
-    if (!topo && ex > 0 && h < p.n) enqueue(p, r, round_id, v);
-  }
-  if (topo) agg_add_int(&p.ctrl->seen[r % 3], seen);
-}
-
-// recalculate_max_flow_kernel_39 (code/dyn_data.h:208-215) as a reduction:
-// flow = excess(t) + sum of negative excess over v != s, t (per instance in
-// batched mode).
-template <int BLOCK>
-__device__ __forceinline__ void ph_flow(const Params &p, typename BlockGroup<BLOCK>::Temp &btmp) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  long long acc = 0;
-  for (int v = gt; v < p.n; v += nt) {
-    const long long ex = __ldcg(p.excess + v);
-    long long c = 0;
-    if (is_snk(p, v)) c = ex;
-    else if (!is_src(p, v) && ex < 0) c = ex;
-    if (p.inst) {
-      if (c && (!p.inst_active || p.inst_active[__ldg(p.inst + v)])) atomic_add_ll(p.inst_flow + __ldg(p.inst + v), c);
-    } else {
-      acc += c;
-    }
-  }
-  if (p.inst) return;
-  __syncthreads();
-  long long tot = typename BlockGroup<BLOCK>::RedL(btmp.redl).Sum(acc);
-  if (threadIdx.x == 0 && tot) atomic_add_ll(&p.ctrl->flow, tot);
-}
-
-__device__ __forceinline__ void clear_slot(Slot *s) {
-  s->q = 0;
-  s->hq = 0;
-  s->arcs = 0;
-  s->cnt = 0;
-}
-
-// ---- push-pull, phase 1 (code/dyn_pp_bench.cu:6-88, part_pp) --------------------
-// The cut kept from the previous solve splits the vertices into the sink side B
-// (side = 1) and the source side A (side = 0).  Phase 1 works inside each side:
-// B pushes its excess towards t and B's deficits (heights: residual distance to
-// them within B, pp_bfs code/dyn_pp.h:99-120), A pulls its deficits from A's
-// excess (heights: residual distance from an excess vertex within A; pull_kernel
-// code/dyn_pp.h:237-280), both in the same rounds.  Arcs between the sides are
-// not touched.  Phase 2, the general solve, then finishes exactly.
-
-__device__ __forceinline__ bool pp_active(const Params &p, int v, long long ex) {
-  if (is_term(p, v)) return false;
-  return p.side[v] ? ex > 0 : ex < 0;
-}
-
-// Seeds (pp_bfs_init, code/dyn_pp.h:76-83): t, B's deficits and A's excess.
-__device__ __forceinline__ void ph_pp_init(const Params &p, Slot *out) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  Ctrl *c = p.ctrl;
-  if (gt == 0) {
-    c->act_q = 0;
-    c->act_hq = 0;
-    c->wtail[0] = c->whtail[0] = c->seen[0] = 0;
-  }
-  int pos = 0;
-  for (int v = gt; v < p.n; v += nt) {
-    const long long ex = __ldcg(p.excess + v);
-    const int sd = p.side[v];
-    const bool seed = is_snk(p, v) || (!is_src(p, v) && (sd ? ex < 0 : ex > 0));
-    if (seed) {
-      p.height[v] = 0;
-      if (deg_of(p, v) > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
-      else append(p.fq[0], &out->q, v);
-    } else {
-      p.height[v] = UNV;
-    }
-    if (pp_active(p, v, ex)) pos++;
-  }
-  agg_add_int(&c->pos_count, pos);
-}
-
-// One level over the frontier: a B vertex x labels B neighbours w with residual
-// w->x, an A vertex x labels A neighbours w with residual x->w; s and t are
-// never labelled.  All phase-1 actives go to the non-hub active list.
-__device__ __forceinline__ void pp_td_range(const Params &p, Slot *out, int nxt, int x, int first, int end,
-                                            int stride, int L, LStats &ls, VisitAcc &acc) {
-  const int sx = p.side[x];
-  for (int a = first; a < end; a += stride) {
-    const int w = __ldg(p.adj + a);
-    ls.arcs++;
-    if (is_term(p, w) || p.side[w] != sx) continue;
-    if (__ldcg(p.height + w) != UNV) continue;
-    const int r = sx ? __ldcg(p.res + __ldg(p.par + a)) : __ldcg(p.res + a);
-    if (r <= 0 || atomicCAS(p.height + w, UNV, L + 1) != UNV) continue;
-    const int d = deg_of(p, w);
-    if (d > p.hub_deg) append_hub(p, p.fh[nxt], &out->hq, w);
-    else append(p.fq[nxt], &out->q, w);
-    if (pp_active(p, w, __ldcg(p.excess + w))) {
-      append(p.aq, &p.ctrl->act_q, w);
-      acc.reached++;
-    }
-  }
-}
-
-template <int TILE>
-__device__ __forceinline__ void ph_pp_bfs(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
-  const int cur = L & 1, nxt = cur ^ 1;
-  const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
-  VisitAcc acc;
-  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = spread_group<32>(); i < nh; i += nwarps) {
-    const int2 it = __ldcg(p.fh[cur] + i);
-    int beg, end;
-    chunk_range(p, it, beg, end);
-    pp_td_range(p, out, nxt, it.x, beg + lane, end, 32, L, ls, acc);
-  }
-  for_tiered<TILE>(p, ls, p.fq[cur], nn, [&](auto &g, int x) {
-    const int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
-    pp_td_range(p, out, nxt, x, beg + g.rank(), end, g.size(), L, ls, acc);
-  });
-  flush_visits(p, out, acc);
-}
-
-// Unlabelled vertices cannot reach a target within their side: inactive for
-// phase 1 (not dead: the general solve decides that).
-__device__ __forceinline__ void ph_pp_finalize(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gt == 0) p.ctrl->pos_count = 0;  // read by every block before this phase
-  for (int v = gt; v < p.n; v += nt)
-    if (__ldcg(p.height + v) == UNV) p.height[v] = p.n;
-}
-
-__device__ __forceinline__ void pp_enqueue(const Params &p, int r, unsigned round_id, int v) {
-  if (atomicExch(p.stamp + v, (int)round_id) == (int)round_id) return;
-  append(p.wq[r & 1], &p.ctrl->wtail[r % 3], v);
-}
-
-// Push (B vertex, to B neighbours) or pull (A vertex, from A neighbours) of one
-// vertex by a group, two passes per cycle as in discharge: pass 1 sums the
-// admissible residual (head / tail labelled below h) and the minimum label over
-// the other residual arcs; a group prefix sum gives lane budgets; pass 2 moves
-// them.  A pull of d from w along w->v lowers res(w->v) and excess(w).
-template <class G>
-__device__ __forceinline__ void pp_discharge(G &g, const Params &p, int v, int r, unsigned round_id, LStats &ls) {
-  long long e0 = 0;
-  int hh = 0;
-  if (g.rank() == 0) {
-    e0 = __ldcg(p.excess + v);
-    hh = __ldcg(p.height + v);
-  }
-  long long ex0;
-  int h;
-  if constexpr (G::size() == 1) {
-    ex0 = e0;
-    h = hh;
-  } else {
-    ex0 = g.g.shfl(e0, 0);
-    h = g.g.shfl(hh, 0);
-  }
-  const bool pull = p.side[v] == 0;
-  if (!pp_active(p, v, ex0) || h >= p.n) return;
-  if (g.rank() == 0) ls.visits++;
-  long long need = pull ? -ex0 : ex0;
-  const long long need0 = need;
-  const int beg = __ldg(p.off + v), end = __ldg(p.off + v + 1);
-  constexpr int S = G::size();
-  for (int cyc = 0; cyc < p.cycles && need > 0 && h < p.n; cyc++) {
-    long long tsum = 0;
-    int tmin = INT_MAX;
-    for (int a = beg + g.rank(); a < end; a += S) {
-      const int w = __ldg(p.adj + a);
-      ls.arcs++;
-      // B pushes to B (t included); A pulls from A (s excluded: its arcs are saturated)
-      if (is_src(p, w) || p.side[w] != (pull ? 0 : 1)) continue;
-      const int rr = pull ? __ldcg(p.res + __ldg(p.par + a)) : __ldcg(p.res + a);
-      if (rr <= 0) continue;
-      const int hw = __ldcg(p.height + w);
-      if (hw < h) tsum += rr;
-      else tmin = min(tmin, hw);
-    }
-    long long tot;
-    const long long pre = g.scan(tsum, tot);
-    long long budget = need - pre;
-    budget = budget < 0 ? 0 : (budget > tsum ? tsum : budget);
-    long long done = 0;
-    for (int a = beg + g.rank(); a < end && budget > 0; a += S) {
-      const int w = __ldg(p.adj + a);
-      if (is_src(p, w) || p.side[w] != (pull ? 0 : 1)) continue;
-      const int pa = __ldg(p.par + a);
-      const int rr = pull ? __ldcg(p.res + pa) : __ldcg(p.res + a);
-      if (rr <= 0 || __ldcg(p.height + w) >= h) continue;
-      const int d = (int)(rr < budget ? rr : budget);
-      if (pull) {
-        atomicSub(p.res + pa, d);
-        atomicAdd(p.res + a, d);
-        const long long old = atomic_add_ll(p.excess + w, -(long long)d);
-        if (old - d < 0 && old >= 0) pp_enqueue(p, r, round_id, w);  // w now has a deficit
-      } else {
-        atomicSub(p.res + a, d);
-        atomicAdd(p.res + pa, d);
-        const long long old = atomic_add_ll(p.excess + w, (long long)d);
-        if (old + d > 0 && old <= 0) pp_enqueue(p, r, round_id, w);  // w now has excess
-      }
-      ls.pushes++;
-      budget -= d;
-      done += d;
-    }
-    const long long moved = g.sum_all(done);
-    need -= moved;
-    if (need > 0 && moved == tot) {
-      const int mh = g.min_all(tmin);
-      h = mh >= p.n ? p.n : mh + 1;
-      if (g.rank() == 0) {
-        p.height[v] = h;
-        ls.relabels++;
-      }
-    }
-  }
-  if (g.rank() == 0) {
-    const long long moved_total = need0 - need;
-    if (moved_total) atomic_add_ll(p.excess + v, pull ? moved_total : -moved_total);
-    if (need > 0 && h < p.n) pp_enqueue(p, r, round_id, v);
-  }
-}
-
-template <int TILE>
-__device__ __forceinline__ void ph_pp_round(const Params &p, const Ctrl *sc, int r, unsigned round_id, LStats &ls) {
-  Ctrl *c = p.ctrl;
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gt == 0) c->wtail[(r + 1) % 3] = c->whtail[(r + 1) % 3] = c->seen[(r + 1) % 3] = 0;
-  const int *list = r == 0 ? p.aq : p.wq[(r - 1) & 1];
-  const int nn = r == 0 ? sc->act_q : sc->wtail[(r - 1) % 3];
-  // small vertices by a lane, medium ones by a tile; hubs wait for phase 2
-  const int nt = gridDim.x * blockDim.x;
-  for (int i = spread_thread(rot_threads()); i < nn; i += nt) {
-    const int v = __ldcg(list + i);
-    if (deg_of(p, v) > p.small_deg) continue;
-    ThreadGroup th;
-    pp_discharge(th, p, v, r, round_id, ls);
-  }
-  TileGroup<TILE> tg;
-  for (int i = spread_group<TILE>(rot_tiles()); i < nn; i += nt / TILE) {
-    int v = 0, d = 0;
-    if (tg.rank() == 0) {
-      v = __ldcg(list + i);
-      d = deg_of(p, v);
-    }
-    v = tg.g.shfl(v, 0);
-    d = tg.g.shfl(d, 0);
-    if (d <= p.small_deg || d > p.hub_deg) continue;  // hubs are left to the general solve
-    pp_discharge(tg, p, v, r, round_id, ls);
-  }
-}
-
-template <int TILE, int BLOCK>
-__device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockGroup<BLOCK>::Temp &btmp, int *bci,
-                    long long *bcl, Ctrl *sc) {
-  // c: the control block in global memory (atomics, writes by the lead);
-  // sc: this block's copy taken at the last barrier, for every read of a count
-  // the previous phase produced
-  Ctrl *c = p.ctrl;
-  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
-  int ph = 0;
-  int kind = 0;  // phase kind, recorded in the optional timeline
-  long long items = 0, hubitems = 0;  // work of the phase, recorded with it
-  auto slot_out = [&]() { return &c->slot[ph % 3]; };
-  auto slot_in = [&]() { return &sc->slot[(ph + 2) % 3]; };
-  auto record = [&]() {
-    if (lead && p.trace && ph < p.trace_cap) {
-      p.trace[4 * ph] = (unsigned long long)kind | ((unsigned long long)(items & 0xffffffffll) << 8) |
-                        ((unsigned long long)(hubitems & 0xffffff) << 40);
-      p.trace[4 * ph + 1] = globaltimer();
-      p.trace[4 * ph + 2] = ph > 0 ? ld_vol((const long long *)&c->probe[(ph + 1) & 1]) : 0;
-      p.trace[4 * ph + 3] = ph > 0 ? ld_vol((const long long *)&c->blk[(ph + 1) & 1]) : 0;
-      c->probe[(ph + 1) & 1] = 0;
-      c->blk[(ph + 1) & 1] = 0;
-    }
-  };
-  auto next = [&]() -> bool {
-    if (p.probe) {  // longest item of the phase that is ending
-      cg::thread_block_tile<32> w = cg::tiled_partition<32>(cg::this_thread_block());
-      const unsigned long long mx = cg::reduce(w, ls.probe, cg::greater<unsigned long long>());
-      if (w.thread_rank() == 0 && mx) atomicMax(&c->probe[ph & 1], mx);
-      ls.probe = 0;
-      __syncthreads();  // the block's work of this phase is done
-      if (threadIdx.x == 0 && ls.t_phase) atomicMax(&c->blk[ph & 1], globaltimer() - ls.t_phase);
-    }
-    if (!grid_barrier(c, sc)) return false;
-    if (p.probe && threadIdx.x == 0) ls.t_phase = globaltimer();
-    ph++;
-    record();
-    if (lead) clear_slot(&c->slot[(ph + 1) % 3]);
-    return true;
-  };
-  record();
-  if (lead) clear_slot(&c->slot[1]);
-
-  // ---- prologue --------------------------------------------------------------
-  if (p.mode == MODE_STATIC) {
-    kind = TR_INIT_RES;
-    ph_init_res(p);
-    if (!next()) return;
-    kind = TR_SATURATE;
-    ph_saturate(p);
-    if (!next()) return;
-  } else if (p.mode == MODE_DYNAMIC) {
-    kind = TR_LOOKUP;
-    ph_lookup(p);
-    if (!next()) return;
-    kind = TR_APPLY;
-    ph_apply(p, true);
-    if (!next()) return;
-    kind = TR_REPAIR;
-    ph_repair(p);
-    if (!next()) return;
-    if (p.variant == DMF_VARIANT_PP) {
-      kind = TR_CUT_SATURATE;
-      ph_cut_saturate(p);
-      if (!next()) return;
-    }
-    kind = TR_SATURATE;
-    ph_saturate(p);
-    if (!next()) return;
-  } else if (p.mode == MODE_RECOMPUTE) {
-    kind = TR_LOOKUP;
-    ph_lookup(p);
-    if (!next()) return;
-    kind = TR_APPLY;
-    ph_apply(p, false);
-    if (!next()) return;
-    kind = TR_INIT_RES;
-    ph_init_res(p);
-    if (!next()) return;
-    kind = TR_SATURATE;
-    ph_saturate(p);
-    if (!next()) return;
-  }
-
-  unsigned round_id = p.round_base;
-
-  // ---- push-pull phase 1 (dynamic batches of the push-pull variant) ----------------
-  if (p.variant == DMF_VARIANT_PP && p.mode == MODE_DYNAMIC) {
-    for (int it1 = 0; it1 < kPPIters; it1++) {
-      kind = TR_PP_INIT;
-      items = hubitems = 0;
-      ph_pp_init(p, slot_out());
-      if (!next()) return;
-      const int P = sc->pos_count;
-      int reached = 0;
-      for (int L = 0;; L++) {
-        const Slot *in = slot_in();
-        const int F = in->q + in->hq;
-        reached += in->cnt;
-        if (F == 0 || P == 0 || reached == P) break;
-        kind = TR_PP_BFS;
-        items = in->q;
-        hubitems = in->hq;
-        ph_pp_bfs<TILE>(p, in, slot_out(), L, ls);
-        if (!next()) return;
-      }
-      kind = TR_PP_FINALIZE;
-      items = hubitems = 0;
-      ph_pp_finalize(p);
-      if (!next()) return;
-      const int A = sc->act_q;
-      if (A == 0) break;
-      for (int r = 0; r < p.interval; r++) {
-        round_id++;
-        kind = TR_PP_ROUND;
-        items = r == 0 ? A : sc->wtail[(r - 1) % 3];
-        hubitems = 0;
-        ph_pp_round<TILE>(p, sc, r, round_id, ls);
-        if (!next()) return;
-        if (lead) c->rounds_used = round_id - p.round_base;
-        if (sc->wtail[r % 3] == 0) break;
-      }
-    }
-  }
-
-  // ---- global relabel / push rounds ---------------------------------------------
-  const bool cut_only = p.mode == MODE_CUT;
-  const bool topo = p.variant == DMF_VARIANT_TOPO;
-  for (int it = 0;; it++) {
-    if (it >= p.max_iters) {
-      if (lead) set_err(c, ERR_NO_CONV, it);
-      return;
-    }
-    kind = TR_BFS_INIT;
-    items = hubitems = 0;
-    ph_bfs_init(p, slot_out(), it == 0);
-    if (!next()) return;
-    if (lead) c->st_outer++;
-    const int P = sc->pos_count;
-    const bool want_cut = p.need_cut || cut_only;
-    if (P == 0 && !want_cut) break;
-    long long m_u = sc->unexplored;
-    bool bu = false, full = true;
-    int L = 0, reached = 0;
-    for (;; L++) {
-      const Slot *in = slot_in();
-      const int F = in->q + in->hq;
-      const long long m_f = in->arcs;
-      reached += in->cnt;
-      if (F == 0) break;  // complete
-      if (!cut_only && P > 0 && reached == P) {
-        full = false;  // every active vertex has its exact distance
-        break;
-      }
-      if (L > 0) m_u -= m_f;
-      if (!bu && p.bu_alpha > 0 && m_f * p.bu_alpha > m_u) bu = true;
-      else if (bu && (long long)F * 24 < p.n) bu = false;
-      kind = bu ? TR_BFS_BU : TR_BFS_TD;
-      items = in->q;
-      hubitems = in->hq;
-      if (bu) ph_bfs_bu<TILE>(p, slot_out(), L, ls);
-      else ph_bfs_td<TILE>(p, in, slot_out(), L, ls);
-      if (!next()) return;
-      if (lead) c->st_levels++;
-    }
-    kind = TR_BFS_FINALIZE;
-    items = hubitems = 0;
-    ph_bfs_finalize(p, full, L + 1, full && want_cut);
-    if (!next()) return;
-    const int A = sc->act_q + sc->act_hq;
-    if (A == 0 || cut_only) break;
-    // a global relabel costs about one phase per BFS level and a push round moves
-    // excess about one hop: on deep graphs (grids) allow as many rounds as the
-    // relabel had levels before relabelling again (the loop ends early when the
-    // worklist empties)
-    const int rounds = (p.interval > L || !p.adaptive) ? p.interval : L;
-    for (int r = 0; r < rounds; r++) {
-      round_id++;
-      const RoundIn in = round_inputs(p, sc, r);
-      kind = TR_PUSH;
-      items = in.nn;
-      hubitems = in.nh;
-      ph_push1<TILE, BLOCK>(p, in, r, round_id, p.relabel_base + it, ls, btmp, bci, bcl);
-      if (!next()) return;
-      if (in.nh > 0) {
-        kind = TR_PUSH_HUB_FINISH;
-        ph_push3(p, in, r, round_id, ls);
-        if (!next()) return;
-      }
-      if (lead) {
-        c->st_rounds++;
-        c->rounds_used = round_id - p.round_base;
-      }
-      const int W = topo ? sc->seen[r % 3] : sc->wtail[r % 3] + sc->whtail[r % 3];
-      if (W == 0) break;
-    }
-  }
-  kind = TR_FLOW;
-  items = hubitems = 0;
-  ph_flow<BLOCK>(p, btmp);
-  if (lead) c->rounds_used = round_id - p.round_base;
-  // the flow phase ends without a barrier; its end is the kernel's end
-  if (lead && p.trace && ph + 1 < p.trace_cap) c->trace_len = ph + 1;
-}
-
-template <int TILE, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_solve(Params p) {
-  __shared__ typename BlockGroup<BLOCK>::Temp btmp;
-  __shared__ int bci;
-  __shared__ long long bcl;
-  __shared__ Ctrl snap;
-  LStats ls;
-  run<TILE, BLOCK>(p, ls, btmp, &bci, &bcl, &snap);
-  // statistics: one atomic per block and counter
-  __syncthreads();
-  typedef cub::BlockReduce<unsigned long long, BLOCK> R;
-  __shared__ typename R::TempStorage rt;
-  unsigned long long v[4] = {ls.pushes, ls.relabels, ls.arcs, ls.visits};
-  unsigned long long *dst[4] = {&p.ctrl->st_pushes, &p.ctrl->st_relabels, &p.ctrl->st_arcs, &p.ctrl->st_visits};
-  for (int i = 0; i < 4; i++) {
-    unsigned long long s = R(rt).Sum(v[i]);
-    if (threadIdx.x == 0 && s) atomicAdd(dst[i], s);
-    __syncthreads();
-  }
-}
 
 // Raw feature sums of an update batch against the current residual state, for
 // the schedule picker (nothing is modified).  Updates the solver would reject
 // (bad ids, unknown arcs) are skipped here; the solve reports them.
-__global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, const int *__restrict__ adj,
+__global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, const int *__restrict__ shead,
                                                   const int *__restrict__ sidx, const int *cap, const int *res, int n,
                                                   int k, const int *usrc, const int *udst, const int *uw,
                                                   dmfs::FeatAcc *acc) {
@@ -1666,7 +29,7 @@ __global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, c
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
     const int u = __ldg(usrc + i), v = __ldg(udst + i), w = __ldg(uw + i);
     if (u < 0 || u >= n || v < 0 || v >= n || u == v) continue;
-    const int e = find_arc_dev(off, adj, sidx, u, v);
+    const int e = find_arc_dev(off, shead, sidx, u, v);
     if (e < 0) continue;
     valid++;
     const int c0 = __ldcg(cap + e), r = __ldcg(res + e);
@@ -1709,24 +72,14 @@ __global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, c
   }
 }
 
-using KernelFn = void (*)(Params);
-
 // minb = resident blocks per SM the register budget is sized for (1: up to 128
 // registers a thread, 2: up to 64).
 KernelFn pick_kernel(int tile, int minb) {
-  if (minb == 1) {
-    switch (tile) {
-      case 4: return k_solve<4, kBlock, 1>;
-      case 8: return k_solve<8, kBlock, 1>;
-      case 16: return k_solve<16, kBlock, 1>;
-      default: return k_solve<32, kBlock, 1>;
-    }
-  }
   switch (tile) {
-    case 4: return k_solve<4, kBlock, 2>;
-    case 8: return k_solve<8, kBlock, 2>;
-    case 16: return k_solve<16, kBlock, 2>;
-    default: return k_solve<32, kBlock, 2>;
+    case 4: return solve_kernel_t4(minb);
+    case 8: return solve_kernel_t8(minb);
+    case 16: return solve_kernel_t16(minb);
+    default: return solve_kernel_t32(minb);
   }
 }
 
@@ -1746,10 +99,11 @@ struct dmf_solver {
   dmf_opts opts{};
   int tile = 32, grid = 0, block = kBlock, hub_deg = 256, small_deg = 8, minb = 2, bu_alpha = 2;
   int *off = nullptr, *adj = nullptr, *par = nullptr, *sidx = nullptr, *cap = nullptr, *res = nullptr;
+  int *shead = nullptr;  // heads in per-vertex sorted order (shead[i] = adj[sidx[i]])
   int *height = nullptr, *stamp = nullptr, *astamp = nullptr, *uarc = nullptr;
   long long *excess = nullptr;
   unsigned char *dead = nullptr, *side = nullptr;
-  int *qbuf = nullptr;    // 5 vertex queues (frontier x2, worklist x2, active)
+  int *qbuf = nullptr;    // 6 vertex queues (frontier x2, worklist x2, active, dead-set candidates)
   int2 *hqbuf = nullptr;  // 5 hub-chunk queues, same roles
   int2 *hch = nullptr;    // every hub's chunks
   int nchunk = 0;         // total hub chunks = capacity of each hub-chunk queue
@@ -1920,6 +274,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.adj = sv->adj;
   p.par = sv->par;
   p.sidx = sv->sidx;
+  p.shead = sv->shead;
   p.cap = sv->cap;
   p.res = sv->res;
   p.height = sv->height;
@@ -1938,6 +293,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
     p.wh[i] = sv->hqbuf + (2 + i) * NC;
   }
   p.aq = sv->qbuf + 4 * N;
+  p.dq = sv->qbuf + 5 * N;
   p.ah = sv->hqbuf + 4 * NC;
   p.hch = sv->hch;
   p.nhch = sv->nchunk;
@@ -1973,6 +329,10 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.bu_alpha = sv->bu_alpha;
   p.adaptive = (sv->opts.flags & DMF_FLAG_FIXED_INTERVAL) ? 0 : 1;
   p.need_cut = sv->opts.variant == DMF_VARIANT_PP ? 1 : 0;
+  p.keep_dead = mode == MODE_DYNAMIC && !(sv->opts.flags & DMF_FLAG_REVIVE_DEAD) ? 1 : 0;
+  const bool hook = (sv->opts.flags & DMF_FLAG_TEST_BARRIER_TIMEOUT) != 0;
+  p.barrier_ns = hook ? kTestBarrierTimeoutNs : kBarrierTimeoutNs;
+  p.absent_block = hook && sv->grid > 1 ? sv->grid - 1 : -1;
   p.round_base = sv->round_base;
   p.trace = (sv->opts.flags & DMF_FLAG_TRACE) ? sv->trace : nullptr;
   p.probe = (sv->opts.flags & DMF_FLAG_PROBE) && p.trace ? 1 : 0;
@@ -2013,6 +373,9 @@ int finish(dmf_solver *sv, int64_t *flow, bool need_cut_valid) {
   sv->st.arcs_scanned = (int64_t)c.st_arcs;
   sv->st.vertices_visited = (int64_t)c.st_visits;
   sv->st.dead_vertices = (int64_t)c.st_dead;
+  sv->st.bfs_arcs = (int64_t)c.st_barcs;
+  sv->st.dead_deficits = (int64_t)c.st_dseeds;
+  sv->st.dead_kept = c.dkept;
   sv->st.grid_blocks = sv->grid;
   sv->st.block_threads = sv->block;
   sv->st.tile = sv->tile;
@@ -2093,20 +456,21 @@ void stage_copy(int32_t *to, const int32_t *from, size_t count) {
 
 // Copies a host batch into the device staging buffers through pinned memory;
 // each array's H2D starts while the next one is copied.  The solve's start
-// event is recorded before the first H2D (the copies are part of its time).
+// event is recorded behind the last H2D, so the call's device time (last_ms)
+// is the solve alone, as for a batch already on the device; the copies show
+// in the caller's wall-clock time.
 int stage_batch(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w) {
   int st;
   CK(cudaSetDevice(sv->dev), "cudaSetDevice");
   if ((st = ensure_ubuf(sv, k)) || (st = ensure_host_ubuf(sv, k))) return st;
   const size_t K = (size_t)sv->kcap, HK = (size_t)sv->h_kcap;
   const int32_t *from[3] = {src, dst, w};
-  for (int a = 0; a < 3; a++) {
-    if (k > 0) stage_copy(sv->h_ubuf + a * HK, from[a], (size_t)k);
-    if (a == 0) CK(cudaEventRecord(sv->ev0, sv->stream), "event record");
-    if (k > 0)
-      CK(cudaMemcpyAsync(sv->ubuf + a * K, sv->h_ubuf + a * HK, 4 * (size_t)k, cudaMemcpyHostToDevice, sv->stream),
-         "H2D batch");
+  for (int a = 0; a < 3 && k > 0; a++) {
+    stage_copy(sv->h_ubuf + a * HK, from[a], (size_t)k);
+    CK(cudaMemcpyAsync(sv->ubuf + a * K, sv->h_ubuf + a * HK, 4 * (size_t)k, cudaMemcpyHostToDevice, sv->stream),
+       "H2D batch");
   }
+  CK(cudaEventRecord(sv->ev0, sv->stream), "event record");
   return DMF_OK;
 }
 
@@ -2127,7 +491,7 @@ int batch_features(dmf_solver *sv, dmf_sched *sched, int k, float *feat, int *ac
   if (k > 0) {
     const size_t K = (size_t)sv->kcap;
     const int blocks = std::min((k + 255) / 256, 4 * 148);
-    k_features<<<blocks, 256, 0, sv->stream>>>(sv->off, sv->adj, sv->sidx, sv->cap, sv->res, sv->n, k, sv->ubuf,
+    k_features<<<blocks, 256, 0, sv->stream>>>(sv->off, sv->shead, sv->sidx, sv->cap, sv->res, sv->n, k, sv->ubuf,
                                                sv->ubuf + K, sv->ubuf + 2 * K, sv->facc);
     CK(cudaGetLastError(), "feature launch");
   }
@@ -2145,17 +509,14 @@ int batch_features(dmf_solver *sv, dmf_sched *sched, int k, float *feat, int *ac
 // own options are restored afterwards.
 int apply_action(dmf_solver *sv, int action, int k, int64_t *flow) {
   const dmf_opts saved = sv->opts;
-  const int saved_small = sv->small_deg;
   int mode = MODE_DYNAMIC;
   switch (action) {
     case DMF_ACTION_SHORT:
       sv->opts.relabel_interval = 2;
       sv->opts.flags |= DMF_FLAG_FIXED_INTERVAL;
       break;
-    case DMF_ACTION_WARP:
-      sv->opts.relabel_interval = 12;
-      sv->opts.flags |= DMF_FLAG_FIXED_INTERVAL;
-      sv->small_deg = 0;
+    case DMF_ACTION_REVIVE:
+      sv->opts.flags |= DMF_FLAG_REVIVE_DEAD;
       break;
     case DMF_ACTION_RECOMPUTE:
       mode = MODE_RECOMPUTE;
@@ -2166,7 +527,6 @@ int apply_action(dmf_solver *sv, int action, int k, int64_t *flow) {
   const size_t K = (size_t)sv->kcap;
   const int st = run_mode(sv, mode, k, sv->ubuf, sv->ubuf + K, sv->ubuf + 2 * K, flow, true);
   sv->opts = saved;
-  sv->small_deg = saved_small;
   return st;
 }
 
@@ -2220,25 +580,18 @@ constexpr size_t kNoAllocV = (size_t)kNoAllocMaxVertices + 1;
 constexpr size_t kNoAllocBytes = na_round(sizeof(Ctrl)) + na_round(4 * kNoAllocV) /* height */ +
                                  na_round(4 * kNoAllocV) /* stamp */ + na_round(8 * kNoAllocV) /* excess */ +
                                  na_round(kNoAllocV) /* dead */ + na_round(kNoAllocV) /* side */ +
-                                 5 * na_round(4 * kNoAllocV) /* queues */ + 4 * kNoAllocAlign /* unused hub slots */ +
-                                 kNoAllocAlign /* source list */;
+                                 5 * na_round(4 * kNoAllocV) /* queues */ + 4 * kNoAllocAlign /* unused hub slots */;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// Device address of g_noalloc_scratch, looked up once per device (the name is
-// only a host-side stand-in for the array; a kernel must be given this address).
-std::mutex g_noalloc_mu;
-void *g_noalloc_addr[128] = {};
-
-int noalloc_scratch(int dev, unsigned char **out) {
-  if (dev < 0 || dev >= 128) return fail(DMF_ERR_CUDA, "device ordinal %d out of range", dev);
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess || !ptr) return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
-    g_noalloc_addr[dev] = ptr;
-  }
-  *out = (unsigned char *)g_noalloc_addr[dev];
+// Device address of g_noalloc_scratch on the current device (the name is only a
+// host-side stand-in for the array; a kernel must be given this address).  It
+// is looked up on every call: the lookup allocates nothing, and a context that
+// was reset and re-created may have loaded the array at another address.
+int noalloc_scratch(unsigned char **out) {
+  void *ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess || !ptr) return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
+  *out = (unsigned char *)ptr;
   return DMF_OK;
 }
 
@@ -2249,111 +602,115 @@ extern "C" {
 int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, const int32_t *d_adj,
                                const int32_t *d_cap, const int32_t *d_par, int32_t s, int32_t t, int32_t *d_res,
                                int64_t *flow, void *stream) {
-  if (n < 2 || m < 0 || !d_index || !flow || (m > 0 && (!d_adj || !d_cap || !d_par || !d_res)))
-    return fail(DMF_ERR_INVALID_ARG, "bad arguments");
-  if (n > kNoAllocMaxVertices)
-    return fail(DMF_ERR_INVALID_ARG, "n=%d exceeds the %d vertices the allocation-free scratch holds", n,
-                kNoAllocMaxVertices);
-  if (s < 0 || t < 0 || s >= n || t >= n || s == t)
-    return fail(DMF_ERR_INVALID_ARG, "need distinct s, t in [0, n): s=%d t=%d", s, t);
-  int dev = 0;
-  CK(cudaGetDevice(&dev), "cudaGetDevice");
-  unsigned char *base = nullptr;
-  int st = noalloc_scratch(dev, &base);
-  if (st) return st;
-  const int tile = n > 0 && (double)m / n <= 6 ? 4 : (double)m / n <= 12 ? 8 : (double)m / n <= 24 ? 16 : 32;
-  KernelFn fn = pick_kernel(tile, 2);
-  int per_sm = 0, sms = 0, coop = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kBlock, 0), "occupancy");
-  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
-  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "coop attr");
-  if (!coop || per_sm < 1) return fail(DMF_ERR_CUDA, "device does not support cooperative launch of the solver");
-  // carve the scratch
-  size_t off = 0;
-  auto carve = [&](size_t bytes) {
-    unsigned char *q = base + off;
-    off += na_round(bytes);
-    return q;
-  };
-  const size_t N = (size_t)n + 1;
-  Ctrl *ctrl = (Ctrl *)carve(sizeof(Ctrl));
-  Params p{};
-  p.height = (int *)carve(4 * N);
-  p.stamp = (int *)carve(4 * N);
-  p.excess = (long long *)carve(8 * N);
-  p.dead = carve(N);
-  p.side = carve(N);
-  p.fq[0] = (int *)carve(4 * N);
-  p.fq[1] = (int *)carve(4 * N);
-  p.wq[0] = (int *)carve(4 * N);
-  p.wq[1] = (int *)carve(4 * N);
-  p.aq = (int *)carve(4 * N);
-  // no hubs in this mode (hub_deg = INT_MAX): the hub structures are never read
-  int2 *hub_dummy = (int2 *)carve(kNoAllocAlign);
-  long long *ll_dummy = (long long *)carve(kNoAllocAlign);
-  int *int_dummy = (int *)carve(kNoAllocAlign);
-  unsigned long long *mark_dummy = (unsigned long long *)carve(kNoAllocAlign);
-  int *src_list = (int *)carve(kNoAllocAlign);
-  if (off > kNoAllocBytes) return fail(DMF_ERR_CUDA, "internal: scratch layout exceeds the array");
-  p.srcs = src_list;  // one source; filled below by a plain copy (no allocation)
-  p.nsrc = 1;
-  p.role = nullptr;
-  p.inst = nullptr;
-  p.inst_flow = nullptr;
-  p.fh[0] = p.fh[1] = p.wh[0] = p.wh[1] = p.ah = hub_dummy;
-  p.hch = hub_dummy;
-  p.nhch = 0;
-  p.hc_moved = p.hc_alloc = ll_dummy;
-  p.hc_min = p.hc_done = int_dummy;
-  p.hub_base = int_dummy;
-  p.chunk_mark = mark_dummy;
-  p.chunk_tmin = int_dummy;
-  p.n = n;
-  p.m = m;
-  p.s = s;
-  p.t = t;
-  p.off = d_index;
-  p.adj = d_adj;
-  p.par = d_par;
-  p.sidx = nullptr;
-  p.cap = const_cast<int *>(d_cap);  // read only in static mode
-  p.res = d_res;
-  p.astamp = nullptr;
-  p.uarc = nullptr;
-  p.ctrl = ctrl;
-  p.mode = MODE_STATIC;
-  p.variant = DMF_VARIANT_DATA;
-  p.cycles = 2;
-  p.interval = 6;
-  p.max_iters = 100000;
-  p.hub_deg = INT_MAX;
-  p.small_deg = 8;
-  p.bu_alpha = 2;
-  p.need_cut = 0;
-  p.round_base = 1;
-  p.relabel_base = 1;
-  p.epoch = 1;
-  p.trace = nullptr;
-  p.trace_cap = 0;
-  p.probe = 0;
-  cudaStream_t S = (cudaStream_t)stream;
-  // the array keeps the previous call's contents: the control block and the
-  // worklist stamps must start at zero (everything else is written before use)
-  CK(cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), S), "memset control");
-  CK(cudaMemsetAsync(p.stamp, 0, 4 * N, S), "memset stamps");
-  const int32_t src_host = s;
-  CK(cudaMemcpyAsync(src_list, &src_host, sizeof(src_host), cudaMemcpyHostToDevice, S), "H2D source");
-  void *args[] = {&p};
-  CK(cudaLaunchCooperativeKernel((const void *)fn, dim3(per_sm * sms), dim3(kBlock), args, 0, S),
-     "cooperative launch");
-  Ctrl hc;
-  CK(cudaMemcpyAsync(&hc, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, S), "D2H control");
-  CK(cudaStreamSynchronize(S), "solve");
-  if (hc.err & ERR_TIMEOUT) return fail(DMF_ERR_TIMEOUT, "a grid-barrier wait timed out");
-  if (hc.err & ERR_NO_CONV) return fail(DMF_ERR_NO_CONVERGENCE, "no convergence");
-  if (hc.err) return fail(DMF_ERR_CUDA, "device error flags 0x%x", hc.err);
-  *flow = hc.flow;
-  return ok();
+  return guarded([&]() -> int {
+    if (n < 2 || m < 0 || !d_index || !flow || (m > 0 && (!d_adj || !d_cap || !d_par || !d_res)))
+      return fail(DMF_ERR_INVALID_ARG, "bad arguments");
+    if (n > kNoAllocMaxVertices)
+      return fail(DMF_ERR_INVALID_ARG, "n=%d exceeds the %d vertices the allocation-free scratch holds", n,
+                  kNoAllocMaxVertices);
+    if (s < 0 || t < 0 || s >= n || t >= n || s == t)
+      return fail(DMF_ERR_INVALID_ARG, "need distinct s, t in [0, n): s=%d t=%d", s, t);
+    int dev = 0;
+    CK(cudaGetDevice(&dev), "cudaGetDevice");
+    unsigned char *base = nullptr;
+    int st = noalloc_scratch(&base);
+    if (st) return st;
+    const int tile = n > 0 && (double)m / n <= 6 ? 4 : (double)m / n <= 12 ? 8 : (double)m / n <= 24 ? 16 : 32;
+    KernelFn fn = pick_kernel(tile, 2);
+    int per_sm = 0, sms = 0, coop = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kBlock, 0), "occupancy");
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "coop attr");
+    if (!coop || per_sm < 1) return fail(DMF_ERR_CUDA, "device does not support cooperative launch of the solver");
+    // carve the scratch
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+      unsigned char *q = base + off;
+      off += na_round(bytes);
+      return q;
+    };
+    const size_t N = (size_t)n + 1;
+    Ctrl *ctrl = (Ctrl *)carve(sizeof(Ctrl));
+    Params p{};
+    p.height = (int *)carve(4 * N);
+    p.stamp = (int *)carve(4 * N);
+    p.excess = (long long *)carve(8 * N);
+    p.dead = carve(N);
+    p.side = carve(N);
+    p.fq[0] = (int *)carve(4 * N);
+    p.fq[1] = (int *)carve(4 * N);
+    p.wq[0] = (int *)carve(4 * N);
+    p.wq[1] = (int *)carve(4 * N);
+    p.aq = (int *)carve(4 * N);
+    p.dq = nullptr;  // static solves never keep a dead set
+    // no hubs in this mode (hub_deg = INT_MAX): the hub structures are never read
+    int2 *hub_dummy = (int2 *)carve(kNoAllocAlign);
+    long long *ll_dummy = (long long *)carve(kNoAllocAlign);
+    int *int_dummy = (int *)carve(kNoAllocAlign);
+    unsigned long long *mark_dummy = (unsigned long long *)carve(kNoAllocAlign);
+    if (off > kNoAllocBytes) return fail(DMF_ERR_CUDA, "internal: scratch layout exceeds the array");
+    p.srcs = nullptr;  // one source: the kernel takes it from p.s
+    p.nsrc = 1;
+    p.role = nullptr;
+    p.inst = nullptr;
+    p.inst_flow = nullptr;
+    p.fh[0] = p.fh[1] = p.wh[0] = p.wh[1] = p.ah = hub_dummy;
+    p.hch = hub_dummy;
+    p.nhch = 0;
+    p.hc_moved = p.hc_alloc = ll_dummy;
+    p.hc_min = p.hc_done = int_dummy;
+    p.hub_base = int_dummy;
+    p.chunk_mark = mark_dummy;
+    p.chunk_tmin = int_dummy;
+    p.n = n;
+    p.m = m;
+    p.s = s;
+    p.t = t;
+    p.off = d_index;
+    p.adj = d_adj;
+    p.par = d_par;
+    p.sidx = nullptr;
+    p.shead = nullptr;
+    p.cap = const_cast<int *>(d_cap);  // read only in static mode
+    p.res = d_res;
+    p.astamp = nullptr;
+    p.uarc = nullptr;
+    p.ctrl = ctrl;
+    p.mode = MODE_STATIC;
+    p.variant = DMF_VARIANT_DATA;
+    p.cycles = 2;
+    p.interval = 6;
+    p.max_iters = 100000;
+    p.hub_deg = INT_MAX;
+    p.small_deg = 8;
+    p.bu_alpha = 2;
+    p.need_cut = 0;
+    p.keep_dead = 0;
+    p.barrier_ns = kBarrierTimeoutNs;
+    p.absent_block = -1;
+    p.round_base = 1;
+    p.relabel_base = 1;
+    p.epoch = 1;
+    p.trace = nullptr;
+    p.trace_cap = 0;
+    p.probe = 0;
+    cudaStream_t S = (cudaStream_t)stream;
+    // the array keeps the previous call's contents: the control block and the
+    // worklist stamps must start at zero (everything else is written before use)
+    CK(cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), S), "memset control");
+    CK(cudaMemsetAsync(p.stamp, 0, 4 * N, S), "memset stamps");
+    void *args[] = {&p};
+    CK(cudaLaunchCooperativeKernel((const void *)fn, dim3(per_sm * sms), dim3(kBlock), args, 0, S),
+       "cooperative launch");
+    Ctrl hc;
+    CK(cudaMemcpyAsync(&hc, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, S), "D2H control");
+    CK(cudaStreamSynchronize(S), "solve");
+    if (hc.err & ERR_TIMEOUT) return fail(DMF_ERR_TIMEOUT, "a grid-barrier wait timed out");
+    if (hc.err & ERR_NO_CONV) return fail(DMF_ERR_NO_CONVERGENCE, "no convergence");
+    if (hc.err) return fail(DMF_ERR_CUDA, "device error flags 0x%x", hc.err);
+    *flow = hc.flow;
+    return ok();
+  });
 }
 
 int dmf_device_count(void) {
@@ -2426,10 +783,11 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   if ((st = configure(sv))) return st;
   const size_t N = (size_t)g->n + 1, M = (size_t)g->m;
   if ((st = dalloc(sv, &sv->off, N)) || (st = dalloc(sv, &sv->adj, M)) || (st = dalloc(sv, &sv->par, M)) ||
-      (st = dalloc(sv, &sv->sidx, M)) || (st = dalloc(sv, &sv->cap, M)) || (st = dalloc(sv, &sv->res, M)) ||
+      (st = dalloc(sv, &sv->sidx, M)) || (st = dalloc(sv, &sv->shead, M)) || (st = dalloc(sv, &sv->cap, M)) ||
+      (st = dalloc(sv, &sv->res, M)) ||
       (st = dalloc(sv, &sv->astamp, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
       (st = dalloc(sv, &sv->excess, N)) || (st = dalloc(sv, &sv->dead, N)) || (st = dalloc(sv, &sv->side, N)) ||
-      (st = dalloc(sv, &sv->qbuf, 5 * N)) || (st = dalloc(sv, &sv->ctrl, 1)))
+      (st = dalloc(sv, &sv->qbuf, 6 * N)) || (st = dalloc(sv, &sv->ctrl, 1)))
     return st;
   std::vector<int2> hub_chunks;
   std::vector<int> hub_base(g->n, -1);
@@ -2457,6 +815,10 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   up(sv->adj, g->adj.data(), 4 * M);
   up(sv->par, g->par.data(), 4 * M);
   up(sv->sidx, g->sidx.data(), 4 * M);
+  std::vector<int32_t> shead(M);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)M; i++) shead[i] = g->adj[g->sidx[i]];
+  up(sv->shead, shead.data(), 4 * M);
   up(sv->cap, g->w.data(), 4 * M);
   up(sv->hch, hub_chunks.data(), sizeof(int2) * hub_chunks.size());
   up(sv->hub_base, hub_base.data(), 4 * (size_t)g->n);

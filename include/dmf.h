@@ -61,6 +61,14 @@ typedef enum {
 /* dmf_opts.flags bits */
 #define DMF_FLAG_TRACE 1 /* record a per-phase device timeline (dmf_trace_get) */
 #define DMF_FLAG_PROBE 2 /* with TRACE: also time every work item (dmf_trace_items) */
+#define DMF_FLAG_REVIVE_DEAD 8 /* batches revive every vertex at their first global relabel
+                                  instead of keeping the dead set of the last solve */
+#define DMF_FLAG_TEST_BARRIER_TIMEOUT 16 /* failure-injection hook for tests: one block of
+                                  the persistent grid leaves at once and never arrives
+                                  at a grid barrier, and the barrier wait limit drops
+                                  from 4 s to 20 ms, so the call returns
+                                  DMF_ERR_TIMEOUT (every wait stays bounded; the
+                                  next call without the flag solves normally) */
 #define DMF_FLAG_FIXED_INTERVAL 4 /* exactly relabel_interval push rounds per global relabel
                                      (default: at least the depth of the last relabel BFS) */
 
@@ -95,11 +103,18 @@ typedef struct {
   int64_t arcs_scanned;     /* adjacency entries read in the last solve */
   int64_t vertices_visited; /* vertex visits (BFS + push) in the last solve */
   int64_t dead_vertices;    /* vertices proven unable to reach t or a deficit */
-  double last_ms;           /* device time of the last solve call (CUDA events) */
+  double last_ms;           /* device time of the last solve call (CUDA events), from
+                               the batch on the device to the result (host-array
+                               calls: the H2D of the batch is not included) */
   int32_t grid_blocks;      /* persistent-kernel grid */
   int32_t block_threads;
   int32_t tile;
   int32_t pad;
+  int64_t bfs_arcs;         /* adjacency entries read by global-relabel BFS levels
+                               (included in arcs_scanned) */
+  int64_t dead_deficits;    /* deficits a batch left inside the kept dead set */
+  int32_t dead_kept;        /* 1: the batch kept the dead set of the last solve */
+  int32_t pad2;
 } dmf_stats;
 
 /* ---- errors and options ------------------------------------------------- */
@@ -313,10 +328,10 @@ int dmf_autotune(dmf_solver *sv, int32_t repeats, dmf_opts *chosen);
 #define DMF_SCHED_WEIGHTS 5120 /* bf16: W1[64][12], W2[64][64], W3[4][64] (row = output unit) */
 #define DMF_SCHED_BIASES 132   /* fp32: b1[64], b2[64], b3[4] */
 /* actions */
-#define DMF_ACTION_PLAIN 0       /* incremental repair, engine defaults */
+#define DMF_ACTION_PLAIN 0       /* incremental repair, engine defaults (dead set kept) */
 #define DMF_ACTION_SHORT 1       /* incremental, global relabel every 2 push rounds */
-#define DMF_ACTION_WARP 2        /* incremental, every non-hub vertex by a tile (no
-                                    thread-per-vertex tier), 12 rounds per relabel */
+#define DMF_ACTION_REVIVE 2      /* incremental, every vertex revived at the batch's first
+                                    global relabel (DMF_FLAG_REVIVE_DEAD) */
 #define DMF_ACTION_RECOMPUTE 3   /* set the capacities and solve from scratch */
 
 typedef struct dmf_sched dmf_sched; /* MLP 12-64-64-4, bf16 weights, fp32 accumulation */
@@ -375,10 +390,13 @@ int dmf_solver_copy_state(dmf_solver *dst, const dmf_solver *src);
  * other scratch lives in one static device array inside the library, sized for
  * n <= 262144 vertices (about 10 MiB, held by every GPU that loads the library
  * until the process exits); larger n is rejected with DMF_ERR_INVALID_ARG.
- * The first call on a device looks up that array's device address (so make it
- * before any stream capture).  Calls share the array: calls that overlap on the
- * GPU race and give wrong results, so serialise them.  The call waits for the
- * result on `stream` (a cudaStream_t, NULL = legacy default stream). */
+ * Every call looks up the array's device address on the current device (the
+ * lookup allocates nothing, and stays right if the context was reset).  Calls
+ * share the array and each clears what must start at zero: calls that overlap
+ * on the GPU race and give wrong results, so serialise them.  The call blocks
+ * until the result is back: it waits for `stream` (a cudaStream_t, NULL =
+ * legacy default stream), so work queued on it before the call is waited for
+ * too. */
 int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index,
                                const int32_t *d_adj, const int32_t *d_cap,
                                const int32_t *d_par, int32_t s, int32_t t,

@@ -23,7 +23,7 @@ def test_constants_match_header(dmf):
     assert d["DMF_SCHED_ACTIONS"] == dmf.N_ACTIONS == len(dmf.ACTIONS) == 4
     assert d["DMF_SCHED_WEIGHTS"] == dmf.N_WEIGHTS == 64 * 12 + 64 * 64 + 4 * 64
     assert d["DMF_SCHED_BIASES"] == dmf.N_BIASES == 64 + 64 + 4
-    assert [d["DMF_ACTION_PLAIN"], d["DMF_ACTION_SHORT"], d["DMF_ACTION_WARP"], d["DMF_ACTION_RECOMPUTE"]] == [0, 1, 2, 3]
+    assert [d["DMF_ACTION_PLAIN"], d["DMF_ACTION_SHORT"], d["DMF_ACTION_REVIVE"], d["DMF_ACTION_RECOMPUTE"]] == [0, 1, 2, 3]
     from dyn_maxflow_b200 import sched
     assert len(sched.FEATURE_NAMES) == dmf.N_FEATURES
 
