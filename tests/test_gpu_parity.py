@@ -106,6 +106,33 @@ def test_rmat_successive_batches(dmf, oracle, name, variant):
         assert sv.recompute() == want
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("name", ["rmat14", "grid256", "rmat16"])
+def test_kept_dead_set_matches_revived(dmf, oracle, name, variant):
+    """Batches keep the dead set of the last solve (the deficits a batch leaves
+    inside it are covered there); every flow equals Dinic and the flow of a
+    solver that revives every vertex at each batch, and every kept state is
+    certified."""
+    g, s, t, batches = make_config(name)
+    if name == "grid256":  # more than the one configured batch
+        batches = batches + dmf.gen_batches(g, 4, frac=0.01, p_inc=0.4, p_dec=0.4, p_ins=0.0, delta_hi=50, seed=7)
+    off, adj, w, par = g.arrays()
+    n = g.num_nodes()
+    cur = w.copy()
+    kept_batches = 0
+    with dmf.Solver(g, s, t, variant=variant) as kept, dmf.Solver(g, s, t, variant=variant, revive_dead=True) as rev:
+        assert kept.static_maxflow() == rev.static_maxflow()
+        for b in batches:
+            apply_host(g, cur, b)
+            want = oracle.dinic(n, off, adj, cur, par, s, t)
+            assert kept.apply_updates(*b) == want
+            assert rev.apply_updates(*b) == want
+            kept_batches += kept.stats()["dead_kept"]
+            assert rev.stats()["dead_kept"] == 0
+            certify(oracle, g, kept, s, t, want)
+    assert kept_batches > 0
+
+
 @pytest.mark.parametrize("tile", [4, 8, 16, 32])
 def test_tile_sizes_agree(dmf, oracle, tile):
     g, s, t, batches = make_config("rmat12")
