@@ -109,6 +109,7 @@ _sig("dmf_multi_run_batches", C.c_int, VP, C.c_int32, I64P, VP, VP, VP, C.c_int3
 _sig("dmf_autotune", C.c_int, VP, C.c_int32, C.POINTER(Opts))
 _sig("dmf_server_create", C.c_int, C.c_int32, C.POINTER(C.c_void_p), I32P, I32P, C.c_int64, C.POINTER(Opts), PP)
 _sig("dmf_server_info", C.c_int, VP, C.POINTER(C.c_int32), C.POINTER(C.c_int64))
+_sig("dmf_server_lane", C.c_int, VP, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32))
 _sig("dmf_server_submit", C.c_int, VP, C.c_int32, C.c_int32, I32P, I32P, I32P, C.POINTER(C.c_int64))
 _sig("dmf_server_wait", C.c_int, VP, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double))
 _sig("dmf_server_stats", C.c_int, VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_double))
@@ -634,6 +635,12 @@ class Server:
         a, b, c = C.c_int64(), C.c_int64(), C.c_double()
         _check(_L.dmf_server_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return {"ticks": a.value, "served": b.value, "mean_requests_per_tick": c.value}
+
+    def lane(self, graph: int) -> dict:
+        """dmf_server_lane: the lane serving `graph` and its share of resident blocks."""
+        ln, lns, gb = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(_L.dmf_server_lane(self._h, graph, C.byref(ln), C.byref(lns), C.byref(gb)))
+        return {"lane": ln.value, "lanes": lns.value, "grid_blocks": gb.value}
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

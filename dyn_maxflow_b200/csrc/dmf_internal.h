@@ -57,4 +57,8 @@ int64_t find_arc(const dmf_graph &g, int32_t src, int32_t dst);
 int build_from_edges(int64_t k, const int32_t *u, const int32_t *v,
                      const int32_t *w, dmf_graph **out);
 
+// Blocks of the persistent solve kernel that the current device holds at once
+// (the grid of a solver without a grid_blocks cap).
+int resident_solve_blocks(int32_t *blocks);
+
 }  // namespace dmf

@@ -5,14 +5,24 @@
 // stays resident for the server's life, and every batch a request carries is
 // applied to it (successive batches per graph, in submission order).
 //
-// Continuous batching: all admitted graphs live in one batched-instance solver
-// (dmf_multi_*).  A worker thread runs ticks; a tick takes, for every graph,
-// its oldest waiting request (while the tick's batch stays inside the staging
-// budget) and serves them all with one persistent launch, which relabels and
-// pushes only inside the touched graphs.  Requests that arrive during a tick
-// join the next one.  Instances are independent, so each result equals the
-// result of the same request sequence served alone.  No counterpart in the
-// reference (a one-shot bench).
+// Lanes (continuous batching over device slots): the admitted graphs are split
+// into lanes.  A graph with at least a quarter of the admitted arcs gets a lane
+// of its own (at most kMaxLanes - 1 such lanes); the others share one lane whose
+// graphs live in one batched-instance solver (dmf_multi_*).  Every lane has its
+// own solver, CUDA stream, worker thread and a fixed share of the persistent
+// grid (dmf_opts.grid_blocks), in proportion to its arcs.  The shares add up to
+// at most the blocks the GPU holds at once (every solve kernel is launched for
+// 2 blocks of 512 threads per SM, which fill its register file), so the lanes'
+// cooperative launches are always resident together and never wait for one
+// another: a request for a small graph is served while a large graph's solve is
+// in flight, not after it.  A lane's worker runs ticks: it takes the oldest
+// waiting request of each of its graphs, while the tick's updates fit the
+// lane's staging budget, and serves them with one launch; requests arriving
+// meanwhile join its next tick.  Instances are independent, so each result
+// equals the result of the same request sequence served alone.  No counterpart
+// in the reference (a one-shot bench).
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <climits>
 #include <parallel/algorithm>
@@ -24,6 +34,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <numeric>
 #include <thread>
 #include <vector>
 
@@ -34,6 +45,8 @@ using dmf::guarded;
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+constexpr int kMaxLanes = 4;
 
 struct Request {
   int64_t ticket;
@@ -48,25 +61,37 @@ struct Request {
   double latency_ms = 0;
 };
 
+struct Lane {
+  std::vector<int32_t> graphs;  // server graph ids, in instance order
+  bool multi = false;           // batched-instance solver (else one graph, plain solver)
+  dmf_solver *sv = nullptr;
+  cudaStream_t stream = nullptr;
+  int32_t grid_blocks = 0;
+  int64_t stage_budget = 0;
+  std::condition_variable cv_work;
+  std::thread worker;
+  // worker-owned, reused from tick to tick (they grow, never shrink)
+  std::vector<Request *> batch;
+  std::vector<int64_t> flows;
+  std::vector<int32_t> I, A, B, W;
+};
+
 }  // namespace
 
 struct dmf_server {
   std::vector<const dmf_graph *> graphs;  // admitted (borrowed; caller keeps them alive)
   std::vector<int32_t> s, t;
-  int64_t budget = 0, device_bytes = 0, stage_budget = 0;
-  dmf_solver *sv = nullptr;
+  int64_t budget = 0, device_bytes = 0;
+  std::vector<std::unique_ptr<Lane>> lanes;
+  std::vector<int32_t> lane_of, inst_of;  // per graph: its lane and its instance in the lane
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
+  std::condition_variable cv_done;
   std::vector<std::deque<Request *>> pending;  // per graph, FIFO
   std::map<int64_t, Request *> all;
   int64_t next_ticket = 1;
-  bool stop = false;  // destroy(): serve what is pending, then end the worker
+  bool stop = false;  // destroy(): serve what is pending, then end the workers
   int waiters = 0;    // threads inside wait()
-  std::thread worker;
   int64_t ticks = 0, served = 0, batched_sum = 0;
-  // worker-owned staging, sized at create so a tick's selection never allocates
-  std::vector<Request *> batch;
-  std::vector<int64_t> flows;
 };
 
 static int64_t footprint(const dmf_graph *g) {
@@ -74,43 +99,50 @@ static int64_t footprint(const dmf_graph *g) {
   return 28LL * g->m + 64LL * g->n;
 }
 
-static void tick_loop(dmf_server *S) {
-  const int G = (int)S->graphs.size();
-  std::vector<Request *> &batch = S->batch;
+static void tick_loop(dmf_server *S, Lane *L) {
+  std::vector<Request *> &batch = L->batch;
   for (;;) {
-    batch.clear();  // capacity G: the selection below never allocates
+    batch.clear();  // capacity = the lane's graphs: the selection below never allocates
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      S->cv_work.wait(lk, [&] {
+      L->cv_work.wait(lk, [&] {
         if (S->stop) return true;
-        for (auto &q : S->pending)
-          if (!q.empty()) return true;
+        for (int32_t g : L->graphs)
+          if (!S->pending[g].empty()) return true;
         return false;
       });
       int64_t bytes = 0;
-      for (int g = 0; g < G; g++) {
+      for (int32_t g : L->graphs) {
         if (S->pending[g].empty()) continue;
         Request *r = S->pending[g].front();
         const int64_t b = 16LL * (int64_t)r->src.size();
-        if (!batch.empty() && bytes + b > S->stage_budget) continue;  // waits for the next tick
+        if (!batch.empty() && bytes + b > L->stage_budget) continue;  // waits for the next tick
         bytes += b;
         S->pending[g].pop_front();
         batch.push_back(r);
       }
       if (batch.empty()) return;  // stopping, and every submitted request is served
     }
-    // a failure here (staging allocation included) fails this tick's requests
-    // and leaves the worker running
+    // a failure here (staging growth included) fails this tick's requests and
+    // leaves the worker running
     int st = guarded([&]() -> int {
-      std::vector<int32_t> I, A, B, W;
-      for (Request *r : batch) {
-        I.insert(I.end(), r->src.size(), r->graph);
-        A.insert(A.end(), r->src.begin(), r->src.end());
-        B.insert(B.end(), r->dst.begin(), r->dst.end());
-        W.insert(W.end(), r->w.begin(), r->w.end());
+      if (!L->multi) {
+        Request *r = batch[0];
+        return dmf_apply_updates(L->sv, (int32_t)r->src.size(), r->src.data(), r->dst.data(), r->w.data(),
+                                 &L->flows[0]);
       }
-      return dmf_multi_apply_updates(S->sv, (int32_t)A.size(), I.data(), A.data(), B.data(), W.data(),
-                                     S->flows.data());
+      L->I.clear();
+      L->A.clear();
+      L->B.clear();
+      L->W.clear();
+      for (Request *r : batch) {
+        L->I.insert(L->I.end(), r->src.size(), S->inst_of[r->graph]);
+        L->A.insert(L->A.end(), r->src.begin(), r->src.end());
+        L->B.insert(L->B.end(), r->dst.begin(), r->dst.end());
+        L->W.insert(L->W.end(), r->w.begin(), r->w.end());
+      }
+      return dmf_multi_apply_updates(L->sv, (int32_t)L->A.size(), L->I.data(), L->A.data(), L->B.data(),
+                                     L->W.data(), L->flows.data());
     });
     const char *err = st ? dmf_last_error() : "";
     const auto now = Clock::now();
@@ -123,7 +155,7 @@ static void tick_loop(dmf_server *S) {
         } catch (...) {
           // the status alone reaches the waiter
         }
-        r->flow = S->flows[r->graph];
+        r->flow = L->flows[L->multi ? S->inst_of[r->graph] : 0];
         r->latency_ms = std::chrono::duration<double, std::milli>(now - r->t_submit).count();
         r->done = true;
       }
@@ -133,6 +165,75 @@ static void tick_loop(dmf_server *S) {
     }
     S->cv_done.notify_all();
   }
+}
+
+// Splits the admitted graphs into lanes and gives each its share of `grid`
+// resident blocks (see the file comment).
+static void plan_lanes(dmf_server *S, int32_t grid) {
+  const int G = (int)S->graphs.size();
+  int64_t total = 0;
+  for (const dmf_graph *g : S->graphs) total += g->m;
+  std::vector<int32_t> order(G);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return S->graphs[a]->m > S->graphs[b]->m; });
+  std::vector<std::vector<int32_t>> parts;
+  std::vector<int32_t> rest;
+  for (int32_t g : order) {
+    const bool own = (int)parts.size() < kMaxLanes - 1 && 4 * (int64_t)S->graphs[g]->m >= total;
+    if (own) parts.push_back({g});
+    else rest.push_back(g);
+  }
+  if (!rest.empty()) {
+    std::sort(rest.begin(), rest.end());
+    parts.push_back(rest);
+  }
+  S->lane_of.assign(G, 0);
+  S->inst_of.assign(G, 0);
+  std::vector<int64_t> weight;
+  for (size_t l = 0; l < parts.size(); l++) {
+    std::unique_ptr<Lane> L(new Lane());
+    L->graphs = parts[l];
+    L->multi = parts[l].size() > 1;
+    int64_t w = 1;
+    for (size_t i = 0; i < parts[l].size(); i++) {
+      S->lane_of[parts[l][i]] = (int32_t)l;
+      S->inst_of[parts[l][i]] = (int32_t)i;
+      w += S->graphs[parts[l][i]]->m;
+    }
+    weight.push_back(w);
+    L->batch.reserve(parts[l].size());
+    L->flows.resize(parts[l].size());
+    S->lanes.push_back(std::move(L));
+  }
+  // shares in proportion to the arcs, at least 1/16 of the grid each, summing to <= grid
+  const int nl = (int)S->lanes.size();
+  const int32_t floor_share = std::max<int32_t>(1, grid / 16);
+  int64_t wsum = 0;
+  for (int64_t w : weight) wsum += w;
+  int32_t used = 0;
+  for (int l = 0; l < nl; l++) {
+    const int32_t share = nl == 1 ? grid : std::max<int32_t>(floor_share, (int32_t)((__int128)grid * weight[l] / wsum));
+    S->lanes[l]->grid_blocks = share;
+    used += share;
+  }
+  while (used > grid) {  // take the excess from the largest shares
+    auto it = std::max_element(S->lanes.begin(), S->lanes.end(),
+                               [](const std::unique_ptr<Lane> &a, const std::unique_ptr<Lane> &b) {
+                                 return a->grid_blocks < b->grid_blocks;
+                               });
+    (*it)->grid_blocks--;
+    used--;
+  }
+  const int64_t spare = std::max<int64_t>(S->budget - S->device_bytes, 0);
+  for (auto &L : S->lanes) L->stage_budget = std::max<int64_t>(spare / nl, 16LL << 20);
+}
+
+static void free_server(dmf_server *S) {
+  for (auto &L : S->lanes) {
+    if (L->sv) dmf_solver_destroy(L->sv);
+    if (L->stream) cudaStreamDestroy(L->stream);
+  }
+  delete S;
 }
 
 extern "C" {
@@ -157,23 +258,55 @@ int dmf_server_create(int32_t count, const dmf_graph *const *graphs, const int32
     }
     if (S->graphs.empty())
       return dmf::fail(DMF_ERR_OOM, "no graph fits the HBM budget of %lld bytes", (long long)hbm_budget);
-    S->stage_budget = std::max<int64_t>(hbm_budget - S->device_bytes, 16LL << 20);
-    const size_t G = S->graphs.size();
-    S->pending.resize(G);
-    S->batch.reserve(G);
-    S->flows.resize(G);
-    int rc = dmf_multi_create((int32_t)G, S->graphs.data(), S->s.data(), S->t.data(), opts, nullptr, &S->sv);
-    if (rc) return rc;
-    if ((rc = dmf_multi_static_maxflow(S->sv, S->flows.data()))) return rc;
-    S->worker = std::thread(tick_loop, S);
+    S->pending.resize(S->graphs.size());
+    dmf_opts o;
+    if (opts) o = *opts;
+    else dmf_opts_default(&o);
+    if (o.device >= 0 && cudaSetDevice(o.device) != cudaSuccess)
+      return dmf::fail(DMF_ERR_CUDA, "cudaSetDevice(%d) failed", o.device);
+    int32_t grid = 0;  // the blocks the GPU holds at once
+    if (int rc = dmf::resident_solve_blocks(&grid)) return rc;
+    const int32_t cap = o.grid_blocks > 0 ? std::min(o.grid_blocks, grid) : grid;
+    plan_lanes(S, cap);
+    for (auto &L : S->lanes) {
+      if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return dmf::fail(DMF_ERR_CUDA, "cudaStreamCreate failed");
+      dmf_opts lo = o;
+      lo.grid_blocks = L->grid_blocks;
+      int rc;
+      if (L->multi) {
+        std::vector<const dmf_graph *> gs;
+        std::vector<int32_t> ss, ts;
+        for (int32_t g : L->graphs) {
+          gs.push_back(S->graphs[g]);
+          ss.push_back(S->s[g]);
+          ts.push_back(S->t[g]);
+        }
+        rc = dmf_multi_create((int32_t)gs.size(), gs.data(), ss.data(), ts.data(), &lo, L->stream, &L->sv);
+        if (!rc) rc = dmf_multi_static_maxflow(L->sv, L->flows.data());
+      } else {
+        const int32_t g = L->graphs[0];
+        rc = dmf_solver_create(S->graphs[g], S->s[g], S->t[g], &lo, L->stream, &L->sv);
+        if (!rc) rc = dmf_static_maxflow(L->sv, &L->flows[0]);
+      }
+      if (rc) return rc;
+    }
+    for (auto &L : S->lanes) L->worker = std::thread(tick_loop, S, L.get());
     return dmf::ok();
   });
   if (st) {
     if (S) {
       char msg[1024];
       std::snprintf(msg, sizeof msg, "%s", dmf_last_error());
-      dmf_solver_destroy(S->sv);
-      delete S;
+      {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+      }
+      for (auto &L : S->lanes) {
+        L->cv_work.notify_all();
+        if (L->worker.joinable()) L->worker.join();
+      }
+      free_server(S);
       dmf::fail(st, "%s", msg);
     }
     return st;
@@ -186,6 +319,17 @@ int dmf_server_info(const dmf_server *S, int32_t *admitted, int64_t *device_byte
   if (!S) return dmf::fail(DMF_ERR_INVALID_ARG, "null server");
   if (admitted) *admitted = (int32_t)S->graphs.size();
   if (device_bytes) *device_bytes = S->device_bytes;
+  return dmf::ok();
+}
+
+int dmf_server_lane(const dmf_server *S, int32_t graph, int32_t *lane, int32_t *lanes, int32_t *grid_blocks) {
+  if (!S) return dmf::fail(DMF_ERR_INVALID_ARG, "null server");
+  if (graph < 0 || graph >= (int32_t)S->graphs.size())
+    return dmf::fail(DMF_ERR_INVALID_ARG, "graph %d was not admitted", graph);
+  const int32_t l = S->lane_of[graph];
+  if (lane) *lane = l;
+  if (lanes) *lanes = (int32_t)S->lanes.size();
+  if (grid_blocks) *grid_blocks = S->lanes[l]->grid_blocks;
   return dmf::ok();
 }
 
@@ -250,7 +394,7 @@ int dmf_server_submit(dmf_server *S, int32_t graph, int32_t k, const int32_t *sr
       *ticket = tk;
       r.release();  // owned by the server until its wait() returns
     }
-    S->cv_work.notify_one();
+    S->lanes[S->lane_of[graph]]->cv_work.notify_one();
     return dmf::ok();
   });
 }
@@ -293,17 +437,17 @@ int dmf_server_destroy(dmf_server *S) {
     std::lock_guard<std::mutex> lk(S->mu);
     S->stop = true;
   }
-  S->cv_work.notify_all();
-  // the worker serves every request already submitted before it ends, so a
+  // the workers serve every request already submitted before they end, so a
   // thread blocked in wait() gets its result; no call may start after this one
-  if (S->worker.joinable()) S->worker.join();
+  for (auto &L : S->lanes) L->cv_work.notify_all();
+  for (auto &L : S->lanes)
+    if (L->worker.joinable()) L->worker.join();
   {
     std::unique_lock<std::mutex> lk(S->mu);
     S->cv_done.wait(lk, [&] { return S->waiters == 0; });
   }
   for (auto &kv : S->all) delete kv.second;  // served, never waited on
-  dmf_solver_destroy(S->sv);
-  delete S;
+  free_server(S);
   return dmf::ok();
 }
 

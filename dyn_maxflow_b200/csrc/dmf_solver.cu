@@ -875,6 +875,16 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
 
 }  // namespace
 
+int dmf::resident_solve_blocks(int32_t *blocks) {
+  int dev = 0, per_sm = 0, sms = 0;
+  CK(cudaGetDevice(&dev), "cudaGetDevice");
+  // every instantiation has the same launch bounds (kBlock threads, 2 blocks per SM)
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)pick_kernel(32, 2), kBlock, 0), "occupancy");
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+  *blocks = per_sm * sms;
+  return DMF_OK;
+}
+
 extern "C" {
 
 int dmf_solver_create(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, void *stream,

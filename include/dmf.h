@@ -280,11 +280,17 @@ int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs,
  * (28 B per arc + 64 B per vertex) fits `hbm_budget` bytes; the rest are not
  * admitted (ids of admitted graphs are their positions among the admitted ones,
  * dmf_server_info).  The caller keeps the graphs alive until destroy.
- * Continuous batching: a worker thread serves, per tick, the oldest waiting
- * request of every graph with one persistent launch (dmf_multi_apply_updates),
- * while the tick's batch stays inside the staging budget (what the graphs leave
- * of hbm_budget, at least 16 MiB); requests arriving during a tick join the
- * next.  Batches of one graph apply in submission order.  submit() validates a
+ * Lanes: a graph with at least a quarter of the admitted arcs gets a lane of
+ * its own (at most 3 such lanes), the others share one lane.  Each lane has
+ * its own solver, CUDA stream and worker thread, and a fixed share of the
+ * GPU's resident solve blocks (in proportion to its arcs; `opts->grid_blocks`,
+ * when > 0, caps the total), so the lanes' launches run side by side: a
+ * request for a small graph is served while a large graph's solve is in flight.
+ * Continuous batching within a lane: its worker serves, per tick, the oldest
+ * waiting request of each of its graphs with one persistent launch, while the
+ * tick's updates stay inside the lane's staging budget (its share of what the
+ * graphs leave of hbm_budget, at least 16 MiB); requests arriving during a tick
+ * join the next.  Batches of one graph apply in submission order.  submit() validates a
  * request on the host (vertex ranges, existing arcs, no repeats) and copies it;
  * wait() blocks until it is served and returns the graph's exact max-flow after
  * it and its latency from the start of its submit() call (validation
@@ -298,6 +304,10 @@ int dmf_server_create(int32_t count, const dmf_graph *const *graphs,
                       const int32_t *s, const int32_t *t, int64_t hbm_budget,
                       const dmf_opts *opts, dmf_server **out);
 int dmf_server_info(const dmf_server *srv, int32_t *admitted, int64_t *device_bytes);
+/* The lane that serves admitted graph `graph`, the number of lanes, and that
+ * lane's share of resident solve blocks (any output may be NULL). */
+int dmf_server_lane(const dmf_server *srv, int32_t graph, int32_t *lane, int32_t *lanes,
+                    int32_t *grid_blocks);
 int dmf_server_submit(dmf_server *srv, int32_t graph, int32_t k, const int32_t *src,
                       const int32_t *dst, const int32_t *w, int64_t *ticket);
 int dmf_server_wait(dmf_server *srv, int64_t ticket, int64_t *flow, double *latency_ms);

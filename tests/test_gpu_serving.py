@@ -186,3 +186,48 @@ def make_config_rmat14_one():
     g, s, t = D.gen_rmat(14, narcs, 0.57, 0.19, 0.19, seed=0, cap_lo=1, cap_hi=1000, reserve=narcs // 50)
     b = D.gen_batches(g, 1, frac=0.08, p_inc=0.4, p_dec=0.4, p_ins=0.1, delta_hi=500, ins_lo=1, ins_hi=1000, seed=3)
     return g, s, t, b
+
+
+def test_small_request_overlaps_large_one(dmf, oracle):
+    """A graph with most of the arcs gets a lane of its own; a request for a small
+    graph, submitted while a large request (1M updates) is in flight on it, is
+    served on the other lane and completes first, with the flow it has alone."""
+    import dyn_maxflow_b200 as D
+    narcs = 16 << 18
+    big, bs, bt = D.gen_rmat(18, narcs, 0.57, 0.19, 0.19, seed=5, cap_lo=1, cap_hi=1000, reserve=narcs // 100)
+    positive = int((big.arrays()[2] > 0).sum())
+    (bb,) = D.gen_batches(big, 1, frac=min(0.5, 1_050_000 / positive), p_inc=0.4, p_dec=0.4, p_ins=0.0,
+                          delta_hi=500, seed=6)
+    assert len(bb[0]) >= 1_000_000
+    inst = _graphs(dmf)
+    graphs = [big] + [x[0] for x in inst]
+    S, T = [bs] + [x[1] for x in inst], [bt] + [x[2] for x in inst]
+    # alone
+    with dmf.Solver(big, bs, bt) as sv:
+        sv.static_maxflow()
+        capacity = sv.stats()["grid_blocks"]  # resident blocks of an uncapped solver
+        want_big = sv.apply_updates(*bb)
+    g1, s1, t1, b1 = inst[0]
+    with dmf.Solver(g1, s1, t1) as sv:
+        sv.static_maxflow()
+        want_small = sv.apply_updates(*b1[0])
+    off, adj, w, par = g1.arrays()
+    cur = w.copy()
+    for a, c, x in zip(*b1[0]):
+        if a != c:
+            cur[g1.find_arc(int(a), int(c))] = x
+    assert want_small == oracle.dinic(g1.num_nodes(), off, adj, cur, par, s1, t1)
+    with dmf.Server(graphs, S, T, 1 << 36) as srv:
+        lb, ls = srv.lane(0), srv.lane(1)
+        assert lb["lanes"] == 2 and lb["lane"] != ls["lane"]
+        assert lb["grid_blocks"] + ls["grid_blocks"] <= capacity
+        t0 = time.perf_counter()
+        tk_big = srv.submit(0, *bb)
+        t1_ = time.perf_counter()
+        tk_small = srv.submit(1, *b1[0])
+        f_small, lat_small = srv.wait(tk_small)
+        f_big, lat_big = srv.wait(tk_big)
+    assert f_small == want_small and f_big == want_big
+    # completion times from the first submit: the small request finished first
+    done_small = (t1_ - t0) * 1e3 + lat_small
+    assert done_small < lat_big, (done_small, lat_big)
