@@ -1,23 +1,29 @@
 #!/usr/bin/env python
 """Benchmark: milliseconds to the exact max-flow per update batch.
 
-Workload (the reference's GPU-scale configuration): R-MAT scale 20
-(1,048,576 vertices, 16,777,216 directed samples, a=0.57 b=0.19 c=0.19,
-self-loops and duplicates dropped, capacities uniform [1,1000], source = max
-out-degree vertex, sink = max in-degree other vertex), then successive 1% update
-batches (40% increases, 40% decreases, 10% inserts into reserved zero-capacity
-slots, 10% deletes).  Inputs are synthetic and seeded.  One step = one batch.
+Workload (the target configuration): R-MAT scale 24 (16,777,216 vertices,
+268,435,456 directed samples, a=0.57 b=0.19 c=0.19, self-loops and duplicates
+dropped, capacities uniform [1,1000], source = max out-degree vertex, sink = max
+in-degree other vertex; about 526 M CSR arcs), then successive 1% update batches
+(40% increases, 40% decreases, 10% inserts into reserved zero-capacity slots,
+10% deletes).  Inputs are synthetic and seeded.  One step = one batch.
+`--scale 20` gives the reference's GPU-scale configuration.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--variant data|pp|topo]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--scale S] [--variant data|pp|topo]
   python bench.py --impl reference ...   (the reference algorithm restated on the
                                           host cores: oracle/, OpenMP)
 
 Prints one JSON line (rank 0).  `value` is the p50 device time per batch with the
 batch already in HBM (dmf_apply_updates_device, CUDA events on the solver's
-stream); `e2e` is the same metric through the host-array entry point
-dmf_apply_updates (pinned staging, H2D of the batch, D2H of the flow value)
-timed by the host clock.  Every batch's final device state is certified by the
-oracle's certificate checker outside the timed region.
+stream, no instrumentation); `e2e` is the same metric through the host-array
+entry point dmf_apply_updates (pinned staging, H2D of the batch, D2H of the flow
+value) timed by the host clock.  Beside it, on the same batches and from the
+same pre-batch states: the engine's own from-scratch recompute
+(`recompute_p50_ms`, `speedup_vs_recompute`), the learned schedule picker
+against the plain schedule (`learned_vs_plain`), and the phase timeline of a
+traced copy (`phases_us_per_batch`, `roofline_bfs`).  The device states after
+the first and the last timed batch are certified by the oracle's certificate
+checker, and every batch's flow must agree across all the solvers.
 """
 from __future__ import annotations
 
@@ -34,7 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "ms to exact maxflow per update batch (p50)"
-PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_solve_rmat20_traffic.json")
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_solve_traffic.json")
 
 
 def parse_args():
@@ -44,7 +50,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variant", default="data", choices=["data", "topo", "pp"])
-    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--scale", type=int, default=24)
     ap.add_argument("--kernel-cycles", type=int, default=0)
     ap.add_argument("--relabel-interval", type=int, default=0)
     ap.add_argument("--tile", type=int, default=0)
@@ -52,9 +58,14 @@ def parse_args():
                     help="exactly --relabel-interval push rounds per global relabel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-certify", action="store_true")
-    ap.add_argument("--cpu-batches", type=int, default=3)
-    ap.add_argument("--workload", default="rmat20", choices=["rmat20", "grid256", "batched", "learned", "serving"],
-                    help="rmat20: the headline single-graph workload (scale from --scale); batched: 256 "
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0,
+                    help="CPU baseline: batches of the port are timed until they took this long in all")
+    ap.add_argument("--ref-budget-s", type=float, default=150.0,
+                    help="--impl reference: batches are timed until they took this long in all")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain pairs")
+    ap.add_argument("--phase-batches", type=int, default=3, help="timed batches replayed on a traced copy")
+    ap.add_argument("--workload", default="rmat", choices=["rmat", "grid256", "batched", "learned", "serving"],
+                    help="rmat: the headline single-graph workload (scale from --scale); batched: 256 "
                          "independent instances in one device state, 5 successive batches; learned: the "
                          "learned schedule picker against the plain schedule on held-out R-MAT instances")
     ap.add_argument("--learn-scale", type=int, default=22)
@@ -84,7 +95,7 @@ def workload(scale: int, nbatches: int):
 
 def config_dict(args, g, s, t, batches):
     return {
-        "workload": f"rmat{args.scale}-10x1pct-mixed",
+        "workload": f"rmat{args.scale}-1pct-mixed-successive",
         "graph": f"R-MAT scale {args.scale} a=0.57 b=0.19 c=0.19, 16*2^scale samples, caps U[1,1000]",
         "vertices": g.num_nodes(), "csr_arcs": g.num_edges(), "source": s, "sink": t,
         "batch_updates": int(len(batches[0][0])), "batch_mix": "40% inc / 40% dec / 10% insert / 10% delete",
@@ -103,15 +114,18 @@ def pct(xs, q):
 
 
 # ---------------------------------------------------------------------------
-def cpu_port_run(g, s, t, batches, nthreads):
-    """The reference's data-driven algorithm restated in oracle/ (OpenMP)."""
+def cpu_port_run(g, s, t, batches, nthreads, budget_ms=0.0):
+    """The reference's data-driven algorithm restated in oracle/ (OpenMP): a
+    static solve, then the batches in order (stopping once they took budget_ms
+    in all, when it is > 0)."""
     from oracle import build as OB
     OB.build_oracle()
     from oracle import oracle as O
     off, adj, w, par = g.arrays()
     n = g.num_nodes()
     kc = max(1, g.num_edges() // n)
-    _, flows, ms = O.ref_run_successive("data", n, off, adj, w, par, s, t, kc, batches, nthreads=nthreads)
+    _, flows, ms = O.ref_run_successive("data", n, off, adj, w, par, s, t, kc, batches, nthreads=nthreads,
+                                        budget_ms=budget_ms)
     return list(flows), list(ms)
 
 
@@ -179,7 +193,51 @@ def load_measured_peak():
     return 6650.0, "fallback"
 
 
+def bfs_roofline(stats: list, phases: dict, n: int, peak: float) -> dict | None:
+    """Roofline of the global relabel alone (the BFS from t and the deficits):
+    algorithmic bytes per relabel 16*V (offsets, label write) + 12 per adjacency
+    entry scanned (head, residual, head label), over the time of the BFS phases
+    (seed pass, top-down and bottom-up levels, finalize) in the traced pass."""
+    t_us = sum(phases.get(k, {}).get("us", 0.0) for k in ("bfs_init", "bfs_td", "bfs_bu", "bfs_finalize"))
+    if not stats or t_us <= 0:
+        return None
+    relabels = sum(st["outer_iters"] for st in stats) / len(stats)
+    barcs = sum(st["bfs_arcs"] for st in stats) / len(stats)
+    nbytes = 16.0 * n * relabels + 12.0 * barcs
+    achieved = nbytes / (t_us * 1e-6) / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "bytes_per_batch": int(nbytes), "bfs_us_per_batch": round(t_us, 1),
+            "relabels_per_batch": round(relabels, 2), "bfs_arcs_per_batch": int(barcs)}
+
+
+def recorded_reference_cuda(g, s, t, scale: int):
+    """The reference's own CUDA binaries on this workload's graph (cumulative
+    update file 1), as recorded on a B200 by tests/golden/make_golden.py."""
+    path = os.path.join(ROOT, "tests", "golden", "reference_flows.json")
+    if not os.path.exists(path):
+        return None
+    rec = json.load(open(path)).get(f"rmat{scale}")
+    if not rec or (rec["n"], rec["m"], rec["source"], rec["sink"]) != (g.num_nodes(), g.num_edges(), s, t):
+        return None
+    out = {"source": "tests/golden/reference_flows.json (reference binaries built from its code/, B200)",
+           "graph_sha256": rec["sha256"]}
+    for key, per_file in rec["runs"].items():
+        runs = [r for f in per_file if f["file"] == 1 and f["rc"] == 0 for r in f["runs"]]
+        if runs:
+            out[key] = {"dyn_per_batch_ms": [r["dyn_ms"] for r in runs],
+                        "static_update_ms": [r["recompute_ms"] for r in runs],
+                        "flow": runs[0]["dynamic_flow"]}
+    return out
+
+
 def run_ours(args, rank: int, world: int):
+    """The headline workload.  One step = one 1% batch applied to the resident
+    state.  Per timed batch, from copies of the same pre-batch state: the batch
+    (value; device pointers, no instrumentation), the engine's own from-scratch
+    recompute of the same capacities (dmf_recompute_device), the learned and the
+    plain schedule through the scheduled entry point, and a traced pass for the
+    phase breakdown.  A second solver replays every batch through the host-array
+    entry point (e2e)."""
     import numpy as np
     import torch
     import dyn_maxflow_b200 as D
@@ -188,50 +246,85 @@ def run_ours(args, rank: int, world: int):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     nb = args.warmup + args.steps
+    t_gen = time.perf_counter()
     g, s, t, batches = workload(args.scale, nb)
+    gen_s = time.perf_counter() - t_gen
     n = g.num_nodes()
     off, adj, w, par = g.arrays()
     deg_s = int(off[s + 1] - off[s])
     stream = torch.cuda.Stream()
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")  # 256 MiB > 126 MB L2
-    # ---- device-resident pass (value) ----
     dbat = [[torch.as_tensor(x, dtype=torch.int32).cuda() for x in b] for b in batches]
     torch.cuda.synchronize()
-    sv = D.Solver(g, s, t, variant=args.variant, kernel_cycles=args.kernel_cycles,
-                  relabel_interval=args.relabel_interval, tile=args.tile, stream=stream, trace=True,
-                  fixed_interval=args.fixed_interval)
-    static_flow = sv.static_maxflow()
-    phase_us = {}
-    flows, times, stats = [], [], []
+    kw = dict(variant=args.variant, kernel_cycles=args.kernel_cycles, relabel_interval=args.relabel_interval,
+              tile=args.tile, stream=stream, fixed_interval=args.fixed_interval)
+    A = D.Solver(g, s, t, **kw)
+    static_flow = A.static_maxflow()
+    static_ms = A.stats()["last_ms"]
+    sched = None
+    if not args.no_learned and os.path.exists(args.sched_weights):
+        sched = D.Scheduler.load(args.sched_weights)
+    R = D.Solver(g, s, t, **kw)
+    P = D.Solver(g, s, t, trace=True, **kw)
+    B = D.Solver(g, s, t, **kw)
+    B.copy_state_from(A)
+    Ls = [D.Solver(g, s, t, **kw), D.Solver(g, s, t, **kw)] if sched is not None else []
+
+    def flushed():
+        flush.fill_(1)
+        torch.cuda.synchronize()
+
+    flows, times, stats, rec_ms, rec_flows = [], [], [], [], []
+    learned_ms, plain_ms, picks, learned_ok = [], [], [], True
+    phase_us, pstats = {}, []
     certified = True
-    sampler = None
-    t_region = None
+    sampler, t_region = None, None
     for i, b in enumerate(dbat):
         timed = i >= args.warmup
-        if timed and sampler is None:
-            if world > 1:
-                torch.distributed.barrier()
-            torch.cuda.synchronize()
-            sampler = ClockSampler(dev)
-            t_region = time.perf_counter()
-        flush.fill_(i)
-        torch.cuda.synchronize()
+        args_d = (b[0].data_ptr(), b[1].data_ptr(), b[2].data_ptr(), int(b[0].numel()))
+        if timed:
+            for other in [R] + Ls + ([P] if len(pstats) < args.phase_batches else []):
+                other.copy_state_from(A)
+            if sampler is None:
+                if world > 1:
+                    torch.distributed.barrier()
+                torch.cuda.synchronize()
+                sampler = ClockSampler(dev)
+                t_region = time.perf_counter()
+        flushed()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        f = sv.apply_updates_device(b[0].data_ptr(), b[1].data_ptr(), b[2].data_ptr(), int(b[0].numel()))
+        f = A.apply_updates_device(*args_d)
         e1.record(stream)
         e1.synchronize()
-        if timed:
-            times.append(e0.elapsed_time(e1))
-            stats.append(sv.stats())
-            tr = sv.trace()
+        flows.append(f)
+        if not timed:
+            continue
+        times.append(e0.elapsed_time(e1))
+        stats.append(A.stats())
+        flushed()
+        rec_flows.append(R.recompute_device(*args_d))
+        rec_ms.append(R.stats()["last_ms"])
+        if Ls:
+            flushed()
+            fl, act = Ls[0].apply_updates_scheduled(sched, *batches[i])
+            learned_ms.append(Ls[0].stats()["last_ms"])
+            flushed()
+            fp, _ = Ls[1].apply_updates_scheduled(None, *batches[i])
+            plain_ms.append(Ls[1].stats()["last_ms"])
+            picks.append(act)
+            learned_ok &= fl == fp == f
+        if len(pstats) < args.phase_batches:
+            flushed()
+            P.apply_updates_device(*args_d)
+            pstats.append(P.stats())
+            tr = P.trace()
             for (k0, t0_), (k1, t1_) in zip(tr, tr[1:]):
                 d = phase_us.setdefault(k1, [0.0, 0])
                 d[0] += t1_ - t0_
                 d[1] += 1
-        flows.append(f)
-        if not args.no_certify and timed:
-            cap, res, ex, _ = sv.state()
+        if not args.no_certify and (i == args.warmup or i == nb - 1):
+            cap, res, ex, _ = A.state()
             rc, val, cut = O.certify(n, off, adj, cap, par, res, s, t)
             certified &= (rc == 0 and val == f == cut)
     torch.cuda.synchronize()
@@ -239,25 +332,21 @@ def run_ours(args, rank: int, world: int):
         torch.distributed.barrier()
     region_s = time.perf_counter() - t_region
     clocks = sampler.stop() if sampler else None
-    sv.close()
+    for x in [A, R, P] + Ls:
+        x.close()
+    if sched is not None:
+        sched.close()
     # ---- end-to-end pass through the host-array entry point ----
-    sv2 = D.Solver(g, s, t, variant=args.variant, kernel_cycles=args.kernel_cycles,
-                   relabel_interval=args.relabel_interval, tile=args.tile, stream=stream,
-                   fixed_interval=args.fixed_interval)
-    assert sv2.static_maxflow() == static_flow
-    e2e = []
-    flows2 = []
+    e2e, flows2 = [], []
     for i, b in enumerate(batches):
-        flush.fill_(i)
-        torch.cuda.synchronize()
+        flushed()
         t0 = time.perf_counter()
-        f = sv2.apply_updates(*b)
+        flows2.append(B.apply_updates(*b))
         dt = (time.perf_counter() - t0) * 1e3
-        flows2.append(f)
         if i >= args.warmup:
             e2e.append(dt)
-    sv2.close()
-    consistent = flows == flows2
+    B.close()
+    consistent = flows == flows2 and rec_flows == flows[args.warmup:]
     # ---- roofline of the solve kernel ----
     abytes = [algorithmic_bytes(st, n, int(len(batches[args.warmup + j][0])), deg_s) for j, st in enumerate(stats)]
     avg_bytes = sum(abytes) / len(abytes)
@@ -267,18 +356,26 @@ def run_ours(args, rank: int, world: int):
     traffic = None
     if os.path.exists(PROFILE_SUMMARY):
         try:
-            traffic = json.load(open(PROFILE_SUMMARY)).get("dram_bytes_per_launch")
+            prof = json.load(open(PROFILE_SUMMARY))
+            if prof.get("workload") == f"rmat{args.scale}":
+                traffic = prof.get("dram_bytes_per_launch")
         except ValueError:
             traffic = None
+    phases = {k: {"us": round(v[0] / max(1, len(pstats)), 1), "count": round(v[1] / max(1, len(pstats)), 1)}
+              for k, v in sorted(phase_us.items(), key=lambda kv: -kv[1][0])}
     p50, p99 = pct(times, 0.5), pct(times, 0.99)
+    rec_p50 = pct(rec_ms, 0.5)
     res = {
         "metric": METRIC, "value": round(p50, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(avg_ms, 4), "p50_ms": round(p50, 4), "p99_ms": round(p99, 4),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int32 (int64 excess)",
         "data": "synthetic (seeded R-MAT and update generators)", "config": config_dict(args, g, s, t, batches),
         "parallelism": "replicas" if world > 1 else "single",
-        "static_flow": static_flow, "flows": flows[args.warmup:], "certified": bool(certified and consistent),
-        "timed_region_s": round(region_s, 3),
+        "static_flow": static_flow, "static_ms": round(static_ms, 3), "flows": flows[args.warmup:],
+        "certified": bool(certified and consistent), "timed_region_s": round(region_s, 3),
+        "generation_s": round(gen_s, 1),
+        "recompute_p50_ms": round(rec_p50, 4), "recompute_p99_ms": round(pct(rec_ms, 0.99), 4),
+        "speedup_vs_recompute": round(rec_p50 / p50, 2),
         "e2e": {"value": round(pct(e2e, 0.5), 4), "unit": "ms", "p99": round(pct(e2e, 0.99), 4),
                 "h2d_bytes_per_step": int(12 * len(batches[-1][0])), "d2h_bytes_per_step": 8,
                 "api": "dmf_apply_updates (host arrays)"},
@@ -286,13 +383,27 @@ def run_ours(args, rank: int, world: int):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "k_solve", "algorithmic_bytes_per_launch": int(avg_bytes)},
+        "roofline_bfs": bfs_roofline(pstats, phases, n, peak),
         "solver_stats_mean": {k: round(sum(st[k] for st in stats) / len(stats), 1)
                               for k in ("outer_iters", "bfs_levels", "push_rounds", "pushes", "relabels",
-                                        "arcs_scanned", "vertices_visited", "dead_vertices")},
+                                        "arcs_scanned", "bfs_arcs", "vertices_visited", "dead_vertices",
+                                        "dead_deficits", "dead_kept")},
         "clocks": clocks,
-        "phases_us_per_batch": {k: {"us": round(v[0] / len(times), 1), "count": round(v[1] / len(times), 1)}
-                                for k, v in sorted(phase_us.items(), key=lambda kv: -kv[1][0])},
+        "phases_us_per_batch": phases,
+        "phases_source": f"separate traced solver, state copied before each of the first {len(pstats)} timed batches",
     }
+    if Ls:
+        lp, pp = pct(learned_ms, 0.5), pct(plain_ms, 0.5)
+        res["learned_vs_plain"] = {
+            "learned_p50_ms": round(lp, 4), "plain_p50_ms": round(pp, 4), "learned_p99_ms": round(pct(learned_ms, 0.99), 4),
+            "plain_p99_ms": round(pct(plain_ms, 0.99), 4), "ratio_plain_over_learned": round(pp / lp, 4),
+            "picks": dict(zip(D.ACTIONS, np.bincount(picks, minlength=D.N_ACTIONS).tolist())),
+            "equal_flows": bool(learned_ok),
+            "timing": "dmf_apply_updates_scheduled from copies of the same pre-batch state (features, decision and "
+                      "solve; H2D of the batch not included)"}
+    refc = recorded_reference_cuda(g, s, t, args.scale)
+    if refc is not None:
+        res["reference_cuda"] = refc
     if world > 1:
         from dyn_maxflow_b200.replicas import replica_summary
         rs = replica_summary(p50, avg_ms, pct(e2e, 0.5), world)
@@ -301,13 +412,14 @@ def run_ours(args, rank: int, world: int):
         res["throughput_batches_per_s"] = round(rs["throughput_batches_per_s"], 2)
     if rank == 0 and not args.no_cpu_baseline:
         nth = os.cpu_count() or 1
-        k = max(1, min(args.cpu_batches, len(batches)))
         t0 = time.perf_counter()
-        cflows, cms = cpu_port_run(g, s, t, batches[:k], nth)
+        cflows, cms = cpu_port_run(g, s, t, batches, nth, budget_ms=args.cpu_budget_s * 1e3)
+        k = len(cms)
         res["cpu_baseline"] = {"value": round(statistics.median(cms), 3), "unit": "ms", "cores": nth,
                                "kind": "port",
-                               "sample": f"first {k} successive batches of the same workload after an untimed "
-                                         f"static solve ({time.perf_counter() - t0:.1f} s total)",
+                               "sample": f"first {k} successive batches of the same workload (a {args.cpu_budget_s:.0f} s "
+                                         f"budget) after an untimed static solve; {time.perf_counter() - t0:.1f} s "
+                                         "of CPU work in all",
                                "flows_match": [int(x) for x in cflows] == flows[:k]}
     return res
 
@@ -552,6 +664,10 @@ def run_serving(args, rank: int, world: int):
     gen_s = time.time() - t_gen
     srv = D.Server(graphs, srcs, snks, int(args.serve_budget_gb * (1 << 30)))
     admitted = srv.admitted
+    lanes = {}
+    for gi in range(admitted):
+        ln = srv.lane(gi)
+        lanes.setdefault(ln["lane"], {"graphs": 0, "grid_blocks": ln["grid_blocks"]})["graphs"] += 1
     # warm-up: one request per admitted graph
     for gi in range(admitted):
         srv.wait(srv.submit(gi, *pools[gi][0]))
@@ -608,6 +724,7 @@ def run_serving(args, rank: int, world: int):
         "config": {"workload": f"serving-rmat{args.serve_scale}+{args.serve_small}x(16-18)",
                    "graphs": len(graphs), "admitted": admitted, "device_bytes": srv.device_bytes,
                    "big_graph": {"vertices": graphs[0].num_nodes(), "csr_arcs": graphs[0].num_edges()},
+                   "lanes": [lanes[k] for k in sorted(lanes)],
                    "rate_req_s": args.serve_rate, "stream_s": args.serve_seconds,
                    "request_sizes": "log-uniform [1e3, 1e6] updates, <= m/2",
                    "l2": "device state (large graph) far larger than L2"},
@@ -620,25 +737,34 @@ def run_serving(args, rank: int, world: int):
 
 
 def run_reference(args, rank: int):
+    """The reference's data-driven algorithm (restated in oracle/, OpenMP on all
+    host cores) on the same workload: static solve (untimed), then the batches in
+    order until they took --ref-budget-s in all (a batch of the full graph takes
+    seconds on the host, so the step count is bounded by time, not by --steps)."""
     if rank != 0:
         return None
     nb = args.warmup + args.steps
     g, s, t, batches = workload(args.scale, nb)
     nth = os.cpu_count() or 1
-    flows, ms = cpu_port_run(g, s, t, batches, nth)
-    timed = ms[args.warmup:]
+    t0 = time.perf_counter()
+    flows, ms = cpu_port_run(g, s, t, batches, nth, budget_ms=args.ref_budget_s * 1e3)
+    wall = time.perf_counter() - t0
+    wu = min(args.warmup, 1 if len(ms) > 2 else 0)
+    timed = ms[wu:]
     p50 = pct(timed, 0.5)
     return {
         "impl": "reference", "metric": METRIC, "value": round(p50, 3), "unit": "ms", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sum(timed) / len(timed), 3),
+        "steps": len(timed), "warmup": wu, "ms_per_step": round(sum(timed) / len(timed), 3),
         "p99_ms": round(pct(timed, 0.99), 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32 (int64 excess)", "data": "synthetic (seeded R-MAT and update generators)",
         "config": config_dict(args, g, s, t, batches),
         "cpu_baseline": {"value": round(p50, 3), "unit": "ms", "cores": nth, "kind": "port",
-                         "sample": f"{args.steps} timed successive batches (after {args.warmup} warm-up) of the "
-                                   "full workload, reference data-driven algorithm restated in oracle/ (OpenMP)"},
+                         "sample": f"{len(timed)} timed successive batches (after {wu} untimed) of the full workload, "
+                                   f"as many as fit a {args.ref_budget_s:.0f} s budget of batch time ({args.steps} "
+                                   f"requested), after an untimed static solve; reference data-driven algorithm "
+                                   f"restated in oracle/ (OpenMP); {wall:.1f} s in all"},
         "e2e": {"value": round(p50, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "flows": [int(x) for x in flows[args.warmup:]],
+        "flows": [int(x) for x in flows[wu:]],
     }
 
 

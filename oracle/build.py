@@ -3,7 +3,8 @@
 * ``build_oracle()`` compiles oracle/oracle.c (the CPU restatement, Dinic and the
   certificate checker) into oracle/liboracle.so.
 * ``build_ref()`` compiles the reference's own sources, read in place under the
-  reference checkout (default /root/reference, override with DMF_REFERENCE), into
+  reference checkout (DMF_REFERENCE, else a `reference` directory beside the
+  repository; nothing is built when neither exists), into
   oracle/_ref/: its input tools with g++ (input_create/weight.cpp, create_bin.cpp,
   create_update_bin.cpp) and its CUDA benches with nvcc, once with the flags of
   code/Makefile (no -arch) and once with -arch=sm_100a.  Nothing is copied from
@@ -21,7 +22,11 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 
 
 def reference_root() -> str:
-    return os.environ.get("DMF_REFERENCE", "/root/reference")
+    """The reference checkout: $DMF_REFERENCE, else `reference` beside the repository."""
+    env = os.environ.get("DMF_REFERENCE")
+    if env:
+        return env
+    return os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 
 
 def _stale(out: str, srcs: list[str]) -> bool:

@@ -5,9 +5,11 @@ import subprocess
 import numpy as np
 import pytest
 
+from oracle.build import reference_root
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 TOOL = os.path.join(ROOT, "dyn_maxflow_b200", "bin", "dmf_tool")
-MTX = os.path.join(os.environ.get("DMF_REFERENCE", "/root/reference"), "data", "raw_dataset", "johnson8-2-4.mtx")
+MTX = os.path.join(reference_root(), "data", "raw_dataset", "johnson8-2-4.mtx")
 
 pytestmark = pytest.mark.skipif(not os.path.exists(TOOL), reason="dmf_tool not built")
 
