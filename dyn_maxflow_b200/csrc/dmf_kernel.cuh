@@ -493,10 +493,12 @@ __device__ __forceinline__ void chunk_range(const Params &p, int2 it, int &beg, 
 // than s get height 0; all other live vertices become unvisited.  reset_dead
 // revives every vertex (the first relabel of a solve that does not keep the
 // dead set); clean_dead puts the kept dead vertices back at height V after the
-// local repair labelled some of them.  Vertices of instances outside the call's
-// mask are not touched at all: their labels and dead set stay as their own last
-// solve left them.
-__device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead, bool clean_dead) {
+// local repair labelled some of them.  count_kept adds the kept dead vertices to
+// the dead-vertex statistic (first relabel of a batch that kept them).  Vertices
+// of instances outside the call's mask are not touched at all: their labels and
+// dead set stay as their own last solve left them.
+__device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead, bool clean_dead,
+                                            bool count_kept) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   Ctrl *c = p.ctrl;
   if (gt == 0) {
@@ -504,7 +506,7 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
     c->act_hq = 0;
     c->wtail[0] = c->whtail[0] = c->seen[0] = 0;  // written by push round 0
   }
-  int pos = 0;
+  int pos = 0, kept = 0;
   long long unexpl = 0, seed_arcs = 0;
   for (int v = gt; v < p.n; v += nt) {
     if (p.inst_active && !p.inst_active[__ldg(p.inst + v)]) continue;
@@ -512,6 +514,7 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
       if (__ldcg(p.dead + v)) p.dead[v] = 0;
     } else if (__ldcg(p.dead + v)) {
       if (clean_dead) p.height[v] = p.n;
+      kept++;
       continue;
     }
     long long ex = __ldcg(p.excess + v);
@@ -547,6 +550,7 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
   block_add_int(&c->pos_count, pos);
   block_add_ll(&c->unexplored, unexpl);
   block_add_ll(&out->arcs, seed_arcs);
+  if (count_kept) block_add_ll((long long *)&c->st_dead, kept);
 }
 
 // Reserves `cnt` consecutive slots behind *tail for this thread with one atomic
@@ -1808,7 +1812,7 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     }
     kind = TR_BFS_INIT;
     items = hubitems = 0;
-    ph_bfs_init(p, slot_out(), it == 0 && revive, it == 0 && clean && !revive);
+    ph_bfs_init(p, slot_out(), it == 0 && revive, it == 0 && clean && !revive, it == 0 && !revive);
     if (!next()) return;
     if (lead) c->st_outer++;
     const int P = sc->pos_count;
