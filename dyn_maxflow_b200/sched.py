@@ -67,11 +67,12 @@ def next_batch(g, frac: float, seed: int):
     return b
 
 
-def record(specs, batches: int, frac_lo: float, frac_hi: float, verbose=True):
+def record(specs, batches: int, frac_lo: float, frac_hi: float, verbose=True, out=None, save_every=8):
     """Traces of (features, per-action log2 ms) over R-MAT instances `specs` =
-    [(scale, seed), ...].  Returns X[n,12], T[n,4] (ms), meta list."""
+    [(scale, seed), ...].  Returns X[n,12], T[n,4] (ms), meta list.  With `out`,
+    the traces so far are saved there every `save_every` instances."""
     X, T, meta = [], [], []
-    for scale, seed in specs:
+    for done, (scale, seed) in enumerate(specs, 1):
         t0 = time.time()
         g, s, t = rmat_instance(scale, seed)
         trunk = D.Solver(g, s, t)
@@ -104,6 +105,8 @@ def record(specs, batches: int, frac_lo: float, frac_hi: float, verbose=True):
         scratch.close()
         if verbose:
             print(f"recorded scale {scale} seed {seed}: {batches} batches in {time.time() - t0:.1f}s", flush=True)
+        if out and (done % save_every == 0 or done == len(specs)):
+            np.savez(out, X=np.array(X, np.float32), T=np.array(T, np.float32), meta=json.dumps(meta))
     return np.array(X, np.float32), np.array(T, np.float32), meta
 
 
@@ -266,7 +269,10 @@ def forward_reference(weights: np.ndarray, biases: np.ndarray, X: np.ndarray) ->
     return h2 @ W3.T + b3
 
 
-def _specs(scales, seeds):
+def _specs(scales, seeds, spread=False):
+    """Every seed at every scale, or (spread) seed i at scales[i % len(scales)]."""
+    if spread:
+        return [(scales[i % len(scales)], sd) for i, sd in enumerate(seeds)]
     return [(sc, sd) for sd in seeds for sc in scales]
 
 
@@ -281,6 +287,8 @@ def main(argv=None):
     r.add_argument("--batches", type=int, default=10)
     r.add_argument("--frac-lo", type=float, default=5e-4)
     r.add_argument("--frac-hi", type=float, default=0.1)
+    r.add_argument("--spread", action="store_true",
+                   help="one graph per seed, the scales taken in turn (200 seeds over 7 scales = 200 graphs)")
     t = sub.add_parser("train")
     t.add_argument("--traces", required=True, nargs="+")
     t.add_argument("--out", required=True)
@@ -296,8 +304,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     if a.cmd == "record":
         scales = [int(x) for x in a.scales.split(",")]
-        specs = _specs(scales, range(a.seed_base, a.seed_base + a.seeds))
-        X, T, meta = record(specs, a.batches, a.frac_lo, a.frac_hi)
+        specs = _specs(scales, range(a.seed_base, a.seed_base + a.seeds), spread=a.spread)
+        X, T, meta = record(specs, a.batches, a.frac_lo, a.frac_hi, out=a.out)
         np.savez(a.out, X=X, T=T, meta=json.dumps(meta))
         print(f"{len(X)} records -> {a.out}")
     elif a.cmd == "train":
