@@ -38,7 +38,6 @@ struct Slot {
   long long arcs;    // sum of degrees of appended vertices
   int cnt;           // generic counter (BFS: active vertices labelled; topo push: active seen)
   int pad;
-  long long exsum;   // BFS inside the dead set: excess of the active vertices labelled
 };
 
 // Control block of one solver (device memory, cleared before every launch).
@@ -64,8 +63,8 @@ struct Ctrl {
   unsigned long long probe[2];  // longest work item of a phase, (ns << 32) | vertex
   unsigned long long blk[2];    // longest block work of a phase (ns), barrier exit to arrival
   // kept dead set (dynamic batches): vertices of the dead set whose excess a batch
-  // lowered (candidates for deficits), the deficits found among them, and those
-  // left after the local repair inside the dead set
+  // lowered or that a pull moved a deficit to (candidates for deficits), the
+  // deficits found among them, and those left after the local repair
   int dcand;
   int dseeds;
   long long dneed;

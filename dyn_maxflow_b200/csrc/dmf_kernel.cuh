@@ -20,9 +20,10 @@
 // A dynamic batch keeps the dead set of the last solve (the vertices proven
 // unable to reach t or a deficit): updated arcs that open residual from it to
 // the live side are saturated at once (ph_reopen), the deficits this leaves
-// inside the dead set are covered there by a short local push-relabel
-// (ph_dead_seed .. ph_dead_check), and the global relabels then only visit
-// live vertices.  A deficit the local pass cannot cover revives every vertex.
+// inside the dead set are covered there by pulls from the excess parked in it
+// (ph_dead_seed, ph_dead_pull, ph_dead_check), and the global relabels then
+// only visit live vertices.  A deficit the pulls cannot cover revives every
+// vertex.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -46,11 +47,11 @@ enum TraceKind : int {
   TR_START = 0, TR_INIT_RES = 1, TR_SATURATE = 2, TR_LOOKUP = 3, TR_APPLY = 4, TR_REPAIR = 5,
   TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
   TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14, TR_PP_INIT = 15, TR_PP_BFS = 16, TR_PP_FINALIZE = 17,
-  TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_BFS = 21, TR_DEAD_PUSH = 22, TR_DEAD_CHECK = 23
+  TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_PULL = 21, TR_DEAD_CHECK = 23
 };
 
-// Local repair inside a kept dead set: at most this many BFS levels.
-constexpr int kDeadLevels = 4;
+// Local repair inside a kept dead set: at most this many pull rounds.
+constexpr int kDeadRounds = 8;
 
 // Largest capacity an update may set: keeps cap(e) + cap(partner) < 2^31 when
 // both arcs of a pair change in one batch.
@@ -492,13 +493,11 @@ __device__ __forceinline__ void chunk_range(const Params &p, int2 it, int &beg, 
 // Seeds (my_init_1, code/dyn_data.h:60-67): t and every deficit vertex other
 // than s get height 0; all other live vertices become unvisited.  reset_dead
 // revives every vertex (the first relabel of a solve that does not keep the
-// dead set); clean_dead puts the kept dead vertices back at height V after the
-// local repair labelled some of them.  count_kept adds the kept dead vertices to
-// the dead-vertex statistic (first relabel of a batch that kept them).  Vertices
-// of instances outside the call's mask are not touched at all: their labels and
-// dead set stay as their own last solve left them.
-__device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead, bool clean_dead,
-                                            bool count_kept) {
+// dead set); count_kept adds the kept dead vertices to the dead-vertex
+// statistic (first relabel of a batch that kept them).  Vertices of instances
+// outside the call's mask are not touched at all: their labels and dead set
+// stay as their own last solve left them.
+__device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead, bool count_kept) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   Ctrl *c = p.ctrl;
   if (gt == 0) {
@@ -513,7 +512,6 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
     if (reset_dead) {
       if (__ldcg(p.dead + v)) p.dead[v] = 0;
     } else if (__ldcg(p.dead + v)) {
-      if (clean_dead) p.height[v] = p.n;
       kept++;
       continue;
     }
@@ -566,7 +564,6 @@ __device__ __forceinline__ int reserve(int *tail, int cnt) {
 struct VisitAcc {
   long long arcs = 0;
   int reached = 0;
-  long long exsum = 0;  // excess of the active vertices labelled (dead-set levels)
 };
 
 __device__ __forceinline__ void bfs_visit(const Params &p, Slot *out, int nxt, int w, VisitAcc &acc) {
@@ -584,11 +581,9 @@ __device__ __forceinline__ void bfs_visit(const Params &p, Slot *out, int nxt, i
 
 // Counts go to the phase's own slot: a cross-phase counter would be read by a
 // slow block after a fast block already added to it in the next phase.
-template <bool DM = false>
 __device__ __forceinline__ void flush_visits(const Params &p, Slot *out, VisitAcc &acc) {
   block_add_ll(&out->arcs, acc.arcs);
   block_add_int(&out->cnt, acc.reached);
-  if (DM) block_add_ll(&out->exsum, acc.exsum);
 }
 
 // Top-down level (staticMaxFlow_kernel_11, code/dyn_data.h:72-87, run over the
@@ -599,15 +594,10 @@ __device__ __forceinline__ void flush_visits(const Params &p, Slot *out, VisitAc
 // batches of kBatch so that the gathers of a batch are in flight together:
 // heads, then head labels, then the reverse residuals, then the claims, then
 // the claimed heads' degree and excess.
-//
-// DM (local repair inside a kept dead set): the level claims dead vertices,
-// which sit at height V between solves, instead of unvisited live ones.
 constexpr int kBatch = 8;   // arcs per lane per batch (a hub chunk is one batch)
 constexpr int kTdBatch = 4;  // smaller for top-down, which keeps more state per arc
-template <bool DM = false>
 __device__ __forceinline__ void td_range(const Params &p, Slot *out, int nxt, int first, int end, int stride, int L,
                                          LStats &ls, VisitAcc &acc) {
-  const int unv = DM ? p.n : UNV;
   for (int a0 = first; a0 < end; a0 += kTdBatch * stride) {
     int w[kTdBatch];
     bool c[kTdBatch];
@@ -617,18 +607,13 @@ __device__ __forceinline__ void td_range(const Params &p, Slot *out, int nxt, in
       w[k] = a < end ? __ldg(p.adj + a) : -1;
     }
 #pragma unroll
-    for (int k = 0; k < kTdBatch; k++) c[k] = w[k] >= 0 && __ldcg(p.height + w[k]) == unv;
-    if (DM) {
-#pragma unroll
-      for (int k = 0; k < kTdBatch; k++)
-        if (c[k]) c[k] = __ldcg(p.dead + w[k]) != 0;
-    }
+    for (int k = 0; k < kTdBatch; k++) c[k] = w[k] >= 0 && __ldcg(p.height + w[k]) == UNV;
 #pragma unroll
     for (int k = 0; k < kTdBatch; k++)
       if (c[k]) c[k] = __ldcg(p.res + __ldg(p.par + a0 + k * stride)) > 0;
 #pragma unroll
     for (int k = 0; k < kTdBatch; k++)
-      if (c[k]) c[k] = atomicCAS(p.height + w[k], unv, L + 1) == unv;
+      if (c[k]) c[k] = atomicCAS(p.height + w[k], UNV, L + 1) == UNV;
     int d[kTdBatch];
     long long ex[kTdBatch];
 #pragma unroll
@@ -649,10 +634,7 @@ __device__ __forceinline__ void td_range(const Params &p, Slot *out, int nxt, in
       if (!c[k]) continue;
       acc.arcs += d[k];
       const bool act = !is_term(p, w[k]) && ex[k] > 0;
-      if (act) {
-        acc.reached++;
-        if (DM) acc.exsum += ex[k];
-      }
+      if (act) acc.reached++;
       if (d[k] > p.hub_deg) {
         append_hub(p, p.fh[nxt], &out->hq, w[k]);
         if (act) append_hub(p, p.ah, &p.ctrl->act_hq, w[k]);
@@ -680,7 +662,7 @@ __device__ __forceinline__ void td_range(const Params &p, Slot *out, int nxt, in
   }
 }
 
-template <int TILE, bool DM = false>
+template <int TILE>
 __device__ __forceinline__ void ph_bfs_td(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
   const int cur = L & 1, nxt = cur ^ 1;
   const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
@@ -691,14 +673,14 @@ __device__ __forceinline__ void ph_bfs_td(const Params &p, const Slot *in, Slot 
     const int2 it = __ldcg(p.fh[cur] + i);
     ItemTimer tm(p);
     chunk_range(p, it, beg, end);
-    td_range<DM>(p, out, nxt, beg + lane, end, 32, L, ls, acc);
+    td_range(p, out, nxt, beg + lane, end, 32, L, ls, acc);
     tm.done(ls, it.x);
   }
   for_tiered<TILE>(p, ls, p.fq[cur], nn, [&](auto &g, int x) {
     const int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
-    td_range<DM>(p, out, nxt, beg + g.rank(), end, g.size(), L, ls, acc);
+    td_range(p, out, nxt, beg + g.rank(), end, g.size(), L, ls, acc);
   });
-  flush_visits<DM>(p, out, acc);
+  flush_visits(p, out, acc);
 }
 
 // Whether one of the arcs first, first+stride, ... < end (at most kBatch of them)
@@ -784,24 +766,24 @@ __device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int 
 
 // ---- local repair inside a kept dead set ------------------------------------------
 // The batch left deficits on some dead vertices (candidates in dq).  They are
-// covered from the excess parked inside the dead set, without reviving it: a
-// short BFS from the deficits over residual arcs between dead vertices (at
-// most kDeadLevels levels, stopping once the excess it reached is twice the
-// deficit), then push rounds of the vertices it labelled.  Every residual arc
-// out of a dead vertex ends at a dead vertex, so these pushes stay inside the
-// dead set.  A deficit left over makes the first global relabel revive every
-// vertex (the solve then proceeds as from a reset dead set).
+// covered from the excess parked inside the dead set, without reviving it, by
+// pulls: a deficit y takes what it lacks over residual arcs x->y from dead
+// in-neighbours x, first from those holding excess (exactly the amount missing,
+// so parked excess is not flooded around), then, for what is still missing,
+// from dead in-neighbours not yet touched by this repair, which take that part
+// of the deficit over and pull in the next round.  A vertex is stamped the
+// first time a deficit reaches it, so deficits only move to fresh vertices and
+// the rounds end (at most kDeadRounds).  Only dead vertices are pulled from, so
+// the pulled flow stays inside the dead set and every arc it adds residual to
+// (y->x) lies inside it: the set stays closed.  A deficit left over makes the
+// first global relabel revive every vertex (the solve then proceeds as from a
+// reset dead set).
 
-// Seeds: candidates with a deficit get height 0.
+// Seeds: the candidates with a deficit.  (Candidates are stamped with the
+// repair's wave, round_base, when they join dq.)
 __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Slot *out) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   Ctrl *c = p.ctrl;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    c->act_q = 0;
-    c->act_hq = 0;
-    c->wtail[0] = c->whtail[0] = c->seen[0] = 0;
-    c->dleft = 0;
-  }
   int seeds = 0;
   long long need = 0;
   const int nc = sc->dcand;
@@ -809,9 +791,7 @@ __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Sl
     const int v = __ldcg(p.dq + i);
     const long long ex = __ldcg(p.excess + v);
     if (ex >= 0 || is_term(p, v)) continue;
-    p.height[v] = 0;
-    if (deg_of(p, v) > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
-    else append(p.fq[0], &out->q, v);
+    append(p.fq[0], &out->q, v);
     seeds++;
     need -= ex;
   }
@@ -819,8 +799,78 @@ __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Sl
   block_add_ll(&c->dneed, need);
 }
 
-// Counts the dead deficits left (pushes never create a deficit, so only
-// candidates can be one).
+// One pull round: a warp per deficit of the list, lanes over its arcs.
+__device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, int nn, int *nxt, Slot *out,
+                                             LStats &ls) {
+  const unsigned wave = p.round_base;
+  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = spread_group<32>(); i < nn; i += nwarps) {
+    int y = 0;
+    long long need = 0;
+    if (lane == 0) {
+      y = __ldcg(list + i);
+      need = -__ldcg(p.excess + y);
+    }
+    y = __shfl_sync(0xffffffffu, y, 0);
+    need = __shfl_sync(0xffffffffu, need, 0);
+    if (need <= 0) continue;
+    const int beg = __ldg(p.off + y), end = __ldg(p.off + y + 1);
+    long long got = 0;
+    for (int pass = 0; pass < 2 && need > 0; pass++) {
+      for (int a0 = beg; a0 < end && need > 0; a0 += 32) {
+        const int a = a0 + lane;
+        int x = -1, pa = -1;
+        long long cand = 0;
+        if (a < end) {
+          x = __ldg(p.adj + a);
+          pa = __ldg(p.par + a);
+          const int r = __ldcg(p.res + pa);  // residual x -> y
+          if (r > 0 && __ldcg(p.dead + x) && !is_term(p, x)) {
+            if (pass == 0) {
+              const long long ex = __ldcg(p.excess + x);
+              if (ex > 0) cand = ex < r ? ex : r;
+            } else if (__ldcg(p.stamp + x) != (int)wave) {
+              cand = r;
+            }
+          }
+          ls.arcs++;
+        }
+        const long long pre = cg::exclusive_scan(cg::tiled_partition<32>(cg::this_thread_block()), cand,
+                                                 cg::plus<long long>());
+        long long take = need - pre;
+        take = take < 0 ? 0 : (take > cand ? cand : take);
+        if (take > 0) {
+          const long long old = atomic_add_ll(p.excess + x, -take);
+          if (pass == 0) {
+            // only parked excess: hand back what another puller took first
+            if (old < take) {
+              const long long back = take - (old > 0 ? old : 0);
+              atomic_add_ll(p.excess + x, back);
+              take -= back;
+            }
+          } else if (old - take < 0 && atomicExch(p.stamp + x, (int)wave) != (int)wave) {
+            // x takes this part of the deficit over: it pulls next round and is checked at the end
+            append(nxt, &out->q, x);
+            append(p.dq, &p.ctrl->dcand, x);
+          }
+          if (take > 0) {
+            atomicSub(p.res + pa, (int)take);
+            atomicAdd(p.res + a, (int)take);
+            ls.pushes++;
+          }
+        }
+        const long long moved = cg::reduce(cg::tiled_partition<32>(cg::this_thread_block()), take,
+                                           cg::plus<long long>());
+        need -= moved;
+        got += moved;
+      }
+    }
+    if (lane == 0 && got) atomic_add_ll(p.excess + y, got);
+  }
+}
+
+// Counts the dead deficits left (pulls and pushes never create a deficit
+// outside dq: every vertex a pull moves a deficit to joins it).
 __device__ __forceinline__ void ph_dead_check(const Params &p, const Ctrl *sc) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   Ctrl *c = p.ctrl;
@@ -1393,7 +1443,6 @@ __device__ __forceinline__ void clear_slot(Slot *s) {
   s->hq = 0;
   s->arcs = 0;
   s->cnt = 0;
-  s->exsum = 0;
 }
 
 // ---- push-pull, phase 1 (code/dyn_pp_bench.cu:6-88, part_pp) --------------------
@@ -1703,9 +1752,7 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
   unsigned round_id = p.round_base;
 
   // ---- local repair inside the kept dead set ------------------------------------
-  bool revive = true;   // the first global relabel revives every vertex
-  bool clean = false;   // kept dead vertices need their height put back to V
-  int epoch_off = 0;    // relabel epochs the local repair used
+  bool revive = true;  // the first global relabel revives every vertex
   if (p.mode == MODE_DYNAMIC && p.keep_dead) {
     revive = false;
     kind = TR_DEAD_SEED;
@@ -1715,42 +1762,14 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     if (!next()) return;
     if (lead) c->st_dseeds = (unsigned long long)sc->dseeds;
     if (sc->dseeds > 0) {
-      clean = true;
-      epoch_off = 1;
-      const long long need = sc->dneed;
-      long long got = 0;
-      int L = 0;
-      for (;; L++) {
+      for (int r = 0; r < kDeadRounds; r++) {
         const Slot *in = slot_in();
-        got += in->exsum;
-        if (in->q + in->hq == 0 || got >= 2 * need || L >= kDeadLevels) break;
-        kind = TR_DEAD_BFS;
+        if (in->q == 0) break;
+        kind = TR_DEAD_PULL;
         items = in->q;
-        hubitems = in->hq;
-        ph_bfs_td<TILE, true>(p, in, slot_out(), L, ls);
+        hubitems = 0;
+        ph_dead_pull(p, p.fq[r & 1], in->q, p.fq[(r + 1) & 1], slot_out(), ls);
         if (!next()) return;
-        if (lead) c->st_levels++;
-      }
-      const int A = sc->act_q + sc->act_hq;
-      const int rounds = A == 0 ? 0 : 2 * (L + 1) + p.interval;
-      for (int r = 0; r < rounds; r++) {
-        round_id++;
-        const RoundIn in = round_inputs(p, sc, r, true);
-        kind = TR_DEAD_PUSH;
-        items = in.nn;
-        hubitems = in.nh;
-        ph_push1<TILE, BLOCK>(p, in, r, round_id, p.relabel_base, ls, btmp, bci, bcl, true);
-        if (!next()) return;
-        if (in.nh > 0) {
-          kind = TR_PUSH_HUB_FINISH;
-          ph_push3(p, in, r, round_id, ls, true);
-          if (!next()) return;
-        }
-        if (lead) {
-          c->st_rounds++;
-          c->rounds_used = round_id - p.round_base;
-        }
-        if (sc->wtail[r % 3] + sc->whtail[r % 3] == 0) break;
       }
       kind = TR_DEAD_CHECK;
       items = hubitems = 0;
@@ -1812,7 +1831,7 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     }
     kind = TR_BFS_INIT;
     items = hubitems = 0;
-    ph_bfs_init(p, slot_out(), it == 0 && revive, it == 0 && clean && !revive, it == 0 && !revive);
+    ph_bfs_init(p, slot_out(), it == 0 && revive, it == 0 && !revive);
     if (!next()) return;
     if (lead) c->st_outer++;
     const int P = sc->pos_count;
@@ -1862,7 +1881,7 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
       kind = TR_PUSH;
       items = in.nn;
       hubitems = in.nh;
-      ph_push1<TILE, BLOCK>(p, in, r, round_id, p.relabel_base + epoch_off + it, ls, btmp, bci, bcl, false);
+      ph_push1<TILE, BLOCK>(p, in, r, round_id, p.relabel_base + it, ls, btmp, bci, bcl, false);
       if (!next()) return;
       if (in.nh > 0) {
         kind = TR_PUSH_HUB_FINISH;
