@@ -64,6 +64,7 @@ struct Params {
   const int *__restrict__ par;
   const int *__restrict__ sidx;
   const int *__restrict__ shead;  // heads in per-vertex sorted order (arc lookup)
+  const int *__restrict__ ssamp;  // every kSampleStride-th entry of shead (ssamp[j] = shead[j * stride])
   int *cap, *res, *height, *stamp, *astamp, *uarc;
   long long *excess;
   unsigned char *dead, *side;
@@ -231,10 +232,36 @@ __device__ __forceinline__ void ph_saturate(const Params &p) {
 // (shead[i] = adj[sidx[i]]), so a search step is one load; sidx maps the found
 // position back to the arc.  Equal heads (a CSR with duplicate arcs) resolve to
 // the last arc among them, as OnAdd_kernel's linear scan keeps the last match.
+// A long adjacency is searched in two steps: first over `ssamp`, every
+// kSampleStride-th head (m / 32 entries, small enough to stay in L2), then
+// within the window of kSampleStride heads that sample opens, so a search
+// reads about one DRAM sector of shead instead of one per step.
+constexpr int kSampleStride = 32;
+
+// The window [lo, hi) of u's sorted heads [b, e) that holds the last head <= v.
+struct SearchRange {
+  int lo, hi;
+};
+
+__device__ __forceinline__ SearchRange sample_window(const int *__restrict__ ssamp, int b, int e, int v) {
+  if (e - b <= kSampleStride) return {b, e};
+  int jlo = (b + kSampleStride - 1) / kSampleStride, jhi = (e - 1) / kSampleStride + 1;  // samples in [b, e)
+  if (__ldg(ssamp + jlo) > v) return {b, jlo * kSampleStride};
+  while (jhi - jlo > 1) {  // last sample <= v
+    const int mid = (jlo + jhi) >> 1;
+    if (__ldg(ssamp + mid) <= v) jlo = mid;
+    else jhi = mid;
+  }
+  const int lo = jlo * kSampleStride;
+  return {lo, min(e, lo + kSampleStride)};
+}
+
 __device__ __forceinline__ int find_arc_dev(const int *__restrict__ off, const int *__restrict__ shead,
-                                            const int *__restrict__ sidx, int u, int v) {
+                                            const int *__restrict__ ssamp, const int *__restrict__ sidx, int u,
+                                            int v) {
   const int first = __ldg(off + u);
-  int lo = first, hi = __ldg(off + u + 1);
+  const SearchRange w = sample_window(ssamp, first, __ldg(off + u + 1), v);
+  int lo = w.lo, hi = w.hi;
   while (lo < hi) {  // last position with head <= v
     const int mid = (lo + hi) >> 1;
     if (__ldg(shead + mid) <= v) lo = mid + 1;
@@ -279,7 +306,51 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
       hi[j] = on[j] ? __ldg(p.off + u[j] + 1) : 0;
       lo[j] = first[j];
     }
-    for (;;) {  // last position with head <= v, all searches one step at a time
+    // step 1, long adjacencies: the sample that opens the window, all searches
+    // in lockstep (jlo/jhi index ssamp; a search over [b, e) uses the samples in it)
+    int jlo[kLookupBatch], jhi[kLookupBatch];
+#pragma unroll
+    for (int j = 0; j < kLookupBatch; j++) {
+      jlo[j] = jhi[j] = 0;
+      if (hi[j] - lo[j] > kSampleStride) {
+        jlo[j] = (lo[j] + kSampleStride - 1) / kSampleStride;
+        jhi[j] = (hi[j] - 1) / kSampleStride + 1;
+      }
+    }
+    int s0[kLookupBatch];
+#pragma unroll
+    for (int j = 0; j < kLookupBatch; j++) s0[j] = jhi[j] > jlo[j] ? __ldg(p.ssamp + jlo[j]) : 0;
+#pragma unroll
+    for (int j = 0; j < kLookupBatch; j++)
+      if (jhi[j] > jlo[j] && s0[j] > v[j]) {  // v below every sample: the window before the first
+        hi[j] = jlo[j] * kSampleStride;
+        jhi[j] = jlo[j];
+      }
+    for (;;) {
+      int mid[kLookupBatch], sv[kLookupBatch];
+      bool any = false;
+#pragma unroll
+      for (int j = 0; j < kLookupBatch; j++)
+        if (jhi[j] - jlo[j] > 1) {
+          mid[j] = (jlo[j] + jhi[j]) >> 1;
+          sv[j] = __ldg(p.ssamp + mid[j]);
+          any = true;
+        }
+      if (!any) break;
+#pragma unroll
+      for (int j = 0; j < kLookupBatch; j++)
+        if (jhi[j] - jlo[j] > 1) {
+          if (sv[j] <= v[j]) jlo[j] = mid[j];
+          else jhi[j] = mid[j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kLookupBatch; j++)
+      if (jhi[j] - jlo[j] == 1) {
+        lo[j] = jlo[j] * kSampleStride;
+        hi[j] = min(hi[j], lo[j] + kSampleStride);
+      }
+    for (;;) {  // step 2: last position with head <= v in the window
       int mid[kLookupBatch], hv[kLookupBatch];
       bool any = false;
 #pragma unroll

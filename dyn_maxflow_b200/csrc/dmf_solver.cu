@@ -21,7 +21,8 @@ namespace {
 // the schedule picker (nothing is modified).  Updates the solver would reject
 // (bad ids, unknown arcs) are skipped here; the solve reports them.
 __global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, const int *__restrict__ shead,
-                                                  const int *__restrict__ sidx, const int *cap, const int *res, int n,
+                                                  const int *__restrict__ ssamp, const int *__restrict__ sidx,
+                                                  const int *cap, const int *res, int n,
                                                   int k, const int *usrc, const int *udst, const int *uw,
                                                   dmfs::FeatAcc *acc) {
   unsigned long long valid = 0, dec = 0, satdec = 0, incsat = 0, ins = 0, del = 0, sdeg = 0, mdeg = 0;
@@ -29,7 +30,7 @@ __global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, c
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
     const int u = __ldg(usrc + i), v = __ldg(udst + i), w = __ldg(uw + i);
     if (u < 0 || u >= n || v < 0 || v >= n || u == v) continue;
-    const int e = find_arc_dev(off, shead, sidx, u, v);
+    const int e = find_arc_dev(off, shead, ssamp, sidx, u, v);
     if (e < 0) continue;
     valid++;
     const int c0 = __ldcg(cap + e), r = __ldcg(res + e);
@@ -100,6 +101,7 @@ struct dmf_solver {
   int tile = 32, grid = 0, block = kBlock, hub_deg = 256, small_deg = 8, minb = 2, bu_alpha = 2;
   int *off = nullptr, *adj = nullptr, *par = nullptr, *sidx = nullptr, *cap = nullptr, *res = nullptr;
   int *shead = nullptr;  // heads in per-vertex sorted order (shead[i] = adj[sidx[i]])
+  int *ssamp = nullptr;  // every kSampleStride-th entry of shead
   int *height = nullptr, *stamp = nullptr, *astamp = nullptr, *uarc = nullptr;
   long long *excess = nullptr;
   unsigned char *dead = nullptr, *side = nullptr;
@@ -275,6 +277,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.par = sv->par;
   p.sidx = sv->sidx;
   p.shead = sv->shead;
+  p.ssamp = sv->ssamp;
   p.cap = sv->cap;
   p.res = sv->res;
   p.height = sv->height;
@@ -491,8 +494,8 @@ int batch_features(dmf_solver *sv, dmf_sched *sched, int k, float *feat, int *ac
   if (k > 0) {
     const size_t K = (size_t)sv->kcap;
     const int blocks = std::min((k + 255) / 256, 4 * 148);
-    k_features<<<blocks, 256, 0, sv->stream>>>(sv->off, sv->shead, sv->sidx, sv->cap, sv->res, sv->n, k, sv->ubuf,
-                                               sv->ubuf + K, sv->ubuf + 2 * K, sv->facc);
+    k_features<<<blocks, 256, 0, sv->stream>>>(sv->off, sv->shead, sv->ssamp, sv->sidx, sv->cap, sv->res, sv->n, k,
+                                               sv->ubuf, sv->ubuf + K, sv->ubuf + 2 * K, sv->facc);
     CK(cudaGetLastError(), "feature launch");
   }
   dmfs::FeatScalars sc;
@@ -671,6 +674,7 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
     p.par = d_par;
     p.sidx = nullptr;
     p.shead = nullptr;
+    p.ssamp = nullptr;
     p.cap = const_cast<int *>(d_cap);  // read only in static mode
     p.res = d_res;
     p.astamp = nullptr;
@@ -783,7 +787,8 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   if ((st = configure(sv))) return st;
   const size_t N = (size_t)g->n + 1, M = (size_t)g->m;
   if ((st = dalloc(sv, &sv->off, N)) || (st = dalloc(sv, &sv->adj, M)) || (st = dalloc(sv, &sv->par, M)) ||
-      (st = dalloc(sv, &sv->sidx, M)) || (st = dalloc(sv, &sv->shead, M)) || (st = dalloc(sv, &sv->cap, M)) ||
+      (st = dalloc(sv, &sv->sidx, M)) || (st = dalloc(sv, &sv->shead, M)) ||
+      (st = dalloc(sv, &sv->ssamp, M / kSampleStride + 1)) || (st = dalloc(sv, &sv->cap, M)) ||
       (st = dalloc(sv, &sv->res, M)) ||
       (st = dalloc(sv, &sv->astamp, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
       (st = dalloc(sv, &sv->excess, N)) || (st = dalloc(sv, &sv->dead, N)) || (st = dalloc(sv, &sv->side, N)) ||
@@ -819,6 +824,9 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < (int64_t)M; i++) shead[i] = g->adj[g->sidx[i]];
   up(sv->shead, shead.data(), 4 * M);
+  std::vector<int32_t> ssamp(M / kSampleStride + 1, INT_MAX);
+  for (size_t j = 0; j * kSampleStride < M; j++) ssamp[j] = shead[j * kSampleStride];
+  up(sv->ssamp, ssamp.data(), 4 * ssamp.size());
   up(sv->cap, g->w.data(), 4 * M);
   up(sv->hch, hub_chunks.data(), sizeof(int2) * hub_chunks.size());
   up(sv->hub_base, hub_base.data(), 4 * (size_t)g->n);
