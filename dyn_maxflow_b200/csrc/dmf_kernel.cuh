@@ -20,8 +20,9 @@
 // A dynamic batch keeps the dead set of the last solve (the vertices proven
 // unable to reach t or a deficit): updated arcs that open residual from it to
 // the live side are saturated at once (ph_reopen), the deficits this leaves
-// inside the dead set are covered there by pulls from the excess parked in it
-// (ph_dead_seed, ph_dead_pull, ph_dead_check), and the global relabels then
+// inside the dead set are covered there by pulls from excess inside it, along
+// labels of a short BFS from that excess (ph_dead_seed, ph_dead_bfs,
+// ph_dead_pull, ph_dead_check), and the global relabels then
 // only visit live vertices.  A deficit the pulls cannot cover revives every
 // vertex.
 #pragma once
@@ -47,11 +48,12 @@ enum TraceKind : int {
   TR_START = 0, TR_INIT_RES = 1, TR_SATURATE = 2, TR_LOOKUP = 3, TR_APPLY = 4, TR_REPAIR = 5,
   TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
   TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14, TR_PP_INIT = 15, TR_PP_BFS = 16, TR_PP_FINALIZE = 17,
-  TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_PULL = 21, TR_DEAD_CHECK = 23
+  TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_PULL = 21, TR_DEAD_BFS = 22, TR_DEAD_CHECK = 23
 };
 
-// Local repair inside a kept dead set: at most this many pull rounds.
-constexpr int kDeadRounds = 8;
+// Local repair inside a kept dead set: BFS levels from the excess, pull rounds.
+constexpr int kDeadLevels = 6;
+constexpr int kDeadRounds = kDeadLevels + 2;
 
 // Largest capacity an update may set: keeps cap(e) + cap(partner) < 2^31 when
 // both arcs of a pair change in one batch.
@@ -69,7 +71,8 @@ struct Params {
   long long *excess;
   unsigned char *dead, *side;
   int *fq[2], *wq[2], *aq;     // non-hub vertex queues
-  int *dq;                     // dead vertices whose excess the batch lowered (kept dead set)
+  int *dq;                     // dead vertices whose excess the batch changed (kept dead set)
+  int *dlab;                   // distance from excess inside the dead set, (wave << 4) | level
   int2 *fh[2], *wh[2], *ah;    // hub chunk queues
   const int2 *hch;             // every hub's chunks (bottom-up BFS, topology-driven rounds)
   int nhch;
@@ -426,7 +429,10 @@ __device__ __forceinline__ void ph_repair(const Params &p) {
       const int v = __ldg(p.adj + e);
       atomic_add_ll(p.excess + __ldg(p.usrc + i), -(long long)r);
       atomic_add_ll(p.excess + v, (long long)r);
-      if (p.keep_dead && __ldcg(p.dead + v)) add_dead_cand(p, v);
+      if (p.keep_dead) {  // the overflow returns to the tail: excess that can cover the head's deficit
+        if (__ldcg(p.dead + v)) add_dead_cand(p, v);
+        if (__ldcg(p.dead + __ldg(p.usrc + i))) add_dead_cand(p, __ldg(p.usrc + i));
+      }
     }
   }
 }
@@ -836,22 +842,41 @@ __device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int 
 }
 
 // ---- local repair inside a kept dead set ------------------------------------------
-// The batch left deficits on some dead vertices (candidates in dq).  They are
-// covered from the excess parked inside the dead set, without reviving it, by
-// pulls: a deficit y takes what it lacks over residual arcs x->y from dead
-// in-neighbours x, first from those holding excess (exactly the amount missing,
-// so parked excess is not flooded around), then, for what is still missing,
-// from dead in-neighbours not yet touched by this repair, which take that part
-// of the deficit over and pull in the next round.  A vertex is stamped the
-// first time a deficit reaches it, so deficits only move to fresh vertices and
-// the rounds end (at most kDeadRounds).  Only dead vertices are pulled from, so
-// the pulled flow stays inside the dead set and every arc it adds residual to
-// (y->x) lies inside it: the set stays closed.  A deficit left over makes the
-// first global relabel revive every vertex (the solve then proceeds as from a
-// reset dead set).
+// The batch changed the excess of some dead vertices (candidates in dq): the
+// heads of repaired arcs got deficits, their tails the returned overflow, the
+// tails of reopened arcs deficits.  The deficits are covered from excess inside
+// the dead set, without reviving it:
+//  1. a short BFS forward from the candidates holding excess, over residual
+//     arcs between dead vertices, labels dead vertices with their distance from
+//     that excess (dlab, tagged with the call's wave so that no reset is
+//     needed; at most kDeadLevels levels, ending once every deficit is labelled);
+//  2. pull rounds: a deficit takes what it lacks over residual arcs x->y from
+//     dead in-neighbours holding excess (exactly the missing amount, so parked
+//     excess is not flooded around), and moves the rest to in-neighbours with a
+//     smaller label, which pull in the next round.  Labels fall along every
+//     move, so deficits head for the excess and never cycle.
+// Only dead vertices are pulled from, so every arc that gains residual (y->x)
+// lies inside the dead set: it stays closed.  A deficit left over (an O(n)
+// check) makes the first global relabel revive every vertex.
 
-// Seeds: the candidates with a deficit.  (Candidates are stamped with the
-// repair's wave, round_base, when they join dq.)
+__device__ __forceinline__ unsigned dead_wave(const Params &p) { return ((unsigned)p.epoch & 0x0fffffffu) << 4; }
+
+// Claims dead vertex v for BFS level `lv` of this call's wave; true if this thread did.
+__device__ __forceinline__ bool dead_label(const Params &p, int v, int lv) {
+  const unsigned wave = dead_wave(p);
+  const unsigned old = (unsigned)__ldcg(p.dlab + v);
+  if ((old & ~15u) == wave) return false;
+  return (unsigned)atomicCAS(p.dlab + v, (int)old, (int)(wave | (unsigned)lv)) == old;
+}
+
+// Level of v in this call's BFS, or 16 when it was not reached.
+__device__ __forceinline__ int dead_level(const Params &p, int v) {
+  const unsigned l = (unsigned)__ldcg(p.dlab + v);
+  return (l & ~15u) == dead_wave(p) ? (int)(l & 15u) : 16;
+}
+
+// Seeds: candidates with excess start the BFS (level 0), candidates with a
+// deficit form the first pull list (aq).
 __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Slot *out) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   Ctrl *c = p.ctrl;
@@ -861,20 +886,67 @@ __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Sl
   for (int i = gt; i < nc; i += nt) {
     const int v = __ldcg(p.dq + i);
     const long long ex = __ldcg(p.excess + v);
-    if (ex >= 0 || is_term(p, v)) continue;
-    append(p.fq[0], &out->q, v);
-    seeds++;
-    need -= ex;
+    if (is_term(p, v) || ex == 0) continue;
+    if (ex > 0) {
+      if (dead_label(p, v, 0)) {
+        if (deg_of(p, v) > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
+        else append(p.fq[0], &out->q, v);
+      }
+    } else {
+      append(p.aq, &c->act_q, v);
+      seeds++;
+      need -= ex;
+    }
   }
   block_add_int(&c->dseeds, seeds);
   block_add_ll(&c->dneed, need);
 }
 
-// One pull round: a warp per deficit of the list, lanes over its arcs.
-__device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, int nn, int *nxt, Slot *out,
-                                             LStats &ls) {
-  const unsigned wave = p.round_base;
+// Out-arcs first, first+stride, ... < end of frontier vertex x at level L.
+__device__ __forceinline__ void dead_bfs_range(const Params &p, Slot *out, int nxt, int first, int end, int stride,
+                                               int L, LStats &ls, int &reached) {
+  for (int a = first; a < end; a += stride) {
+    const int y = __ldg(p.adj + a);
+    ls.barcs++;
+    if (__ldcg(p.res + a) <= 0 || !__ldcg(p.dead + y) || is_term(p, y)) continue;
+    if (!dead_label(p, y, L + 1)) continue;
+    if (deg_of(p, y) > p.hub_deg) append_hub(p, p.fh[nxt], &out->hq, y);
+    else append(p.fq[nxt], &out->q, y);
+    if (__ldcg(p.excess + y) < 0) reached++;
+  }
+}
+
+template <int TILE>
+__device__ __forceinline__ void ph_dead_bfs(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
+  const int cur = L & 1, nxt = cur ^ 1;
+  const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
+  int reached = 0;
   const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = spread_group<32>(); i < nh; i += nwarps) {
+    int beg, end;
+    const int2 it = __ldcg(p.fh[cur] + i);
+    chunk_range(p, it, beg, end);
+    dead_bfs_range(p, out, nxt, beg + lane, end, 32, L, ls, reached);
+  }
+  for_tiered<TILE>(p, ls, p.fq[cur], nn, [&](auto &g, int x) {
+    const int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
+    dead_bfs_range(p, out, nxt, beg + g.rank(), end, g.size(), L, ls, reached);
+  });
+  block_add_int(&out->cnt, reached);
+}
+
+// Pull round r: a warp per deficit of the round's list, lanes over its arcs.
+// List r = 0 is aq (act_q), list r > 0 is wq[(r-1) & 1] (wtail[(r-1) % 3]);
+// vertices a deficit moves to go to wq[r & 1] (wtail[r % 3]), once per round.
+__device__ __forceinline__ void ph_dead_pull(const Params &p, const Ctrl *sc, int r, unsigned round_id, LStats &ls) {
+  Ctrl *c = p.ctrl;
+  if (blockIdx.x == 0 && threadIdx.x == 0) c->wtail[(r + 1) % 3] = 0;
+  const int *list = r == 0 ? p.aq : p.wq[(r - 1) & 1];
+  const int nn = r == 0 ? sc->act_q : sc->wtail[(r - 1) % 3];
+  int *nxt = p.wq[r & 1];
+  int *ntail = &c->wtail[r % 3];
+  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
+  cg::thread_block_tile<32> warp = cg::tiled_partition<32>(cg::this_thread_block());
   for (int i = spread_group<32>(); i < nn; i += nwarps) {
     int y = 0;
     long long need = 0;
@@ -882,12 +954,14 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
       y = __ldcg(list + i);
       need = -__ldcg(p.excess + y);
     }
-    y = __shfl_sync(0xffffffffu, y, 0);
-    need = __shfl_sync(0xffffffffu, need, 0);
+    y = warp.shfl(y, 0);
+    need = warp.shfl(need, 0);
     if (need <= 0) continue;
+    const int ly = dead_level(p, y);
     const int beg = __ldg(p.off + y), end = __ldg(p.off + y + 1);
     long long got = 0;
     for (int pass = 0; pass < 2 && need > 0; pass++) {
+      if (pass == 1 && ly == 0) break;  // nothing below it to move the deficit to
       for (int a0 = beg; a0 < end && need > 0; a0 += 32) {
         const int a = a0 + lane;
         int x = -1, pa = -1;
@@ -895,19 +969,18 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
         if (a < end) {
           x = __ldg(p.adj + a);
           pa = __ldg(p.par + a);
-          const int r = __ldcg(p.res + pa);  // residual x -> y
-          if (r > 0 && __ldcg(p.dead + x) && !is_term(p, x)) {
+          const int rr = __ldcg(p.res + pa);  // residual x -> y
+          if (rr > 0 && __ldcg(p.dead + x) && !is_term(p, x)) {
             if (pass == 0) {
               const long long ex = __ldcg(p.excess + x);
-              if (ex > 0) cand = ex < r ? ex : r;
-            } else if (__ldcg(p.stamp + x) != (int)wave) {
-              cand = r;
+              if (ex > 0) cand = ex < rr ? ex : rr;
+            } else if (dead_level(p, x) < ly) {
+              cand = rr;
             }
           }
           ls.arcs++;
         }
-        const long long pre = cg::exclusive_scan(cg::tiled_partition<32>(cg::this_thread_block()), cand,
-                                                 cg::plus<long long>());
+        const long long pre = cg::exclusive_scan(warp, cand, cg::plus<long long>());
         long long take = need - pre;
         take = take < 0 ? 0 : (take > cand ? cand : take);
         if (take > 0) {
@@ -919,10 +992,8 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
               atomic_add_ll(p.excess + x, back);
               take -= back;
             }
-          } else if (old - take < 0 && atomicExch(p.stamp + x, (int)wave) != (int)wave) {
-            // x takes this part of the deficit over: it pulls next round and is checked at the end
-            append(nxt, &out->q, x);
-            append(p.dq, &p.ctrl->dcand, x);
+          } else if (old - take < 0 && atomicExch(p.stamp + x, (int)round_id) != (int)round_id) {
+            append(nxt, ntail, x);  // x pulls its part next round
           }
           if (take > 0) {
             atomicSub(p.res + pa, (int)take);
@@ -930,8 +1001,7 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
             ls.pushes++;
           }
         }
-        const long long moved = cg::reduce(cg::tiled_partition<32>(cg::this_thread_block()), take,
-                                           cg::plus<long long>());
+        const long long moved = cg::reduce(warp, take, cg::plus<long long>());
         need -= moved;
         got += moved;
       }
@@ -940,18 +1010,14 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
   }
 }
 
-// Counts the dead deficits left (pulls and pushes never create a deficit
-// outside dq: every vertex a pull moves a deficit to joins it).
-__device__ __forceinline__ void ph_dead_check(const Params &p, const Ctrl *sc) {
-  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
-  Ctrl *c = p.ctrl;
+// Counts the deficits left inside the dead set (every dead vertex is looked at:
+// the check cannot miss one the pulls moved).
+__device__ __forceinline__ void ph_dead_check(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   int left = 0;
-  const int nc = sc->dcand;
-  for (int i = gt; i < nc; i += nt) {
-    const int v = __ldcg(p.dq + i);
-    if (__ldcg(p.excess + v) < 0 && !is_term(p, v)) left++;
-  }
-  block_add_int(&c->dleft, left);
+  for (int v = gt; v < p.n; v += nt)
+    if (__ldcg(p.dead + v) && inst_on(p, v) && !is_term(p, v) && __ldcg(p.excess + v) < 0) left++;
+  block_add_int(&p.ctrl->dleft, left);
 }
 
 // ---- push rounds ---------------------------------------------------------------
@@ -1829,22 +1895,37 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     kind = TR_DEAD_SEED;
     items = sc->dcand;
     hubitems = 0;
-    ph_dead_seed(p, sc, slot_out());
+    ph_dead_seed(p, sc, slot_out());  // act_q and wtail[0] are still 0 from the launch
     if (!next()) return;
     if (lead) c->st_dseeds = (unsigned long long)sc->dseeds;
-    if (sc->dseeds > 0) {
-      for (int r = 0; r < kDeadRounds; r++) {
+    const int nseeds = sc->dseeds;
+    if (nseeds > 0) {
+      int reached = 0;
+      for (int L = 0;; L++) {
         const Slot *in = slot_in();
-        if (in->q == 0) break;
-        kind = TR_DEAD_PULL;
+        reached += in->cnt;
+        if (in->q + in->hq == 0 || reached >= nseeds || L >= kDeadLevels) break;
+        kind = TR_DEAD_BFS;
         items = in->q;
-        hubitems = 0;
-        ph_dead_pull(p, p.fq[r & 1], in->q, p.fq[(r + 1) & 1], slot_out(), ls);
+        hubitems = in->hq;
+        ph_dead_bfs<TILE>(p, in, slot_out(), L, ls);
         if (!next()) return;
+        if (lead) c->st_levels++;
+      }
+      for (int r = 0; r < kDeadRounds; r++) {
+        const int nn = r == 0 ? sc->act_q : sc->wtail[(r - 1) % 3];
+        if (nn == 0) break;
+        round_id++;
+        kind = TR_DEAD_PULL;
+        items = nn;
+        hubitems = 0;
+        ph_dead_pull(p, sc, r, round_id, ls);
+        if (!next()) return;
+        if (lead) c->rounds_used = round_id - p.round_base;
       }
       kind = TR_DEAD_CHECK;
       items = hubitems = 0;
-      ph_dead_check(p, sc);
+      ph_dead_check(p);
       if (!next()) return;
       revive = sc->dleft > 0;
     }

@@ -105,6 +105,7 @@ struct dmf_solver {
   int *height = nullptr, *stamp = nullptr, *astamp = nullptr, *uarc = nullptr;
   long long *excess = nullptr;
   unsigned char *dead = nullptr, *side = nullptr;
+  int *dlab = nullptr;    // dead-set repair labels, tagged with the launch epoch
   int *qbuf = nullptr;    // 6 vertex queues (frontier x2, worklist x2, active, dead-set candidates)
   int2 *hqbuf = nullptr;  // 5 hub-chunk queues, same roles
   int2 *hch = nullptr;    // every hub's chunks
@@ -297,6 +298,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   }
   p.aq = sv->qbuf + 4 * N;
   p.dq = sv->qbuf + 5 * N;
+  p.dlab = sv->dlab;
   p.ah = sv->hqbuf + 4 * NC;
   p.hch = sv->hch;
   p.nhch = sv->nchunk;
@@ -646,6 +648,7 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
     p.wq[1] = (int *)carve(4 * N);
     p.aq = (int *)carve(4 * N);
     p.dq = nullptr;  // static solves never keep a dead set
+    p.dlab = nullptr;
     // no hubs in this mode (hub_deg = INT_MAX): the hub structures are never read
     int2 *hub_dummy = (int2 *)carve(kNoAllocAlign);
     long long *ll_dummy = (long long *)carve(kNoAllocAlign);
@@ -792,7 +795,7 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
       (st = dalloc(sv, &sv->res, M)) ||
       (st = dalloc(sv, &sv->astamp, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
       (st = dalloc(sv, &sv->excess, N)) || (st = dalloc(sv, &sv->dead, N)) || (st = dalloc(sv, &sv->side, N)) ||
-      (st = dalloc(sv, &sv->qbuf, 6 * N)) || (st = dalloc(sv, &sv->ctrl, 1)))
+      (st = dalloc(sv, &sv->qbuf, 6 * N)) || (st = dalloc(sv, &sv->dlab, N)) || (st = dalloc(sv, &sv->ctrl, 1)))
     return st;
   std::vector<int2> hub_chunks;
   std::vector<int> hub_base(g->n, -1);
@@ -837,6 +840,7 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->hc_moved, 0, 8 * NC, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->stamp, 0, 4 * N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->dead, 0, N, S);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->dlab, 0, 4 * N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->side, 0, N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->excess, 0, 8 * N, S);
   if (e == cudaSuccess) e = cudaMallocHost(&sv->h_ctrl, sizeof(Ctrl));
