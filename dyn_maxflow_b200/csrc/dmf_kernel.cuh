@@ -567,6 +567,29 @@ __device__ __forceinline__ void chunk_range(const Params &p, int2 it, int &beg, 
 
 #define UNV (p.n + 1)
 
+// Every vertex v of the call (instances outside the mask skipped) with its dead
+// flag, f(v, dead): a thread takes vertices v0, v0 + nt, ... (coalesced across
+// the warp), U at a time with their flag loads in flight together.  With a
+// kept dead set nearly every vertex is dead and costs just that load, so the
+// loop is bound by load latency unless several are outstanding.
+template <int U, class F>
+__device__ __forceinline__ void for_vertices(const Params &p, F &&f) {
+  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int v0 = gt; v0 < p.n; v0 += U * nt) {
+    unsigned char dd[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      const int v = v0 + j * nt;
+      dd[j] = v < p.n ? __ldcg(p.dead + v) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      const int v = v0 + j * nt;
+      if (v < p.n && inst_on(p, v)) f(v, dd[j] != 0);
+    }
+  }
+}
+
 // Seeds (my_init_1, code/dyn_data.h:60-67): t and every deficit vertex other
 // than s get height 0; all other live vertices become unvisited.  reset_dead
 // revives every vertex (the first relabel of a solve that does not keep the
@@ -575,7 +598,7 @@ __device__ __forceinline__ void chunk_range(const Params &p, int2 it, int &beg, 
 // outside the call's mask are not touched at all: their labels and dead set
 // stay as their own last solve left them.
 __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool reset_dead, bool count_kept) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   Ctrl *c = p.ctrl;
   if (gt == 0) {
     c->act_q = 0;
@@ -584,13 +607,12 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
   }
   int pos = 0, kept = 0;
   long long unexpl = 0, seed_arcs = 0;
-  for (int v = gt; v < p.n; v += nt) {
-    if (p.inst_active && !p.inst_active[__ldg(p.inst + v)]) continue;
+  for_vertices<4>(p, [&](int v, bool is_dead) {
     if (reset_dead) {
-      if (__ldcg(p.dead + v)) p.dead[v] = 0;
-    } else if (__ldcg(p.dead + v)) {
+      if (is_dead) p.dead[v] = 0;
+    } else if (is_dead) {
       kept++;
-      continue;
+      return;
     }
     long long ex = __ldcg(p.excess + v);
     int d = deg_of(p, v);
@@ -621,7 +643,7 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
       unexpl += d;
     }
     if (!is_term(p, v) && ex > 0) pos++;
-  }
+  });
   block_add_int(&c->pos_count, pos);
   block_add_ll(&c->unexplored, unexpl);
   block_add_ll(&out->arcs, seed_arcs);
@@ -822,11 +844,13 @@ __device__ __forceinline__ void ph_bfs_bu(const Params &p, Slot *out, int L, LSt
 // After the BFS: a complete BFS proves every unvisited vertex unreachable
 // (dead for the rest of this solve; the reference gives them height V); an
 // early-stopped BFS gives them the valid lower bound `floor`.
+// Vertices already dead are skipped: they sit at height V and side 0 since the
+// BFS that proved them dead.
 __device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int floor_h, bool write_side) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   int nd = 0;
-  for (int v = gt; v < p.n; v += nt) {
-    int h = __ldcg(p.height + v);
+  for_vertices<8>(p, [&](int v, bool is_dead) {
+    if (is_dead) return;
+    const int h = __ldcg(p.height + v);
     if (h == UNV) {
       if (full) {
         p.dead[v] = 1;
@@ -836,8 +860,8 @@ __device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int 
         p.height[v] = floor_h;
       }
     }
-    if (write_side && (!p.inst_active || p.inst_active[__ldg(p.inst + v)])) p.side[v] = h < p.n ? 1 : 0;
-  }
+    if (write_side) p.side[v] = h < p.n ? 1 : 0;
+  });
   block_add_ll((long long *)&p.ctrl->st_dead, nd);
 }
 
@@ -1013,10 +1037,10 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const Ctrl *sc, in
 // Counts the deficits left inside the dead set (every dead vertex is looked at:
 // the check cannot miss one the pulls moved).
 __device__ __forceinline__ void ph_dead_check(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   int left = 0;
-  for (int v = gt; v < p.n; v += nt)
-    if (__ldcg(p.dead + v) && inst_on(p, v) && !is_term(p, v) && __ldcg(p.excess + v) < 0) left++;
+  for_vertices<8>(p, [&](int v, bool is_dead) {
+    if (is_dead && !is_term(p, v) && __ldcg(p.excess + v) < 0) left++;
+  });
   block_add_int(&p.ctrl->dleft, left);
 }
 
@@ -1555,20 +1579,22 @@ __device__ __forceinline__ void ph_push3(const Params &p, const RoundIn &in, int
 // flow = excess(t) + sum of negative excess over v != s, t (per instance in
 // batched mode).
 template <int BLOCK>
+// Dead vertices are skipped: a sink or a deficit is a seed of every global
+// relabel, so it is never proven dead.
 __device__ __forceinline__ void ph_flow(const Params &p, typename BlockGroup<BLOCK>::Temp &btmp) {
-  const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
   long long acc = 0;
-  for (int v = gt; v < p.n; v += nt) {
+  for_vertices<8>(p, [&](int v, bool is_dead) {
+    if (is_dead) return;
     const long long ex = __ldcg(p.excess + v);
     long long c = 0;
     if (is_snk(p, v)) c = ex;
     else if (!is_src(p, v) && ex < 0) c = ex;
     if (p.inst) {
-      if (c && (!p.inst_active || p.inst_active[__ldg(p.inst + v)])) atomic_add_ll(p.inst_flow + __ldg(p.inst + v), c);
+      if (c) atomic_add_ll(p.inst_flow + __ldg(p.inst + v), c);
     } else {
       acc += c;
     }
-  }
+  });
   if (p.inst) return;
   __syncthreads();
   long long tot = typename BlockGroup<BLOCK>::RedL(btmp.redl).Sum(acc);
