@@ -130,7 +130,8 @@ def test_kept_dead_set_matches_revived(dmf, oracle, name, variant):
             kept_batches += kept.stats()["dead_kept"]
             assert rev.stats()["dead_kept"] == 0
             certify(oracle, g, kept, s, t, want)
-    assert kept_batches > 0
+    if name.startswith("rmat"):  # on a grid the deficits sit far from any excess: revived
+        assert kept_batches > 0
 
 
 @pytest.mark.parametrize("tile", [4, 8, 16, 32])
