@@ -72,6 +72,7 @@ struct Ctrl {
   int dkept;                    // 1: the dead set was kept for the global relabels
   unsigned long long st_barcs;  // adjacency entries read by global-relabel BFS levels
   unsigned long long st_dseeds; // deficits inside the kept dead set (first local pass)
+  unsigned long long st_revived; // dead vertices revived because they reach a deficit left over
 };
 
 // ---- memory helpers ---------------------------------------------------------

@@ -48,7 +48,8 @@ enum TraceKind : int {
   TR_START = 0, TR_INIT_RES = 1, TR_SATURATE = 2, TR_LOOKUP = 3, TR_APPLY = 4, TR_REPAIR = 5,
   TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
   TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14, TR_PP_INIT = 15, TR_PP_BFS = 16, TR_PP_FINALIZE = 17,
-  TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_PULL = 21, TR_DEAD_BFS = 22, TR_DEAD_CHECK = 23
+  TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_PULL = 21, TR_DEAD_BFS = 22, TR_DEAD_CHECK = 23,
+  TR_DEAD_REVIVE = 24
 };
 
 // Local repair inside a kept dead set: BFS levels from the excess, pull rounds.
@@ -1034,14 +1035,69 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const Ctrl *sc, in
   }
 }
 
+// Claims dead vertex v for the partial revival of this call (tag level 15).
+__device__ __forceinline__ bool revive_claim(const Params &p, int v) {
+  const int tag = (int)(dead_wave(p) | 15u);
+  const int old = __ldcg(p.dlab + v);
+  if (old == tag) return false;
+  return atomicCAS(p.dlab + v, old, tag) == old;
+}
+
 // Counts the deficits left inside the dead set (every dead vertex is looked at:
-// the check cannot miss one the pulls moved).
-__device__ __forceinline__ void ph_dead_check(const Params &p) {
+// the check cannot miss one the pulls moved).  Each of them is revived (made
+// live: it is a seed of the global relabels) and starts the partial revival.
+__device__ __forceinline__ void ph_dead_check(const Params &p, Slot *out) {
   int left = 0;
   for_vertices<8>(p, [&](int v, bool is_dead) {
-    if (is_dead && !is_term(p, v) && __ldcg(p.excess + v) < 0) left++;
+    if (is_dead && !is_term(p, v) && __ldcg(p.excess + v) < 0 && revive_claim(p, v)) {
+      left++;
+      p.dead[v] = 0;
+      if (deg_of(p, v) > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
+      else append(p.fq[0], &out->q, v);
+    }
   });
   block_add_int(&p.ctrl->dleft, left);
+}
+
+// Partial revival, one level: every dead vertex with a residual arc into the
+// frontier can reach a revived deficit, so it is revived too (made live).  Run
+// to completion, the dead vertices left cannot reach any revived vertex, and
+// the dead set stays closed.  The arcs scanned go to out->arcs (the caller
+// gives up past a budget and revives every vertex instead).
+__device__ __forceinline__ void dead_revive_range(const Params &p, Slot *out, int nxt, int first, int end,
+                                                  int stride, LStats &ls, long long &scanned, int &revived) {
+  for (int a = first; a < end; a += stride) {
+    const int x = __ldg(p.adj + a);
+    ls.barcs++;
+    scanned++;
+    if (__ldcg(p.res + __ldg(p.par + a)) <= 0 || !__ldcg(p.dead + x) || is_term(p, x)) continue;
+    if (!revive_claim(p, x)) continue;
+    p.dead[x] = 0;
+    revived++;
+    if (deg_of(p, x) > p.hub_deg) append_hub(p, p.fh[nxt], &out->hq, x);
+    else append(p.fq[nxt], &out->q, x);
+  }
+}
+
+template <int TILE>
+__device__ __forceinline__ void ph_dead_revive(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
+  const int cur = L & 1, nxt = cur ^ 1;
+  const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
+  long long scanned = 0;
+  int revived = 0;
+  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = spread_group<32>(); i < nh; i += nwarps) {
+    int beg, end;
+    const int2 it = __ldcg(p.fh[cur] + i);
+    chunk_range(p, it, beg, end);
+    dead_revive_range(p, out, nxt, beg + lane, end, 32, ls, scanned, revived);
+  }
+  for_tiered<TILE>(p, ls, p.fq[cur], nn, [&](auto &g, int z) {
+    const int beg = __ldg(p.off + z), end = __ldg(p.off + z + 1);
+    dead_revive_range(p, out, nxt, beg + g.rank(), end, g.size(), ls, scanned, revived);
+  });
+  block_add_ll(&out->arcs, scanned);
+  block_add_ll((long long *)&p.ctrl->st_revived, revived);
 }
 
 // ---- push rounds ---------------------------------------------------------------
@@ -1951,9 +2007,28 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
       }
       kind = TR_DEAD_CHECK;
       items = hubitems = 0;
-      ph_dead_check(p);
+      ph_dead_check(p, slot_out());
       if (!next()) return;
-      revive = sc->dleft > 0;
+      if (sc->dleft > 0) {
+        // deficits left: revive what can reach them (partial), unless that
+        // grows past a budget of arcs, then every vertex
+        const long long budget = (long long)p.m / 16;
+        long long scanned = 0;
+        for (int L = 0;; L++) {
+          const Slot *in = slot_in();
+          if (L > 0) scanned += in->arcs;
+          if (in->q + in->hq == 0) break;
+          if (scanned > budget) {
+            revive = true;
+            break;
+          }
+          kind = TR_DEAD_REVIVE;
+          items = in->q;
+          hubitems = in->hq;
+          ph_dead_revive<TILE>(p, in, slot_out(), L, ls);
+          if (!next()) return;
+        }
+      }
     }
     if (lead) c->dkept = revive ? 0 : 1;
   }

@@ -380,6 +380,7 @@ int finish(dmf_solver *sv, int64_t *flow, bool need_cut_valid) {
   sv->st.dead_vertices = (int64_t)c.st_dead;
   sv->st.bfs_arcs = (int64_t)c.st_barcs;
   sv->st.dead_deficits = (int64_t)c.st_dseeds;
+  sv->st.dead_revived = (int64_t)c.st_revived;
   sv->st.dead_kept = c.dkept;
   sv->st.grid_blocks = sv->grid;
   sv->st.block_threads = sv->block;

@@ -113,7 +113,10 @@ typedef struct {
   int64_t bfs_arcs;         /* adjacency entries read by global-relabel BFS levels
                                (included in arcs_scanned) */
   int64_t dead_deficits;    /* deficits a batch left inside the kept dead set */
-  int32_t dead_kept;        /* 1: the batch kept the dead set of the last solve */
+  int64_t dead_revived;     /* dead vertices revived because they reach a deficit the
+                               local repair left (partial revival) */
+  int32_t dead_kept;        /* 1: the batch kept the dead set of the last solve
+                               (all of it but the partially revived vertices) */
   int32_t pad2;
 } dmf_stats;
 
