@@ -20,11 +20,11 @@
 // A dynamic batch keeps the dead set of the last solve (the vertices proven
 // unable to reach t or a deficit): updated arcs that open residual from it to
 // the live side are saturated at once (ph_reopen), the deficits this leaves
-// inside the dead set are covered there by pulls from excess inside it, along
-// labels of a short BFS from that excess (ph_dead_seed, ph_dead_bfs,
-// ph_dead_pull, ph_dead_check), and the global relabels then
-// only visit live vertices.  A deficit the pulls cannot cover revives every
-// vertex.
+// inside the dead set are covered there by pulls from excess inside it
+// (ph_dead_seed, ph_dead_pull), and the global relabels then only visit live
+// vertices.  A deficit the pulls cannot cover revives the dead vertices that
+// can reach it (ph_dead_check, ph_dead_revive), or every vertex when those are
+// too many.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -48,13 +48,12 @@ enum TraceKind : int {
   TR_START = 0, TR_INIT_RES = 1, TR_SATURATE = 2, TR_LOOKUP = 3, TR_APPLY = 4, TR_REPAIR = 5,
   TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
   TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14, TR_PP_INIT = 15, TR_PP_BFS = 16, TR_PP_FINALIZE = 17,
-  TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_PULL = 21, TR_DEAD_BFS = 22, TR_DEAD_CHECK = 23,
+  TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_PULL = 21, TR_DEAD_CHECK = 23,
   TR_DEAD_REVIVE = 24
 };
 
-// Local repair inside a kept dead set: BFS levels from the excess, pull rounds.
-constexpr int kDeadLevels = 6;
-constexpr int kDeadRounds = kDeadLevels + 2;
+// Local repair inside a kept dead set: at most this many pull rounds.
+constexpr int kDeadRounds = 8;
 
 // Largest capacity an update may set: keeps cap(e) + cap(partner) < 2^31 when
 // both arcs of a pair change in one batch.
@@ -867,41 +866,25 @@ __device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int 
 }
 
 // ---- local repair inside a kept dead set ------------------------------------------
-// The batch changed the excess of some dead vertices (candidates in dq): the
-// heads of repaired arcs got deficits, their tails the returned overflow, the
-// tails of reopened arcs deficits.  The deficits are covered from excess inside
-// the dead set, without reviving it:
-//  1. a short BFS forward from the candidates holding excess, over residual
-//     arcs between dead vertices, labels dead vertices with their distance from
-//     that excess (dlab, tagged with the call's wave so that no reset is
-//     needed; at most kDeadLevels levels, ending once every deficit is labelled);
-//  2. pull rounds: a deficit takes what it lacks over residual arcs x->y from
-//     dead in-neighbours holding excess (exactly the missing amount, so parked
-//     excess is not flooded around), and moves the rest to in-neighbours with a
-//     smaller label, which pull in the next round.  Labels fall along every
-//     move, so deficits head for the excess and never cycle.
-// Only dead vertices are pulled from, so every arc that gains residual (y->x)
-// lies inside the dead set: it stays closed.  A deficit left over (an O(n)
-// check) makes the first global relabel revive every vertex.
+// The batch changed the excess of some dead vertices (candidates in dq, stamped
+// with the repair's wave, round_base): the heads of repaired arcs got deficits,
+// their tails the returned overflow, the tails of reopened arcs deficits.  The
+// deficits are covered from excess inside the dead set, without reviving it,
+// by pulls: a deficit y takes what it lacks over residual arcs x->y from dead
+// in-neighbours x, first from those holding excess (exactly the amount
+// missing, so parked excess is not flooded around), then, for what is still
+// missing, from dead in-neighbours not yet touched by this repair, which take
+// that part of the deficit over and pull in the next round.  A vertex is
+// stamped the first time a deficit reaches it, so deficits only move to fresh
+// vertices and the rounds end (at most kDeadRounds).  Only dead vertices are
+// pulled from, so every arc that gains residual (y->x) lies inside the dead
+// set: it stays closed.  Deficits left over revive the dead vertices that can
+// reach them (ph_dead_check, ph_dead_revive).
 
+// Wave tag of this call in dlab (partial revival claims).
 __device__ __forceinline__ unsigned dead_wave(const Params &p) { return ((unsigned)p.epoch & 0x0fffffffu) << 4; }
 
-// Claims dead vertex v for BFS level `lv` of this call's wave; true if this thread did.
-__device__ __forceinline__ bool dead_label(const Params &p, int v, int lv) {
-  const unsigned wave = dead_wave(p);
-  const unsigned old = (unsigned)__ldcg(p.dlab + v);
-  if ((old & ~15u) == wave) return false;
-  return (unsigned)atomicCAS(p.dlab + v, (int)old, (int)(wave | (unsigned)lv)) == old;
-}
-
-// Level of v in this call's BFS, or 16 when it was not reached.
-__device__ __forceinline__ int dead_level(const Params &p, int v) {
-  const unsigned l = (unsigned)__ldcg(p.dlab + v);
-  return (l & ~15u) == dead_wave(p) ? (int)(l & 15u) : 16;
-}
-
-// Seeds: candidates with excess start the BFS (level 0), candidates with a
-// deficit form the first pull list (aq).
+// Seeds: the candidates with a deficit.
 __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Slot *out) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   Ctrl *c = p.ctrl;
@@ -911,65 +894,19 @@ __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Sl
   for (int i = gt; i < nc; i += nt) {
     const int v = __ldcg(p.dq + i);
     const long long ex = __ldcg(p.excess + v);
-    if (is_term(p, v) || ex == 0) continue;
-    if (ex > 0) {
-      if (dead_label(p, v, 0)) {
-        if (deg_of(p, v) > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
-        else append(p.fq[0], &out->q, v);
-      }
-    } else {
-      append(p.aq, &c->act_q, v);
-      seeds++;
-      need -= ex;
-    }
+    if (ex >= 0 || is_term(p, v)) continue;
+    append(p.fq[0], &out->q, v);
+    seeds++;
+    need -= ex;
   }
   block_add_int(&c->dseeds, seeds);
   block_add_ll(&c->dneed, need);
 }
 
-// Out-arcs first, first+stride, ... < end of frontier vertex x at level L.
-__device__ __forceinline__ void dead_bfs_range(const Params &p, Slot *out, int nxt, int first, int end, int stride,
-                                               int L, LStats &ls, int &reached) {
-  for (int a = first; a < end; a += stride) {
-    const int y = __ldg(p.adj + a);
-    ls.barcs++;
-    if (__ldcg(p.res + a) <= 0 || !__ldcg(p.dead + y) || is_term(p, y)) continue;
-    if (!dead_label(p, y, L + 1)) continue;
-    if (deg_of(p, y) > p.hub_deg) append_hub(p, p.fh[nxt], &out->hq, y);
-    else append(p.fq[nxt], &out->q, y);
-    if (__ldcg(p.excess + y) < 0) reached++;
-  }
-}
-
-template <int TILE>
-__device__ __forceinline__ void ph_dead_bfs(const Params &p, const Slot *in, Slot *out, int L, LStats &ls) {
-  const int cur = L & 1, nxt = cur ^ 1;
-  const int nn = ld_vol(&in->q), nh = ld_vol(&in->hq);
-  int reached = 0;
-  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = spread_group<32>(); i < nh; i += nwarps) {
-    int beg, end;
-    const int2 it = __ldcg(p.fh[cur] + i);
-    chunk_range(p, it, beg, end);
-    dead_bfs_range(p, out, nxt, beg + lane, end, 32, L, ls, reached);
-  }
-  for_tiered<TILE>(p, ls, p.fq[cur], nn, [&](auto &g, int x) {
-    const int beg = __ldg(p.off + x), end = __ldg(p.off + x + 1);
-    dead_bfs_range(p, out, nxt, beg + g.rank(), end, g.size(), L, ls, reached);
-  });
-  block_add_int(&out->cnt, reached);
-}
-
-// Pull round r: a warp per deficit of the round's list, lanes over its arcs.
-// List r = 0 is aq (act_q), list r > 0 is wq[(r-1) & 1] (wtail[(r-1) % 3]);
-// vertices a deficit moves to go to wq[r & 1] (wtail[r % 3]), once per round.
-__device__ __forceinline__ void ph_dead_pull(const Params &p, const Ctrl *sc, int r, unsigned round_id, LStats &ls) {
-  Ctrl *c = p.ctrl;
-  if (blockIdx.x == 0 && threadIdx.x == 0) c->wtail[(r + 1) % 3] = 0;
-  const int *list = r == 0 ? p.aq : p.wq[(r - 1) & 1];
-  const int nn = r == 0 ? sc->act_q : sc->wtail[(r - 1) % 3];
-  int *nxt = p.wq[r & 1];
-  int *ntail = &c->wtail[r % 3];
+// One pull round: a warp per deficit of the list, lanes over its arcs.
+__device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, int nn, int *nxt, Slot *out,
+                                             LStats &ls) {
+  const unsigned wave = p.round_base;
   const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
   cg::thread_block_tile<32> warp = cg::tiled_partition<32>(cg::this_thread_block());
   for (int i = spread_group<32>(); i < nn; i += nwarps) {
@@ -982,11 +919,9 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const Ctrl *sc, in
     y = warp.shfl(y, 0);
     need = warp.shfl(need, 0);
     if (need <= 0) continue;
-    const int ly = dead_level(p, y);
     const int beg = __ldg(p.off + y), end = __ldg(p.off + y + 1);
     long long got = 0;
     for (int pass = 0; pass < 2 && need > 0; pass++) {
-      if (pass == 1 && ly == 0) break;  // nothing below it to move the deficit to
       for (int a0 = beg; a0 < end && need > 0; a0 += 32) {
         const int a = a0 + lane;
         int x = -1, pa = -1;
@@ -994,13 +929,13 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const Ctrl *sc, in
         if (a < end) {
           x = __ldg(p.adj + a);
           pa = __ldg(p.par + a);
-          const int rr = __ldcg(p.res + pa);  // residual x -> y
-          if (rr > 0 && __ldcg(p.dead + x) && !is_term(p, x)) {
+          const int r = __ldcg(p.res + pa);  // residual x -> y
+          if (r > 0 && __ldcg(p.dead + x) && !is_term(p, x)) {
             if (pass == 0) {
               const long long ex = __ldcg(p.excess + x);
-              if (ex > 0) cand = ex < rr ? ex : rr;
-            } else if (dead_level(p, x) < ly) {
-              cand = rr;
+              if (ex > 0) cand = ex < r ? ex : r;
+            } else if (__ldcg(p.stamp + x) != (int)wave) {
+              cand = r;
             }
           }
           ls.arcs++;
@@ -1017,8 +952,8 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const Ctrl *sc, in
               atomic_add_ll(p.excess + x, back);
               take -= back;
             }
-          } else if (old - take < 0 && atomicExch(p.stamp + x, (int)round_id) != (int)round_id) {
-            append(nxt, ntail, x);  // x pulls its part next round
+          } else if (old - take < 0 && atomicExch(p.stamp + x, (int)wave) != (int)wave) {
+            append(nxt, &out->q, x);  // x takes this part of the deficit over: it pulls next round
           }
           if (take > 0) {
             atomicSub(p.res + pa, (int)take);
@@ -1977,33 +1912,18 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     kind = TR_DEAD_SEED;
     items = sc->dcand;
     hubitems = 0;
-    ph_dead_seed(p, sc, slot_out());  // act_q and wtail[0] are still 0 from the launch
+    ph_dead_seed(p, sc, slot_out());
     if (!next()) return;
     if (lead) c->st_dseeds = (unsigned long long)sc->dseeds;
-    const int nseeds = sc->dseeds;
-    if (nseeds > 0) {
-      int reached = 0;
-      for (int L = 0;; L++) {
-        const Slot *in = slot_in();
-        reached += in->cnt;
-        if (in->q + in->hq == 0 || reached >= nseeds || L >= kDeadLevels) break;
-        kind = TR_DEAD_BFS;
-        items = in->q;
-        hubitems = in->hq;
-        ph_dead_bfs<TILE>(p, in, slot_out(), L, ls);
-        if (!next()) return;
-        if (lead) c->st_levels++;
-      }
+    if (sc->dseeds > 0) {
       for (int r = 0; r < kDeadRounds; r++) {
-        const int nn = r == 0 ? sc->act_q : sc->wtail[(r - 1) % 3];
-        if (nn == 0) break;
-        round_id++;
+        const Slot *in = slot_in();
+        if (in->q == 0) break;
         kind = TR_DEAD_PULL;
-        items = nn;
+        items = in->q;
         hubitems = 0;
-        ph_dead_pull(p, sc, r, round_id, ls);
+        ph_dead_pull(p, p.fq[r & 1], in->q, p.fq[(r + 1) & 1], slot_out(), ls);
         if (!next()) return;
-        if (lead) c->rounds_used = round_id - p.round_base;
       }
       kind = TR_DEAD_CHECK;
       items = hubitems = 0;
