@@ -53,7 +53,7 @@ enum TraceKind : int {
 };
 
 // Local repair inside a kept dead set: at most this many pull rounds.
-constexpr int kDeadRounds = 8;
+constexpr int kDeadRounds = 16;
 
 // Largest capacity an update may set: keeps cap(e) + cap(partner) < 2^31 when
 // both arcs of a pair change in one batch.
@@ -866,25 +866,38 @@ __device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int 
 }
 
 // ---- local repair inside a kept dead set ------------------------------------------
-// The batch changed the excess of some dead vertices (candidates in dq, stamped
-// with the repair's wave, round_base): the heads of repaired arcs got deficits,
-// their tails the returned overflow, the tails of reopened arcs deficits.  The
-// deficits are covered from excess inside the dead set, without reviving it,
-// by pulls: a deficit y takes what it lacks over residual arcs x->y from dead
-// in-neighbours x, first from those holding excess (exactly the amount
-// missing, so parked excess is not flooded around), then, for what is still
-// missing, from dead in-neighbours not yet touched by this repair, which take
-// that part of the deficit over and pull in the next round.  A vertex is
-// stamped the first time a deficit reaches it, so deficits only move to fresh
-// vertices and the rounds end (at most kDeadRounds).  Only dead vertices are
-// pulled from, so every arc that gains residual (y->x) lies inside the dead
-// set: it stays closed.  Deficits left over revive the dead vertices that can
-// reach them (ph_dead_check, ph_dead_revive).
+// The batch changed the excess of some dead vertices (candidates in dq): the
+// heads of repaired arcs got deficits, their tails the returned overflow, the
+// tails of reopened arcs deficits.  The deficits are covered from excess inside
+// the dead set, without reviving it, by pull-relabel rounds -- push-relabel run
+// backwards, a deficit being moved instead of an excess.  A deficit y takes
+// what it lacks over residual arcs x->y from dead in-neighbours holding excess
+// (exactly the amount missing, so parked excess is not flooded around); it
+// moves the rest to dead in-neighbours with a lower label, which pull in the
+// next round; if some is still missing it relabels to 1 + the lowest label of
+// its dead in-neighbours with residual and tries again next round.  Labels
+// (dlab, tagged with the launch so nothing is reset; 0 until set, deficits
+// start at 1) only rise, so deficits never cycle, and vertices can be passed
+// through by many deficits.  Only dead vertices are pulled from, so every arc
+// that gains residual (y->x) lies inside the dead set: it stays closed.
+// Deficits left after kDeadRounds revive the dead vertices that can reach them
+// (ph_dead_check, ph_dead_revive).
 
-// Wave tag of this call in dlab (partial revival claims).
-__device__ __forceinline__ unsigned dead_wave(const Params &p) { return ((unsigned)p.epoch & 0x0fffffffu) << 4; }
+constexpr int kDeadRevived = 255;  // dlab label of a vertex the partial revival claimed
 
-// Seeds: the candidates with a deficit.
+__device__ __forceinline__ unsigned dlab_tag(const Params &p) { return ((unsigned)p.epoch & 0xffffffu) << 8; }
+
+// Label of dead vertex v in this launch's repair (0 when not set yet).
+__device__ __forceinline__ int dead_label(const Params &p, int v) {
+  const unsigned l = (unsigned)__ldcg(p.dlab + v);
+  return (l & ~255u) == dlab_tag(p) ? (int)(l & 255u) : 0;
+}
+
+__device__ __forceinline__ void set_dead_label(const Params &p, int v, int h) {
+  p.dlab[v] = (int)(dlab_tag(p) | (unsigned)(h < kDeadRevived - 1 ? h : kDeadRevived - 1));
+}
+
+// Seeds: the candidates with a deficit, at label 1.
 __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Slot *out) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   Ctrl *c = p.ctrl;
@@ -895,6 +908,7 @@ __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Sl
     const int v = __ldcg(p.dq + i);
     const long long ex = __ldcg(p.excess + v);
     if (ex >= 0 || is_term(p, v)) continue;
+    set_dead_label(p, v, 1);
     append(p.fq[0], &out->q, v);
     seeds++;
     need -= ex;
@@ -903,10 +917,10 @@ __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Sl
   block_add_ll(&c->dneed, need);
 }
 
-// One pull round: a warp per deficit of the list, lanes over its arcs.
+// One pull-relabel round: a warp per deficit of the list, lanes over its arcs.
+// A vertex joins the next round's list once (stamp = this round's id).
 __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, int nn, int *nxt, Slot *out,
-                                             LStats &ls) {
-  const unsigned wave = p.round_base;
+                                             unsigned round_id, LStats &ls) {
   const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
   cg::thread_block_tile<32> warp = cg::tiled_partition<32>(cg::this_thread_block());
   for (int i = spread_group<32>(); i < nn; i += nwarps) {
@@ -919,23 +933,27 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
     y = warp.shfl(y, 0);
     need = warp.shfl(need, 0);
     if (need <= 0) continue;
+    const int hy = dead_label(p, y);
     const int beg = __ldg(p.off + y), end = __ldg(p.off + y + 1);
     long long got = 0;
+    int hmin = INT_MAX;  // lowest label over the dead in-neighbours still residual (pass 1)
     for (int pass = 0; pass < 2 && need > 0; pass++) {
       for (int a0 = beg; a0 < end && need > 0; a0 += 32) {
         const int a = a0 + lane;
-        int x = -1, pa = -1;
+        int x = -1, pa = -1, r = 0;
         long long cand = 0;
         if (a < end) {
           x = __ldg(p.adj + a);
           pa = __ldg(p.par + a);
-          const int r = __ldcg(p.res + pa);  // residual x -> y
+          r = __ldcg(p.res + pa);  // residual x -> y
           if (r > 0 && __ldcg(p.dead + x) && !is_term(p, x)) {
             if (pass == 0) {
               const long long ex = __ldcg(p.excess + x);
               if (ex > 0) cand = ex < r ? ex : r;
-            } else if (__ldcg(p.stamp + x) != (int)wave) {
-              cand = r;
+            } else {
+              const int hx = dead_label(p, x);
+              if (hx < hy) cand = r;
+              else hmin = min(hmin, hx);
             }
           }
           ls.arcs++;
@@ -952,7 +970,7 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
               atomic_add_ll(p.excess + x, back);
               take -= back;
             }
-          } else if (old - take < 0 && atomicExch(p.stamp + x, (int)wave) != (int)wave) {
+          } else if (old - take < 0 && atomicExch(p.stamp + x, (int)round_id) != (int)round_id) {
             append(nxt, &out->q, x);  // x takes this part of the deficit over: it pulls next round
           }
           if (take > 0) {
@@ -961,18 +979,27 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
             ls.pushes++;
           }
         }
+        if (pass == 1 && cand > 0 && take < cand) hmin = min(hmin, dead_label(p, x));  // still residual
         const long long moved = cg::reduce(warp, take, cg::plus<long long>());
         need -= moved;
         got += moved;
+      }
+    }
+    if (need > 0) {  // relabel and try again next round (nowhere to go: stays for the check)
+      hmin = cg::reduce(warp, hmin, cg::less<int>());
+      if (lane == 0 && hmin != INT_MAX) {
+        set_dead_label(p, y, hmin + 1);
+        ls.relabels++;
+        if (atomicExch(p.stamp + y, (int)round_id) != (int)round_id) append(nxt, &out->q, y);
       }
     }
     if (lane == 0 && got) atomic_add_ll(p.excess + y, got);
   }
 }
 
-// Claims dead vertex v for the partial revival of this call (tag level 15).
+// Claims dead vertex v for the partial revival of this launch.
 __device__ __forceinline__ bool revive_claim(const Params &p, int v) {
-  const int tag = (int)(dead_wave(p) | 15u);
+  const int tag = (int)(dlab_tag(p) | (unsigned)kDeadRevived);
   const int old = __ldcg(p.dlab + v);
   if (old == tag) return false;
   return atomicCAS(p.dlab + v, old, tag) == old;
@@ -1919,11 +1946,13 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
       for (int r = 0; r < kDeadRounds; r++) {
         const Slot *in = slot_in();
         if (in->q == 0) break;
+        round_id++;
         kind = TR_DEAD_PULL;
         items = in->q;
         hubitems = 0;
-        ph_dead_pull(p, p.fq[r & 1], in->q, p.fq[(r + 1) & 1], slot_out(), ls);
+        ph_dead_pull(p, p.fq[r & 1], in->q, p.fq[(r + 1) & 1], slot_out(), round_id, ls);
         if (!next()) return;
+        if (lead) c->rounds_used = round_id - p.round_base;
       }
       kind = TR_DEAD_CHECK;
       items = hubitems = 0;
