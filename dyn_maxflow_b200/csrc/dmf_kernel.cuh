@@ -111,6 +111,9 @@ struct Params {
   // dead unless the batch gives them a deficit that cannot be covered inside
   // the dead set (then the first global relabel revives every vertex).
   int keep_dead;
+  // every capacity is at most kMaxUpdateCap, so a pair's sum cannot overflow
+  // and the lookup need not read the partner's capacity
+  int caps_bounded;
   int bu_alpha;  // bottom-up when frontier arcs * bu_alpha > unexplored arcs (0: never)
   int adaptive;  // push rounds per relabel at least the depth of the last relabel BFS
   unsigned round_base;
@@ -389,7 +392,7 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
         set_err(p.ctrl, ERR_DUP_ARC, i);
         continue;
       }
-      if ((long long)w[j] + __ldcg(p.cap + __ldg(p.par + e[j])) > INT_MAX) {
+      if (!p.caps_bounded && (long long)w[j] + __ldcg(p.cap + __ldg(p.par + e[j])) > INT_MAX) {
         set_err(p.ctrl, ERR_BAD_UPDATE, i);
         continue;
       }
@@ -412,27 +415,32 @@ __device__ __forceinline__ void ph_apply(const Params &p, bool residual) {
   }
 }
 
-// Over-capacity repair driven by the batch: replaces the O(m) sweeps
-// incremental_kernel_20 / _22 (code/dyn_data.h:157-183).  An arc whose residual
-// went negative carries more flow than its new capacity; the excess is returned
-// to its tail and taken from its head.  At most one arc of a pair can be
-// negative because res(e) + res(partner) = cap(e) + cap(partner) >= 0.
-__device__ __forceinline__ void ph_repair(const Params &p) {
+// Capacity apply and over-capacity repair in one pass (dynamic batches).  The
+// repair replaces the O(m) sweeps incremental_kernel_20 / _22
+// (code/dyn_data.h:157-183): an arc whose residual went negative carries more
+// flow than its new capacity; the overflow returns to its tail and is taken
+// from its head.  An arc's residual changes only by its own apply here, and at
+// most one arc of a pair goes negative (res(e) + res(partner) = cap(e) +
+// cap(partner) >= 0), so the repair can follow each apply at once.
+__device__ __forceinline__ void ph_apply_repair(const Params &p) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   for (int i = gt; i < p.k; i += nt) {
-    int e = __ldcg(p.uarc + i);
+    const int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
-    int r = __ldcg(p.res + e);
-    if (r < 0) {
-      p.res[e] = 0;
-      atomicAdd(p.res + __ldg(p.par + e), r);
-      const int v = __ldg(p.adj + e);
-      atomic_add_ll(p.excess + __ldg(p.usrc + i), -(long long)r);
-      atomic_add_ll(p.excess + v, (long long)r);
-      if (p.keep_dead) {  // the overflow returns to the tail: excess that can cover the head's deficit
-        if (__ldcg(p.dead + v)) add_dead_cand(p, v);
-        if (__ldcg(p.dead + __ldg(p.usrc + i))) add_dead_cand(p, __ldg(p.usrc + i));
-      }
+    const int w = __ldg(p.uw + i);
+    const int delta = w - __ldcg(p.cap + e);
+    p.cap[e] = w;
+    if (!delta) continue;
+    const int r = atomicAdd(p.res + e, delta) + delta;
+    if (r >= 0) continue;
+    atomicAdd(p.res + e, -r);
+    atomicAdd(p.res + __ldg(p.par + e), r);
+    const int u = __ldg(p.usrc + i), v = __ldg(p.adj + e);
+    atomic_add_ll(p.excess + u, -(long long)r);
+    atomic_add_ll(p.excess + v, (long long)r);
+    if (p.keep_dead) {  // the overflow returns to the tail: excess that can cover the head's deficit
+      if (__ldcg(p.dead + v)) add_dead_cand(p, v);
+      if (__ldcg(p.dead + u)) add_dead_cand(p, u);
     }
   }
 }
@@ -1897,24 +1905,19 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     ph_lookup(p);
     if (!next()) return;
     kind = TR_APPLY;
-    ph_apply(p, true);
-    if (!next()) return;
-    kind = TR_REPAIR;
-    ph_repair(p);
+    ph_apply_repair(p);
     if (!next()) return;
     if (p.variant == DMF_VARIANT_PP && !p.keep_dead) {  // with the dead set kept, ph_reopen does it
       kind = TR_CUT_SATURATE;
       ph_cut_saturate(p);
       if (!next()) return;
     }
+    // source saturation and reopening touch disjoint arcs (a reopened arc's
+    // tail is dead, so neither it nor its partner is a source arc): one phase
     kind = TR_SATURATE;
     ph_saturate(p);
+    if (p.keep_dead) ph_reopen(p);
     if (!next()) return;
-    if (p.keep_dead) {
-      kind = TR_REOPEN;
-      ph_reopen(p);
-      if (!next()) return;
-    }
   } else if (p.mode == MODE_RECOMPUTE) {
     kind = TR_LOOKUP;
     ph_lookup(p);

@@ -106,6 +106,7 @@ struct dmf_solver {
   long long *excess = nullptr;
   unsigned char *dead = nullptr, *side = nullptr;
   int *dlab = nullptr;    // dead-set repair labels, tagged with the launch epoch
+  bool caps_bounded = false;  // every capacity <= 2^30 - 1 (updates keep it so)
   int *qbuf = nullptr;    // 6 vertex queues (frontier x2, worklist x2, active, dead-set candidates)
   int2 *hqbuf = nullptr;  // 5 hub-chunk queues, same roles
   int2 *hch = nullptr;    // every hub's chunks
@@ -335,6 +336,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.adaptive = (sv->opts.flags & DMF_FLAG_FIXED_INTERVAL) ? 0 : 1;
   p.need_cut = sv->opts.variant == DMF_VARIANT_PP ? 1 : 0;
   p.keep_dead = mode == MODE_DYNAMIC && !(sv->opts.flags & DMF_FLAG_REVIVE_DEAD) ? 1 : 0;
+  p.caps_bounded = sv->caps_bounded ? 1 : 0;
   const bool hook = (sv->opts.flags & DMF_FLAG_TEST_BARRIER_TIMEOUT) != 0;
   p.barrier_ns = hook ? kTestBarrierTimeoutNs : kBarrierTimeoutNs;
   p.absent_block = hook && sv->grid > 1 ? sv->grid - 1 : -1;
@@ -694,6 +696,7 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
     p.bu_alpha = 2;
     p.need_cut = 0;
     p.keep_dead = 0;
+    p.caps_bounded = 0;
     p.barrier_ns = kBarrierTimeoutNs;
     p.absent_block = -1;
     p.round_base = 1;
@@ -832,6 +835,12 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   for (size_t j = 0; j * kSampleStride < M; j++) ssamp[j] = shead[j * kSampleStride];
   up(sv->ssamp, ssamp.data(), 4 * ssamp.size());
   up(sv->cap, g->w.data(), 4 * M);
+  {
+    int32_t mx = 0;
+#pragma omp parallel for schedule(static) reduction(max : mx)
+    for (int64_t i = 0; i < (int64_t)M; i++) mx = std::max(mx, g->w[i]);
+    sv->caps_bounded = mx <= kMaxUpdateCap;
+  }
   up(sv->hch, hub_chunks.data(), sizeof(int2) * hub_chunks.size());
   up(sv->hub_base, hub_base.data(), 4 * (size_t)g->n);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->chunk_mark, 0, 8 * NC, S);
