@@ -332,6 +332,16 @@ def run_ours(args, rank: int, world: int):
         torch.distributed.barrier()
     region_s = time.perf_counter() - t_region
     clocks = sampler.stop() if sampler else None
+    # the BFS of a from-scratch solve (every vertex live), on the traced solver, untimed
+    flushed()
+    P.static_maxflow()
+    static_stats = [P.stats()]
+    static_phase = {}
+    tr = P.trace()
+    for (k0, t0_), (k1, t1_) in zip(tr, tr[1:]):
+        static_phase.setdefault(k1, {"us": 0.0, "count": 0})
+        static_phase[k1]["us"] += t1_ - t0_
+        static_phase[k1]["count"] += 1
     for x in [A, R, P] + Ls:
         x.close()
     if sched is not None:
@@ -384,6 +394,7 @@ def run_ours(args, rank: int, world: int):
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "k_solve", "algorithmic_bytes_per_launch": int(avg_bytes)},
         "roofline_bfs": bfs_roofline(pstats, phases, n, peak),
+        "roofline_bfs_static": bfs_roofline(static_stats, static_phase, n, peak),
         "solver_stats_mean": {k: round(sum(st[k] for st in stats) / len(stats), 1)
                               for k in ("outer_iters", "bfs_levels", "push_rounds", "pushes", "relabels",
                                         "arcs_scanned", "bfs_arcs", "vertices_visited", "dead_vertices",
