@@ -174,12 +174,18 @@ class ClockSampler:
 def algorithmic_bytes(st: dict, n: int, k: int, deg_s: int) -> int:
     """Bytes a single solve must move, from the solver's own counters:
     64 B per update (triple, lookup probes, stamps, apply, repair), 16 B per source
-    arc, 36 B per vertex per global relabel (seed/init + finalize passes), 12 B per
-    adjacency entry scanned (head, residual, neighbour label), 16 B per vertex
-    discharge, 24 B per push (two residual atomics, one 8-byte excess atomic), and
-    8 B per vertex for the flow reduction."""
-    return int(64 * k + 16 * deg_s + 36 * n * max(1, st["outer_iters"]) + 12 * st["arcs_scanned"]
-               + 16 * st["vertices_visited"] + 24 * st["pushes"] + 8 * n)
+    arc, per global relabel 36 B per live vertex and 2 B per dead one (seed and
+    finalize passes; a dead vertex costs its flag), 12 B per adjacency entry
+    scanned (head, residual, neighbour label; BFS, pushes and the dead-set pulls),
+    16 B per vertex discharge, 24 B per push or pull (two residual atomics, one
+    8-byte excess atomic), the flow reduction (8 B per live vertex, 1 B per dead
+    one) and, when the batch left deficits in the kept dead set, its check (9 B
+    per vertex)."""
+    dead = min(n, int(st["dead_vertices"]))
+    live = n - dead
+    check = 9 * n if st.get("dead_deficits", 0) > 0 else 0
+    return int(64 * k + 16 * deg_s + (36 * live + 2 * dead) * max(1, st["outer_iters"]) + 12 * st["arcs_scanned"]
+               + 16 * st["vertices_visited"] + 24 * st["pushes"] + 8 * live + dead + check)
 
 
 def load_measured_peak():
