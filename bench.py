@@ -201,15 +201,18 @@ def load_measured_peak():
 
 def bfs_roofline(stats: list, phases: dict, n: int, peak: float) -> dict | None:
     """Roofline of the global relabel alone (the BFS from t and the deficits):
-    algorithmic bytes per relabel 16*V (offsets, label write) + 12 per adjacency
-    entry scanned (head, residual, head label), over the time of the BFS phases
-    (seed pass, top-down and bottom-up levels, finalize) in the traced pass."""
+    algorithmic bytes per relabel 16 per live vertex (offsets, label write) and
+    2 per dead one (its flag, read by the seed and finalize passes), plus 12 per
+    adjacency entry scanned (head, residual, head label), over the time of the
+    BFS phases (seed pass, top-down and bottom-up levels, finalize) in the
+    traced pass."""
     t_us = sum(phases.get(k, {}).get("us", 0.0) for k in ("bfs_init", "bfs_td", "bfs_bu", "bfs_finalize"))
     if not stats or t_us <= 0:
         return None
     relabels = sum(st["outer_iters"] for st in stats) / len(stats)
     barcs = sum(st["bfs_arcs"] for st in stats) / len(stats)
-    nbytes = 16.0 * n * relabels + 12.0 * barcs
+    dead = sum(min(n, st["dead_vertices"]) for st in stats) / len(stats)
+    nbytes = (16.0 * (n - dead) + 2.0 * dead) * relabels + 12.0 * barcs
     achieved = nbytes / (t_us * 1e-6) / 1e9
     return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "bytes_per_batch": int(nbytes), "bfs_us_per_batch": round(t_us, 1),
@@ -681,9 +684,10 @@ def run_serving(args, rank: int, world: int):
     gen_s = time.time() - t_gen
     srv = D.Server(graphs, srcs, snks, int(args.serve_budget_gb * (1 << 30)))
     admitted = srv.admitted
-    lanes = {}
+    lanes, srv_lanes = {}, []
     for gi in range(admitted):
         ln = srv.lane(gi)
+        srv_lanes.append(ln["lane"])
         lanes.setdefault(ln["lane"], {"graphs": 0, "grid_blocks": ln["grid_blocks"]})["graphs"] += 1
     # warm-up: one request per admitted graph
     for gi in range(admitted):
@@ -733,6 +737,18 @@ def run_serving(args, rank: int, world: int):
                 exact &= sv.apply_updates(*pools[gi][pick[i]]) == flows[i]
     lat_ms = [x for x in lat if x is not None]
     p50, p99 = pct(lat_ms, 0.5), pct(lat_ms, 0.99)
+    # where the tail comes from: latency per lane, and the slowest requests
+    lane_of = [srv_lanes[gi] for gi in range(admitted)]
+    per_lane = {}
+    for i in range(n_req):
+        if lat[i] is not None:
+            per_lane.setdefault(lane_of[choice[i]], []).append(lat[i])
+    lane_lat = {str(k): {"requests": len(v), "p50_ms": round(pct(v, 0.5), 3), "p99_ms": round(pct(v, 0.99), 3),
+                         "max_ms": round(max(v), 3)} for k, v in sorted(per_lane.items())}
+    worst = sorted((i for i in range(n_req) if lat[i] is not None), key=lambda i: -lat[i])[:8]
+    slowest = [{"graph": int(choice[i]), "lane": lane_of[choice[i]], "updates": len(pools[choice[i]][pick[i]][0]),
+                "graph_arcs": graphs[choice[i]].num_edges(), "ms": round(lat[i], 3),
+                "arrival_s": round(float(np.sum(gaps[:i + 1])), 3)} for i in worst]
     return {
         "metric": "ms from request to exact maxflow, serving (p50)", "value": round(p50, 3), "unit": "ms",
         "n_gpus": world, "steps": n_req, "warmup": admitted, "ms_per_step": round(float(np.mean(lat_ms)), 3),
@@ -746,7 +762,8 @@ def run_serving(args, rank: int, world: int):
                    "request_sizes": "log-uniform [1e3, 1e6] updates, <= m/2",
                    "l2": "device state (large graph) far larger than L2"},
         "sustained_updates_per_s": round(updates / wall, 1), "requests_per_s": round(n_req / wall, 2),
-        "server": st, "exact_replay_check": bool(exact), "generation_s": round(gen_s, 1),
+        "server": st, "latency_by_lane": lane_lat, "slowest_requests": slowest,
+        "exact_replay_check": bool(exact), "generation_s": round(gen_s, 1),
         "e2e": {"value": round(p50, 3), "unit": "ms", "h2d_bytes_per_step": int(12 * updates / n_req),
                 "d2h_bytes_per_step": 8},
         "clocks": clk, "gpu_launches": int(st["ticks"]),
