@@ -182,6 +182,16 @@ __device__ __forceinline__ void append(int *q, int *tail, int v) {
   q[base + g.thread_rank()] = v;
 }
 
+// append() into a queue of `cap` entries: *tail still counts every append, so
+// *tail > cap afterwards tells that entries were dropped.
+__device__ __forceinline__ void append_bounded(int *q, int *tail, int v, int cap) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  int base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(tail, (int)g.size());
+  base = g.shfl(base, 0);
+  if (base + (int)g.thread_rank() < cap) q[base + g.thread_rank()] = v;
+}
+
 __device__ __forceinline__ void agg_add_ll(long long *p, long long v) {
   cg::coalesced_group g = cg::coalesced_threads();
   long long s = cg::reduce(g, v, cg::plus<long long>());
@@ -289,5 +299,58 @@ struct BlockGroup {
     return *bcast_l;
   }
 };
+
+
+// ---- arc table: (tail, head) -> arc ------------------------------------------
+// Open addressing with linear probing over `nslots` 16-byte slots.  An empty
+// slot has tail == kEmptyTail (the table is cleared with 0xFF bytes, which also
+// sets arc = -1 and stamp = -1, an epoch no launch uses).  The stamp is the
+// launch epoch of the last batch that named the slot's arc.
+struct __align__(16) ArcSlot {
+  int tail, head, arc, stamp;
+};
+constexpr int kEmptyTail = -1;
+
+// Slots per arc count: load factor at most about 0.62, so a found key takes
+// two probes on average, most of them in the first slot's DRAM sector.
+__host__ __device__ constexpr long long arc_table_slots(long long m) { return m + m / 2 + m / 8 + 64; }
+
+// The 64-bit key as it lies in the slot's first two words (tail low, head high).
+__device__ __forceinline__ unsigned long long arc_key(int u, int v) {
+  return ((unsigned long long)(unsigned)v << 32) | (unsigned)u;
+}
+
+// First slot of a key: the SplitMix64 finaliser (Steele, Lea and Flood,
+// "Fast splittable pseudorandom number generators", OOPSLA 2014) mixes the
+// key, and the high half of its product with nslots maps it onto [0, nslots)
+// (Lemire's multiply-shift range reduction) without a division.
+__device__ __forceinline__ long long arc_slot0(int u, int v, long long nslots) {
+  unsigned long long x = arc_key(u, v);
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return (long long)__umul64hi(x, (unsigned long long)nslots);
+}
+
+// One slot through L2 (the stamp word changes during a batch; tail, head and
+// arc never do after the build).
+__device__ __forceinline__ ArcSlot load_slot(const ArcSlot *s) {
+  const int4 x = __ldcg(reinterpret_cast<const int4 *>(s));
+  return ArcSlot{x.x, x.y, x.z, x.w};
+}
+
+// Arc u->v, or -1 (read-only probe).
+__device__ __forceinline__ int find_arc_table(const ArcSlot *tab, long long nslots, int u, int v) {
+  long long sl = arc_slot0(u, v, nslots);
+  for (long long probe = 0; probe < nslots; probe++) {
+    const ArcSlot s = load_slot(tab + sl);
+    if (s.tail == u && s.head == v) return s.arc;
+    if (s.tail == kEmptyTail) return -1;
+    sl = sl + 1 == nslots ? 0 : sl + 1;
+  }
+  return -1;
+}
 
 }  // namespace dmfd

@@ -61,4 +61,14 @@ int build_from_edges(int64_t k, const int32_t *u, const int32_t *v,
 // (the grid of a solver without a grid_blocks cap).
 int resident_solve_blocks(int32_t *blocks);
 
+// Device bytes of one solver's per-arc and per-vertex state for a graph of n
+// vertices and m arcs: heads, partners, capacities, residuals and the arc
+// table per arc; labels, excess, marks and queues per vertex.
+int64_t solver_footprint(int64_t n, int64_t m);
+
+// Grows a solver's device and pinned staging for batches of up to k updates
+// now, so that later calls of that size allocate nothing (an allocation or a
+// free in the middle of serving waits for every stream of the device).
+int reserve_updates(dmf_solver *sv, int32_t k);
+
 }  // namespace dmf

@@ -64,10 +64,9 @@ struct Params {
   const int *__restrict__ off;
   const int *__restrict__ adj;
   const int *__restrict__ par;
-  const int *__restrict__ sidx;
-  const int *__restrict__ shead;  // heads in per-vertex sorted order (arc lookup)
-  const int *__restrict__ ssamp;  // every kSampleStride-th entry of shead (ssamp[j] = shead[j * stride])
-  int *cap, *res, *height, *stamp, *astamp, *uarc;
+  ArcSlot *atab;    // (tail, head) -> arc table with the per-arc batch stamps
+  long long nslots;  // its slots
+  int *cap, *res, *height, *stamp, *uarc;
   long long *excess;
   unsigned char *dead, *side;
   int *fq[2], *wq[2], *aq;     // non-hub vertex queues
@@ -166,10 +165,14 @@ __device__ __forceinline__ void set_err(Ctrl *c, int bit, int info) {
 }
 
 // A dead vertex whose excess a batch lowers joins the candidate list once
-// (stamp = round_base, a value no push round of this call uses).
+// (stamp = round_base, a value no push round of this call uses).  The pull
+// rounds later append the dead vertices they take below zero, so after them
+// the list holds every dead vertex that can hold a deficit (dead vertices end
+// every solve with excess >= 0).  The list has n + 1 entries; a count past
+// that means some were dropped, and the dead check then sweeps every vertex.
 __device__ __forceinline__ void add_dead_cand(const Params &p, int v) {
   if (atomicExch(p.stamp + v, (int)p.round_base) == (int)p.round_base) return;
-  append(p.dq, &p.ctrl->dcand, v);
+  append_bounded(p.dq, &p.ctrl->dcand, v, p.n + 1);
 }
 
 // ---- prologue phases ----------------------------------------------------------
@@ -233,59 +236,25 @@ __device__ __forceinline__ void ph_saturate(const Params &p) {
   if (same.thread_rank() == 0 && cur >= 0 && sum) atomic_add_ll(p.excess + __ldg(p.srcs + cur), -sum);
 }
 
-// Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201) by binary search; also
-// validates the batch.  `shead` holds every vertex's heads in sorted order
-// (shead[i] = adj[sidx[i]]), so a search step is one load; sidx maps the found
-// position back to the arc.  Equal heads (a CSR with duplicate arcs) resolve to
-// the last arc among them, as OnAdd_kernel's linear scan keeps the last match.
-// A long adjacency is searched in two steps: first over `ssamp`, every
-// kSampleStride-th head (m / 32 entries, small enough to stay in L2), then
-// within the window of kSampleStride heads that sample opens, so a search
-// reads about one DRAM sector of shead instead of one per step.
-constexpr int kSampleStride = 32;
+// Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201), which scans the tail's
+// adjacency for the head; here one probe of an open-addressing table keyed by
+// (tail, head) (dmfd::ArcSlot, built once per solver by k_arc_table_build).
+// A slot holds the key, the arc and the batch stamp that detects an arc named
+// twice in one batch, in one 16-byte line: a found update costs one DRAM
+// sector (two when the probe crosses a sector) instead of a search of the
+// tail's adjacency.  Equal (tail, head) pairs in a CSR with duplicate arcs
+// resolve to the last arc among them, as OnAdd_kernel's scan keeps the last
+// match.  The lookup also validates the batch.
 
-// The window [lo, hi) of u's sorted heads [b, e) that holds the last head <= v.
-struct SearchRange {
-  int lo, hi;
-};
-
-__device__ __forceinline__ SearchRange sample_window(const int *__restrict__ ssamp, int b, int e, int v) {
-  if (e - b <= kSampleStride) return {b, e};
-  int jlo = (b + kSampleStride - 1) / kSampleStride, jhi = (e - 1) / kSampleStride + 1;  // samples in [b, e)
-  if (__ldg(ssamp + jlo) > v) return {b, jlo * kSampleStride};
-  while (jhi - jlo > 1) {  // last sample <= v
-    const int mid = (jlo + jhi) >> 1;
-    if (__ldg(ssamp + mid) <= v) jlo = mid;
-    else jhi = mid;
-  }
-  const int lo = jlo * kSampleStride;
-  return {lo, min(e, lo + kSampleStride)};
-}
-
-__device__ __forceinline__ int find_arc_dev(const int *__restrict__ off, const int *__restrict__ shead,
-                                            const int *__restrict__ ssamp, const int *__restrict__ sidx, int u,
-                                            int v) {
-  const int first = __ldg(off + u);
-  const SearchRange w = sample_window(ssamp, first, __ldg(off + u + 1), v);
-  int lo = w.lo, hi = w.hi;
-  while (lo < hi) {  // last position with head <= v
-    const int mid = (lo + hi) >> 1;
-    if (__ldg(shead + mid) <= v) lo = mid + 1;
-    else hi = mid;
-  }
-  if (lo > first && __ldg(shead + lo - 1) == v) return __ldg(sidx + lo - 1);
-  return -1;
-}
-
-// Updates a thread looks up side by side: their searches advance in lockstep,
-// so the loads of one step are in flight together.
+// Updates a thread looks up side by side: their probes are in flight together.
 constexpr int kLookupBatch = 4;
 
 __device__ __forceinline__ void ph_lookup(const Params &p) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   for (int i0 = gt; i0 < p.k; i0 += kLookupBatch * nt) {
-    int u[kLookupBatch], v[kLookupBatch], w[kLookupBatch], lo[kLookupBatch], hi[kLookupBatch], first[kLookupBatch];
-    bool on[kLookupBatch];
+    int u[kLookupBatch], v[kLookupBatch], w[kLookupBatch], e[kLookupBatch];
+    long long slot[kLookupBatch];
+    bool on[kLookupBatch], pend[kLookupBatch];
 #pragma unroll
     for (int j = 0; j < kLookupBatch; j++) {
       const int i = i0 + j * nt;
@@ -296,6 +265,8 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
     }
 #pragma unroll
     for (int j = 0; j < kLookupBatch; j++) {
+      e[j] = -1;
+      pend[j] = false;
       if (!on[j]) continue;
       const int i = i0 + j * nt;
       p.uarc[i] = -1;
@@ -304,81 +275,33 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
         on[j] = false;
       } else if (u[j] == v[j]) {
         on[j] = false;  // ignored, as OnAdd_kernel does (code/dyn_data.h:194)
+      } else {
+        slot[j] = arc_slot0(u[j], v[j], p.nslots);
+        pend[j] = true;
       }
     }
+    // linear probing; the table always has an empty slot, so every probe
+    // sequence ends (the bound only guards a corrupt table)
+    for (long long probe = 0; probe < p.nslots; probe++) {
+      ArcSlot s[kLookupBatch];
 #pragma unroll
-    for (int j = 0; j < kLookupBatch; j++) {
-      first[j] = on[j] ? __ldg(p.off + u[j]) : 0;
-      hi[j] = on[j] ? __ldg(p.off + u[j] + 1) : 0;
-      lo[j] = first[j];
-    }
-    // step 1, long adjacencies: the sample that opens the window, all searches
-    // in lockstep (jlo/jhi index ssamp; a search over [b, e) uses the samples in it)
-    int jlo[kLookupBatch], jhi[kLookupBatch];
-#pragma unroll
-    for (int j = 0; j < kLookupBatch; j++) {
-      jlo[j] = jhi[j] = 0;
-      if (hi[j] - lo[j] > kSampleStride) {
-        jlo[j] = (lo[j] + kSampleStride - 1) / kSampleStride;
-        jhi[j] = (hi[j] - 1) / kSampleStride + 1;
-      }
-    }
-    int s0[kLookupBatch];
-#pragma unroll
-    for (int j = 0; j < kLookupBatch; j++) s0[j] = jhi[j] > jlo[j] ? __ldg(p.ssamp + jlo[j]) : 0;
-#pragma unroll
-    for (int j = 0; j < kLookupBatch; j++)
-      if (jhi[j] > jlo[j] && s0[j] > v[j]) {  // v below every sample: the window before the first
-        hi[j] = jlo[j] * kSampleStride;
-        jhi[j] = jlo[j];
-      }
-    for (;;) {
-      int mid[kLookupBatch], sv[kLookupBatch];
+      for (int j = 0; j < kLookupBatch; j++)
+        if (pend[j]) s[j] = load_slot(p.atab + slot[j]);
       bool any = false;
 #pragma unroll
-      for (int j = 0; j < kLookupBatch; j++)
-        if (jhi[j] - jlo[j] > 1) {
-          mid[j] = (jlo[j] + jhi[j]) >> 1;
-          sv[j] = __ldg(p.ssamp + mid[j]);
+      for (int j = 0; j < kLookupBatch; j++) {
+        if (!pend[j]) continue;
+        if (s[j].tail == u[j] && s[j].head == v[j]) {
+          e[j] = s[j].arc;
+          pend[j] = false;
+        } else if (s[j].tail == kEmptyTail) {
+          pend[j] = false;
+        } else {
+          slot[j] = slot[j] + 1 == p.nslots ? 0 : slot[j] + 1;
           any = true;
         }
-      if (!any) break;
-#pragma unroll
-      for (int j = 0; j < kLookupBatch; j++)
-        if (jhi[j] - jlo[j] > 1) {
-          if (sv[j] <= v[j]) jlo[j] = mid[j];
-          else jhi[j] = mid[j];
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < kLookupBatch; j++)
-      if (jhi[j] - jlo[j] == 1) {
-        lo[j] = jlo[j] * kSampleStride;
-        hi[j] = min(hi[j], lo[j] + kSampleStride);
       }
-    for (;;) {  // step 2: last position with head <= v in the window
-      int mid[kLookupBatch], hv[kLookupBatch];
-      bool any = false;
-#pragma unroll
-      for (int j = 0; j < kLookupBatch; j++)
-        if (lo[j] < hi[j]) {
-          mid[j] = (lo[j] + hi[j]) >> 1;
-          hv[j] = __ldg(p.shead + mid[j]);
-          any = true;
-        }
       if (!any) break;
-#pragma unroll
-      for (int j = 0; j < kLookupBatch; j++)
-        if (lo[j] < hi[j]) {
-          if (hv[j] <= v[j]) lo[j] = mid[j] + 1;
-          else hi[j] = mid[j];
-        }
-    }
-    int e[kLookupBatch];
-#pragma unroll
-    for (int j = 0; j < kLookupBatch; j++) {
-      e[j] = -1;
-      if (on[j] && lo[j] > first[j] && __ldg(p.shead + lo[j] - 1) == v[j]) e[j] = __ldg(p.sidx + lo[j] - 1);
     }
 #pragma unroll
     for (int j = 0; j < kLookupBatch; j++) {
@@ -388,7 +311,7 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
         set_err(p.ctrl, ERR_UNKNOWN_ARC, i);
         continue;
       }
-      if (atomicExch(p.astamp + e[j], p.epoch) == p.epoch) {
+      if (atomicExch(&p.atab[slot[j]].stamp, p.epoch) == p.epoch) {
         set_err(p.ctrl, ERR_DUP_ARC, i);
         continue;
       }
@@ -435,7 +358,7 @@ __device__ __forceinline__ void ph_apply_repair(const Params &p) {
     if (r >= 0) continue;
     atomicAdd(p.res + e, -r);
     atomicAdd(p.res + __ldg(p.par + e), r);
-    const int u = __ldg(p.usrc + i), v = __ldg(p.adj + e);
+    const int u = __ldg(p.usrc + i), v = __ldg(p.udst + i);  // the lookup matched adj[e] == udst[i]
     atomic_add_ll(p.excess + u, -(long long)r);
     atomic_add_ll(p.excess + v, (long long)r);
     if (p.keep_dead) {  // the overflow returns to the tail: excess that can cover the head's deficit
@@ -456,7 +379,7 @@ __device__ __forceinline__ void ph_reopen(const Params &p) {
   for (int i = gt; i < p.k; i += nt) {
     const int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
-    const int u = __ldg(p.usrc + i), v = __ldg(p.adj + e);
+    const int u = __ldg(p.usrc + i), v = __ldg(p.udst + i);  // adj[e] == udst[i]
     if (!__ldcg(p.dead + u) || __ldcg(p.dead + v) || is_src(p, v)) continue;
     const int r = __ldcg(p.res + e);
     if (r <= 0) continue;
@@ -476,7 +399,7 @@ __device__ __forceinline__ void ph_cut_saturate(const Params &p) {
   for (int i = gt; i < p.k; i += nt) {
     int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
-    int u = __ldg(p.usrc + i), v = __ldg(p.adj + e);
+    int u = __ldg(p.usrc + i), v = __ldg(p.udst + i);  // adj[e] == udst[i]
     if (is_term(p, u) || is_term(p, v)) continue;
     if (p.side[u] == 0 && p.side[v] == 1) {
       int r = __ldcg(p.res + e);
@@ -598,6 +521,64 @@ __device__ __forceinline__ void for_vertices(const Params &p, F &&f) {
   }
 }
 
+// Every live vertex of the call, f(v); returns how many dead vertices this
+// thread passed over.  A warp takes windows of 512 vertices and first reads
+// their dead flags as one 16-byte load per lane: a window with no live vertex
+// (nearly all of them when a batch keeps the dead set) costs that load and a
+// vote.  Other windows are walked like for_vertices (v = window + 32 j + lane,
+// coalesced), the flags coming again from L2.  Calls with an instance mask
+// take the plain per-vertex walk.
+constexpr int kWindow = 512;
+
+template <int U, class F>
+__device__ __forceinline__ int for_live_vertices(const Params &p, F &&f) {
+  int dead_seen = 0;
+  if (p.inst_active) {
+    for_vertices<U>(p, [&](int v, bool is_dead) {
+      if (is_dead) dead_seen++;
+      else f(v);
+    });
+    return dead_seen;
+  }
+  const int lane = threadIdx.x & 31;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long w0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kWindow; w0 < p.n;
+       w0 += nw * kWindow) {
+    const long long b = w0 + 16 * lane;  // this lane's 16 flags; b is 16-byte aligned
+    bool all_dead;
+    int mine;  // vertices < n among the 16
+    if (b + 16 <= p.n) {
+      const uint4 x = __ldcg(reinterpret_cast<const uint4 *>(p.dead + b));
+      all_dead = (x.x & x.y & x.z & x.w) == 0x01010101u && (x.x | x.y | x.z | x.w) == 0x01010101u;
+      mine = 16;
+    } else {
+      mine = b < p.n ? (int)(p.n - b) : 0;
+      all_dead = true;
+      for (int i = 0; i < mine; i++) all_dead &= __ldcg(p.dead + b + i) != 0;
+    }
+    if (__all_sync(0xffffffffu, all_dead)) {
+      dead_seen += mine;
+      continue;
+    }
+    for (int j0 = 0; j0 < kWindow / 32; j0 += U) {
+      unsigned char dd[U];
+#pragma unroll
+      for (int j = 0; j < U; j++) {
+        const long long v = w0 + (j0 + j) * 32 + lane;
+        dd[j] = v < p.n ? __ldcg(p.dead + v) : 1;
+      }
+#pragma unroll
+      for (int j = 0; j < U; j++) {
+        const long long v = w0 + (j0 + j) * 32 + lane;
+        if (v >= p.n) continue;
+        if (dd[j]) dead_seen++;
+        else f((int)v);
+      }
+    }
+  }
+  return dead_seen;
+}
+
 // Seeds (my_init_1, code/dyn_data.h:60-67): t and every deficit vertex other
 // than s get height 0; all other live vertices become unvisited.  reset_dead
 // revives every vertex (the first relabel of a solve that does not keep the
@@ -615,13 +596,7 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
   }
   int pos = 0, kept = 0;
   long long unexpl = 0, seed_arcs = 0;
-  for_vertices<4>(p, [&](int v, bool is_dead) {
-    if (reset_dead) {
-      if (is_dead) p.dead[v] = 0;
-    } else if (is_dead) {
-      kept++;
-      return;
-    }
+  auto seed = [&](int v) {
     long long ex = __ldcg(p.excess + v);
     int d = deg_of(p, v);
     if (d > p.hub_deg) {  // the hub's round totals start clean
@@ -651,7 +626,15 @@ __device__ __forceinline__ void ph_bfs_init(const Params &p, Slot *out, bool res
       unexpl += d;
     }
     if (!is_term(p, v) && ex > 0) pos++;
-  });
+  };
+  if (reset_dead) {
+    for_vertices<4>(p, [&](int v, bool is_dead) {
+      if (is_dead) p.dead[v] = 0;
+      seed(v);
+    });
+  } else {
+    kept = for_live_vertices<4>(p, seed);
+  }
   block_add_int(&c->pos_count, pos);
   block_add_ll(&c->unexplored, unexpl);
   block_add_ll(&out->arcs, seed_arcs);
@@ -856,8 +839,7 @@ __device__ __forceinline__ void ph_bfs_bu(const Params &p, Slot *out, int L, LSt
 // BFS that proved them dead.
 __device__ __forceinline__ void ph_bfs_finalize(const Params &p, bool full, int floor_h, bool write_side) {
   int nd = 0;
-  for_vertices<8>(p, [&](int v, bool is_dead) {
-    if (is_dead) return;
+  for_live_vertices<8>(p, [&](int v) {
     const int h = __ldcg(p.height + v);
     if (h == UNV) {
       if (full) {
@@ -911,7 +893,7 @@ __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Sl
   Ctrl *c = p.ctrl;
   int seeds = 0;
   long long need = 0;
-  const int nc = sc->dcand;
+  const int nc = min(sc->dcand, p.n + 1);
   for (int i = gt; i < nc; i += nt) {
     const int v = __ldcg(p.dq + i);
     const long long ex = __ldcg(p.excess + v);
@@ -980,6 +962,7 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
             }
           } else if (old - take < 0 && atomicExch(p.stamp + x, (int)round_id) != (int)round_id) {
             append(nxt, &out->q, x);  // x takes this part of the deficit over: it pulls next round
+            append_bounded(p.dq, &p.ctrl->dcand, x, p.n + 1);  // and may keep it: the check looks at x
           }
           if (take > 0) {
             atomicSub(p.res + pa, (int)take);
@@ -1013,19 +996,31 @@ __device__ __forceinline__ bool revive_claim(const Params &p, int v) {
   return atomicCAS(p.dlab + v, old, tag) == old;
 }
 
-// Counts the deficits left inside the dead set (every dead vertex is looked at:
-// the check cannot miss one the pulls moved).  Each of them is revived (made
-// live: it is a seed of the global relabels) and starts the partial revival.
-__device__ __forceinline__ void ph_dead_check(const Params &p, Slot *out) {
+// Counts the deficits left inside the dead set: the candidate list holds every
+// dead vertex whose excess the batch or the pulls lowered (a vertex may appear
+// more than once; the claim counts it once); past its capacity every vertex is
+// looked at.  Each deficit found is revived (made live: it is a seed of the
+// global relabels) and starts the partial revival.
+__device__ __forceinline__ void ph_dead_check(const Params &p, const Ctrl *sc, Slot *out) {
   int left = 0;
-  for_vertices<8>(p, [&](int v, bool is_dead) {
+  auto check = [&](int v, bool is_dead) {
     if (is_dead && !is_term(p, v) && __ldcg(p.excess + v) < 0 && revive_claim(p, v)) {
       left++;
       p.dead[v] = 0;
       if (deg_of(p, v) > p.hub_deg) append_hub(p, p.fh[0], &out->hq, v);
       else append(p.fq[0], &out->q, v);
     }
-  });
+  };
+  const int nc = sc->dcand;
+  if (nc <= p.n + 1) {
+    const int nt = gridDim.x * blockDim.x, gt = spread_thread();
+    for (int i = gt; i < nc; i += nt) {
+      const int v = __ldcg(p.dq + i);
+      check(v, __ldcg(p.dead + v) != 0);
+    }
+  } else {
+    for_vertices<8>(p, check);
+  }
   block_add_int(&p.ctrl->dleft, left);
 }
 
@@ -1609,8 +1604,7 @@ template <int BLOCK>
 // relabel, so it is never proven dead.
 __device__ __forceinline__ void ph_flow(const Params &p, typename BlockGroup<BLOCK>::Temp &btmp) {
   long long acc = 0;
-  for_vertices<8>(p, [&](int v, bool is_dead) {
-    if (is_dead) return;
+  for_live_vertices<8>(p, [&](int v) {
     const long long ex = __ldcg(p.excess + v);
     long long c = 0;
     if (is_snk(p, v)) c = ex;
@@ -1958,8 +1952,9 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
         if (lead) c->rounds_used = round_id - p.round_base;
       }
       kind = TR_DEAD_CHECK;
-      items = hubitems = 0;
-      ph_dead_check(p, slot_out());
+      items = sc->dcand;
+      hubitems = 0;
+      ph_dead_check(p, sc, slot_out());
       if (!next()) return;
       if (sc->dleft > 0) {
         // deficits left: revive what can reach them (partial), unless that

@@ -47,6 +47,11 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr int kMaxLanes = 4;
+// Updates per tick a lane's staging is sized for at creation.
+constexpr int64_t kStageReserve = 1 << 20;
+// Host threads that validate one request (the lanes' workers and other
+// submitters run beside them).
+constexpr int kSubmitThreads = 8;
 
 struct Request {
   int64_t ticket;
@@ -94,10 +99,7 @@ struct dmf_server {
   int64_t ticks = 0, served = 0, batched_sum = 0;
 };
 
-static int64_t footprint(const dmf_graph *g) {
-  // residual state bytes per arc and per vertex (see the solver's data layout)
-  return 28LL * g->m + 64LL * g->n;
-}
+static int64_t footprint(const dmf_graph *g) { return dmf::solver_footprint(g->n, g->m); }
 
 static void tick_loop(dmf_server *S, Lane *L) {
   std::vector<Request *> &batch = L->batch;
@@ -289,6 +291,11 @@ int dmf_server_create(int32_t count, const dmf_graph *const *graphs, const int32
         rc = dmf_solver_create(S->graphs[g], S->s[g], S->t[g], &lo, L->stream, &L->sv);
         if (!rc) rc = dmf_static_maxflow(L->sv, &L->flows[0]);
       }
+      // staging for the usual tick up front (a lane that shares graphs batches
+      // several requests per tick); larger ticks still grow it
+      int64_t arcs = 0;
+      for (int32_t g : L->graphs) arcs += S->graphs[g]->m;
+      if (!rc) rc = dmf::reserve_updates(L->sv, (int32_t)std::min<int64_t>(arcs, L->multi ? kStageReserve * 4 : kStageReserve));
       if (rc) return rc;
     }
     for (auto &L : S->lanes) L->worker = std::thread(tick_loop, S, L.get());
@@ -345,7 +352,8 @@ int dmf_server_submit(dmf_server *S, int32_t graph, int32_t k, const int32_t *sr
   // arc ids are sorted to find repeats.  The first bad update is reported.
   std::vector<int64_t> arcs((size_t)k);
   int32_t bad_range = INT32_MAX, bad_cap = INT32_MAX, bad_arc = INT32_MAX;
-#pragma omp parallel for schedule(static) reduction(min : bad_range, bad_cap, bad_arc) if (k >= 16384)
+#pragma omp parallel for num_threads(kSubmitThreads) schedule(static) reduction(min : bad_range, bad_cap, bad_arc) \
+    if (k >= 16384)
   for (int32_t i = 0; i < k; i++) {
     arcs[i] = -1;
     if (src[i] < 0 || dst[i] < 0 || src[i] >= g->n || dst[i] >= g->n) {

@@ -20,9 +20,8 @@ namespace {
 // Raw feature sums of an update batch against the current residual state, for
 // the schedule picker (nothing is modified).  Updates the solver would reject
 // (bad ids, unknown arcs) are skipped here; the solve reports them.
-__global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, const int *__restrict__ shead,
-                                                  const int *__restrict__ ssamp, const int *__restrict__ sidx,
-                                                  const int *cap, const int *res, int n,
+__global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, const ArcSlot *atab,
+                                                  long long nslots, const int *cap, const int *res, int n,
                                                   int k, const int *usrc, const int *udst, const int *uw,
                                                   dmfs::FeatAcc *acc) {
   unsigned long long valid = 0, dec = 0, satdec = 0, incsat = 0, ins = 0, del = 0, sdeg = 0, mdeg = 0;
@@ -30,7 +29,7 @@ __global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, c
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
     const int u = __ldg(usrc + i), v = __ldg(udst + i), w = __ldg(uw + i);
     if (u < 0 || u >= n || v < 0 || v >= n || u == v) continue;
-    const int e = find_arc_dev(off, shead, ssamp, sidx, u, v);
+    const int e = find_arc_table(atab, nslots, u, v);
     if (e < 0) continue;
     valid++;
     const int c0 = __ldcg(cap + e), r = __ldcg(res + e);
@@ -93,16 +92,43 @@ using dmf::fail;
 using dmf::ok;
 using dmf::guarded;
 
+// Fills the arc table: a warp per tail vertex, a lane per arc.  Equal
+// (tail, head) pairs keep the largest arc index.  Every insert ends: the table
+// has more slots than arcs, so an empty slot or the key is always found.
+__global__ void __launch_bounds__(256) k_arc_table_build(const int *__restrict__ off, const int *__restrict__ adj,
+                                                         int n, ArcSlot *tab, long long nslots) {
+  const int lane = threadIdx.x & 31;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long u = warp; u < n; u += nwarps) {
+    const int b = __ldg(off + u), e = __ldg(off + u + 1);
+    for (int a = b + lane; a < e; a += 32) {
+      const int v = __ldg(adj + a);
+      const unsigned long long key = arc_key((int)u, v);
+      long long sl = arc_slot0((int)u, v, nslots);
+      for (long long probe = 0; probe < nslots; probe++) {
+        const unsigned long long old =
+            atomicCAS(reinterpret_cast<unsigned long long *>(tab + sl), ~0ull, key);
+        if (old == ~0ull || old == key) {
+          atomicMax(&tab[sl].arc, a);
+          break;
+        }
+        sl = sl + 1 == nslots ? 0 : sl + 1;
+      }
+    }
+  }
+}
+
 struct dmf_solver {
   int dev = 0;
   cudaStream_t stream = nullptr;
   int n = 0, m = 0, s = 0, t = 0;
   dmf_opts opts{};
   int tile = 32, grid = 0, block = kBlock, hub_deg = 256, small_deg = 8, minb = 2, bu_alpha = 2;
-  int *off = nullptr, *adj = nullptr, *par = nullptr, *sidx = nullptr, *cap = nullptr, *res = nullptr;
-  int *shead = nullptr;  // heads in per-vertex sorted order (shead[i] = adj[sidx[i]])
-  int *ssamp = nullptr;  // every kSampleStride-th entry of shead
-  int *height = nullptr, *stamp = nullptr, *astamp = nullptr, *uarc = nullptr;
+  int *off = nullptr, *adj = nullptr, *par = nullptr, *cap = nullptr, *res = nullptr;
+  ArcSlot *atab = nullptr;  // (tail, head) -> arc, with the per-arc batch stamps
+  long long nslots = 0;
+  int *height = nullptr, *stamp = nullptr, *uarc = nullptr;
   long long *excess = nullptr;
   unsigned char *dead = nullptr, *side = nullptr;
   int *dlab = nullptr;    // dead-set repair labels, tagged with the launch epoch
@@ -277,14 +303,12 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.off = sv->off;
   p.adj = sv->adj;
   p.par = sv->par;
-  p.sidx = sv->sidx;
-  p.shead = sv->shead;
-  p.ssamp = sv->ssamp;
+  p.atab = sv->atab;
+  p.nslots = sv->nslots;
   p.cap = sv->cap;
   p.res = sv->res;
   p.height = sv->height;
   p.stamp = sv->stamp;
-  p.astamp = sv->astamp;
   p.uarc = sv->ubuf ? sv->ubuf + 3 * (size_t)sv->kcap : nullptr;
   p.excess = sv->excess;
   p.dead = sv->dead;
@@ -499,7 +523,7 @@ int batch_features(dmf_solver *sv, dmf_sched *sched, int k, float *feat, int *ac
   if (k > 0) {
     const size_t K = (size_t)sv->kcap;
     const int blocks = std::min((k + 255) / 256, 4 * 148);
-    k_features<<<blocks, 256, 0, sv->stream>>>(sv->off, sv->shead, sv->ssamp, sv->sidx, sv->cap, sv->res, sv->n, k,
+    k_features<<<blocks, 256, 0, sv->stream>>>(sv->off, sv->atab, sv->nslots, sv->cap, sv->res, sv->n, k,
                                                sv->ubuf, sv->ubuf + K, sv->ubuf + 2 * K, sv->facc);
     CK(cudaGetLastError(), "feature launch");
   }
@@ -678,12 +702,10 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
     p.off = d_index;
     p.adj = d_adj;
     p.par = d_par;
-    p.sidx = nullptr;
-    p.shead = nullptr;
-    p.ssamp = nullptr;
+    p.atab = nullptr;
+    p.nslots = 0;
     p.cap = const_cast<int *>(d_cap);  // read only in static mode
     p.res = d_res;
-    p.astamp = nullptr;
     p.uarc = nullptr;
     p.ctrl = ctrl;
     p.mode = MODE_STATIC;
@@ -752,7 +774,6 @@ int create_impl(const dmf_graph *g, int32_t s, int32_t t, const dmf_opts *opts, 
   if (!g || !out) return fail(DMF_ERR_INVALID_ARG, "null argument");
   if (g->n < 2 || s < 0 || t < 0 || s >= g->n || t >= g->n || s == t)
     return fail(DMF_ERR_INVALID_ARG, "need n >= 2 and distinct s, t in [0, n): n=%d s=%d t=%d", g->n, s, t);
-  if ((int64_t)g->sidx.size() != g->m) return fail(DMF_ERR_INVALID_ARG, "graph has no arc index");
   int ndev = dmf_device_count();
   if (ndev == 0) return fail(DMF_ERR_CUDA, "no CUDA device is visible; the solver runs only on the GPU");
   if (opts && (opts->variant < 0 || opts->variant > 2))
@@ -794,10 +815,8 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   if ((st = configure(sv))) return st;
   const size_t N = (size_t)g->n + 1, M = (size_t)g->m;
   if ((st = dalloc(sv, &sv->off, N)) || (st = dalloc(sv, &sv->adj, M)) || (st = dalloc(sv, &sv->par, M)) ||
-      (st = dalloc(sv, &sv->sidx, M)) || (st = dalloc(sv, &sv->shead, M)) ||
-      (st = dalloc(sv, &sv->ssamp, M / kSampleStride + 1)) || (st = dalloc(sv, &sv->cap, M)) ||
-      (st = dalloc(sv, &sv->res, M)) ||
-      (st = dalloc(sv, &sv->astamp, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
+      (st = dalloc(sv, &sv->atab, (size_t)arc_table_slots((long long)M))) || (st = dalloc(sv, &sv->cap, M)) ||
+      (st = dalloc(sv, &sv->res, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
       (st = dalloc(sv, &sv->excess, N)) || (st = dalloc(sv, &sv->dead, N)) || (st = dalloc(sv, &sv->side, N)) ||
       (st = dalloc(sv, &sv->qbuf, 6 * N)) || (st = dalloc(sv, &sv->dlab, N)) || (st = dalloc(sv, &sv->ctrl, 1)))
     return st;
@@ -826,14 +845,13 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   up(sv->off, g->off.data(), 4 * N);
   up(sv->adj, g->adj.data(), 4 * M);
   up(sv->par, g->par.data(), 4 * M);
-  up(sv->sidx, g->sidx.data(), 4 * M);
-  std::vector<int32_t> shead(M);
-#pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < (int64_t)M; i++) shead[i] = g->adj[g->sidx[i]];
-  up(sv->shead, shead.data(), 4 * M);
-  std::vector<int32_t> ssamp(M / kSampleStride + 1, INT_MAX);
-  for (size_t j = 0; j * kSampleStride < M; j++) ssamp[j] = shead[j * kSampleStride];
-  up(sv->ssamp, ssamp.data(), 4 * ssamp.size());
+  sv->nslots = arc_table_slots((long long)M);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->atab, 0xFF, sizeof(ArcSlot) * (size_t)sv->nslots, S);
+  if (e == cudaSuccess && g->n > 0) {
+    const int warps = 8, blocks = (int)std::min<long long>(((long long)g->n + warps - 1) / warps, 16LL * 148);
+    k_arc_table_build<<<blocks, 32 * warps, 0, S>>>(sv->off, sv->adj, g->n, sv->atab, sv->nslots);
+    e = cudaGetLastError();
+  }
   up(sv->cap, g->w.data(), 4 * M);
   {
     int32_t mx = 0;
@@ -844,7 +862,6 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   up(sv->hch, hub_chunks.data(), sizeof(int2) * hub_chunks.size());
   up(sv->hub_base, hub_base.data(), 4 * (size_t)g->n);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->chunk_mark, 0, 8 * NC, S);
-  if (e == cudaSuccess) e = cudaMemsetAsync(sv->astamp, 0, 4 * M, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->hc_done, 0, 4 * NC, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->hc_alloc, 0, 8 * NC, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->hc_moved, 0, 8 * NC, S);
@@ -897,6 +914,19 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
 
 }  // namespace
 
+int64_t dmf::solver_footprint(int64_t n, int64_t m) {
+  // adj, par, cap, res; the arc table; off, labels, stamps, excess, marks,
+  // repair labels, hub bases and six vertex queues (rounded up)
+  return 16 * m + (int64_t)sizeof(ArcSlot) * arc_table_slots(m) + 64 * n;
+}
+
+int dmf::reserve_updates(dmf_solver *sv, int32_t k) {
+  CK(cudaSetDevice(sv->dev), "cudaSetDevice");
+  int st = ensure_ubuf(sv, k);
+  if (!st) st = ensure_host_ubuf(sv, k);
+  return st;
+}
+
 int dmf::resident_solve_blocks(int32_t *blocks) {
   int dev = 0, per_sm = 0, sms = 0;
   CK(cudaGetDevice(&dev), "cudaGetDevice");
@@ -922,7 +952,6 @@ int dmf_multi_create(int32_t count, const dmf_graph *const *graphs, const int32_
     const dmf_graph *g = graphs[i];
     if (!g || g->n < 2 || s[i] < 0 || t[i] < 0 || s[i] >= g->n || t[i] >= g->n || s[i] == t[i])
       return fail(DMF_ERR_INVALID_ARG, "instance %d: need a graph with n >= 2 and distinct s, t in [0, n)", i);
-    if ((int64_t)g->sidx.size() != g->m) return fail(DMF_ERR_INVALID_ARG, "instance %d has no arc index", i);
     N += g->n;
     M += g->m;
   }
@@ -935,7 +964,6 @@ int dmf_multi_create(int32_t count, const dmf_graph *const *graphs, const int32_
     U.adj.resize((size_t)M);
     U.w.resize((size_t)M);
     U.par.resize((size_t)M);
-    U.sidx.resize((size_t)M);
     MultiSpec ms;
     ms.count = count;
     ms.vbase.resize((size_t)count + 1);
@@ -963,7 +991,6 @@ int dmf_multi_create(int32_t count, const dmf_graph *const *graphs, const int32_
         U.adj[ab + e] = vb_i + g.adj[e];
         U.w[ab + e] = g.w[e];
         U.par[ab + e] = ab + g.par[e];
-        U.sidx[ab + e] = ab + g.sidx[e];
       }
     }
     U.off[N] = (int32_t)M;
@@ -1401,7 +1428,6 @@ int dmf_solver_copy_state(dmf_solver *dst, const dmf_solver *src) {
     cudaStream_t S = dst->stream;
     CK(cudaMemcpyAsync(dst->cap, src->cap, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D cap");
     CK(cudaMemcpyAsync(dst->res, src->res, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D res");
-    CK(cudaMemcpyAsync(dst->astamp, src->astamp, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D astamp");
     CK(cudaMemcpyAsync(dst->excess, src->excess, 8 * N, cudaMemcpyDeviceToDevice, S), "D2D excess");
     CK(cudaMemcpyAsync(dst->height, src->height, 4 * N, cudaMemcpyDeviceToDevice, S), "D2D height");
     CK(cudaMemcpyAsync(dst->stamp, src->stamp, 4 * N, cudaMemcpyDeviceToDevice, S), "D2D stamp");
@@ -1412,7 +1438,9 @@ int dmf_solver_copy_state(dmf_solver *dst, const dmf_solver *src) {
     CK(cudaStreamSynchronize(S), "copy state");
     dst->round_base = src->round_base;
     dst->relabel_base = src->relabel_base;
-    dst->epoch = src->epoch;
+    // later than every epoch either solver used: no stale batch stamp or
+    // repair-label tag in dst's own arrays can equal a future launch's epoch
+    dst->epoch = std::max(dst->epoch, src->epoch);
     dst->solved = src->solved;
     dst->side_valid = src->side_valid;
     dst->st = src->st;

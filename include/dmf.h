@@ -280,7 +280,7 @@ int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs,
 /* ---- serving loop ------------------------------------------------------------ */
 /* Device-resident graphs serving update-batch requests.  Graphs are admitted in
  * the given order while the estimated device footprint of their residual state
- * (28 B per arc + 64 B per vertex) fits `hbm_budget` bytes; the rest are not
+ * (42 B per arc + 64 B per vertex) fits `hbm_budget` bytes; the rest are not
  * admitted (ids of admitted graphs are their positions among the admitted ones,
  * dmf_server_info).  The caller keeps the graphs alive until destroy.
  * Lanes: a graph with at least a quarter of the admitted arcs gets a lane of
