@@ -17,11 +17,11 @@ Prints one JSON line (rank 0).  `value` is the p50 device time per batch with th
 batch already in HBM (dmf_apply_updates_device, CUDA events on the solver's
 stream, no instrumentation); `e2e` is the same metric through the host-array
 entry point dmf_apply_updates (pinned staging, H2D of the batch, D2H of the flow
-value) timed by the host clock.  Beside it, on the same batches and from the
-same pre-batch states: the engine's own from-scratch recompute
+value) timed by the host clock.  Beside it, on the same batch sequence, one
+solver at a time: the engine's own from-scratch recompute
 (`recompute_p50_ms`, `speedup_vs_recompute`), the learned schedule picker
 against the plain schedule (`learned_vs_plain`), and the phase timeline of a
-traced copy (`phases_us_per_batch`, `roofline_bfs`).  The device states after
+traced solver (`phases_us_per_batch`, `roofline_bfs`).  The device states after
 the first and the last timed batch are certified by the oracle's certificate
 checker, and every batch's flow must agree across all the solvers.
 """
@@ -241,12 +241,14 @@ def recorded_reference_cuda(g, s, t, scale: int):
 
 def run_ours(args, rank: int, world: int):
     """The headline workload.  One step = one 1% batch applied to the resident
-    state.  Per timed batch, from copies of the same pre-batch state: the batch
-    (value; device pointers, no instrumentation), the engine's own from-scratch
-    recompute of the same capacities (dmf_recompute_device), the learned and the
-    plain schedule through the scheduled entry point, and a traced pass for the
-    phase breakdown.  A second solver replays every batch through the host-array
-    entry point (e2e)."""
+    state.  The timed solver takes every batch in order, alone on the GPU (L2
+    flushed before each), as a resident solver serving a stream of batches
+    would.  The same batch sequence then runs, one solver at a time, through
+    the engine's own from-scratch recompute (dmf_recompute_device), the
+    learned and the plain schedule (dmf_apply_updates_scheduled), a traced
+    solver for the phase breakdown, and the host-array entry point (e2e).
+    Every solver reaches the same capacities before each batch, so every flow
+    must agree."""
     import numpy as np
     import torch
     import dyn_maxflow_b200 as D
@@ -267,43 +269,33 @@ def run_ours(args, rank: int, world: int):
     torch.cuda.synchronize()
     kw = dict(variant=args.variant, kernel_cycles=args.kernel_cycles, relabel_interval=args.relabel_interval,
               tile=args.tile, stream=stream, fixed_interval=args.fixed_interval)
-    A = D.Solver(g, s, t, **kw)
-    static_flow = A.static_maxflow()
-    static_ms = A.stats()["last_ms"]
-    sched = None
-    if not args.no_learned and os.path.exists(args.sched_weights):
-        sched = D.Scheduler.load(args.sched_weights)
-    R = D.Solver(g, s, t, **kw)
-    P = D.Solver(g, s, t, trace=True, **kw)
-    B = D.Solver(g, s, t, **kw)
-    B.copy_state_from(A)
-    Ls = [D.Solver(g, s, t, **kw), D.Solver(g, s, t, **kw)] if sched is not None else []
 
     def flushed():
         flush.fill_(1)
         torch.cuda.synchronize()
 
-    flows, times, stats, rec_ms, rec_flows = [], [], [], [], []
-    learned_ms, plain_ms, picks, learned_ok = [], [], [], True
-    phase_us, pstats = {}, []
+    def arg_ptrs(b):
+        return (b[0].data_ptr(), b[1].data_ptr(), b[2].data_ptr(), int(b[0].numel()))
+
+    # ---- headline pass: one resident solver, every batch in order ----
+    A = D.Solver(g, s, t, **kw)
+    static_flow = A.static_maxflow()
+    static_ms = A.stats()["last_ms"]
+    flows, times, stats = [], [], []
     certified = True
-    sampler, t_region = None, None
+    sampler, t_region, t_check = None, None, 0.0
     for i, b in enumerate(dbat):
         timed = i >= args.warmup
-        args_d = (b[0].data_ptr(), b[1].data_ptr(), b[2].data_ptr(), int(b[0].numel()))
-        if timed:
-            for other in [R] + Ls + ([P] if len(pstats) < args.phase_batches else []):
-                other.copy_state_from(A)
-            if sampler is None:
-                if world > 1:
-                    torch.distributed.barrier()
-                torch.cuda.synchronize()
-                sampler = ClockSampler(dev)
-                t_region = time.perf_counter()
+        if timed and sampler is None:
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            sampler = ClockSampler(dev)
+            t_region = time.perf_counter()
         flushed()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        f = A.apply_updates_device(*args_d)
+        f = A.apply_updates_device(*arg_ptrs(b))
         e1.record(stream)
         e1.synchronize()
         flows.append(f)
@@ -311,36 +303,67 @@ def run_ours(args, rank: int, world: int):
             continue
         times.append(e0.elapsed_time(e1))
         stats.append(A.stats())
-        flushed()
-        rec_flows.append(R.recompute_device(*args_d))
-        rec_ms.append(R.stats()["last_ms"])
-        if Ls:
-            flushed()
-            fl, act = Ls[0].apply_updates_scheduled(sched, *batches[i])
-            learned_ms.append(Ls[0].stats()["last_ms"])
-            flushed()
-            fp, _ = Ls[1].apply_updates_scheduled(None, *batches[i])
-            plain_ms.append(Ls[1].stats()["last_ms"])
-            picks.append(act)
-            learned_ok &= fl == fp == f
-        if len(pstats) < args.phase_batches:
-            flushed()
-            P.apply_updates_device(*args_d)
-            pstats.append(P.stats())
-            tr = P.trace()
-            for (k0, t0_), (k1, t1_) in zip(tr, tr[1:]):
-                d = phase_us.setdefault(k1, [0.0, 0])
-                d[0] += t1_ - t0_
-                d[1] += 1
         if not args.no_certify and (i == args.warmup or i == nb - 1):
+            t_c = time.perf_counter()
             cap, res, ex, _ = A.state()
             rc, val, cut = O.certify(n, off, adj, cap, par, res, s, t)
             certified &= (rc == 0 and val == f == cut)
+            t_check += time.perf_counter() - t_c
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    region_s = time.perf_counter() - t_region
+    region_s = time.perf_counter() - t_region - t_check
     clocks = sampler.stop() if sampler else None
+    A.close()
+
+    # ---- the same batch sequence on other solvers, one pass each ----
+    # from-scratch recompute of the same capacities (dmf_recompute_device)
+    R = D.Solver(g, s, t, **kw)
+    R.static_maxflow()
+    rec_ms, rec_flows = [], []
+    for i, b in enumerate(dbat):
+        flushed()
+        f = R.recompute_device(*arg_ptrs(b))
+        if i >= args.warmup:
+            rec_flows.append(f)
+            rec_ms.append(R.stats()["last_ms"])
+    R.close()
+    # learned and plain schedules through the scheduled entry point
+    sched = None
+    if not args.no_learned and os.path.exists(args.sched_weights):
+        sched = D.Scheduler.load(args.sched_weights)
+    learned_ms, plain_ms, picks, learned_ok = [], [], [], True
+    if sched is not None:
+        lflows = {}
+        for name, sc in (("learned", sched), ("plain", None)):
+            L = D.Solver(g, s, t, **kw)
+            L.static_maxflow()
+            for i, b in enumerate(batches):
+                flushed()
+                fl, act = L.apply_updates_scheduled(sc, *b)
+                if i >= args.warmup:
+                    lflows.setdefault(name, []).append(fl)
+                    (learned_ms if name == "learned" else plain_ms).append(L.stats()["last_ms"])
+                    if name == "learned":
+                        picks.append(act)
+            L.close()
+        learned_ok = lflows["learned"] == lflows["plain"] == flows[args.warmup:]
+        sched.close()
+    # phase timeline of a traced solver over the first timed batches
+    P = D.Solver(g, s, t, trace=True, **kw)
+    P.static_maxflow()
+    phase_us, pstats = {}, []
+    for i, b in enumerate(dbat[:args.warmup + args.phase_batches]):
+        flushed()
+        P.apply_updates_device(*arg_ptrs(b))
+        if i < args.warmup:
+            continue
+        pstats.append(P.stats())
+        tr = P.trace()
+        for (k0, t0_), (k1, t1_) in zip(tr, tr[1:]):
+            d = phase_us.setdefault(k1, [0.0, 0])
+            d[0] += t1_ - t0_
+            d[1] += 1
     # the BFS of a from-scratch solve (every vertex live), on the traced solver, untimed
     flushed()
     P.static_maxflow()
@@ -351,11 +374,10 @@ def run_ours(args, rank: int, world: int):
         static_phase.setdefault(k1, {"us": 0.0, "count": 0})
         static_phase[k1]["us"] += t1_ - t0_
         static_phase[k1]["count"] += 1
-    for x in [A, R, P] + Ls:
-        x.close()
-    if sched is not None:
-        sched.close()
+    P.close()
     # ---- end-to-end pass through the host-array entry point ----
+    B = D.Solver(g, s, t, **kw)
+    B.static_maxflow()
     e2e, flows2 = [], []
     for i, b in enumerate(batches):
         flushed()
@@ -410,16 +432,16 @@ def run_ours(args, rank: int, world: int):
                                         "dead_deficits", "dead_kept")},
         "clocks": clocks,
         "phases_us_per_batch": phases,
-        "phases_source": f"separate traced solver, state copied before each of the first {len(pstats)} timed batches",
+        "phases_source": f"separate traced solver on the same batch sequence, its first {len(pstats)} timed batches",
     }
-    if Ls:
+    if learned_ms:
         lp, pp = pct(learned_ms, 0.5), pct(plain_ms, 0.5)
         res["learned_vs_plain"] = {
             "learned_p50_ms": round(lp, 4), "plain_p50_ms": round(pp, 4), "learned_p99_ms": round(pct(learned_ms, 0.99), 4),
             "plain_p99_ms": round(pct(plain_ms, 0.99), 4), "ratio_plain_over_learned": round(pp / lp, 4),
             "picks": dict(zip(D.ACTIONS, np.bincount(picks, minlength=D.N_ACTIONS).tolist())),
             "equal_flows": bool(learned_ok),
-            "timing": "dmf_apply_updates_scheduled from copies of the same pre-batch state (features, decision and "
+            "timing": "dmf_apply_updates_scheduled, one solver per schedule over the same batch sequence (features, decision and "
                       "solve; H2D of the batch not included)"}
     refc = recorded_reference_cuda(g, s, t, args.scale)
     if refc is not None:

@@ -908,12 +908,93 @@ __device__ __forceinline__ void ph_dead_seed(const Params &p, const Ctrl *sc, Sl
 }
 
 // One pull-relabel round: a warp per deficit of the list, lanes over its arcs.
-// A vertex joins the next round's list once (stamp = this round's id).
-__device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, int nn, int *nxt, Slot *out,
-                                             unsigned round_id, LStats &ls) {
-  const int lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
+// A vertex joins the next round's list once (stamp = this round's id).  A
+// 32-arc step issues the supplier-side loads (the residual x->y, x's dead flag,
+// excess and repair label) together once the arc's head and partner are
+// known.  A row of at most 32 arcs is read once: pass 1 works on the loads of
+// pass 0, with the residual pass 0 left on each arc (only y's warp changes the
+// residual of an arc into y within a round).
+struct PullArc {
+  int x, pa, a, r, hx;
+  long long ex;
+  bool ok;  // residual x -> y from a dead vertex that is not a terminal
+};
+
+__device__ __forceinline__ PullArc pull_load(const Params &p, int a, int end) {
+  PullArc q{-1, 0, a, 0, 0, 0, false};
+  if (a < end) {
+    q.x = __ldg(p.adj + a);
+    q.pa = __ldg(p.par + a);
+    q.r = __ldcg(p.res + q.pa);
+    const bool dx = __ldcg(p.dead + q.x) != 0;
+    q.ex = __ldcg(p.excess + q.x);
+    q.hx = dead_label(p, q.x);
+    q.ok = q.r > 0 && dx && !is_term(p, q.x);
+  }
+  return q;
+}
+
+// Pass 0 on one step: exact claims on parked excess (a claim bounded by an
+// atomic on the supplier's excess; what another puller took first is handed
+// back).  Returns what the warp moved.
+__device__ __forceinline__ long long pull_excess(const Params &p, cg::thread_block_tile<32> &warp, PullArc &q,
+                                                 long long need, LStats &ls) {
+  const long long cand = q.ok && q.ex > 0 ? (q.ex < q.r ? q.ex : (long long)q.r) : 0;
+  const long long pre = cg::exclusive_scan(warp, cand, cg::plus<long long>());
+  long long take = need - pre;
+  take = take < 0 ? 0 : (take > cand ? cand : take);
+  if (take > 0) {
+    const long long old = atomic_add_ll(p.excess + q.x, -take);
+    if (old < take) {
+      const long long back = take - (old > 0 ? old : 0);
+      atomic_add_ll(p.excess + q.x, back);
+      take -= back;
+    }
+    if (take > 0) {
+      atomicSub(p.res + q.pa, (int)take);
+      atomicAdd(p.res + q.a, (int)take);
+      q.r -= (int)take;
+      ls.pushes++;
+    }
+  }
+  return cg::reduce(warp, take, cg::plus<long long>());
+}
+
+// Pass 1 on one step: the rest of the deficit moves to dead in-neighbours with
+// a lower label (they pull it in the next round); hmin collects the labels of
+// in-neighbours still residual.  Returns what the warp moved.
+__device__ __forceinline__ long long pull_lower(const Params &p, cg::thread_block_tile<32> &warp, PullArc &q,
+                                                long long need, int hy, int &hmin, int *nxt, int *ntail,
+                                                unsigned round_id, LStats &ls) {
+  long long cand = 0;
+  if (q.ok && q.r > 0) {
+    if (q.hx < hy) cand = q.r;
+    else hmin = min(hmin, q.hx);
+  }
+  const long long pre = cg::exclusive_scan(warp, cand, cg::plus<long long>());
+  long long take = need - pre;
+  take = take < 0 ? 0 : (take > cand ? cand : take);
+  if (take > 0) {
+    const long long old = atomic_add_ll(p.excess + q.x, -take);
+    if (old - take < 0 && atomicExch(p.stamp + q.x, (int)round_id) != (int)round_id) {
+      append(nxt, ntail, q.x);  // x takes this part of the deficit over: it pulls next round
+      append_bounded(p.dq, &p.ctrl->dcand, q.x, p.n + 1);  // and may keep it: the check looks at x
+    }
+    atomicSub(p.res + q.pa, (int)take);
+    atomicAdd(p.res + q.a, (int)take);
+    ls.pushes++;
+  }
+  if (cand > 0 && take < cand) hmin = min(hmin, q.hx);  // still residual
+  return cg::reduce(warp, take, cg::plus<long long>());
+}
+
+// Warps first_warp, first_warp + nwarps, ... take the list's deficits; the next
+// round's list is appended behind *ntail.
+__device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, int nn, int *nxt, int *ntail,
+                                             int first_warp, int nwarps, unsigned round_id, LStats &ls) {
+  const int lane = threadIdx.x & 31;
   cg::thread_block_tile<32> warp = cg::tiled_partition<32>(cg::this_thread_block());
-  for (int i = spread_group<32>(); i < nn; i += nwarps) {
+  for (int i = first_warp; i < nn; i += nwarps) {
     int y = 0;
     long long need = 0;
     if (lane == 0) {
@@ -926,54 +1007,35 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
     const int hy = dead_label(p, y);
     const int beg = __ldg(p.off + y), end = __ldg(p.off + y + 1);
     long long got = 0;
-    int hmin = INT_MAX;  // lowest label over the dead in-neighbours still residual (pass 1)
-    for (int pass = 0; pass < 2 && need > 0; pass++) {
-      for (int a0 = beg; a0 < end && need > 0; a0 += 32) {
-        const int a = a0 + lane;
-        int x = -1, pa = -1, r = 0;
-        long long cand = 0;
-        if (a < end) {
-          x = __ldg(p.adj + a);
-          pa = __ldg(p.par + a);
-          r = __ldcg(p.res + pa);  // residual x -> y
-          if (r > 0 && __ldcg(p.dead + x) && !is_term(p, x)) {
-            if (pass == 0) {
-              const long long ex = __ldcg(p.excess + x);
-              if (ex > 0) cand = ex < r ? ex : r;
-            } else {
-              const int hx = dead_label(p, x);
-              if (hx < hy) cand = r;
-              else hmin = min(hmin, hx);
-            }
-          }
-          ls.arcs++;
-        }
-        const long long pre = cg::exclusive_scan(warp, cand, cg::plus<long long>());
-        long long take = need - pre;
-        take = take < 0 ? 0 : (take > cand ? cand : take);
-        if (take > 0) {
-          const long long old = atomic_add_ll(p.excess + x, -take);
-          if (pass == 0) {
-            // only parked excess: hand back what another puller took first
-            if (old < take) {
-              const long long back = take - (old > 0 ? old : 0);
-              atomic_add_ll(p.excess + x, back);
-              take -= back;
-            }
-          } else if (old - take < 0 && atomicExch(p.stamp + x, (int)round_id) != (int)round_id) {
-            append(nxt, &out->q, x);  // x takes this part of the deficit over: it pulls next round
-            append_bounded(p.dq, &p.ctrl->dcand, x, p.n + 1);  // and may keep it: the check looks at x
-          }
-          if (take > 0) {
-            atomicSub(p.res + pa, (int)take);
-            atomicAdd(p.res + a, (int)take);
-            ls.pushes++;
+    int hmin = INT_MAX;  // lowest label over the dead in-neighbours still residual
+    if (end - beg <= 32) {
+      PullArc q = pull_load(p, beg + lane, end);
+      if (q.x >= 0) ls.arcs++;
+      long long mv = pull_excess(p, warp, q, need, ls);
+      need -= mv;
+      got += mv;
+      if (need > 0) {
+        mv = pull_lower(p, warp, q, need, hy, hmin, nxt, ntail, round_id, ls);
+        need -= mv;
+        got += mv;
+      }
+    } else {  // two steps' loads in flight at a time
+      for (int pass = 0; pass < 2 && need > 0; pass++) {
+        for (int a0 = beg; a0 < end && need > 0; a0 += 64) {
+          PullArc q0 = pull_load(p, a0 + lane, end);
+          PullArc q1 = pull_load(p, a0 + 32 + lane, end);
+          ls.arcs += (q0.x >= 0) + (q1.x >= 0);
+          long long mv = pass == 0 ? pull_excess(p, warp, q0, need, ls)
+                                   : pull_lower(p, warp, q0, need, hy, hmin, nxt, ntail, round_id, ls);
+          need -= mv;
+          got += mv;
+          if (need > 0 && a0 + 32 < end) {
+            mv = pass == 0 ? pull_excess(p, warp, q1, need, ls)
+                           : pull_lower(p, warp, q1, need, hy, hmin, nxt, ntail, round_id, ls);
+            need -= mv;
+            got += mv;
           }
         }
-        if (pass == 1 && cand > 0 && take < cand) hmin = min(hmin, dead_label(p, x));  // still residual
-        const long long moved = cg::reduce(warp, take, cg::plus<long long>());
-        need -= moved;
-        got += moved;
       }
     }
     if (need > 0) {  // relabel and try again next round (nowhere to go: stays for the check)
@@ -981,10 +1043,30 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
       if (lane == 0 && hmin != INT_MAX) {
         set_dead_label(p, y, hmin + 1);
         ls.relabels++;
-        if (atomicExch(p.stamp + y, (int)round_id) != (int)round_id) append(nxt, &out->q, y);
+        if (atomicExch(p.stamp + y, (int)round_id) != (int)round_id) append(nxt, ntail, y);
       }
     }
     if (lane == 0 && got) atomic_add_ll(p.excess + y, got);
+  }
+}
+
+// Pull rounds from round r0 on, in the calling block alone, once the list is
+// short (at most kPullTail deficits): a block barrier between rounds instead of
+// a grid barrier.  Round r uses id round_base + (r - r0) + 1; the caller
+// reserves the ids of every round up to kDeadRounds.  Deficits still open at the
+// end are found by the dead check like any other.
+constexpr int kPullTail = 64;
+
+__device__ __forceinline__ void pull_tail_rounds(const Params &p, int r0, int nn, unsigned round_base, LStats &ls) {
+  __shared__ int s_tail;
+  for (int r = r0; r < kDeadRounds && nn > 0; r++) {
+    if (threadIdx.x == 0) s_tail = 0;
+    __syncthreads();
+    ph_dead_pull(p, p.fq[r & 1], nn, p.fq[(r + 1) & 1], &s_tail, threadIdx.x >> 5, blockDim.x >> 5,
+                 round_base + (unsigned)(r - r0) + 1, ls);
+    __syncthreads();
+    nn = s_tail;
+    __syncthreads();
   }
 }
 
@@ -1940,14 +2022,23 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     if (!next()) return;
     if (lead) c->st_dseeds = (unsigned long long)sc->dseeds;
     if (sc->dseeds > 0) {
+      const int nwarps = (gridDim.x * blockDim.x) >> 5;
       for (int r = 0; r < kDeadRounds; r++) {
         const Slot *in = slot_in();
         if (in->q == 0) break;
-        round_id++;
         kind = TR_DEAD_PULL;
         items = in->q;
         hubitems = 0;
-        ph_dead_pull(p, p.fq[r & 1], in->q, p.fq[(r + 1) & 1], slot_out(), round_id, ls);
+        if (in->q <= kPullTail) {  // the remaining rounds in one block
+          if (blockIdx.x == 0) pull_tail_rounds(p, r, in->q, round_id, ls);
+          round_id += (unsigned)(kDeadRounds - r);
+          if (!next()) return;
+          if (lead) c->rounds_used = round_id - p.round_base;
+          break;
+        }
+        round_id++;
+        ph_dead_pull(p, p.fq[r & 1], in->q, p.fq[(r + 1) & 1], &slot_out()->q, spread_group<32>(), nwarps, round_id,
+                     ls);
         if (!next()) return;
         if (lead) c->rounds_used = round_id - p.round_base;
       }
