@@ -334,20 +334,27 @@ def run_ours(args, rank: int, world: int):
         sched = D.Scheduler.load(args.sched_weights)
     learned_ms, plain_ms, picks, learned_ok = [], [], [], True
     if sched is not None:
-        lflows = {}
-        for name, sc in (("learned", sched), ("plain", None)):
-            L = D.Solver(g, s, t, **kw)
-            L.static_maxflow()
-            for i, b in enumerate(batches):
+        # a trunk solver carries the batch sequence; before each timed batch its
+        # state is copied into both schedule solvers, so the two are timed on
+        # the same pre-batch state
+        T = D.Solver(g, s, t, **kw)
+        T.static_maxflow()
+        Ll, Lp = D.Solver(g, s, t, **kw), D.Solver(g, s, t, **kw)
+        for i, b in enumerate(batches):
+            if i >= args.warmup:
+                Ll.copy_state_from(T)
+                Lp.copy_state_from(T)
                 flushed()
-                fl, act = L.apply_updates_scheduled(sc, *b)
-                if i >= args.warmup:
-                    lflows.setdefault(name, []).append(fl)
-                    (learned_ms if name == "learned" else plain_ms).append(L.stats()["last_ms"])
-                    if name == "learned":
-                        picks.append(act)
-            L.close()
-        learned_ok = lflows["learned"] == lflows["plain"] == flows[args.warmup:]
+                fl, act = Ll.apply_updates_scheduled(sched, *b)
+                learned_ms.append(Ll.stats()["last_ms"])
+                flushed()
+                fp, _ = Lp.apply_updates_scheduled(None, *b)
+                plain_ms.append(Lp.stats()["last_ms"])
+                picks.append(act)
+                learned_ok &= fl == fp == flows[i]
+            T.apply_updates_device(*arg_ptrs(dbat[i]))
+        for x in (T, Ll, Lp):
+            x.close()
         sched.close()
     # phase timeline of a traced solver over the first timed batches
     P = D.Solver(g, s, t, trace=True, **kw)
@@ -441,7 +448,7 @@ def run_ours(args, rank: int, world: int):
             "plain_p99_ms": round(pct(plain_ms, 0.99), 4), "ratio_plain_over_learned": round(pp / lp, 4),
             "picks": dict(zip(D.ACTIONS, np.bincount(picks, minlength=D.N_ACTIONS).tolist())),
             "equal_flows": bool(learned_ok),
-            "timing": "dmf_apply_updates_scheduled, one solver per schedule over the same batch sequence (features, decision and "
+            "timing": "dmf_apply_updates_scheduled from copies of the same pre-batch state (features, decision and "
                       "solve; H2D of the batch not included)"}
     refc = recorded_reference_cuda(g, s, t, args.scale)
     if refc is not None:

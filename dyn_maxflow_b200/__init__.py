@@ -423,7 +423,7 @@ class Solver:
                    6: "cut_saturate", 7: "bfs_init", 8: "bfs_td", 9: "bfs_bu", 10: "bfs_finalize", 11: "push",
                    12: "flow", 13: "push_hub", 14: "push_hub_finish", 15: "pp_init", 16: "pp_bfs",
                    17: "pp_finalize", 18: "pp_round", 19: "reopen", 20: "dead_seed", 21: "dead_pull",
-                   23: "dead_check", 24: "dead_revive"}
+                   23: "dead_check", 24: "dead_revive", 25: "claim"}
 
     def trace(self):
         """[(phase kind, end time in us since kernel start)] of the last solve (trace=True)."""

@@ -49,7 +49,7 @@ enum TraceKind : int {
   TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
   TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14, TR_PP_INIT = 15, TR_PP_BFS = 16, TR_PP_FINALIZE = 17,
   TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_PULL = 21, TR_DEAD_CHECK = 23,
-  TR_DEAD_REVIVE = 24
+  TR_DEAD_REVIVE = 24, TR_CLAIM = 25
 };
 
 // Local repair inside a kept dead set: at most this many pull rounds.
@@ -67,6 +67,7 @@ struct Params {
   ArcSlot *atab;    // (tail, head) -> arc table with the per-arc batch stamps
   long long nslots;  // its slots
   int *cap, *res, *height, *stamp, *uarc;
+  int *uold;  // per update: the capacity its claim replaced (sign bit: an earlier update claimed the arc)
   long long *excess;
   unsigned char *dead, *side;
   int *fq[2], *wq[2], *aq;     // non-hub vertex queues
@@ -239,12 +240,12 @@ __device__ __forceinline__ void ph_saturate(const Params &p) {
 // Arc lookup of OnAdd_kernel (code/dyn_data.h:196-201), which scans the tail's
 // adjacency for the head; here one probe of an open-addressing table keyed by
 // (tail, head) (dmfd::ArcSlot, built once per solver by k_arc_table_build).
-// A slot holds the key, the arc and the batch stamp that detects an arc named
-// twice in one batch, in one 16-byte line: a found update costs one DRAM
-// sector (two when the probe crosses a sector) instead of a search of the
-// tail's adjacency.  Equal (tail, head) pairs in a CSR with duplicate arcs
-// resolve to the last arc among them, as OnAdd_kernel's scan keeps the last
-// match.  The lookup also validates the batch.
+// A slot holds the key and the arc in one 16-byte line: a found update costs
+// one DRAM sector (two when the probe crosses a sector) instead of a search of
+// the tail's adjacency, and the line is only read.  Equal (tail, head) pairs
+// in a CSR with duplicate arcs resolve to the last arc among them, as
+// OnAdd_kernel's scan keeps the last match.  The lookup validates vertex ids,
+// capacities and arcs; an arc named twice is found by the claim (ph_claim).
 
 // Updates a thread looks up side by side: their probes are in flight together.
 constexpr int kLookupBatch = 4;
@@ -311,10 +312,6 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
         set_err(p.ctrl, ERR_UNKNOWN_ARC, i);
         continue;
       }
-      if (atomicExch(&p.atab[slot[j]].stamp, p.epoch) == p.epoch) {
-        set_err(p.ctrl, ERR_DUP_ARC, i);
-        continue;
-      }
       if (!p.caps_bounded && (long long)w[j] + __ldcg(p.cap + __ldg(p.par + e[j])) > INT_MAX) {
         set_err(p.ctrl, ERR_BAD_UPDATE, i);
         continue;
@@ -324,17 +321,45 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
   }
 }
 
-// Capacity apply of OnAdd_kernel (code/dyn_data.h:202-205); in recompute mode
-// only the capacity is set (update_kernel, code/dyn_data_bench.cu:300-322).
-__device__ __forceinline__ void ph_apply(const Params &p, bool residual) {
+// Claim: every update swaps its new capacity, with the sign bit set, into its
+// arc's capacity and keeps the old value in uold.  Capacities are never
+// negative, so an update that gets a value with the sign bit back names an arc
+// an earlier update of the batch named: the batch is rejected (Ctrl::dup_at,
+// read after the barrier) and ph_unclaim puts every capacity back.  The apply
+// clears the bit.  This detects duplicates on the capacity's line, which the
+// apply reads and writes anyway, instead of a per-arc stamp.
+constexpr int kClaimBit = INT_MIN;
+
+__device__ __forceinline__ void ph_claim(const Params &p) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
   for (int i = gt; i < p.k; i += nt) {
-    int e = __ldcg(p.uarc + i);
+    const int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
-    int w = __ldg(p.uw + i);
-    int delta = w - __ldcg(p.cap + e);
-    p.cap[e] = w;
-    if (residual && delta) atomicAdd(p.res + e, delta);
+    const int old = atomicExch(p.cap + e, __ldg(p.uw + i) | kClaimBit);
+    p.uold[i] = old;
+    if (old < 0) atomicCAS(&p.ctrl->dup_at, 0, i + 1);
+  }
+}
+
+// A rejected batch: the first claimer of each arc (the one that got a value
+// without the sign bit) restores it.
+__device__ __forceinline__ void ph_unclaim(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
+  for (int i = gt; i < p.k; i += nt) {
+    const int e = __ldcg(p.uarc + i);
+    if (e < 0) continue;
+    const int old = __ldcg(p.uold + i);
+    if (old >= 0) p.cap[e] = old;
+  }
+}
+
+// Capacity apply of update_kernel in recompute mode (the capacity only,
+// code/dyn_data_bench.cu:300-322).
+__device__ __forceinline__ void ph_apply(const Params &p) {
+  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
+  for (int i = gt; i < p.k; i += nt) {
+    const int e = __ldcg(p.uarc + i);
+    if (e >= 0) p.cap[e] = __ldg(p.uw + i);
   }
 }
 
@@ -351,20 +376,31 @@ __device__ __forceinline__ void ph_apply_repair(const Params &p) {
     const int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
     const int w = __ldg(p.uw + i);
-    const int delta = w - __ldcg(p.cap + e);
-    p.cap[e] = w;
-    if (!delta) continue;
-    const int r = atomicAdd(p.res + e, delta) + delta;
-    if (r >= 0) continue;
-    atomicAdd(p.res + e, -r);
-    atomicAdd(p.res + __ldg(p.par + e), r);
     const int u = __ldg(p.usrc + i), v = __ldg(p.udst + i);  // the lookup matched adj[e] == udst[i]
-    atomic_add_ll(p.excess + u, -(long long)r);
-    atomic_add_ll(p.excess + v, (long long)r);
-    if (p.keep_dead) {  // the overflow returns to the tail: excess that can cover the head's deficit
-      if (__ldcg(p.dead + v)) add_dead_cand(p, v);
-      if (__ldcg(p.dead + u)) add_dead_cand(p, u);
+    bool du = false, dv = false;
+    if (p.keep_dead) {
+      du = __ldcg(p.dead + u) != 0;
+      dv = __ldcg(p.dead + v) != 0;
     }
+    const int delta = w - __ldcg(p.uold + i);
+    p.cap[e] = w;  // clears the claim bit
+    int r = 0;  // residual of e after the apply, when it changed
+    if (delta) {
+      r = atomicAdd(p.res + e, delta) + delta;
+      if (r < 0) {
+        atomicAdd(p.res + e, -r);
+        atomicAdd(p.res + __ldg(p.par + e), r);
+        atomic_add_ll(p.excess + u, -(long long)r);
+        atomic_add_ll(p.excess + v, (long long)r);
+        if (p.keep_dead) {  // the overflow returns to the tail: excess that can cover the head's deficit
+          if (dv) add_dead_cand(p, v);
+          if (du) add_dead_cand(p, u);
+        }
+      }
+    }
+    // an arc from the kept dead set to a live head may need reopening once
+    // every apply is done (a partner's repair can still lower its residual)
+    if (du && !dv && r > 0 && !is_src(p, v)) append_bounded(p.aq, &p.ctrl->nreopen, i, p.n + 1);
   }
 }
 
@@ -374,20 +410,29 @@ __device__ __forceinline__ void ph_apply_repair(const Params &p) {
 // now is saturated at once: the flow goes to v (handled by the live solve) and
 // u is charged with it (a deficit inside D, covered by the local repair).  D
 // stays closed, so only the deficits inside it decide whether it stays dead.
-__device__ __forceinline__ void ph_reopen(const Params &p) {
+__device__ __forceinline__ void reopen_update(const Params &p, int i) {
+  const int e = __ldcg(p.uarc + i);
+  if (e < 0) return;
+  const int u = __ldg(p.usrc + i), v = __ldg(p.udst + i);  // adj[e] == udst[i]
+  if (!__ldcg(p.dead + u) || __ldcg(p.dead + v) || is_src(p, v)) return;
+  const int r = __ldcg(p.res + e);
+  if (r <= 0) return;
+  p.res[e] = 0;
+  atomicAdd(p.res + __ldg(p.par + e), r);
+  atomic_add_ll(p.excess + u, -(long long)r);
+  atomic_add_ll(p.excess + v, (long long)r);
+  add_dead_cand(p, u);
+}
+
+// The apply queued the updates that can need it (dead tail, live head,
+// residual left); past the queue's capacity every update is looked at.
+__device__ __forceinline__ void ph_reopen(const Params &p, const Ctrl *sc) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
-  for (int i = gt; i < p.k; i += nt) {
-    const int e = __ldcg(p.uarc + i);
-    if (e < 0) continue;
-    const int u = __ldg(p.usrc + i), v = __ldg(p.udst + i);  // adj[e] == udst[i]
-    if (!__ldcg(p.dead + u) || __ldcg(p.dead + v) || is_src(p, v)) continue;
-    const int r = __ldcg(p.res + e);
-    if (r <= 0) continue;
-    p.res[e] = 0;
-    atomicAdd(p.res + __ldg(p.par + e), r);
-    atomic_add_ll(p.excess + u, -(long long)r);
-    atomic_add_ll(p.excess + v, (long long)r);
-    add_dead_cand(p, u);
+  const int nq = sc->nreopen;
+  if (nq <= p.n + 1) {
+    for (int j = gt; j < nq; j += nt) reopen_update(p, __ldcg(p.aq + j));
+  } else {
+    for (int i = gt; i < p.k; i += nt) reopen_update(p, i);
   }
 }
 
@@ -1052,14 +1097,19 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
 
 // Pull rounds from round r0 on, in the calling block alone, once the list is
 // short (at most kPullTail deficits): a block barrier between rounds instead of
-// a grid barrier.  Round r uses id round_base + (r - r0) + 1; the caller
+// a grid barrier, at most kPullTailRounds of them.  Round r uses id round_base + (r - r0) + 1; the caller
 // reserves the ids of every round up to kDeadRounds.  Deficits still open at the
 // end are found by the dead check like any other.
 constexpr int kPullTail = 64;
+// Block rounds at most: a deficit still bouncing after them has no excess
+// within reach inside the dead set (it relabels by one per round); the check
+// revives it.
+constexpr int kPullTailRounds = 6;
 
 __device__ __forceinline__ void pull_tail_rounds(const Params &p, int r0, int nn, unsigned round_base, LStats &ls) {
   __shared__ int s_tail;
-  for (int r = r0; r < kDeadRounds && nn > 0; r++) {
+  const int r_end = min(kDeadRounds, r0 + kPullTailRounds);
+  for (int r = r0; r < r_end && nn > 0; r++) {
     if (threadIdx.x == 0) s_tail = 0;
     __syncthreads();
     ph_dead_pull(p, p.fq[r & 1], nn, p.fq[(r + 1) & 1], &s_tail, threadIdx.x >> 5, blockDim.x >> 5,
@@ -1976,10 +2026,20 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     kind = TR_SATURATE;
     ph_saturate(p);
     if (!next()) return;
-  } else if (p.mode == MODE_DYNAMIC) {
+  } else if (p.mode == MODE_DYNAMIC || p.mode == MODE_RECOMPUTE) {
     kind = TR_LOOKUP;
     ph_lookup(p);
     if (!next()) return;
+    kind = TR_CLAIM;
+    ph_claim(p);
+    if (!next()) return;
+    if (sc->dup_at) {  // every claim is done: put the capacities back, reject the batch
+      ph_unclaim(p);
+      if (lead) set_err(c, ERR_DUP_ARC, sc->dup_at - 1);
+      return;
+    }
+  }
+  if (p.mode == MODE_DYNAMIC) {
     kind = TR_APPLY;
     ph_apply_repair(p);
     if (!next()) return;
@@ -1992,14 +2052,11 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     // tail is dead, so neither it nor its partner is a source arc): one phase
     kind = TR_SATURATE;
     ph_saturate(p);
-    if (p.keep_dead) ph_reopen(p);
+    if (p.keep_dead) ph_reopen(p, sc);
     if (!next()) return;
   } else if (p.mode == MODE_RECOMPUTE) {
-    kind = TR_LOOKUP;
-    ph_lookup(p);
-    if (!next()) return;
     kind = TR_APPLY;
-    ph_apply(p, false);
+    ph_apply(p);
     if (!next()) return;
     kind = TR_INIT_RES;
     ph_init_res(p);

@@ -269,8 +269,8 @@ int ensure_ubuf(dmf_solver *sv, int k) {
   if (k <= sv->kcap) return DMF_OK;
   int want = std::max(k, 1024);
   int *nb = nullptr;
-  CK(cudaMalloc(&nb, sizeof(int) * 4 * (size_t)want), "cudaMalloc updates");
-  // uarc lives in the 4th quarter
+  CK(cudaMalloc(&nb, sizeof(int) * 5 * (size_t)want), "cudaMalloc updates");
+  // src, dst, w (staged host batches), then the per-update arc and claimed capacity
   if (sv->ubuf) {
     cudaStreamSynchronize(sv->stream);
     cudaFree(sv->ubuf);
@@ -310,6 +310,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.height = sv->height;
   p.stamp = sv->stamp;
   p.uarc = sv->ubuf ? sv->ubuf + 3 * (size_t)sv->kcap : nullptr;
+  p.uold = sv->ubuf ? sv->ubuf + 4 * (size_t)sv->kcap : nullptr;
   p.excess = sv->excess;
   p.dead = sv->dead;
   p.side = sv->side;
@@ -707,6 +708,7 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
     p.cap = const_cast<int *>(d_cap);  // read only in static mode
     p.res = d_res;
     p.uarc = nullptr;
+    p.uold = nullptr;
     p.ctrl = ctrl;
     p.mode = MODE_STATIC;
     p.variant = DMF_VARIANT_DATA;

@@ -232,7 +232,10 @@ int dmf_stats_get(const dmf_solver *sv, dmf_stats *st);
  * t_us[i] microseconds after the start.  Kinds: 1 init residuals, 2 source
  * saturation, 3 arc lookup, 4 capacity apply, 5 over-capacity repair, 6 cut
  * saturation, 7 BFS seeds, 8 BFS top-down level, 9 BFS bottom-up level,
- * 10 BFS finalize, 11 push round.  No counterpart in the reference (which
+ * 10 BFS finalize, 11 push round, 12 flow readout, 13/14 hub push rounds,
+ * 15-18 push-pull phase 1, 19 reopen, 20 dead-set pull seeding, 21 pull round,
+ * 23 dead-set check, 24 partial revival, 25 capacity claim (duplicate-arc
+ * check).  No counterpart in the reference (which
  * times whole calls with cudaEvents, code/dyn_data_bench.cu:246-258). */
 int dmf_trace_get(dmf_solver *sv, int32_t cap, int32_t *kinds, double *t_us,
                   int32_t *count);
@@ -280,7 +283,7 @@ int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs,
 /* ---- serving loop ------------------------------------------------------------ */
 /* Device-resident graphs serving update-batch requests.  Graphs are admitted in
  * the given order while the estimated device footprint of their residual state
- * (42 B per arc + 64 B per vertex) fits `hbm_budget` bytes; the rest are not
+ * (48 B per arc + 64 B per vertex) fits `hbm_budget` bytes; the rest are not
  * admitted (ids of admitted graphs are their positions among the admitted ones,
  * dmf_server_info).  The caller keeps the graphs alive until destroy.
  * Lanes: a graph with at least a quarter of the admitted arcs gets a lane of

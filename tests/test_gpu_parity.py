@@ -202,8 +202,13 @@ def test_edge_cases(dmf, oracle, golden_dir):
         assert sv.apply_updates([3, 3], [3, 3], [5, 9]) == 540  # self-loops ignored
         missing = next((a, b) for a in range(n) for b in range(n) if a != b and g.find_arc(a, b) < 0)
         e0 = int(np.flatnonzero(w > 0)[0])
+        e1 = int(np.flatnonzero(w > 0)[1])
+        cap0, res0, _, _ = sv.state()
         for bad, status in [(([missing[0]], [missing[1]], [5]), 3),
                             (([tail[e0], tail[e0]], [adj[e0], adj[e0]], [1, 2]), 4),
+                            # a valid update beside a repeated arc: the batch is rejected whole
+                            (([tail[e1], tail[e0], tail[e0], tail[e0]], [adj[e1], adj[e0], adj[e0], adj[e0]],
+                              [7, 1, 2, 3]), 4),
                             (([n + 5], [0], [1]), 1),
                             (([tail[e0]], [adj[e0]], [-1]), 1),
                             (([tail[e0]], [adj[e0]], [2**30]), 1)]:
@@ -211,6 +216,9 @@ def test_edge_cases(dmf, oracle, golden_dir):
                 sv.apply_updates(*bad)
             assert ei.value.status == status
             assert sv.flow == 540  # rejected batches change nothing
+            cap1, res1, _, _ = sv.state()
+            np.testing.assert_array_equal(cap1, cap0)
+            np.testing.assert_array_equal(res1, res0)
         assert sv.apply_updates([], [], []) == 540
         # delete every arc out of the source: flow 0
         src_arcs = np.arange(off[25], off[26])
