@@ -75,6 +75,8 @@ struct Ctrl {
   unsigned long long st_revived; // dead vertices revived because they reach a deficit left over
   int dup_at;                   // 1 + an update whose arc an earlier update of the batch names (0: none)
   int nreopen;                  // updates queued for reopening (kept dead set)
+  int nrepair;                  // updates queued for the over-capacity repair
+  int pad3;
 };
 
 // ---- memory helpers ---------------------------------------------------------

@@ -49,7 +49,7 @@ enum TraceKind : int {
   TR_CUT_SATURATE = 6, TR_BFS_INIT = 7, TR_BFS_TD = 8, TR_BFS_BU = 9, TR_BFS_FINALIZE = 10, TR_PUSH = 11,
   TR_FLOW = 12, TR_PUSH_HUB = 13, TR_PUSH_HUB_FINISH = 14, TR_PP_INIT = 15, TR_PP_BFS = 16, TR_PP_FINALIZE = 17,
   TR_PP_ROUND = 18, TR_REOPEN = 19, TR_DEAD_SEED = 20, TR_DEAD_PULL = 21, TR_DEAD_CHECK = 23,
-  TR_DEAD_REVIVE = 24, TR_CLAIM = 25
+  TR_DEAD_REVIVE = 24
 };
 
 // Local repair inside a kept dead set: at most this many pull rounds.
@@ -66,8 +66,10 @@ struct Params {
   const int *__restrict__ par;
   ArcSlot *atab;    // (tail, head) -> arc table with the per-arc batch stamps
   long long nslots;  // its slots
-  int *cap, *res, *height, *stamp, *uarc;
-  int *uold;  // per update: the capacity its claim replaced (sign bit: an earlier update claimed the arc)
+  int *cap;                  // capacities as a plain array (allocation-free static solve only)
+  unsigned long long *capx;  // capacities of a solver: (epoch of the batch that set it << 32) | capacity
+  int *res, *height, *stamp, *uarc;
+  int *uold;  // per update: the capacity it replaced (-1: an earlier update of the batch named the arc)
   long long *excess;
   unsigned char *dead, *side;
   int *fq[2], *wq[2], *aq;     // non-hub vertex queues
@@ -176,12 +178,29 @@ __device__ __forceinline__ void add_dead_cand(const Params &p, int v) {
   append_bounded(p.dq, &p.ctrl->dcand, v, p.n + 1);
 }
 
+// Capacities of a solver live in 8-byte words, capacity in the low half and
+// in the high half the launch epoch of the batch that last set it (0 from the
+// upload).  A batch swaps (epoch, w) in for every update; an update that gets
+// back a word with this launch's epoch names an arc an earlier update of the
+// batch named, so the batch is rejected (Ctrl::dup_at, read after the barrier)
+// and ph_unclaim puts back what was changed.  The duplicate check thus rides on
+// the capacity line the apply reads and writes anyway: no per-arc stamp, and
+// no second write to clear a mark.  The caller-supplied capacities of the
+// allocation-free static solve stay a plain int32 array (capx == nullptr).
+__device__ __forceinline__ int cap_of(const Params &p, int e) {
+  return p.capx ? (int)(unsigned)__ldcg(p.capx + e) : __ldcg(p.cap + e);
+}
+
+__device__ __forceinline__ unsigned long long cap_word(const Params &p, int w) {
+  return ((unsigned long long)(unsigned)p.epoch << 32) | (unsigned)w;
+}
+
 // ---- prologue phases ----------------------------------------------------------
 
 // staticMaxFlow_kernel_1 (code/dyn_data.h:25-35): residual = capacity, excess 0.
 __device__ __forceinline__ void ph_init_res(const Params &p) {
   const int nt = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
-  for (int e = gt; e < p.m; e += nt) p.res[e] = __ldcg(p.cap + e);
+  for (int e = gt; e < p.m; e += nt) p.res[e] = cap_of(p, e);
   for (int v = gt; v < p.n; v += nt) p.excess[v] = 0;
 }
 
@@ -312,7 +331,7 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
         set_err(p.ctrl, ERR_UNKNOWN_ARC, i);
         continue;
       }
-      if (!p.caps_bounded && (long long)w[j] + __ldcg(p.cap + __ldg(p.par + e[j])) > INT_MAX) {
+      if (!p.caps_bounded && (long long)w[j] + cap_of(p, __ldg(p.par + e[j])) > INT_MAX) {
         set_err(p.ctrl, ERR_BAD_UPDATE, i);
         continue;
       }
@@ -321,86 +340,89 @@ __device__ __forceinline__ void ph_lookup(const Params &p) {
   }
 }
 
-// Claim: every update swaps its new capacity, with the sign bit set, into its
-// arc's capacity and keeps the old value in uold.  Capacities are never
-// negative, so an update that gets a value with the sign bit back names an arc
-// an earlier update of the batch named: the batch is rejected (Ctrl::dup_at,
-// read after the barrier) and ph_unclaim puts every capacity back.  The apply
-// clears the bit.  This detects duplicates on the capacity's line, which the
-// apply reads and writes anyway, instead of a per-arc stamp.
-constexpr int kClaimBit = INT_MIN;
-
-__device__ __forceinline__ void ph_claim(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
-  for (int i = gt; i < p.k; i += nt) {
-    const int e = __ldcg(p.uarc + i);
-    if (e < 0) continue;
-    const int old = atomicExch(p.cap + e, __ldg(p.uw + i) | kClaimBit);
-    p.uold[i] = old;
-    if (old < 0) atomicCAS(&p.ctrl->dup_at, 0, i + 1);
-  }
-}
-
-// A rejected batch: the first claimer of each arc (the one that got a value
-// without the sign bit) restores it.
-__device__ __forceinline__ void ph_unclaim(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
-  for (int i = gt; i < p.k; i += nt) {
-    const int e = __ldcg(p.uarc + i);
-    if (e < 0) continue;
-    const int old = __ldcg(p.uold + i);
-    if (old >= 0) p.cap[e] = old;
-  }
-}
-
-// Capacity apply of update_kernel in recompute mode (the capacity only,
+// Claim and capacity apply of OnAdd_kernel (code/dyn_data.h:202-205) in one
+// pass: the new capacity goes in, the residual moves by the difference.  An
+// arc whose residual went negative carries more flow than its new capacity;
+// it is queued for the repair (ph_repair) rather than repaired here, so that a
+// rejected batch only has to undo additions.  With the dead set kept, an arc
+// from a dead tail to a live head that has residual now is queued for
+// reopening.  In recompute mode only the capacity changes (update_kernel,
 // code/dyn_data_bench.cu:300-322).
-__device__ __forceinline__ void ph_apply(const Params &p) {
+__device__ __forceinline__ void ph_claim_apply(const Params &p, bool residual) {
   const int nt = gridDim.x * blockDim.x, gt = spread_thread();
-  for (int i = gt; i < p.k; i += nt) {
-    const int e = __ldcg(p.uarc + i);
-    if (e >= 0) p.cap[e] = __ldg(p.uw + i);
-  }
-}
-
-// Capacity apply and over-capacity repair in one pass (dynamic batches).  The
-// repair replaces the O(m) sweeps incremental_kernel_20 / _22
-// (code/dyn_data.h:157-183): an arc whose residual went negative carries more
-// flow than its new capacity; the overflow returns to its tail and is taken
-// from its head.  An arc's residual changes only by its own apply here, and at
-// most one arc of a pair goes negative (res(e) + res(partner) = cap(e) +
-// cap(partner) >= 0), so the repair can follow each apply at once.
-__device__ __forceinline__ void ph_apply_repair(const Params &p) {
-  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
+  const unsigned ep = (unsigned)p.epoch;
   for (int i = gt; i < p.k; i += nt) {
     const int e = __ldcg(p.uarc + i);
     if (e < 0) continue;
     const int w = __ldg(p.uw + i);
-    const int u = __ldg(p.usrc + i), v = __ldg(p.udst + i);  // the lookup matched adj[e] == udst[i]
     bool du = false, dv = false;
-    if (p.keep_dead) {
+    int u = 0, v = 0;
+    if (residual && p.keep_dead) {
+      u = __ldg(p.usrc + i);
+      v = __ldg(p.udst + i);  // the lookup matched adj[e] == udst[i]
       du = __ldcg(p.dead + u) != 0;
       dv = __ldcg(p.dead + v) != 0;
     }
-    const int delta = w - __ldcg(p.uold + i);
-    p.cap[e] = w;  // clears the claim bit
-    int r = 0;  // residual of e after the apply, when it changed
-    if (delta) {
-      r = atomicAdd(p.res + e, delta) + delta;
-      if (r < 0) {
-        atomicAdd(p.res + e, -r);
-        atomicAdd(p.res + __ldg(p.par + e), r);
-        atomic_add_ll(p.excess + u, -(long long)r);
-        atomic_add_ll(p.excess + v, (long long)r);
-        if (p.keep_dead) {  // the overflow returns to the tail: excess that can cover the head's deficit
-          if (dv) add_dead_cand(p, v);
-          if (du) add_dead_cand(p, u);
-        }
-      }
+    const unsigned long long old = atomicExch(p.capx + e, cap_word(p, w));
+    if ((unsigned)(old >> 32) == ep) {  // named twice: this update changes nothing
+      p.uold[i] = -1;
+      atomicCAS(&p.ctrl->dup_at, 0, i + 1);
+      continue;
     }
-    // an arc from the kept dead set to a live head may need reopening once
-    // every apply is done (a partner's repair can still lower its residual)
-    if (du && !dv && r > 0 && !is_src(p, v)) append_bounded(p.aq, &p.ctrl->nreopen, i, p.n + 1);
+    const int oc = (int)(unsigned)old;
+    p.uold[i] = oc;
+    const int delta = w - oc;
+    if (!residual || !delta) continue;
+    const int r = atomicAdd(p.res + e, delta) + delta;
+    if (r < 0) append_bounded(p.wq[0], &p.ctrl->nrepair, i, p.n + 1);
+    else if (r > 0 && du && !dv && !is_src(p, v)) append_bounded(p.aq, &p.ctrl->nreopen, i, p.n + 1);
+  }
+}
+
+// A rejected batch: every update that changed its arc (the first to name it)
+// puts the capacity and the residual back.
+__device__ __forceinline__ void ph_unclaim(const Params &p, bool residual) {
+  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
+  for (int i = gt; i < p.k; i += nt) {
+    const int e = __ldcg(p.uarc + i);
+    if (e < 0) continue;
+    const int oc = __ldcg(p.uold + i);
+    if (oc < 0) continue;
+    p.capx[e] = (unsigned long long)(unsigned)oc;
+    const int delta = __ldg(p.uw + i) - oc;
+    if (residual && delta) atomicSub(p.res + e, delta);
+  }
+}
+
+// Over-capacity repair of the queued arcs; replaces the O(m) sweeps
+// incremental_kernel_20 / _22 (code/dyn_data.h:157-183): the overflow returns
+// to the tail and is taken from the head.  Only an arc's own apply changed its
+// residual, and at most one arc of a pair is negative (res(e) + res(partner) =
+// cap(e) + cap(partner) >= 0), so the residual read here is the apply's.  Past
+// the queue's capacity every update is looked at.
+__device__ __forceinline__ void repair_update(const Params &p, int i) {
+  const int e = __ldcg(p.uarc + i);
+  if (e < 0) return;
+  const int r = __ldcg(p.res + e);
+  if (r >= 0) return;
+  atomicAdd(p.res + e, -r);
+  atomicAdd(p.res + __ldg(p.par + e), r);
+  const int u = __ldg(p.usrc + i), v = __ldg(p.udst + i);
+  atomic_add_ll(p.excess + u, -(long long)r);
+  atomic_add_ll(p.excess + v, (long long)r);
+  if (p.keep_dead) {  // the overflow returns to the tail: excess that can cover the head's deficit
+    if (__ldcg(p.dead + v)) add_dead_cand(p, v);
+    if (__ldcg(p.dead + u)) add_dead_cand(p, u);
+  }
+}
+
+__device__ __forceinline__ void ph_repair(const Params &p, const Ctrl *sc) {
+  const int nt = gridDim.x * blockDim.x, gt = spread_thread();
+  const int nq = sc->nrepair;
+  if (nq <= p.n + 1) {
+    for (int j = gt; j < nq; j += nt) repair_update(p, __ldcg(p.wq[0] + j));
+  } else {
+    for (int i = gt; i < p.k; i += nt) repair_update(p, i);
   }
 }
 
@@ -2027,43 +2049,41 @@ __device__ __forceinline__ void run(const Params &p, LStats &ls, typename BlockG
     ph_saturate(p);
     if (!next()) return;
   } else if (p.mode == MODE_DYNAMIC || p.mode == MODE_RECOMPUTE) {
+    const bool dyn = p.mode == MODE_DYNAMIC;
     kind = TR_LOOKUP;
     ph_lookup(p);
     if (!next()) return;
-    kind = TR_CLAIM;
-    ph_claim(p);
+    kind = TR_APPLY;
+    ph_claim_apply(p, dyn);
     if (!next()) return;
-    if (sc->dup_at) {  // every claim is done: put the capacities back, reject the batch
-      ph_unclaim(p);
+    if (sc->dup_at) {  // every claim is done: undo them, reject the batch
+      ph_unclaim(p, dyn);
       if (lead) set_err(c, ERR_DUP_ARC, sc->dup_at - 1);
       return;
     }
-  }
-  if (p.mode == MODE_DYNAMIC) {
-    kind = TR_APPLY;
-    ph_apply_repair(p);
-    if (!next()) return;
-    if (p.variant == DMF_VARIANT_PP && !p.keep_dead) {  // with the dead set kept, ph_reopen does it
-      kind = TR_CUT_SATURATE;
-      ph_cut_saturate(p);
+    if (dyn) {
+      kind = TR_REPAIR;
+      ph_repair(p, sc);
+      if (!next()) return;
+      if (p.variant == DMF_VARIANT_PP && !p.keep_dead) {  // with the dead set kept, ph_reopen does it
+        kind = TR_CUT_SATURATE;
+        ph_cut_saturate(p);
+        if (!next()) return;
+      }
+      // source saturation and reopening touch disjoint arcs (a reopened arc's
+      // tail is dead, so neither it nor its partner is a source arc): one phase
+      kind = TR_SATURATE;
+      ph_saturate(p);
+      if (p.keep_dead) ph_reopen(p, sc);
+      if (!next()) return;
+    } else {
+      kind = TR_INIT_RES;
+      ph_init_res(p);
+      if (!next()) return;
+      kind = TR_SATURATE;
+      ph_saturate(p);
       if (!next()) return;
     }
-    // source saturation and reopening touch disjoint arcs (a reopened arc's
-    // tail is dead, so neither it nor its partner is a source arc): one phase
-    kind = TR_SATURATE;
-    ph_saturate(p);
-    if (p.keep_dead) ph_reopen(p, sc);
-    if (!next()) return;
-  } else if (p.mode == MODE_RECOMPUTE) {
-    kind = TR_APPLY;
-    ph_apply(p);
-    if (!next()) return;
-    kind = TR_INIT_RES;
-    ph_init_res(p);
-    if (!next()) return;
-    kind = TR_SATURATE;
-    ph_saturate(p);
-    if (!next()) return;
   }
 
   unsigned round_id = p.round_base;

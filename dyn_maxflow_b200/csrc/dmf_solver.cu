@@ -21,7 +21,8 @@ namespace {
 // the schedule picker (nothing is modified).  Updates the solver would reject
 // (bad ids, unknown arcs) are skipped here; the solve reports them.
 __global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, const ArcSlot *atab,
-                                                  long long nslots, const int *cap, const int *res, int n,
+                                                  long long nslots, const unsigned long long *capx, const int *res,
+                                                  int n,
                                                   int k, const int *usrc, const int *udst, const int *uw,
                                                   dmfs::FeatAcc *acc) {
   unsigned long long valid = 0, dec = 0, satdec = 0, incsat = 0, ins = 0, del = 0, sdeg = 0, mdeg = 0;
@@ -32,7 +33,7 @@ __global__ void __launch_bounds__(256) k_features(const int *__restrict__ off, c
     const int e = find_arc_table(atab, nslots, u, v);
     if (e < 0) continue;
     valid++;
-    const int c0 = __ldcg(cap + e), r = __ldcg(res + e);
+    const int c0 = (int)(unsigned)__ldcg(capx + e), r = __ldcg(res + e);
     const long long flow = (long long)c0 - r;  // negative: the partner carries flow
     const unsigned long long d = (unsigned long long)(__ldg(off + u + 1) - __ldg(off + u));
     sdeg += d;
@@ -119,13 +120,26 @@ __global__ void __launch_bounds__(256) k_arc_table_build(const int *__restrict__
   }
 }
 
+// Capacity words from the uploaded int32 capacities (epoch 0: set by no batch).
+__global__ void __launch_bounds__(256) k_cap_widen(const int *__restrict__ w, unsigned long long *capx, long long m) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (long long)gridDim.x * blockDim.x)
+    capx[e] = (unsigned long long)(unsigned)__ldg(w + e);
+}
+
+// The capacities of a range of capacity words.
+__global__ void __launch_bounds__(256) k_cap_low(const unsigned long long *__restrict__ capx, int *out, long long m) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (long long)gridDim.x * blockDim.x)
+    out[e] = (int)(unsigned)__ldg(capx + e);
+}
+
 struct dmf_solver {
   int dev = 0;
   cudaStream_t stream = nullptr;
   int n = 0, m = 0, s = 0, t = 0;
   dmf_opts opts{};
   int tile = 32, grid = 0, block = kBlock, hub_deg = 256, small_deg = 8, minb = 2, bu_alpha = 2;
-  int *off = nullptr, *adj = nullptr, *par = nullptr, *cap = nullptr, *res = nullptr;
+  int *off = nullptr, *adj = nullptr, *par = nullptr, *res = nullptr;
+  unsigned long long *capx = nullptr;  // (epoch of the batch that set it << 32) | capacity
   ArcSlot *atab = nullptr;  // (tail, head) -> arc, with the per-arc batch stamps
   long long nslots = 0;
   int *height = nullptr, *stamp = nullptr, *uarc = nullptr;
@@ -305,7 +319,8 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.par = sv->par;
   p.atab = sv->atab;
   p.nslots = sv->nslots;
-  p.cap = sv->cap;
+  p.cap = nullptr;
+  p.capx = sv->capx;
   p.res = sv->res;
   p.height = sv->height;
   p.stamp = sv->stamp;
@@ -524,7 +539,7 @@ int batch_features(dmf_solver *sv, dmf_sched *sched, int k, float *feat, int *ac
   if (k > 0) {
     const size_t K = (size_t)sv->kcap;
     const int blocks = std::min((k + 255) / 256, 4 * 148);
-    k_features<<<blocks, 256, 0, sv->stream>>>(sv->off, sv->atab, sv->nslots, sv->cap, sv->res, sv->n, k,
+    k_features<<<blocks, 256, 0, sv->stream>>>(sv->off, sv->atab, sv->nslots, sv->capx, sv->res, sv->n, k,
                                                sv->ubuf, sv->ubuf + K, sv->ubuf + 2 * K, sv->facc);
     CK(cudaGetLastError(), "feature launch");
   }
@@ -706,6 +721,7 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
     p.atab = nullptr;
     p.nslots = 0;
     p.cap = const_cast<int *>(d_cap);  // read only in static mode
+    p.capx = nullptr;
     p.res = d_res;
     p.uarc = nullptr;
     p.uold = nullptr;
@@ -817,7 +833,7 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   if ((st = configure(sv))) return st;
   const size_t N = (size_t)g->n + 1, M = (size_t)g->m;
   if ((st = dalloc(sv, &sv->off, N)) || (st = dalloc(sv, &sv->adj, M)) || (st = dalloc(sv, &sv->par, M)) ||
-      (st = dalloc(sv, &sv->atab, (size_t)arc_table_slots((long long)M))) || (st = dalloc(sv, &sv->cap, M)) ||
+      (st = dalloc(sv, &sv->atab, (size_t)arc_table_slots((long long)M))) || (st = dalloc(sv, &sv->capx, M)) ||
       (st = dalloc(sv, &sv->res, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
       (st = dalloc(sv, &sv->excess, N)) || (st = dalloc(sv, &sv->dead, N)) || (st = dalloc(sv, &sv->side, N)) ||
       (st = dalloc(sv, &sv->qbuf, 6 * N)) || (st = dalloc(sv, &sv->dlab, N)) || (st = dalloc(sv, &sv->ctrl, 1)))
@@ -854,7 +870,11 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
     k_arc_table_build<<<blocks, 32 * warps, 0, S>>>(sv->off, sv->adj, g->n, sv->atab, sv->nslots);
     e = cudaGetLastError();
   }
-  up(sv->cap, g->w.data(), 4 * M);
+  up(sv->res, g->w.data(), 4 * M);  // staged in res, widened into capx (epoch 0)
+  if (e == cudaSuccess && M > 0) {
+    k_cap_widen<<<(int)std::min<size_t>((M + 255) / 256, 8 * 148), 256, 0, S>>>(sv->res, sv->capx, (long long)M);
+    e = cudaGetLastError();
+  }
   {
     int32_t mx = 0;
 #pragma omp parallel for schedule(static) reduction(max : mx)
@@ -917,9 +937,9 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
 }  // namespace
 
 int64_t dmf::solver_footprint(int64_t n, int64_t m) {
-  // adj, par, cap, res; the arc table; off, labels, stamps, excess, marks,
-  // repair labels, hub bases and six vertex queues (rounded up)
-  return 16 * m + (int64_t)sizeof(ArcSlot) * arc_table_slots(m) + 64 * n;
+  // adj, par, res, capacity words; the arc table; off, labels, stamps,
+  // excess, marks, repair labels, hub bases and six vertex queues (rounded up)
+  return 20 * m + (int64_t)sizeof(ArcSlot) * arc_table_slots(m) + 64 * n;
 }
 
 int dmf::reserve_updates(dmf_solver *sv, int32_t k) {
@@ -1198,6 +1218,7 @@ int dmf_autotune(dmf_solver *sv, int32_t repeats, dmf_opts *chosen) {
     double best_ms = 0;
     int st = cost(best, &best_ms);
     if (st) return st;
+    if (best.tile <= 0) best.tile = sv->tile;  // the result names the tile the defaults resolved to
     auto try_dim = [&](int32_t dmf_opts::*field, std::initializer_list<int32_t> vals) -> int {
       for (int32_t v : vals) {
         dmf_opts o = best;
@@ -1306,7 +1327,22 @@ int dmf_get_state(dmf_solver *sv, int32_t *cap, int32_t *res, int64_t *excess, i
   if (!sv) return fail(DMF_ERR_INVALID_ARG, "null solver");
   CK(cudaSetDevice(sv->dev), "cudaSetDevice");
   const size_t M = (size_t)sv->m, N = (size_t)sv->n;
-  if (cap) CK(cudaMemcpyAsync(cap, sv->cap, 4 * M, cudaMemcpyDeviceToHost, sv->stream), "D2H cap");
+  if (cap && M > 0) {  // the low halves of the capacity words, through a device buffer in pieces
+    const size_t piece = std::min<size_t>(M, (size_t)1 << 26);
+    int *tmp = nullptr;
+    CK(cudaMalloc(&tmp, 4 * piece), "cudaMalloc capacity readout");
+    cudaError_t e = cudaSuccess;
+    for (size_t b = 0; b < M && e == cudaSuccess; b += piece) {
+      const size_t len = std::min(piece, M - b);
+      k_cap_low<<<(int)std::min<size_t>((len + 255) / 256, 8 * 148), 256, 0, sv->stream>>>(sv->capx + b, tmp,
+                                                                                          (long long)len);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(cap + b, tmp, 4 * len, cudaMemcpyDeviceToHost, sv->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(sv->stream);
+    }
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(e, "D2H cap");
+  }
   if (res) CK(cudaMemcpyAsync(res, sv->res, 4 * M, cudaMemcpyDeviceToHost, sv->stream), "D2H res");
   if (excess) CK(cudaMemcpyAsync(excess, sv->excess, 8 * N, cudaMemcpyDeviceToHost, sv->stream), "D2H excess");
   if (height) CK(cudaMemcpyAsync(height, sv->height, 4 * N, cudaMemcpyDeviceToHost, sv->stream), "D2H height");
@@ -1428,7 +1464,7 @@ int dmf_solver_copy_state(dmf_solver *dst, const dmf_solver *src) {
     CK(cudaStreamSynchronize(src->stream), "source solver");
     const size_t N = (size_t)src->n + 1, M = (size_t)src->m, NC = (size_t)std::max(src->nchunk, 1);
     cudaStream_t S = dst->stream;
-    CK(cudaMemcpyAsync(dst->cap, src->cap, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D cap");
+    CK(cudaMemcpyAsync(dst->capx, src->capx, 8 * M, cudaMemcpyDeviceToDevice, S), "D2D cap");
     CK(cudaMemcpyAsync(dst->res, src->res, 4 * M, cudaMemcpyDeviceToDevice, S), "D2D res");
     CK(cudaMemcpyAsync(dst->excess, src->excess, 8 * N, cudaMemcpyDeviceToDevice, S), "D2D excess");
     CK(cudaMemcpyAsync(dst->height, src->height, 4 * N, cudaMemcpyDeviceToDevice, S), "D2D height");

@@ -283,7 +283,7 @@ int dmf_multi_run_batches(dmf_solver *sv, int32_t steps, const int64_t *ofs,
 /* ---- serving loop ------------------------------------------------------------ */
 /* Device-resident graphs serving update-batch requests.  Graphs are admitted in
  * the given order while the estimated device footprint of their residual state
- * (48 B per arc + 64 B per vertex) fits `hbm_budget` bytes; the rest are not
+ * (52 B per arc + 64 B per vertex) fits `hbm_budget` bytes; the rest are not
  * admitted (ids of admitted graphs are their positions among the admitted ones,
  * dmf_server_info).  The caller keeps the graphs alive until destroy.
  * Lanes: a graph with at least a quarter of the admitted arcs gets a lane of
@@ -327,7 +327,8 @@ int dmf_server_destroy(dmf_server *srv);
  * intervals and cycle counts (coordinate descent, best of `repeats` runs each),
  * keeps the fastest in the solver and returns it in *chosen.  Every candidate
  * computes the same exact flow; the state afterwards is a maximum flow of the
- * current capacities. */
+ * current capacities.  *chosen names the tile width explicitly, also when the
+ * solver's default (tile 0: chosen from the graph) was fastest. */
 int dmf_autotune(dmf_solver *sv, int32_t repeats, dmf_opts *chosen);
 
 /* ---- learned schedule picker ----------------------------------------------- */

@@ -17,9 +17,9 @@ def _graphs(dmf):
 def test_admission_by_budget(dmf):
     inst = _graphs(dmf)
     graphs = [x[0] for x in inst]
-    # per arc: heads, partners, capacities, residuals (16 B) and the arc table
-    # (16-byte slots, 2m + 64 of them); 64 B per vertex
-    need = [16 * g.num_edges() + 16 * (2 * g.num_edges() + 64) + 64 * g.num_nodes() for g in graphs]
+    # per arc: heads, partners, residuals, 8-byte capacity words (20 B) and the
+    # arc table (16-byte slots, 2m + 64 of them); 64 B per vertex
+    need = [20 * g.num_edges() + 16 * (2 * g.num_edges() + 64) + 64 * g.num_nodes() for g in graphs]
     budget = sum(need[:3]) + need[3] // 2  # room for the first three only
     with dmf.Server(graphs, [x[1] for x in inst], [x[2] for x in inst], budget) as srv:
         assert srv.admitted == 3 and srv.device_bytes == sum(need[:3])
