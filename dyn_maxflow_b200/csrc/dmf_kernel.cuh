@@ -75,6 +75,7 @@ struct Params {
   int *fq[2], *wq[2], *aq;     // non-hub vertex queues
   int *dq;                     // dead vertices whose excess the batch changed (kept dead set)
   int *dlab;                   // distance from excess inside the dead set, (wave << 4) | level
+  int *pcur;                   // per vertex: where in its row its last pull found enough (long rows; may be null)
   int2 *fh[2], *wh[2], *ah;    // hub chunk queues
   const int2 *hch;             // every hub's chunks (bottom-up BFS, topology-driven rounds)
   int nhch;
@@ -1071,6 +1072,7 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
     y = warp.shfl(y, 0);
     need = warp.shfl(need, 0);
     if (need <= 0) continue;
+    ItemTimer tm(p);
     const int hy = dead_label(p, y);
     const int beg = __ldg(p.off + y), end = __ldg(p.off + y + 1);
     long long got = 0;
@@ -1086,24 +1088,40 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
         need -= mv;
         got += mv;
       }
-    } else {  // two steps' loads in flight at a time
+    } else {
+      // two steps' loads in flight at a time, starting at the row's cursor:
+      // where the last pass 0 of this deficit was satisfied.  A hub deficit
+      // that comes back batch after batch would otherwise rescan the in-arcs
+      // whose suppliers it drained earlier (at R-MAT 24 the longest item of a
+      // round, a hub of 60-165 k in-arcs, grew from 90 us to 550 us over 16
+      // batches, and every round waits for it).
+      const int deg = end - beg;
+      int cur = p.pcur ? __ldcg(p.pcur + y) : 0;
+      cur = (cur < 0 || cur >= deg) ? 0 : (cur & ~31);
+      int stop = -1;
       for (int pass = 0; pass < 2 && need > 0; pass++) {
-        for (int a0 = beg; a0 < end && need > 0; a0 += 64) {
-          PullArc q0 = pull_load(p, a0 + lane, end);
-          PullArc q1 = pull_load(p, a0 + 32 + lane, end);
-          ls.arcs += (q0.x >= 0) + (q1.x >= 0);
-          long long mv = pass == 0 ? pull_excess(p, warp, q0, need, ls)
-                                   : pull_lower(p, warp, q0, need, hy, hmin, nxt, ntail, round_id, ls);
-          need -= mv;
-          got += mv;
-          if (need > 0 && a0 + 32 < end) {
-            mv = pass == 0 ? pull_excess(p, warp, q1, need, ls)
-                           : pull_lower(p, warp, q1, need, hy, hmin, nxt, ntail, round_id, ls);
+        for (int seg = 0; seg < 2 && need > 0; seg++) {
+          const int sb = seg == 0 ? beg + cur : beg, se = seg == 0 ? end : beg + cur;
+          for (int a0 = sb; a0 < se && need > 0; a0 += 64) {
+            PullArc q0 = pull_load(p, a0 + lane, se);
+            PullArc q1 = pull_load(p, a0 + 32 + lane, se);
+            ls.arcs += (q0.x >= 0) + (q1.x >= 0);
+            long long mv = pass == 0 ? pull_excess(p, warp, q0, need, ls)
+                                     : pull_lower(p, warp, q0, need, hy, hmin, nxt, ntail, round_id, ls);
             need -= mv;
             got += mv;
+            if (pass == 0 && need <= 0) stop = a0;
+            if (need > 0 && a0 + 32 < se) {
+              mv = pass == 0 ? pull_excess(p, warp, q1, need, ls)
+                             : pull_lower(p, warp, q1, need, hy, hmin, nxt, ntail, round_id, ls);
+              need -= mv;
+              got += mv;
+              if (pass == 0 && need <= 0) stop = a0 + 32;
+            }
           }
         }
       }
+      if (p.pcur && lane == 0 && stop >= 0) p.pcur[y] = stop - beg;
     }
     if (need > 0) {  // relabel and try again next round (nowhere to go: stays for the check)
       hmin = cg::reduce(warp, hmin, cg::less<int>());
@@ -1114,6 +1132,7 @@ __device__ __forceinline__ void ph_dead_pull(const Params &p, const int *list, i
       }
     }
     if (lane == 0 && got) atomic_add_ll(p.excess + y, got);
+    tm.done(ls, y);
   }
 }
 

@@ -146,6 +146,7 @@ struct dmf_solver {
   long long *excess = nullptr;
   unsigned char *dead = nullptr, *side = nullptr;
   int *dlab = nullptr;    // dead-set repair labels, tagged with the launch epoch
+  int *pcur = nullptr;    // per vertex: pull scan cursor in its row
   bool caps_bounded = false;  // every capacity <= 2^30 - 1 (updates keep it so)
   int *qbuf = nullptr;    // 6 vertex queues (frontier x2, worklist x2, active, dead-set candidates)
   int2 *hqbuf = nullptr;  // 5 hub-chunk queues, same roles
@@ -340,6 +341,7 @@ Params make_params(dmf_solver *sv, int mode, int k, const int *d_src, const int 
   p.aq = sv->qbuf + 4 * N;
   p.dq = sv->qbuf + 5 * N;
   p.dlab = sv->dlab;
+  p.pcur = sv->pcur;
   p.ah = sv->hqbuf + 4 * NC;
   p.hch = sv->hch;
   p.nhch = sv->nchunk;
@@ -692,6 +694,7 @@ int dmf_static_maxflow_noalloc(int32_t n, int32_t m, const int32_t *d_index, con
     p.aq = (int *)carve(4 * N);
     p.dq = nullptr;  // static solves never keep a dead set
     p.dlab = nullptr;
+    p.pcur = nullptr;
     // no hubs in this mode (hub_deg = INT_MAX): the hub structures are never read
     int2 *hub_dummy = (int2 *)carve(kNoAllocAlign);
     long long *ll_dummy = (long long *)carve(kNoAllocAlign);
@@ -836,7 +839,7 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
       (st = dalloc(sv, &sv->atab, (size_t)arc_table_slots((long long)M))) || (st = dalloc(sv, &sv->capx, M)) ||
       (st = dalloc(sv, &sv->res, M)) || (st = dalloc(sv, &sv->height, N)) || (st = dalloc(sv, &sv->stamp, N)) ||
       (st = dalloc(sv, &sv->excess, N)) || (st = dalloc(sv, &sv->dead, N)) || (st = dalloc(sv, &sv->side, N)) ||
-      (st = dalloc(sv, &sv->qbuf, 6 * N)) || (st = dalloc(sv, &sv->dlab, N)) || (st = dalloc(sv, &sv->ctrl, 1)))
+      (st = dalloc(sv, &sv->qbuf, 6 * N)) || (st = dalloc(sv, &sv->dlab, N)) || (st = dalloc(sv, &sv->pcur, N)) || (st = dalloc(sv, &sv->ctrl, 1)))
     return st;
   std::vector<int2> hub_chunks;
   std::vector<int> hub_base(g->n, -1);
@@ -890,6 +893,7 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->stamp, 0, 4 * N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->dead, 0, N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->dlab, 0, 4 * N, S);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sv->pcur, 0, 4 * N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->side, 0, N, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->excess, 0, 8 * N, S);
   if (e == cudaSuccess) e = cudaMallocHost(&sv->h_ctrl, sizeof(Ctrl));
