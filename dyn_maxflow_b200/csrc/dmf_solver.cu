@@ -93,30 +93,39 @@ using dmf::fail;
 using dmf::ok;
 using dmf::guarded;
 
-// Fills the arc table: a warp per tail vertex, a lane per arc.  Equal
-// (tail, head) pairs keep the largest arc index.  Every insert ends: the table
-// has more slots than arcs, so an empty slot or the key is always found.
+// Fills the arc table: a warp per tail vertex of degree <= hub_deg (a lane per
+// arc), and a warp per hub chunk (kChunk arcs of a longer row), so that one
+// warp never walks a hub's whole row.  Equal (tail, head) pairs keep the
+// largest arc index.  Every insert ends: the table has more slots than arcs,
+// so an empty slot or the key is always found.
+__device__ __forceinline__ void table_insert(ArcSlot *tab, long long nslots, int u, int v, int a) {
+  const unsigned long long key = arc_key(u, v);
+  long long sl = arc_slot0(u, v, nslots);
+  for (long long probe = 0; probe < nslots; probe++) {
+    const unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long *>(tab + sl), ~0ull, key);
+    if (old == ~0ull || old == key) {
+      atomicMax(&tab[sl].arc, a);
+      return;
+    }
+    sl = sl + 1 == nslots ? 0 : sl + 1;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_arc_table_build(const int *__restrict__ off, const int *__restrict__ adj,
-                                                         int n, ArcSlot *tab, long long nslots) {
+                                                         int n, int hub_deg, const int2 *__restrict__ hch,
+                                                         int nchunk, ArcSlot *tab, long long nslots) {
   const int lane = threadIdx.x & 31;
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long u = warp; u < n; u += nwarps) {
     const int b = __ldg(off + u), e = __ldg(off + u + 1);
-    for (int a = b + lane; a < e; a += 32) {
-      const int v = __ldg(adj + a);
-      const unsigned long long key = arc_key((int)u, v);
-      long long sl = arc_slot0((int)u, v, nslots);
-      for (long long probe = 0; probe < nslots; probe++) {
-        const unsigned long long old =
-            atomicCAS(reinterpret_cast<unsigned long long *>(tab + sl), ~0ull, key);
-        if (old == ~0ull || old == key) {
-          atomicMax(&tab[sl].arc, a);
-          break;
-        }
-        sl = sl + 1 == nslots ? 0 : sl + 1;
-      }
-    }
+    if (e - b > hub_deg) continue;  // by chunks below
+    for (int a = b + lane; a < e; a += 32) table_insert(tab, nslots, (int)u, __ldg(adj + a), a);
+  }
+  for (long long c = warp; c < nchunk; c += nwarps) {
+    const int2 it = __ldg(hch + c);
+    const int b = __ldg(off + it.x) + it.y * kChunk, e = min(__ldg(off + it.x + 1), b + kChunk);
+    for (int a = b + lane; a < e; a += 32) table_insert(tab, nslots, it.x, __ldg(adj + a), a);
   }
 }
 
@@ -868,11 +877,6 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   up(sv->par, g->par.data(), 4 * M);
   sv->nslots = arc_table_slots((long long)M);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->atab, 0xFF, sizeof(ArcSlot) * (size_t)sv->nslots, S);
-  if (e == cudaSuccess && g->n > 0) {
-    const int warps = 8, blocks = (int)std::min<long long>(((long long)g->n + warps - 1) / warps, 16LL * 148);
-    k_arc_table_build<<<blocks, 32 * warps, 0, S>>>(sv->off, sv->adj, g->n, sv->atab, sv->nslots);
-    e = cudaGetLastError();
-  }
   up(sv->res, g->w.data(), 4 * M);  // staged in res, widened into capx (epoch 0)
   if (e == cudaSuccess && M > 0) {
     k_cap_widen<<<(int)std::min<size_t>((M + 255) / 256, 8 * 148), 256, 0, S>>>(sv->res, sv->capx, (long long)M);
@@ -886,6 +890,12 @@ int setup_solver(dmf_solver *sv, const dmf_graph *g, int32_t s, int32_t t, const
   }
   up(sv->hch, hub_chunks.data(), sizeof(int2) * hub_chunks.size());
   up(sv->hub_base, hub_base.data(), 4 * (size_t)g->n);
+  if (e == cudaSuccess && g->n > 0) {
+    const int warps = 8, blocks = (int)std::min<long long>(((long long)g->n + warps - 1) / warps, 16LL * 148);
+    k_arc_table_build<<<blocks, 32 * warps, 0, S>>>(sv->off, sv->adj, g->n, sv->hub_deg, sv->hch, sv->nchunk,
+                                                    sv->atab, sv->nslots);
+    e = cudaGetLastError();
+  }
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->chunk_mark, 0, 8 * NC, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->hc_done, 0, 4 * NC, S);
   if (e == cudaSuccess) e = cudaMemsetAsync(sv->hc_alloc, 0, 8 * NC, S);
