@@ -2,11 +2,15 @@
 // of the persistent sm_100a kernel (dmf_kernel.cuh), the batch feature kernel
 // of the schedule picker, and the solver entry points of the C ABI.
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "dmf_kernel.cuh"
 #include "dmf_internal.h"
@@ -497,37 +501,61 @@ int check_updates_args(dmf_solver *sv, int32_t k, const void *a, const void *b, 
   return DMF_OK;
 }
 
-// Host copy into pinned staging: pieces of 64 KiB over up to 8 threads for a
-// large array (a single thread copies well below the DRAM bandwidth).
-void stage_copy(int32_t *to, const int32_t *from, size_t count) {
-  constexpr size_t kPiece = 16384;  // int32 elements
-  const long pieces = (long)((count + kPiece - 1) / kPiece);
-  if (pieces < 4) {
-    std::memcpy(to, from, 4 * count);
-    return;
-  }
-#pragma omp parallel for num_threads(8) schedule(static)
-  for (long i = 0; i < pieces; i++) {
-    const size_t b = (size_t)i * kPiece, e = std::min(count, b + kPiece);
-    std::memcpy(to + b, from + b, 4 * (e - b));
-  }
-}
+// Host batch -> pinned staging -> device, pipelined: the three arrays are cut
+// into pieces of kStagePiece updates; copier threads fill the pinned buffer
+// piece by piece (piece i by thread i mod kStageCopiers, so early pieces finish
+// first) while one issuer thread starts the H2D of each piece as soon as it is
+// in, so the copy engine works while later pieces are still being copied.  A
+// batch of fewer than four pieces is copied and sent whole.
+constexpr size_t kStagePiece = 1 << 18;  // updates (1 MiB of int32)
+constexpr int kStageCopiers = 8;
 
-// Copies a host batch into the device staging buffers through pinned memory;
-// each array's H2D starts while the next one is copied.  The solve's start
-// event is recorded behind the last H2D, so the call's device time (last_ms)
-// is the solve alone, as for a batch already on the device; the copies show
-// in the caller's wall-clock time.
 int stage_batch(dmf_solver *sv, int32_t k, const int32_t *src, const int32_t *dst, const int32_t *w) {
   int st;
   CK(cudaSetDevice(sv->dev), "cudaSetDevice");
   if ((st = ensure_ubuf(sv, k)) || (st = ensure_host_ubuf(sv, k))) return st;
-  const size_t K = (size_t)sv->kcap, HK = (size_t)sv->h_kcap;
+  const size_t K = (size_t)sv->kcap, HK = (size_t)sv->h_kcap, n = (size_t)k;
   const int32_t *from[3] = {src, dst, w};
-  for (int a = 0; a < 3 && k > 0; a++) {
-    stage_copy(sv->h_ubuf + a * HK, from[a], (size_t)k);
-    CK(cudaMemcpyAsync(sv->ubuf + a * K, sv->h_ubuf + a * HK, 4 * (size_t)k, cudaMemcpyHostToDevice, sv->stream),
-       "H2D batch");
+  const size_t per = (n + kStagePiece - 1) / kStagePiece, total = 3 * per;
+  if (total < 4) {
+    for (int a = 0; a < 3 && n > 0; a++) {
+      std::memcpy(sv->h_ubuf + a * HK, from[a], 4 * n);
+      CK(cudaMemcpyAsync(sv->ubuf + a * K, sv->h_ubuf + a * HK, 4 * n, cudaMemcpyHostToDevice, sv->stream),
+         "H2D batch");
+    }
+  } else {
+    std::vector<std::atomic<int>> ready(total);
+    for (auto &r : ready) r.store(0, std::memory_order_relaxed);
+    cudaError_t err = cudaSuccess;
+    auto piece = [&](size_t i, size_t &a, size_t &b, size_t &e) {
+      a = i / per;
+      b = (i % per) * kStagePiece;
+      e = std::min(n, b + kStagePiece);
+    };
+#pragma omp parallel num_threads(kStageCopiers + 1)
+    {
+      const int tid = omp_get_thread_num(), nthr = omp_get_num_threads();
+      if (tid == 0) {  // the issuer (with no other thread it copies too)
+        for (size_t i = 0; i < total; i++) {
+          size_t a, b, e;
+          piece(i, a, b, e);
+          if (nthr == 1) std::memcpy(sv->h_ubuf + a * HK + b, from[a] + b, 4 * (e - b));
+          else
+            while (!ready[i].load(std::memory_order_acquire)) std::this_thread::yield();
+          if (err == cudaSuccess)
+            err = cudaMemcpyAsync(sv->ubuf + a * K + b, sv->h_ubuf + a * HK + b, 4 * (e - b),
+                                  cudaMemcpyHostToDevice, sv->stream);
+        }
+      } else {
+        for (size_t i = (size_t)(tid - 1); i < total; i += (size_t)(nthr - 1)) {
+          size_t a, b, e;
+          piece(i, a, b, e);
+          std::memcpy(sv->h_ubuf + a * HK + b, from[a] + b, 4 * (e - b));
+          ready[i].store(1, std::memory_order_release);
+        }
+      }
+    }
+    if (err != cudaSuccess) return cuda_fail(err, "H2D batch");
   }
   CK(cudaEventRecord(sv->ev0, sv->stream), "event record");
   return DMF_OK;

@@ -66,7 +66,9 @@ def make_config(name: str):
     if m:
         scale = int(m.group(1))
         narcs = 16 << scale
-        nb = 10
+        # scale 24 is the benchmark's headline graph: its reserve is sized for
+        # the benchmark's 3 + 10 batches, so that the graphs are the same
+        nb = 13 if scale >= 24 else 10
         reserve = int(0.1 * 0.01 * narcs * nb) + 16
         g, s, t = D.gen_rmat(scale, narcs, 0.57, 0.19, 0.19, seed=0, cap_lo=1, cap_hi=1000, reserve=reserve)
         b = D.gen_batches(g, nb, frac=0.01, p_inc=0.4, p_dec=0.4, p_ins=0.1, delta_hi=500, ins_lo=1,
