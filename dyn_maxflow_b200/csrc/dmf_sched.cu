@@ -39,22 +39,56 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
   return x ^ (x >> 31);
 }
 
-// Forward pass of one sample by 64 threads (thread j owns hidden unit j).
-__device__ void forward64(const __nv_bfloat16 *__restrict__ W, const float *__restrict__ b, const float *x, float *h1,
-                          float *h2, float *out) {
-  const int j = threadIdx.x;
-  float acc = b[kB1 + j];
+// The network in shared memory: the bf16 weights and fp32 biases are copied in
+// with coalesced 16-byte loads (all of a thread's loads issued before any
+// store), one DRAM round trip for the 10.8 KB, instead of each thread walking
+// its own weight row with 2-byte loads -- a few dependent misses per row when
+// the weights are not in L2, which is the normal case for a decision taken once
+// per batch between solves that stream far more than L2 holds.
+struct NetSmem {
+  alignas(16) __nv_bfloat16 w[kNumW];
+  float b[kNumB];
+};
+constexpr int kStageVec = 8;                                // bf16 per 16-byte load
+constexpr int kStageRounds = kNumW / (kStageVec * kHidden);  // loads per thread
+static_assert(kNumW % (kStageVec * kHidden) == 0, "weights split evenly over the block");
+
+// Called by all kHidden threads of the block; W must be 16-byte aligned
+// (cudaMalloc).  Ends with a block barrier.
+__device__ __forceinline__ void stage_net(const __nv_bfloat16 *__restrict__ W, const float *__restrict__ b,
+                                          NetSmem &S) {
+  const uint4 *src = reinterpret_cast<const uint4 *>(W);
+  uint4 *dst = reinterpret_cast<uint4 *>(S.w);
+  uint4 v[kStageRounds];
 #pragma unroll
-  for (int f = 0; f < kFeatures; f++) acc += __bfloat162float(W[kW1 + j * kFeatures + f]) * x[f];
+  for (int r = 0; r < kStageRounds; r++) v[r] = __ldg(src + r * kHidden + threadIdx.x);
+  for (int i = threadIdx.x; i < kNumB; i += kHidden) S.b[i] = __ldg(b + i);
+#pragma unroll
+  for (int r = 0; r < kStageRounds; r++) dst[r * kHidden + threadIdx.x] = v[r];
+  __syncthreads();
+}
+
+// Forward pass of one sample by 64 threads (thread j owns hidden unit j), from
+// the staged network.  In the 64 x 64 layer thread j starts its row at column
+// j, so the threads of a warp read different shared-memory banks (rows are 128
+// bytes apart: read in step they would all hit one bank).
+__device__ void forward64(const NetSmem &S, const float *x, float *h1, float *h2, float *out) {
+  const int j = threadIdx.x;
+  float acc = S.b[kB1 + j];
+#pragma unroll
+  for (int f = 0; f < kFeatures; f++) acc += __bfloat162float(S.w[kW1 + j * kFeatures + f]) * x[f];
   h1[j] = fmaxf(acc, 0.f);
   __syncthreads();
-  acc = b[kB2 + j];
-  for (int i = 0; i < kHidden; i++) acc += __bfloat162float(W[kW2 + j * kHidden + i]) * h1[i];
+  acc = S.b[kB2 + j];
+  for (int c = 0; c < kHidden; c++) {
+    const int i = (c + j) & (kHidden - 1);
+    acc += __bfloat162float(S.w[kW2 + j * kHidden + i]) * h1[i];
+  }
   h2[j] = fmaxf(acc, 0.f);
   __syncthreads();
   if (j < kActions) {
-    acc = b[kB3 + j];
-    for (int i = 0; i < kHidden; i++) acc += __bfloat162float(W[kW3 + j * kHidden + i]) * h2[i];
+    acc = S.b[kB3 + j];
+    for (int i = 0; i < kHidden; i++) acc += __bfloat162float(S.w[kW3 + j * kHidden + i]) * h2[i];
     out[j] = acc;
   }
   __syncthreads();
@@ -63,11 +97,13 @@ __device__ void forward64(const __nv_bfloat16 *__restrict__ W, const float *__re
 // One sample per block of 64 threads.
 __global__ void __launch_bounds__(kHidden) k_predict(const __nv_bfloat16 *W, const float *b, const float *X, int n,
                                                      float *Y) {
+  __shared__ NetSmem net;
   __shared__ float x[kFeatures], h1[kHidden], h2[kHidden], out[kActions];
+  stage_net(W, b, net);
   for (int s = blockIdx.x; s < n; s += gridDim.x) {
     if (threadIdx.x < kFeatures) x[threadIdx.x] = X[(size_t)s * kFeatures + threadIdx.x];
     __syncthreads();
-    forward64(W, b, x, h1, h2, out);
+    forward64(net, x, h1, h2, out);
     if (threadIdx.x < kActions) Y[(size_t)s * kActions + threadIdx.x] = out[threadIdx.x];
     __syncthreads();
   }
@@ -97,7 +133,9 @@ __device__ void make_features(const FeatAcc &a, const FeatScalars &sc, float *x)
 __global__ void __launch_bounds__(kHidden) k_decide(const __nv_bfloat16 *W, const float *b, const FeatAcc *acc,
                                                     FeatScalars sc, int use_model, float margin, float *feat,
                                                     float *pred, int *action) {
+  __shared__ NetSmem net;
   __shared__ float x[kFeatures], h1[kHidden], h2[kHidden], out[kActions];
+  if (use_model) stage_net(W, b, net);  // uniform over the block: every thread reaches its barrier
   if (threadIdx.x == 0) make_features(*acc, sc, x);
   __syncthreads();
   if (threadIdx.x < kFeatures) feat[threadIdx.x] = x[threadIdx.x];
@@ -106,7 +144,7 @@ __global__ void __launch_bounds__(kHidden) k_decide(const __nv_bfloat16 *W, cons
     if (threadIdx.x == 0) *action = 0;
     return;
   }
-  forward64(W, b, x, h1, h2, out);
+  forward64(net, x, h1, h2, out);
   if (threadIdx.x < kActions) pred[threadIdx.x] = out[threadIdx.x];
   if (threadIdx.x == 0) {
     int best = 0;
