@@ -340,8 +340,9 @@ __device__ __forceinline__ long long arc_slot0(int u, int v, long long nslots) {
   return (long long)__umul64hi(x, (unsigned long long)nslots);
 }
 
-// One slot through L2 (the stamp word changes during a batch; tail, head and
-// arc never do after the build).
+// One slot as one 16-byte load through L2, bypassing L1: a random slot is
+// seldom read twice by one SM, and tail, head and arc never change after the
+// build.
 __device__ __forceinline__ ArcSlot load_slot(const ArcSlot *s) {
   const int4 x = __ldcg(reinterpret_cast<const int4 *>(s));
   return ArcSlot{x.x, x.y, x.z, x.w};
