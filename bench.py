@@ -113,6 +113,14 @@ def pct(xs, q):
     return xs[lo] + (xs[hi] - xs[lo]) * (k - lo)
 
 
+def throughput(batches, warmup: int, times_ms: list) -> dict:
+    """Rates of the timed batches over their summed device time: batches and
+    updates per second (batch `warmup + j` took times_ms[j])."""
+    total_s = sum(times_ms) * 1e-3
+    upd = sum(len(batches[warmup + j][0]) for j in range(len(times_ms)))
+    return {"batches_per_s": round(len(times_ms) / total_s, 2), "updates_per_s": round(upd / total_s, 1)}
+
+
 # ---------------------------------------------------------------------------
 def cpu_port_run(g, s, t, batches, nthreads, budget_ms=0.0):
     """The reference's data-driven algorithm restated in oracle/ (OpenMP): a
@@ -428,6 +436,7 @@ def run_ours(args, rank: int, world: int):
                 "h2d_bytes_per_step": int(12 * len(batches[-1][0])), "d2h_bytes_per_step": 8,
                 "api": "dmf_apply_updates (host arrays)"},
         "gpu_launches": len(times),
+        "throughput": throughput(batches, args.warmup, times),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "k_solve", "algorithmic_bytes_per_launch": int(avg_bytes)},

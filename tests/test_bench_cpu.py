@@ -28,6 +28,13 @@ def test_percentiles_interpolate(bench):
     assert bench.pct([], 0.5) is None
 
 
+def test_throughput_of_the_timed_batches(bench):
+    batches = [([0] * 5, [1] * 5, [2] * 5), ([0] * 10, [1] * 10, [2] * 10), ([0] * 30, [1] * 30, [2] * 30)]
+    # the warm-up batch (5 updates) is not counted; 40 updates in 2 + 3 ms
+    r = bench.throughput(batches, 1, [2.0, 3.0])
+    assert r == {"batches_per_s": 400.0, "updates_per_s": 8000.0}
+
+
 def test_algorithmic_bytes_by_hand(bench):
     st = {"dead_vertices": 90, "outer_iters": 2, "arcs_scanned": 1000, "vertices_visited": 50, "pushes": 20,
           "dead_deficits": 0}
