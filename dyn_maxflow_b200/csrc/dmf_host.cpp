@@ -737,29 +737,56 @@ int dmf_gen_batches(const dmf_graph *g, int32_t nb, double frac, double p_inc, d
         }
       }
     }
-    // list := (list without `drop`) merged with `add` (all sorted, drop within list)
-    auto refresh = [](std::vector<int32_t> &list, const std::vector<int32_t> &drop, const std::vector<int32_t> &add) {
+    // list := (list without `drop`) merged with `add`; all three sorted, `drop`
+    // a subset of `list`, `add` disjoint from it, list entries distinct.  The
+    // list is cut into slices of equal length; a slice's first entry bounds its
+    // value range, which selects its part of `drop` and `add` by binary search,
+    // and each slice merges into its own part of the output: the result is the
+    // sequential merge's, entry for entry.  `spare` is the list's previous
+    // buffer, reused so that the output is not cleared on every batch.
+    auto refresh = [](std::vector<int32_t> &list, std::vector<int32_t> &spare, const std::vector<int32_t> &drop,
+                      const std::vector<int32_t> &add) {
       if (drop.empty() && add.empty()) return;
-      std::vector<int32_t> out;
-      out.reserve(list.size() - drop.size() + add.size());
-      size_t i = 0, d = 0, a = 0;
-      while (i < list.size()) {
-        const int32_t x = list[i];
-        if (d < drop.size() && drop[d] == x) {
-          d++;
-          i++;
-          continue;
-        }
-        if (a < add.size() && add[a] < x) {
-          out.push_back(add[a++]);
-          continue;
-        }
-        out.push_back(x);
-        i++;
+      const int64_t L = (int64_t)list.size();
+      spare.resize((size_t)(L - (int64_t)drop.size() + (int64_t)add.size()));
+      int32_t *out = spare.data();
+      int R = 1;
+#ifdef _OPENMP
+      R = (int)std::max<int64_t>(1, std::min<int64_t>(4 * omp_get_max_threads(), L / 65536));
+#endif
+      std::vector<int64_t> ib((size_t)R + 1), db((size_t)R + 1), ab((size_t)R + 1);
+      for (int r = 0; r <= R; r++) ib[r] = L * r / R;
+      db[0] = ab[0] = 0;
+      db[R] = (int64_t)drop.size();
+      ab[R] = (int64_t)add.size();
+      for (int r = 1; r < R; r++) {
+        const int32_t v = list[ib[r]];
+        db[r] = std::lower_bound(drop.begin(), drop.end(), v) - drop.begin();
+        ab[r] = std::lower_bound(add.begin(), add.end(), v) - add.begin();
       }
-      while (a < add.size()) out.push_back(add[a++]);
-      list.swap(out);
+#pragma omp parallel for schedule(static)
+      for (int r = 0; r < R; r++) {
+        int64_t o = ib[r] - db[r] + ab[r], i = ib[r], d = db[r], a = ab[r];
+        const int64_t ie = ib[r + 1], de = db[r + 1], ae = ab[r + 1];
+        while (i < ie) {
+          const int32_t x = list[i];
+          if (d < de && drop[d] == x) {
+            d++;
+            i++;
+            continue;
+          }
+          if (a < ae && add[a] < x) {
+            out[o++] = add[a++];
+            continue;
+          }
+          out[o++] = x;
+          i++;
+        }
+        while (a < ae) out[o++] = add[a++];
+      }
+      list.swap(spare);
     };
+    std::vector<int32_t> pos_spare, absent_spare;
     Rng rng(seed);
     std::vector<int64_t> O(1, 0);
     std::vector<int32_t> S, D, Wn;
@@ -789,7 +816,11 @@ int dmf_gen_batches(const dmf_graph *g, int32_t nb, double frac, double p_inc, d
       touched.reserve(2 * (picks.size() + ins.size()));
       for (int32_t e : picks) { touched.push_back(e); touched.push_back(g->par[e]); }
       for (int32_t e : ins) { touched.push_back(e); touched.push_back(g->par[e]); }
+#ifdef _OPENMP
+      __gnu_parallel::sort(touched.begin(), touched.end());
+#else
       std::sort(touched.begin(), touched.end());
+#endif
       touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
       std::vector<uint8_t> was((size_t)touched.size());
 #pragma omp parallel for schedule(static)
@@ -827,8 +858,8 @@ int dmf_gen_batches(const dmf_graph *g, int32_t nb, double frac, double p_inc, d
         if (!a0 && a1) aadd.push_back(e);
       }
       if (bi + 1 < nb) {
-        refresh(pos, pdrop, padd);
-        refresh(absent, adrop, aadd);
+        refresh(pos, pos_spare, pdrop, padd);
+        refresh(absent, absent_spare, adrop, aadd);
       }
     }
     size_t kk = S.size();
