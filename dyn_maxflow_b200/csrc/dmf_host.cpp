@@ -136,6 +136,8 @@ int build_from_edges(int64_t k, const int32_t *u, const int32_t *v, const int32_
   }
   if (first_bad != INT64_MAX)
     return fail(DMF_ERR_INVALID_ARG, "negative vertex id at edge %lld", (long long)first_bad);
+  if (maxnode == INT32_MAX)  // the vertex count would not fit int32
+    return fail(DMF_ERR_INVALID_ARG, "vertex id %d leaves no room for the vertex count", maxnode);
   const int32_t n = maxnode + 1;
   std::vector<int64_t> bofs((size_t)n + 1, 0);
 #pragma omp parallel for schedule(static)
@@ -439,15 +441,23 @@ int dmf_graph_from_edges(int64_t k, const int32_t *u, const int32_t *v, const in
   return guarded([&] { return build_from_edges(k, u, v, w, out); });
 }
 
+}  // extern "C"
+
+namespace {
+// `count` int32 words; an empty array writes nothing (its pointer may be null,
+// which fwrite does not accept even for a zero count).
+bool put_words(FILE *f, const int32_t *p, size_t count) { return count == 0 || std::fwrite(p, 4, count, f) == count; }
+}  // namespace
+
+extern "C" {
+
 int dmf_graph_save(const dmf_graph *g, const char *path) {
   if (!g || !path) return fail(DMF_ERR_INVALID_ARG, "null argument");
   FILE *f = std::fopen(path, "wb");
   if (!f) return fail(DMF_ERR_BAD_FILE, "cannot open %s for writing", path);
   bool okw = std::fwrite(&g->n, 4, 1, f) == 1 && std::fwrite(&g->m, 4, 1, f) == 1 &&
-             std::fwrite(g->off.data(), 4, g->off.size(), f) == g->off.size() &&
-             std::fwrite(g->adj.data(), 4, g->m, f) == (size_t)g->m &&
-             std::fwrite(g->w.data(), 4, g->m, f) == (size_t)g->m &&
-             std::fwrite(g->par.data(), 4, g->m, f) == (size_t)g->m;
+             put_words(f, g->off.data(), g->off.size()) && put_words(f, g->adj.data(), (size_t)g->m) &&
+             put_words(f, g->w.data(), (size_t)g->m) && put_words(f, g->par.data(), (size_t)g->m);
   okw = (std::fclose(f) == 0) && okw;
   return okw ? ok() : fail(DMF_ERR_BAD_FILE, "write to %s failed", path);
 }
@@ -524,8 +534,8 @@ int dmf_updates_save(const char *path, int32_t k, const int32_t *src, const int3
   if (!path || k < 0 || (k > 0 && (!src || !dst || !w))) return fail(DMF_ERR_INVALID_ARG, "bad arguments");
   FILE *f = std::fopen(path, "wb");
   if (!f) return fail(DMF_ERR_BAD_FILE, "cannot open %s for writing", path);
-  bool okw = std::fwrite(&k, 4, 1, f) == 1 && std::fwrite(src, 4, k, f) == (size_t)k &&
-             std::fwrite(dst, 4, k, f) == (size_t)k && std::fwrite(w, 4, k, f) == (size_t)k;
+  bool okw = std::fwrite(&k, 4, 1, f) == 1 && put_words(f, src, (size_t)k) && put_words(f, dst, (size_t)k) &&
+             put_words(f, w, (size_t)k);
   okw = (std::fclose(f) == 0) && okw;
   return okw ? ok() : fail(DMF_ERR_BAD_FILE, "write to %s failed", path);
 }

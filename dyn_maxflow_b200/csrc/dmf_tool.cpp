@@ -151,7 +151,10 @@ int main(int argc, char **argv) {
     int32_t *S = nullptr, *D = nullptr, *W = nullptr;
     st = dmf_gen_batches(g, nb, std::atof(argv[4]), 0.4, 0.4, 0.1, 500, 1, 1000, std::strtoull(argv[5], nullptr, 10),
                          &ofs, &S, &D, &W);
-    if (st) return die(st, "gen-batches");
+    if (st) {
+      dmf_graph_free(g);
+      return die(st, "gen-batches");
+    }
     const bool cumulative = argc == 8 && std::strcmp(argv[7], "cumulative") == 0;
     std::map<std::pair<int32_t, int32_t>, int32_t> net;
     for (int b = 0; b < nb && !st; b++) {
@@ -182,8 +185,8 @@ int main(int argc, char **argv) {
   } else {
     return usage();
   }
+  dmf_graph_free(g);  // NULL when generation failed
   if (st) return die(st, c.c_str());
   std::printf("source:%d sink:%d\n", s, t);
-  dmf_graph_free(g);
   return 0;
 }

@@ -126,6 +126,23 @@ static void fuzz_builders(int iters, std::mt19937_64 &rng) {
               caps_ok);
 }
 
+static void extreme_ids() {
+  // the largest vertex id leaves no room for the vertex count
+  const int32_t u1[1] = {2147483647}, v1[1] = {1}, u2[2] = {0, 2147483647}, v2[2] = {2147483647, 2147483647},
+                w[2] = {5, 6};
+  dmf_graph *g = nullptr;
+  if (dmf_graph_from_edges(1, u1, v1, w, &g) == DMF_OK) dmf_graph_free(g);
+  if (dmf_graph_from_edges(2, u2, v2, w, &g) == DMF_OK) dmf_graph_free(g);
+  // an empty graph and an empty update file are written without touching data
+  const int32_t none = 0;
+  if (dmf_graph_from_edges(0, &none, &none, &none, &g) == DMF_OK) {
+    dmf_graph_save(g, "/dev/null");
+    dmf_graph_free(g);
+  }
+  dmf_updates_save("/dev/null", 0, nullptr, nullptr, nullptr);
+  std::printf("extreme ids: done\n");
+}
+
 static void generator_edges() {
   dmf_graph *g = nullptr;
   int32_t s = 0, t = 0;
@@ -158,6 +175,7 @@ int main(int argc, char **argv) {
   std::mt19937_64 rng(1);
   fuzz_loaders(G, U, argv[3], iters, rng);
   fuzz_builders(iters, rng);
+  extreme_ids();
   generator_edges();
   return 0;
 }

@@ -110,6 +110,17 @@ def test_int32_arguments_never_wrap(dmf, golden_dir):
     assert g.arrays()[2][g.find_arc(u, v)] == 7
 
 
+def test_largest_vertex_id_is_rejected(dmf):
+    """A vertex id of 2^31-1 would make the vertex count overflow int32: the
+    builder says so instead of wrapping.  A self-loop on it is dropped before
+    the count, as create_bin drops every self-loop."""
+    with pytest.raises(dmf.DmfError) as ei:
+        dmf.Graph.from_edges([2**31 - 1], [1], [5])
+    assert ei.value.status == 1 and "no room for the vertex count" in str(ei.value)
+    g = dmf.Graph.from_edges([0, 2**31 - 1], [1, 2**31 - 1], [5, 7])
+    assert g.num_nodes() == 2 and g.num_edges() == 2
+
+
 def test_validation_names_the_lowest_bad_arc(dmf, golden_dir):
     """With several defects of one kind, the message names the lowest arc,
     whatever the number of host threads that checked them."""
