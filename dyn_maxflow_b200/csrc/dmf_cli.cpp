@@ -48,7 +48,24 @@ int main(int argc, char **argv) {
   const bool json = std::getenv("DMF_CLI_JSON") && std::atoi(std::getenv("DMF_CLI_JSON"));
   const int source = std::atoi(argv[3]), sink = std::atoi(argv[4]);
   std::printf("source:%d sink:%d\n", source, sink);
+  // what a failing step leaves behind is released before the exit
   dmf_graph *g = nullptr;
+  dmf_solver *sv = nullptr;
+  int32_t *us = nullptr, *ud = nullptr, *uw = nullptr;
+  auto release_batch = [&]() {
+    dmf_solver_destroy(sv);  // NULL is fine
+    sv = nullptr;
+    dmf_free(us);
+    dmf_free(ud);
+    dmf_free(uw);
+    us = ud = uw = nullptr;
+  };
+  auto fail_step = [&](int status, const char *what) {
+    const int r = die(status, what);  // first: a successful destroy clears the last error
+    release_batch();
+    dmf_graph_free(g);
+    return r;
+  };
   int st = dmf_graph_load(argv[1], &g);
   if (st) return die(st, "graph load");
   int32_t V = 0, E = 0;
@@ -63,7 +80,7 @@ int main(int argc, char **argv) {
   for (int i = first; i <= last; i++) {
     std::string fname = std::string(argv[2]) + "_p" + std::to_string(i) + ".bin";
     std::printf("Processing file: %s\n", fname.c_str());
-    int32_t k = 0, *us = nullptr, *ud = nullptr, *uw = nullptr;
+    int32_t k = 0;
     st = dmf_updates_load(fname.c_str(), &k, &us, &ud, &uw);
     if (st) {
       // the reference prints the loader error and continues with an empty batch
@@ -84,31 +101,32 @@ int main(int argc, char **argv) {
       o.variant = variant;
       o.kernel_cycles = kc;
       // dynamic path: recalculate_max_flow (code/dyn_data_bench.cu:171-298)
-      dmf_solver *sv = nullptr;
-      if ((st = dmf_solver_create(g, source, sink, &o, nullptr, &sv))) return die(st, "solver create");
+      if ((st = dmf_solver_create(g, source, sink, &o, nullptr, &sv))) return fail_step(st, "solver create");
       int64_t f0 = 0, dyn = 0, stat = 0;
       dmf_stats sst;
-      if ((st = dmf_static_maxflow(sv, &f0))) return die(st, "static solve");
+      if ((st = dmf_static_maxflow(sv, &f0))) return fail_step(st, "static solve");
       dmf_stats_get(sv, &sst);
       if (variant == DMF_VARIANT_PP) std::printf("static main push cnt:%lld GPU Time: %.6f ms\n",
                                                  (long long)sst.push_rounds, sst.last_ms);
       else std::printf("static GPU Time: %.6f ms\n", sst.last_ms);
       if (variant == DMF_VARIANT_TOPO) std::printf("flow:%lld  kernel cycles:%d\n", (long long)f0, kc);
-      if ((st = dmf_apply_updates(sv, k, us, ud, uw, &dyn))) return die(st, "apply updates");
+      if ((st = dmf_apply_updates(sv, k, us, ud, uw, &dyn))) return fail_step(st, "apply updates");
       dmf_stats dst;
       dmf_stats_get(sv, &dst);
       std::printf("total GPU Time: %.6f ms\n", dst.last_ms);
       std::printf("DYN TIME:%.6fms true_cnt=%d cnt=%d per batch time:%.6f\n", dst.last_ms, 1, 1, dst.last_ms);
       std::printf("Dynamic flow:%lld\n", (long long)dyn);
       dmf_solver_destroy(sv);
+      sv = nullptr;
       // from-scratch path: static_recalculate (code/dyn_data_bench.cu:325-492)
-      if ((st = dmf_solver_create(g, source, sink, &o, nullptr, &sv))) return die(st, "solver create");
-      if ((st = dmf_recompute(sv, k, us, ud, uw, &stat))) return die(st, "recompute");
+      if ((st = dmf_solver_create(g, source, sink, &o, nullptr, &sv))) return fail_step(st, "solver create");
+      if ((st = dmf_recompute(sv, k, us, ud, uw, &stat))) return fail_step(st, "recompute");
       dmf_stats rst;
       dmf_stats_get(sv, &rst);
       if (variant == DMF_VARIANT_PP) std::printf("static  UPDATE GPU Time: %.6f ms\n", rst.last_ms);
       else std::printf("STATIC UPDATE GPU Time: %.6f ms\n", rst.last_ms);
       dmf_solver_destroy(sv);
+      sv = nullptr;
       if (dyn != stat) {
         std::printf("<<<<<<<<<<<<<<<<<<<<<<<<PANIC NOT MATCHING dynflow:%lld statflow:%lld>>>>>>>>>>>>>>>>>>>>>>>>>>>\n",
                     (long long)dyn, (long long)stat);
@@ -121,9 +139,7 @@ int main(int argc, char **argv) {
                     fname.c_str(), DMF_CLI_VARIANT, kc, k, (long long)f0, (long long)dyn, (long long)stat,
                     sst.last_ms, dst.last_ms, rst.last_ms);
     }
-    dmf_free(us);
-    dmf_free(ud);
-    dmf_free(uw);
+    release_batch();
   }
   dmf_graph_free(g);
   return rc;

@@ -76,3 +76,20 @@ def test_cli_usage_without_args():
         pytest.skip("CLI not built")
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 1 and "usage" in r.stderr
+
+
+def test_cli_failure_names_the_cause(dmf, golden_dir):
+    """A failing step prints the library's own message (the release of what the
+    step held must not clear it) and exits 1; the reference's first stdout
+    lines are already out."""
+    exe = os.path.join(ROOT, "dyn_maxflow_b200", "bin", "dyn_pp_bench_large")
+    if not os.path.exists(exe):
+        pytest.skip("CLI not built")
+    graph, prefix = os.path.join(golden_dir, "johnson8-2-4.bin"), os.path.join(golden_dir, "johnson")
+    r = subprocess.run([exe, graph, prefix, "25", "25", "1"], capture_output=True, text=True)
+    assert r.returncode == 1
+    assert "solver create failed: [invalid argument] need n >= 2 and distinct s, t" in r.stderr
+    assert r.stdout.startswith("source:25 sink:25\nProcessing file:")
+    if dmf.device_count() == 0:  # without a GPU the solver itself cannot be created
+        r = subprocess.run([exe, graph, prefix, "25", "2", "1"], capture_output=True, text=True)
+        assert r.returncode == 1 and "solver create failed: [cuda error] no CUDA device is visible" in r.stderr
