@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <random>
@@ -364,9 +365,11 @@ int dmf_sched_create(int32_t device, uint64_t seed, dmf_sched **out) {
     SCK(cudaSetDevice(dev), "cudaSetDevice");
     dmf_sched *s = new dmf_sched();
     s->dev = dev;
-    auto bail = [&](int st) {
+    auto bail = [&](int st) {  // the destroy clears the last error: keep the message across it
+      char msg[1024];
+      std::snprintf(msg, sizeof msg, "%s", dmf_last_error());
       dmf_sched_destroy(s);
-      return st;
+      return fail(st, "%s", msg);
     };
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&s->W, sizeof(__nv_bfloat16) * kNumW) != cudaSuccess ||
